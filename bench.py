@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Throughput of DIABLO's channel RK substep (RKW3 + CN, rk_chan_1) on B200.
+
+Metric: grid-point RK substeps per second, whole job.  A bench step is one
+full RKW3 time step (three substeps) of the 512x257x512 FP64 DNS (infinite
+front, Re 5000, Ri 1, CFL 0.5 with variable dt), state resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
+substep has no data-parallel exchange on one instance, so nothing is sharded
+and no collective sits on the data path; rank timings are reduced with MAX.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt RK substeps/s on 1 B200: FP64 plain vs mixed+learned SGS at stated err"
+UNIT = "grid-pt substeps/s"
+
+
+def workload_params(name: str):
+    from diablo3_b200.params import make_params
+    if name == "config1":
+        return make_params(
+            nx=512, ny=257, nz=512, lx=2 * math.pi, lz=2 * math.pi, ly=2.0,
+            re=5000.0, pr=1.0, ri=1.0, ro=1.0, delta=1.0, grav_y=1.0, ic_type=4, kick=1e-3,
+            delta_t=1e-3, variable_dt=1, cfl=0.5, update_dt=1, time_limit=1e9,
+            u_bc_ymin=0, w_bc_ymin=0, v_bc_ymin=0, th_bc_ymin=1,
+            u_bc_ymax=1, w_bc_ymax=1, v_bc_ymax=0, th_bc_ymax=1,
+            th_bc_ymin_c1=1.0, th_bc_ymax_c1=1.0)
+    if name == "config0":
+        p = workload_params("config1")
+        p.nx, p.ny, p.nz, p.re, p.variable_dt = 64, 65, 64, 1000.0, 0
+        return p
+    raise ValueError(name)
+
+
+WORKLOAD_DESC = {
+    "config1": "plain FP64 DNS, infinite front, 512x257x512 (x,y,z), Re 5000, Ri 1 (M2=N2=f=1), CFL 0.5",
+    "config0": "plain FP64 DNS, infinite front, 64x65x64, Re 1000, fixed dt 1e-3",
+}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the oracle (C restatement of the reference) on host cores
+
+def cpu_baseline(name: str, min_seconds: float = 10.0) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from diablo3_b200.grid import create_grid
+    from diablo3_b200.ic import initial_fields
+    p = workload_params(name)
+    if name == "config1":
+        p.ny = 65  # bounded sample: full x-z planes, fewer wall-normal points
+    gy = create_grid(p.ny, lz=p.ly, cs=1.5, grid_type=1)
+    o = pyoracle.Oracle(p, gy)
+    o.init_from_physical(*initial_fields(p, gy, seed=0))
+    n = p.nx * p.ny * p.nz
+    count, t0 = 0, time.perf_counter()
+    while True:
+        o.rk_substep(count % 3 + 1)
+        count += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or count >= 30:
+            break
+    o.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n * count / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{count} substeps of {p.nx}x{p.ny}x{p.nz} (same x-z planes as the workload, "
+                      f"{p.ny} of its wall-normal points), {el:.1f} s, OpenMP C oracle"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    per = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(args.config, min_seconds=2.0)
+        if i >= args.warmup:
+            per.append(r)
+    v = statistics.median(x["value"] for x in per)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.config], "parallelism": "host cores"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": per[0]["cores"], "kind": "port",
+                         "sample": per[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from diablo3_b200 import lib as L
+    from diablo3_b200 import roofline
+    from diablo3_b200.channel import Channel
+    from diablo3_b200.grid import create_grid
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    p = workload_params(args.config)
+    gy = create_grid(p.ny, lz=p.ly, cs=1.5, grid_type=1)
+    stream = torch.cuda.Stream()
+    ch = Channel(p, gy, stream=stream.cuda_stream)
+    ch.init_flow(seed=rank)
+    npts = p.nx * p.ny * p.nz
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ch.step(1)
+    torch.cuda.synchronize()
+
+    # timed region: K steps, stage events recorded inside the step graph
+    ch._ck(ch.L.db_set_timing(ch.h, 1))
+    ch.step(1)  # capture the timed graph (not timed)
+    torch.cuda.synchronize()
+    n0 = ctypes.c_longlong()
+    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n0)))
+    stage_ms = np.zeros(L.DB_NSTAGES if hasattr(L, "DB_NSTAGES") else len(L.STAGES))
+    buf = (ctypes.c_double * len(L.STAGES))()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ch.step(1)
+        ch._ck(ch.L.db_stage_times(ch.h, buf, len(L.STAGES)))
+        stage_ms += np.array(buf[:])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    n1 = ctypes.c_longlong()
+    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n1)))
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = npts * 3 * args.steps * world / (ms_max / 1e3)
+    st = ch.status()
+    if st.flags & 1:
+        raise SystemExit("non-finite values in the flow: run rejected")
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peak_hbm()
+    per_stage = stage_ms / (3 * args.steps)  # ms per launch (per substep)
+    dom = int(np.argmax(per_stage))
+    dom_name = L.STAGES[dom]
+    alg = roofline.stage_bytes(p)[dom_name]
+    achieved = alg / (per_stage[dom] / 1e3) / 1e9
+    traffic = roofline.profiled_traffic(dom_name, ROOT)
+
+    # end to end through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = {f: torch.empty(ch.new_spectral().shape, dtype=torch.complex128, pin_memory=True).numpy()
+                for f in L.STATE_FIELDS}
+        ke = max(1, min(3, args.steps))
+        dev_bytes = roofline.state_transfer_bytes(p)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        saved = ch.download_state()
+        e0.record(stream)
+        for _ in range(ke):
+            ch.upload_state(saved if _ == 0 else host)
+            ch.step(1)
+            for f in L.STATE_FIELDS:
+                ch._ck(ch.L.db_download_field(ch.h, f, L.dptr(host[f].view(np.float64).reshape(-1))))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": npts * 3 * ke * world / (float(te.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": dev_bytes, "d2h_bytes_per_step": dev_bytes,
+               "steps": ke, "path": "db_upload_state + db_rk_steps(1) + db_download_field x9, reference-layout host arrays"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.config)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded infinite-front IC, no dataset)",
+        "config": {"workload": WORKLOAD_DESC[args.config], "grid_xyz": [p.nx, p.ny, p.nz],
+                   "points": npts, "substeps_per_step": 3,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "state ~10 GB resident in HBM, far above the 126 MB L2 (no flush needed)"},
+        "gpu_launches": int(n1.value - n0.value),
+        "stages_ms_per_substep": {L.STAGES[i]: round(float(per_stage[i]), 4) for i in range(len(L.STAGES))},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "step_alg_bytes": roofline.substep_bytes(p),
+                     "step_frac": roofline.substep_bytes(p) / (ms_max / args.steps / 3 / 1e3) / 1e9 / peak},
+        "clocks": clk,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ch.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+"""Host-side mirror of the reference's channel driver over the C-ABI.
+
+``Channel`` owns one device context (db_init) and exposes the reference's
+subroutines by their names: ``fft_xz_to_fourier``, ``fft_xz_to_physical``,
+``rk_chan_1``, ``rem_div_chan``, ``apply_bc_vel_post``, ``courant``, plus the
+driver's time loop ``step`` (for/diablo.f90:58-69).  Arrays crossing the
+boundary use the reference layout (see include/diablo_b200.h).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import lib as _L
+from .ic import initial_fields, ref_cshape, ref_shape
+from .params import DbParams
+
+
+class Channel:
+    def __init__(self, params: DbParams, gy: np.ndarray, stream: int | None = None):
+        self.L = _L.load()
+        self.p = params.copy()
+        self.gy = np.ascontiguousarray(gy, dtype=np.float64)
+        if self.gy.shape != (params.ny + 1,):
+            raise ValueError(f"gy must hold ny+1 = {params.ny + 1} values")
+        h = ctypes.c_void_p()
+        rc = self.L.db_init(ctypes.byref(self.p), _L.dptr(self.gy),
+                            ctypes.c_void_p(stream) if stream else None, ctypes.byref(h))
+        if rc != 0:
+            raise _L.DiabloError(rc, self.L.db_last_error(None).decode())
+        self.h = h
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.db_finalize(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        _L.check(rc, self.h)
+
+    # -- reference-layout arrays ---------------------------------------------
+    def new_real(self) -> np.ndarray:
+        return np.zeros(ref_shape(self.p))
+
+    def new_spectral(self) -> np.ndarray:
+        return np.zeros(ref_cshape(self.p), dtype=np.complex128)
+
+    @staticmethod
+    def _as_d(a: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a)
+        return a.view(np.float64) if a.dtype == np.complex128 else a
+
+    def upload_field(self, fid: int, arr: np.ndarray):
+        self._ck(self.L.db_upload_field(self.h, fid, _L.dptr(self._as_d(arr).reshape(-1))))
+
+    def download_field(self, fid: int) -> np.ndarray:
+        out = self.new_spectral()
+        self._ck(self.L.db_download_field(self.h, fid, _L.dptr(out.view(np.float64).reshape(-1))))
+        return out
+
+    def upload_state(self, state: dict):
+        for fid in _L.STATE_FIELDS:
+            a = state.get(fid)
+            if a is None:
+                a = self.new_spectral()
+            self.upload_field(fid, a)
+
+    def download_state(self) -> dict:
+        return {fid: self.download_field(fid) for fid in _L.STATE_FIELDS}
+
+    # -- the reference's subroutines -----------------------------------------
+    def fft_xz_to_fourier(self, buf: np.ndarray) -> np.ndarray:
+        """In place on a reference-layout real array; returns its complex view."""
+        assert buf.dtype == np.float64 and buf.flags["C_CONTIGUOUS"]
+        self._ck(self.L.db_fft_xz_to_fourier(self.h, _L.dptr(buf.reshape(-1))))
+        return buf.reshape(-1).view(np.complex128).reshape(ref_cshape(self.p))
+
+    def fft_xz_to_physical(self, cbuf: np.ndarray) -> np.ndarray:
+        """In place on a reference-layout complex array; returns its real view."""
+        d = cbuf.view(np.float64) if cbuf.dtype == np.complex128 else cbuf
+        assert d.flags["C_CONTIGUOUS"]
+        self._ck(self.L.db_fft_xz_to_physical(self.h, _L.dptr(d.reshape(-1))))
+        return d.reshape(-1).reshape(ref_shape(self.p))
+
+    def rk_chan_1(self, rk_step: int):
+        self._ck(self.L.db_rk_substep(self.h, rk_step))
+
+    def step(self, nsteps: int = 1):
+        """nsteps driver steps: time_step += 1, three substeps, time += dt."""
+        self._ck(self.L.db_rk_steps(self.h, nsteps))
+
+    def rem_div_chan(self):
+        self._ck(self.L.db_rem_div(self.h))
+
+    def apply_bc_vel_post(self):
+        self._ck(self.L.db_apply_bc_vel_post(self.h))
+
+    def courant(self) -> float:
+        dt = ctypes.c_double()
+        self._ck(self.L.db_courant(self.h, ctypes.byref(dt)))
+        return dt.value
+
+    def divergence(self) -> float:
+        d = ctypes.c_double()
+        self._ck(self.L.db_divergence(self.h, ctypes.byref(d)))
+        return d.value
+
+    def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
+        self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
+
+    def status(self) -> _L.DbStatus:
+        s = _L.DbStatus()
+        self._ck(self.L.db_get_status(self.h, ctypes.byref(s)))
+        return s
+
+    # -- create_flow_chan ------------------------------------------------------
+    def init_flow(self, seed: int = 0, noise: str = "gaussian", fields=None):
+        """Initial condition as create_flow_chan/create_th_chan build it
+        (for/flow.f90:260-499, 562-659): physical fields -> Fourier,
+        apply_BC_vel_mpi_post, rem_div_chan; cp from a zero pressure."""
+        u1, u2, u3, th = fields if fields is not None else initial_fields(self.p, self.gy, seed, noise)
+        spec = {}
+        for fid, a in ((_L.CU1, u1), (_L.CU2, u2), (_L.CU3, u3), (_L.CTH, th)):
+            b = np.ascontiguousarray(a, dtype=np.float64).copy()
+            spec[fid] = self.fft_xz_to_fourier(b).copy()
+        self.upload_state(spec)
+        self.apply_bc_vel_post()
+        self.rem_div_chan()

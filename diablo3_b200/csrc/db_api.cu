@@ -1,0 +1,638 @@
+// db_api.cu -- C-ABI of include/diablo_b200.h: context, state transfer
+// between the reference layout and the device layout, and the substep
+// orchestration (one CUDA graph per RK step).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/diablo_b200.h"
+#include "db_kernels.cuh"
+
+using namespace db;
+
+struct db_ctx {
+  db_params p;
+  Geom g;
+  Phys ph;
+  State s;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  std::vector<void*> allocs;
+  double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
+  double2* d_tw = nullptr;       // twiddles (Nx then Nz)
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+  double* h_stage = nullptr;     // pinned staging, one physical field
+  size_t stage_doubles = 0;
+  std::vector<double> gy, gyf, dy, dyf, kx, kz;
+  double pi_ref = 0.0;
+  double w_min_c1 = 0.0, w_max_c1 = 0.0;
+  // stage timing: events between the kernels of each substep
+  bool timing = false;
+  cudaEvent_t ev[3][DB_NSTAGES + 1] = {};
+  long long launches = 0;          // kernels issued so far
+  long long graph_kernels = 0;     // kernel nodes in one captured step
+};
+
+static std::string g_init_err;
+
+static void mark(db_ctx* c, int rk, int stage) {
+  if (c->timing) cudaEventRecord(c->ev[rk][stage], c->st);
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      c->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+      return DB_ERR_CUDA;                                                                \
+    }                                                                                    \
+  } while (0)
+
+static int fail(db_ctx* c, int code, const char* msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+extern "C" int db_abi_version(void) { return DB_ABI_VERSION; }
+
+extern "C" const char* db_last_error(const db_ctx* c) {
+  if (!c) return g_init_err.c_str();
+  return c->err.c_str();
+}
+
+// ---------------------------------------------------------------------------
+// init
+
+static int validate(const db_params* p, std::string& why) {
+  if (!pow2(p->nx) || p->nx < 16 || p->nx > 1024) { why = "nx must be a power of two in [16, 1024]"; return DB_ERR_SIZE; }
+  if (!pow2(p->nz) || p->nz < 16 || p->nz > 1024) { why = "nz must be a power of two in [16, 1024]"; return DB_ERR_SIZE; }
+  if (p->ny < 4) { why = "ny must be >= 4"; return DB_ERR_SIZE; }
+  if (p->n_th != 1) { why = "n_th must be 1 (one scalar)"; return DB_ERR_UNSUPPORTED; }
+  if (p->time_ad_meth != 1) { why = "time_ad_meth 2 (rk_chan_2) stops in the reference (solver.f90:1289-1293)"; return DB_ERR_UNSUPPORTED; }
+  if (p->use_les) { why = "LES closure not available in this build"; return DB_ERR_UNSUPPORTED; }
+  if (p->precision != 0) { why = "only the FP64 path (precision 0) is available"; return DB_ERR_UNSUPPORTED; }
+  const int b[8] = {p->u_bc_ymin, p->v_bc_ymin, p->w_bc_ymin, p->th_bc_ymin,
+                    p->u_bc_ymax, p->v_bc_ymax, p->w_bc_ymax, p->th_bc_ymax};
+  for (int i = 0; i < 8; ++i)
+    if (b[i] != 0 && b[i] != 1) { why = "boundary types must be 0 (Dirichlet) or 1 (Neumann)"; return DB_ERR_ARG; }
+  if (p->variable_dt && p->update_dt < 1) { why = "update_dt must be >= 1"; return DB_ERR_ARG; }
+  if (p->re <= 0 || p->pr <= 0 || p->lx <= 0 || p->lz <= 0) { why = "re, pr, lx, lz must be positive"; return DB_ERR_ARG; }
+  return DB_OK;
+}
+
+static void twiddles(int n, std::vector<double2>& out) {
+  const long double PI = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < n; ++k) {
+    long double a = 2.0L * PI * (long double)k / (long double)n;
+    out.push_back(make_double2((double)cosl(a), -(double)sinl(a)));
+  }
+}
+
+template <typename T>
+static int dalloc(db_ctx* c, T** ptr, size_t count) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, count * sizeof(T)));
+  CK(cudaMemset(q, 0, count * sizeof(T)));
+  c->allocs.push_back(q);
+  *ptr = (T*)q;
+  return DB_OK;
+}
+
+extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db_ctx** out) {
+  if (!p || !gy_in || !out) { g_init_err = "db_init: NULL argument"; return DB_ERR_ARG; }
+  *out = nullptr;
+  std::string why;
+  int v = validate(p, why);
+  if (v) { g_init_err = "db_init: " + why; return v; }
+  db_ctx* c = new db_ctx();
+  c->p = *p;
+  cudaGetDevice(&c->device);
+  if (stream) c->st = (cudaStream_t)stream;
+  else {
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+      g_init_err = "db_init: no CUDA device";
+      delete c;
+      return DB_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  const int Nx = p->nx, Nyp = p->ny, Nz = p->nz, np = Nyp + 2;
+  Geom& g = c->g;
+  g.nx = Nx; g.ny = Nyp; g.nz = Nz; g.np = np;
+  g.nkx = Nx / 3; g.nkz = Nz / 3; g.nkzp = 2 * g.nkz + 1;
+  g.kxs = round_up(g.nkx + 1, KT);
+  g.sp = (long long)g.nkzp * g.kxs;
+  g.hp = (long long)Nz * g.kxs;
+  g.pp = (long long)Nz * Nx;
+  // init_chan_mpi, for/domain.f90:321-361 (one rank: lower sets jstart, upper jend)
+  g.jstart = (p->u_bc_ymin == 1) ? 1 : 2;
+  g.jend = (p->u_bc_ymax == 1) ? Nyp : Nyp - 1;
+  g.jstart_th = (p->th_bc_ymin == 1) ? 1 : 2;
+  g.jend_th = (p->th_bc_ymax == 1) ? Nyp : Nyp - 1;
+
+  // grid metrics, for/domain.f90:276-300, 538-565
+  c->gy.assign(np, 0.0); c->gyf.assign(np, 0.0); c->dy.assign(np, 0.0); c->dyf.assign(np, 0.0);
+  for (int j = 1; j <= Nyp + 1; ++j) c->gy[j] = gy_in[j - 1];
+  for (int j = 1; j <= Nyp; ++j) c->gyf[j] = 0.5 * (c->gy[j] + c->gy[j + 1]);
+  c->gyf[0] = 2.0 * c->gyf[1] - c->gyf[2];
+  c->gyf[Nyp + 1] = 2.0 * c->gyf[Nyp] - c->gyf[Nyp - 1];
+  for (int j = 1; j <= Nyp + 1; ++j) c->dy[j] = c->gyf[j] - c->gyf[j - 1];
+  for (int j = 1; j <= Nyp; ++j) c->dyf[j] = c->gy[j + 1] - c->gy[j];
+  c->dyf[0] = c->dyf[1];
+  c->dyf[Nyp + 1] = c->dyf[Nyp];
+  // wavenumbers with the reference's single-precision pi (for/fft.f90:147, 208-225)
+  c->pi_ref = (double)(4.0f * atanf(1.0f));
+  c->kx.assign(g.kxs, 0.0);
+  c->kz.assign(g.nkzp, 0.0);
+  for (int i = 0; i <= g.nkx; ++i) c->kx[i] = i * (2. * c->pi_ref) / p->lx;
+  for (int k = 0; k <= g.nkz; ++k) c->kz[k] = k * (2. * c->pi_ref) / p->lz;
+  for (int k = 1; k <= g.nkz; ++k) c->kz[2 * g.nkz + 1 - k] = -k * (2. * c->pi_ref) / p->lz;
+
+  // physics constants, thermal-wind compensation (for/parameters.f90:255-279)
+  Phys& ph = c->ph;
+  memset(&ph, 0, sizeof(ph));
+  ph.nu = 1.0 / p->re; ph.beta = p->beta; ph.nu_v_scale = p->nu_v_scale; ph.pr = p->pr;
+  ph.ro_inv = 1.0 / p->ro; ph.delta = p->delta;
+  ph.grav_x = p->grav_x; ph.grav_y = p->grav_y; ph.grav_z = p->grav_z;
+  ph.ly = p->ly;
+  ph.front = p->flavor_front ? 1 : 0;
+  ph.front_tw = (p->flavor_front && ph.ro_inv != 0.0) ? 1 : 0;
+  ph.f_type = p->f_type; ph.px0 = p->px0; ph.omega0 = p->omega0;
+  ph.amp_omega0 = p->amp_omega0; ph.force_start = p->force_start; ph.ic_type = p->ic_type;
+  double wmin = p->w_bc_ymin_c1, wmax = p->w_bc_ymax_c1;
+  ph.dthdx = 0.0; ph.dthdz = 0.0;
+  if (p->ic_type == 4 || p->ic_type == 5) {
+    double m2 = isnan(p->dthdx_override) ? ph.ro_inv / p->delta : p->dthdx_override;
+    double shear = m2 * p->delta / ph.ro_inv;
+    if (p->w_bc_ymin == 1) wmin -= shear;
+    if (p->w_bc_ymax == 1) wmax -= shear;
+    ph.dthdx = m2;
+  } else if (p->ic_type >= 6 && p->ic_type <= 8) {
+    if (p->w_bc_ymin == 1) wmin -= 2.0 * p->delta / p->lx;
+    if (p->w_bc_ymax == 1) wmax -= 2.0 * p->delta / p->lx;
+    ph.dthdx = isnan(p->dthdx_override) ? 2.0 / p->lx * ph.ro_inv : p->dthdx_override;
+  }
+  c->w_min_c1 = wmin; c->w_max_c1 = wmax;
+  const int bt[8] = {p->u_bc_ymin, p->v_bc_ymin, p->w_bc_ymin, p->th_bc_ymin,
+                     p->u_bc_ymax, p->v_bc_ymax, p->w_bc_ymax, p->th_bc_ymax};
+  const double bv[8] = {p->u_bc_ymin_c1, p->v_bc_ymin_c1, wmin, p->th_bc_ymin_c1,
+                        p->u_bc_ymax_c1, p->v_bc_ymax_c1, wmax, p->th_bc_ymax_c1};
+  for (int i = 0; i < 8; ++i) { ph.bc_type[i] = bt[i]; ph.bc_c1[i] = bv[i]; }
+  ph.dx = p->lx / Nx; ph.dz = p->lz / Nz;
+  ph.pi_ref = c->pi_ref;
+
+  // device memory
+  int rc;
+  size_t S = (size_t)np * g.sp, H = (size_t)np * g.hp, Pn = (size_t)np * g.pp;
+  double2* sp[11];
+  for (int i = 0; i < 11; ++i)
+    if ((rc = dalloc(c, &sp[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  State& s = c->s;
+  s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
+  s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
+  s.phi_g = sp[9]; s.pfac = sp[10];
+  for (int i = 0; i < 8; ++i)
+    if ((rc = dalloc(c, &s.xh[i], H))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  double* ph_[8];
+  for (int i = 0; i < 8; ++i)
+    if ((rc = dalloc(c, &ph_[i], Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  s.u1 = ph_[0]; s.u2 = ph_[1]; s.u3 = ph_[2]; s.th = ph_[3];
+  s.r1 = ph_[4]; s.r2 = ph_[5]; s.r3 = ph_[6]; s.rth = ph_[7];
+  if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
+  if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
+  size_t ntab = 4 * (size_t)np + g.kxs + g.nkzp;
+  if ((rc = dalloc(c, &c->d_tab, ntab))) { db_finalize(c); g_init_err = c->err; return rc; }
+  std::vector<double> tab;
+  tab.insert(tab.end(), c->gy.begin(), c->gy.end());
+  tab.insert(tab.end(), c->gyf.begin(), c->gyf.end());
+  tab.insert(tab.end(), c->dy.begin(), c->dy.end());
+  tab.insert(tab.end(), c->dyf.begin(), c->dyf.end());
+  tab.insert(tab.end(), c->kx.begin(), c->kx.end());
+  tab.insert(tab.end(), c->kz.begin(), c->kz.end());
+  std::vector<double2> tw;
+  twiddles(Nx, tw);
+  twiddles(Nz, tw);
+  if ((rc = dalloc(c, &c->d_tw, tw.size()))) { db_finalize(c); g_init_err = c->err; return rc; }
+  if (cudaMemcpy(c->d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess) {
+    db_finalize(c);
+    g_init_err = "db_init: table upload failed";
+    return DB_ERR_CUDA;
+  }
+  g.gy = c->d_tab; g.gyf = c->d_tab + np; g.dy = c->d_tab + 2 * np; g.dyf = c->d_tab + 3 * np;
+  g.kx = c->d_tab + 4 * np; g.kz = c->d_tab + 4 * np + g.kxs;
+  g.twx = c->d_tw; g.twz = c->d_tw + Nx;
+
+  // run scalars (for/parameters.f90:176-178)
+  DevScalars h{};
+  h.delta_t = p->delta_t;
+  h.h_bar[0] = p->delta_t * (8.0 / 15.0);
+  h.h_bar[1] = p->delta_t * (2.0 / 15.0);
+  h.h_bar[2] = p->delta_t * (5.0 / 15.0);
+  h.time = 0.0; h.time_step = 0;
+  h.save_stats_time = 1e300; h.save_flow_time = 1e300;
+  h.w_bc_ymax_c1_transient = wmax;
+  union { double d; unsigned long long u; } inf;
+  inf.d = INFINITY;
+  h.dt_min_bits = inf.u;
+  if (cudaMemcpy(s.sc, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) {
+    db_finalize(c);
+    g_init_err = "db_init: scalar upload failed";
+    return DB_ERR_CUDA;
+  }
+  c->stage_doubles = std::max(Pn, 2 * S);
+  if (cudaMallocHost(&c->h_stage, c->stage_doubles * sizeof(double)) != cudaSuccess) {
+    db_finalize(c);
+    g_init_err = "db_init: pinned staging allocation failed";
+    return DB_ERR_CUDA;
+  }
+  if (launch_pfac(g, s, c->st) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
+    g_init_err = std::string("db_init: ") + cudaGetErrorString(cudaGetLastError());
+    db_finalize(c);
+    return DB_ERR_CUDA;
+  }
+  *out = c;
+  return DB_OK;
+}
+
+extern "C" int db_finalize(db_ctx* c) {
+  if (!c) return DB_ERR_ARG;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k <= DB_NSTAGES; ++k)
+      if (c->ev[r][k]) cudaEventDestroy(c->ev[r][k]);
+  for (void* q : c->allocs) cudaFree(q);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return DB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion (host side, into the pinned staging buffer)
+
+static double2* spec_field(db_ctx* c, int id) {
+  State& s = c->s;
+  switch (id) {
+    case DB_CU1: return s.cu1;
+    case DB_CU2: return s.cu2;
+    case DB_CU3: return s.cu3;
+    case DB_CP: return s.cp;
+    case DB_CTH: return s.cth;
+    case DB_CF1: return s.cf1;
+    case DB_CF2: return s.cf2;
+    case DB_CF3: return s.cf3;
+    case DB_CFTH: return s.cfth;
+    default: return nullptr;
+  }
+}
+
+// reference complex (0:Nxp, 0:Nz+1, 0:Nyp+1) -> compact [j][kzp][kx]
+static void ref_to_compact(const db_ctx* c, const double* ref, double2* dst) {
+  const Geom& g = c->g;
+  const int nxp1 = c->p.nx / 2 + 1, nz2 = c->p.nz + 2;
+  for (int j = 0; j < g.np; ++j)
+    for (int k = 0; k < g.nkzp; ++k) {
+      const double* row = ref + 2 * ((long long)(j * nz2 + k) * nxp1);
+      double2* d = dst + (long long)j * g.sp + (long long)k * g.kxs;
+      for (int i = 0; i <= g.nkx; ++i) d[i] = make_double2(row[2 * i], row[2 * i + 1]);
+      for (int i = g.nkx + 1; i < g.kxs; ++i) d[i] = make_double2(0.0, 0.0);
+    }
+}
+
+static void compact_to_ref(const db_ctx* c, const double2* src, double* ref) {
+  const Geom& g = c->g;
+  const int nxp1 = c->p.nx / 2 + 1, nz2 = c->p.nz + 2;
+  for (int j = 0; j < g.np; ++j)
+    for (int k = 0; k < nz2; ++k) {
+      double* row = ref + 2 * ((long long)(j * nz2 + k) * nxp1);
+      if (k < g.nkzp) {
+        const double2* s = src + (long long)j * g.sp + (long long)k * g.kxs;
+        for (int i = 0; i <= g.nkx; ++i) { row[2 * i] = s[i].x; row[2 * i + 1] = s[i].y; }
+        for (int i = g.nkx + 1; i < nxp1; ++i) { row[2 * i] = 0.0; row[2 * i + 1] = 0.0; }
+      } else {
+        for (int i = 0; i < 2 * nxp1; ++i) row[i] = 0.0;
+      }
+    }
+}
+
+static void phys_ref_to_compact(const db_ctx* c, const double* ref, double* dst) {
+  const Geom& g = c->g;
+  const int nx2 = c->p.nx + 2, nz2 = c->p.nz + 2;
+  for (int j = 0; j < g.np; ++j)
+    for (int k = 0; k < g.nz; ++k)
+      memcpy(dst + (long long)j * g.pp + (long long)k * g.nx, ref + (long long)(j * nz2 + k) * nx2,
+             sizeof(double) * g.nx);
+}
+
+static void compact_to_phys_ref(const db_ctx* c, const double* src, double* ref) {
+  const Geom& g = c->g;
+  const int nx2 = c->p.nx + 2, nz2 = c->p.nz + 2;
+  for (int j = 0; j < g.np; ++j)
+    for (int k = 0; k < g.nz; ++k)
+      memcpy(ref + (long long)(j * nz2 + k) * nx2, src + (long long)j * g.pp + (long long)k * g.nx,
+             sizeof(double) * g.nx);
+}
+
+static int upload_spec(db_ctx* c, int id, const double* ref) {
+  double2* d = spec_field(c, id);
+  if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
+  const size_t n = (size_t)c->g.np * c->g.sp;
+  double2* st = (double2*)c->h_stage;
+  if (ref) ref_to_compact(c, ref, st);
+  else memset(st, 0, n * sizeof(double2));
+  CK(cudaMemcpyAsync(d, st, n * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+static int download_spec(db_ctx* c, int id, double* ref) {
+  double2* d = spec_field(c, id);
+  if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
+  if (!ref) return DB_OK;
+  const size_t n = (size_t)c->g.np * c->g.sp;
+  double2* st = (double2*)c->h_stage;
+  CK(cudaMemcpyAsync(st, d, n * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  compact_to_ref(c, st, ref);
+  return DB_OK;
+}
+
+extern "C" int db_upload_state(db_ctx* c, const double* cu1, const double* cu2, const double* cu3,
+                               const double* cp, const double* cth, const double* cf1, const double* cf2,
+                               const double* cf3, const double* cfth) {
+  if (!c) return DB_ERR_ARG;
+  const double* a[9] = {cu1, cu2, cu3, cp, cth, cf1, cf2, cf3, cfth};
+  for (int i = 0; i < 9; ++i) {
+    int rc = upload_spec(c, i, a[i]);
+    if (rc) return rc;
+  }
+  return DB_OK;
+}
+
+extern "C" int db_download_state(db_ctx* c, double* cu1, double* cu2, double* cu3, double* cp, double* cth,
+                                 double* cf1, double* cf2, double* cf3, double* cfth) {
+  if (!c) return DB_ERR_ARG;
+  double* a[9] = {cu1, cu2, cu3, cp, cth, cf1, cf2, cf3, cfth};
+  for (int i = 0; i < 9; ++i) {
+    int rc = download_spec(c, i, a[i]);
+    if (rc) return rc;
+  }
+  return DB_OK;
+}
+
+extern "C" int db_upload_field(db_ctx* c, int field, const double* host) {
+  if (!c || !host) return DB_ERR_ARG;
+  if (field >= DB_CU1 && field <= DB_CFTH) return upload_spec(c, field, host);
+  if (field == DB_NU_T || field == DB_KAPPA_T) return fail(c, DB_ERR_UNSUPPORTED, "LES fields not built");
+  return fail(c, DB_ERR_ARG, "bad field id");
+}
+
+extern "C" int db_download_field(db_ctx* c, int field, double* host) {
+  if (!c || !host) return DB_ERR_ARG;
+  if (field >= DB_CU1 && field <= DB_CFTH) return download_spec(c, field, host);
+  if (field == DB_NU_T || field == DB_KAPPA_T) return fail(c, DB_ERR_UNSUPPORTED, "LES fields not built");
+  return fail(c, DB_ERR_ARG, "bad field id");
+}
+
+// ---------------------------------------------------------------------------
+// clock / status
+
+extern "C" int db_set_clock(db_ctx* c, double time, int32_t time_step, double sst, double sft) {
+  if (!c) return DB_ERR_ARG;
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->s.sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  h.time = time; h.time_step = time_step; h.save_stats_time = sst; h.save_flow_time = sft;
+  CK(cudaMemcpyAsync(c->s.sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+extern "C" int db_get_status(db_ctx* c, db_status* out) {
+  if (!c || !out) return DB_ERR_ARG;
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->s.sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  out->flags = h.flags; out->time_step = h.time_step; out->time = h.time;
+  out->delta_t = h.delta_t; out->max_div = h.max_div;
+  return DB_OK;
+}
+
+extern "C" int db_clear_status(db_ctx* c) {
+  if (!c) return DB_ERR_ARG;
+  CK(cudaMemsetAsync(&c->s.sc->flags, 0, sizeof(int), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// transforms of one host array
+
+extern "C" int db_fft_xz_to_fourier(db_ctx* c, double* buf) {
+  if (!c || !buf) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  phys_ref_to_compact(c, buf, c->h_stage);
+  CK(cudaMemcpyAsync(c->s.r1, c->h_stage, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(launch_fwd_x(g, fset(c->s.r1), fset(c->s.xh[0]), 1, c->st));
+  CK(launch_fwd_z(g, fset(c->s.xh[0]), fset(c->s.phi_g), 1, c->st));
+  CK(cudaMemcpyAsync(c->h_stage, c->s.phi_g, (size_t)g.np * g.sp * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  compact_to_ref(c, (double2*)c->h_stage, buf);
+  return DB_OK;
+}
+
+extern "C" int db_fft_xz_to_physical(db_ctx* c, double* buf) {
+  if (!c || !buf) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  ref_to_compact(c, buf, (double2*)c->h_stage);
+  CK(cudaMemcpyAsync(c->s.phi_g, c->h_stage, (size_t)g.np * g.sp * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+  CK(launch_inv_z(g, fset(c->s.phi_g), fset(c->s.xh[0]), 1, c->st));
+  CK(launch_inv_x(g, fset(c->s.xh[0]), fset(c->s.r1), 1, c->st));
+  CK(cudaMemcpyAsync(c->h_stage, c->s.r1, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  compact_to_phys_ref(c, c->h_stage, buf);
+  return DB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the substep
+
+static cudaError_t substep(db_ctx* c, int rk /* 0-based */) {
+  const Geom& g = c->g;
+  State& s = c->s;
+  cudaStream_t st = c->st;
+  cudaError_t e;
+  long long n = 0;
+  mark(c, rk, 0);
+  // velocity and buoyancy to physical space (solver.f90:635-643)
+  if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
+  mark(c, rk, 1);
+  if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.u1, s.u2, s.u3, s.th), 4, st))) return e;
+  mark(c, rk, 2);
+  // nonlinear products + x-FFT, then z-FFT + spectral RHS + inverse z of cr
+  if ((e = launch_products(g, s, st))) return e;
+  mark(c, rk, 3);
+  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st))) return e;
+  mark(c, rk, 4);
+  // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
+  if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
+  mark(c, rk, 5);
+  // implicit CN solves (solver.f90:1012-1233)
+  if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
+  if ((e = launch_thomas(g, s, st))) return e;
+  mark(c, rk, 6);
+  n += 7;
+  // CFL on the last substep (solver.f90:1241-1244)
+  if (rk == 2 && c->p.variable_dt) {
+    CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
+    if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
+    n += 2;
+  }
+  mark(c, rk, 7);
+  // back to Fourier space (solver.f90:1247-1252) and projection
+  if ((e = launch_fwd_x(g, fset(s.u1, s.u2, s.u3, s.th), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
+  mark(c, rk, 8);
+  if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st))) return e;
+  mark(c, rk, 9);
+  if ((e = launch_rem_div(g, s, rk, 1, st))) return e;
+  mark(c, rk, 10);
+  n += 3;
+  c->launches += n;
+  return cudaSuccess;
+}
+
+extern "C" int db_rk_substep(db_ctx* c, int rk_step) {
+  if (!c) return DB_ERR_ARG;
+  if (rk_step < 1 || rk_step > 3) return fail(c, DB_ERR_ARG, "rk_step must be 1, 2 or 3");
+  const bool t = c->timing;
+  c->timing = false;  // stage events belong to whole steps
+  cudaError_t e = substep(c, rk_step - 1);
+  c->timing = t;
+  CK(e);
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+static cudaError_t one_step(db_ctx* c) {
+  cudaError_t e;
+  if ((e = launch_step_begin(c->s.sc, c->st))) return e;
+  for (int rk = 0; rk < 3; ++rk)
+    if ((e = substep(c, rk))) return e;
+  c->launches += 2;
+  return launch_step_end(c->s.sc, c->st);
+}
+
+extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
+  if (!c) return DB_ERR_ARG;
+  if (nsteps < 0) return fail(c, DB_ERR_ARG, "nsteps must be >= 0");
+  if (!c->graph) {
+    cudaGraph_t gr;
+    const long long before = c->launches;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+    cudaError_t e = one_step(c);
+    c->graph_kernels = c->launches - before;
+    c->launches = before;
+    cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      c->err = std::string("graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2);
+      return DB_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&c->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+      c->graph = nullptr;
+      c->err = std::string("graph instantiate failed: ") + cudaGetErrorString(e);
+      return DB_ERR_CUDA;
+    }
+  }
+  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
+  c->launches += (long long)nsteps * c->graph_kernels;
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+extern "C" int db_set_timing(db_ctx* c, int enable) {
+  if (!c) return DB_ERR_ARG;
+  if (enable && !c->ev[0][0])
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k <= DB_NSTAGES; ++k) CK(cudaEventCreate(&c->ev[r][k]));
+  if ((enable != 0) != c->timing && c->graph) {  // re-capture with/without event nodes
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->timing = enable != 0;
+  return DB_OK;
+}
+
+extern "C" int db_stage_times(db_ctx* c, double* ms, int nstages) {
+  if (!c || !ms || nstages < DB_NSTAGES) return DB_ERR_ARG;
+  if (!c->timing) return fail(c, DB_ERR_STATE, "stage timing is off (db_set_timing)");
+  CK(cudaStreamSynchronize(c->st));
+  for (int k = 0; k < DB_NSTAGES; ++k) {
+    double t = 0.0;
+    for (int r = 0; r < 3; ++r) {
+      float f = 0.f;
+      CK(cudaEventElapsedTime(&f, c->ev[r][k], c->ev[r][k + 1]));
+      t += f;
+    }
+    ms[k] = t;
+  }
+  return DB_OK;
+}
+
+extern "C" int db_kernel_launches(db_ctx* c, long long* count) {
+  if (!c || !count) return DB_ERR_ARG;
+  *count = c->launches;
+  return DB_OK;
+}
+
+extern "C" int db_rem_div(db_ctx* c) {
+  if (!c) return DB_ERR_ARG;
+  CK(launch_rem_div(c->g, c->s, 0, 0, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+extern "C" int db_apply_bc_vel_post(db_ctx* c) {
+  if (!c) return DB_ERR_ARG;
+  CK(launch_bc_vel_post(c->g, c->ph, c->s, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+extern "C" int db_courant(db_ctx* c, double* delta_t_out) {
+  if (!c) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  State& s = c->s;
+  CK(launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3), fset(s.xh[0], s.xh[1], s.xh[2]), 3, c->st));
+  CK(launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2]), fset(s.u1, s.u2, s.u3), 3, c->st));
+  CflCtl ctl{c->p.cfl, c->p.time_limit, 1, 1, 1};
+  CK(launch_courant(g, c->ph, s, ctl, c->st));
+  db_status stt;
+  int rc = db_get_status(c, &stt);
+  if (rc) return rc;
+  if (delta_t_out) *delta_t_out = stt.delta_t;
+  return DB_OK;
+}
+
+extern "C" int db_divergence(db_ctx* c, double* max_div_out) {
+  if (!c) return DB_ERR_ARG;
+  CK(cudaMemsetAsync(&c->s.sc->max_div, 0, sizeof(double), c->st));
+  CK(launch_divergence(c->g, c->s, c->st));
+  db_status stt;
+  int rc = db_get_status(c, &stt);
+  if (rc) return rc;
+  if (max_div_out) *max_div_out = stt.max_div;
+  return DB_OK;
+}

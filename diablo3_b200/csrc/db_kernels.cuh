@@ -1,0 +1,74 @@
+// db_kernels.cuh -- declarations shared by the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "db_common.cuh"
+
+namespace db {
+
+constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple of 4)
+constexpr int MAXF = 12;
+
+struct FieldSet {
+  void* p[MAXF];
+};
+
+inline FieldSet fset(void* a = nullptr, void* b = nullptr, void* c = nullptr, void* d = nullptr,
+                     void* e = nullptr, void* f = nullptr, void* g = nullptr, void* h = nullptr) {
+  FieldSet s{};
+  s.p[0] = a; s.p[1] = b; s.p[2] = c; s.p[3] = d;
+  s.p[4] = e; s.p[5] = f; s.p[6] = g; s.p[7] = h;
+  return s;
+}
+
+// k_fft.cu
+cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+
+// Tridiagonal row description of one implicit equation (one per row j of
+// 0..Nyp+1): coefficients l, d, u; is_bc marks rows whose right-hand side
+// is the constant bc (from apply_BC_*), others take r + CN-explicit term.
+struct TriRow {
+  double l, d, u, bc;
+  double ap;      // forward-eliminated multiplier a'_j (Thomas)
+  double ibp;     // 1 / b'_j
+  double cn_lo, cn_hi;  // explicit CN: term = cn_hi*(u_{j+1}-u_j) - cn_lo*(u_j-u_{j-1})
+  int is_bc, interior;
+  int pad[2];
+};
+
+// Pointers of the full device state for the substep kernels.
+struct State {
+  double2 *cu1, *cu2, *cu3, *cp, *cth;       // spectral
+  double2 *cf1, *cf2, *cf3, *cfth;           // spectral RK history
+  double2* xh[8];                            // x-half scratch
+  double *u1, *u2, *u3, *th;                 // physical
+  double *r1, *r2, *r3, *rth;                // physical RHS
+  double2* phi_g;                            // rem_div forward-sweep scratch (spectral)
+  double2* pfac;                             // rem_div factors (a', 1/b') per (kx,kz,j)
+  TriRow* tri;                               // 4 equations x np rows (th, u2, u1, u3)
+  DevScalars* sc;
+};
+
+// k_substep.cu
+cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
+cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
+cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st);
+struct CflCtl {
+  double cfl, time_limit;
+  int variable_dt, update_dt;
+  int force;               // 1: evaluate regardless of variable_dt/time_step
+};
+cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st);
+cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp, cudaStream_t st);
+cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st);
+cudaError_t launch_step_end(DevScalars* sc, cudaStream_t st);
+cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
+
+}  // namespace db

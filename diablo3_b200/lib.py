@@ -1,0 +1,101 @@
+"""ctypes binding of libdiablo_b200.so (include/diablo_b200.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import DbParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdiablo_b200.so")
+
+# enum db_field
+CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH, NU_T, KAPPA_T = range(11)
+STATE_FIELDS = (CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH)
+
+# exported symbols, in header order
+EXPORTS = (
+    "db_abi_version", "db_last_error", "db_init", "db_finalize",
+    "db_upload_state", "db_download_state", "db_upload_field", "db_download_field",
+    "db_set_clock", "db_get_status", "db_clear_status",
+    "db_fft_xz_to_fourier", "db_fft_xz_to_physical",
+    "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
+    "db_courant", "db_divergence",
+    "db_set_timing", "db_stage_times", "db_kernel_launches",
+)
+STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
+          "fwd_x", "fwd_z", "rem_div")
+
+
+class DbStatus(ctypes.Structure):
+    _fields_ = [
+        ("flags", ctypes.c_int32), ("time_step", ctypes.c_int32),
+        ("time", ctypes.c_double), ("delta_t", ctypes.c_double), ("max_div", ctypes.c_double),
+    ]
+
+
+class DiabloError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[db error {code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load the library (it must have been built: diablo3_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: run `python -m diablo3_b200.build` (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    vp, dp, i32 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32
+    L.db_abi_version.restype = ctypes.c_int
+    L.db_last_error.restype = ctypes.c_char_p
+    L.db_last_error.argtypes = [vp]
+    L.db_init.argtypes = [ctypes.POINTER(DbParams), dp, vp, ctypes.POINTER(vp)]
+    L.db_finalize.argtypes = [vp]
+    L.db_upload_state.argtypes = [vp] + [dp] * 9
+    L.db_download_state.argtypes = [vp] + [dp] * 9
+    L.db_upload_field.argtypes = [vp, ctypes.c_int, dp]
+    L.db_download_field.argtypes = [vp, ctypes.c_int, dp]
+    L.db_set_clock.argtypes = [vp, ctypes.c_double, i32, ctypes.c_double, ctypes.c_double]
+    L.db_get_status.argtypes = [vp, ctypes.POINTER(DbStatus)]
+    L.db_clear_status.argtypes = [vp]
+    L.db_fft_xz_to_fourier.argtypes = [vp, dp]
+    L.db_fft_xz_to_physical.argtypes = [vp, dp]
+    L.db_rk_substep.argtypes = [vp, ctypes.c_int]
+    L.db_rk_steps.argtypes = [vp, ctypes.c_int]
+    L.db_rem_div.argtypes = [vp]
+    L.db_apply_bc_vel_post.argtypes = [vp]
+    L.db_courant.argtypes = [vp, dp]
+    L.db_divergence.argtypes = [vp, dp]
+    L.db_set_timing.argtypes = [vp, ctypes.c_int]
+    L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
+    L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    for name in EXPORTS:
+        if name not in ("db_abi_version", "db_last_error"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def check(rc: int, handle=None):
+    if rc != 0:
+        raise DiabloError(rc, load().db_last_error(handle).decode())

@@ -1,0 +1,83 @@
+"""Algorithmic HBM bytes of the FP64 substep, per stage (one place).
+
+Units per wall-normal plane set (Nyp+2 planes, ghosts included):
+  P  = Nx * Nz * 8 B             one physical field
+  Xh = (Nkx+1) * Nz * 16 B       one x-transformed, not z-transformed field
+  S  = (Nkx+1) * (2Nkz+1) * 16 B one dealiased packed spectral field
+Each stage counts the bytes it must read and write once when everything
+inside it is fused (neighbour planes in y are L2 hits):
+
+  inv_z      4 S  -> 4 Xh           cu1, cu2, cu3, cth to x-half
+  inv_x      4 Xh -> 4 P            to physical u1, u2, u3, th
+  products   4 P  -> 8 Xh           11 products + x-FFT, x-derivatives folded
+  zpass_rhs  8 Xh + 9 S -> 4 S + 4 Xh   z-FFT, spectral RHS (cu, cp, cth,
+                                        cf_old in; cf out), inverse z of cr
+  inv_x_r    4 Xh -> 4 P            r1, r2, r3, rth
+  thomas     8 P  -> 4 P            r and u in (CN explicit), u out
+  courant    3 P  -> 0              only on the third substep (averaged /3)
+  fwd_x      4 P  -> 4 Xh
+  fwd_z      4 Xh -> 4 S
+  rem_div    4 S  -> 4 S            cu1, cu2, cu3, cp in and out
+At 512x257x512 this is ~67 P, i.e. ~540 B per grid point and substep.
+"""
+from __future__ import annotations
+
+import os
+import re
+
+
+def units(p) -> dict:
+    nplanes = p.ny + 2
+    nkx, nkz = p.nx // 3, p.nz // 3
+    return {
+        "P": p.nx * p.nz * 8 * nplanes,
+        "Xh": (nkx + 1) * p.nz * 16 * nplanes,
+        "S": (nkx + 1) * (2 * nkz + 1) * 16 * nplanes,
+    }
+
+
+def stage_bytes(p) -> dict:
+    u = units(p)
+    P, X, S = u["P"], u["Xh"], u["S"]
+    cour = (3 * P / 3.0) if p.variable_dt else 0.0
+    return {
+        "inv_z": 4 * S + 4 * X,
+        "inv_x": 4 * X + 4 * P,
+        "products": 4 * P + 8 * X,
+        "zpass_rhs": 8 * X + 9 * S + 4 * S + 4 * X,
+        "inv_x_r": 4 * X + 4 * P,
+        "thomas": 12 * P,
+        "courant": cour,
+        "fwd_x": 4 * P + 4 * X,
+        "fwd_z": 4 * X + 4 * S,
+        "rem_div": 8 * S,
+    }
+
+
+def substep_bytes(p) -> float:
+    return float(sum(stage_bytes(p).values()))
+
+
+def state_transfer_bytes(p) -> int:
+    """Bytes one db_upload_state (or 9 db_download_field) moves over PCIe:
+    nine spectral fields in the device's packed layout."""
+    kxs = ((p.nx // 3 + 1) + 3) // 4 * 4
+    return 9 * (p.ny + 2) * (2 * (p.nz // 3) + 1) * kxs * 16
+
+
+def profiled_traffic(stage: str, root: str):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch of a stage,
+    from the ncu summary committed under profiles/ (a line
+    ``traffic_per_launch <stage> <bytes>``), or None."""
+    d = os.path.join(root, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(d, fn)) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_per_launch\s+(\w+)\s+([0-9.eE+]+)", line)
+                if m and m.group(1) == stage:
+                    return float(m.group(2))
+    return None

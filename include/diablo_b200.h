@@ -1,0 +1,217 @@
+/*
+ * diablo_b200.h -- C-ABI of the B200 (sm_100a) channel time step.
+ *
+ * This is the drop-in boundary for DIABLO 3.0's channel solver
+ * (wienkers/diablo3, Fortran 90).  Each entry point replaces one Fortran
+ * subroutine; the reference interface it stands in for is cited beside it.
+ * A Fortran caller binds these through ISO_C_BINDING (interface block in
+ * INTEGRATION.md); Python binds them through ctypes (diablo3_b200/lib.py).
+ *
+ * Conventions
+ *  - Coordinates follow the Fortran code: x streamwise (periodic), y
+ *    wall-normal (finite differences on a stretched grid), z spanwise
+ *    (periodic).  nx, ny, nz are the code's Nx, NY (= Nyp on one rank), Nz.
+ *  - "Reference spectral layout" is the Fortran array
+ *    complex(8) cu(0:Nxp, 0:Nz+1, 0:Nyp+1), Nxp = Nx/2, column-major, passed
+ *    as double* of 2*(Nxp+1)*(Nz+2)*(Nyp+2) values (re, im interleaved).
+ *    "Reference physical layout" is real(8) u(0:Nx+1, 0:Nz+1, 0:Nyp+1);
+ *    both views alias the same number of doubles (for/fft.f90:71-96).
+ *  - Every entry point returns int: 0 on success, a DB_ERR_* code otherwise.
+ *    Nothing aborts the process; db_last_error() gives the message.
+ *  - A context is not thread-safe: one host thread per context.  All work
+ *    is issued on the stream given to db_init (NULL = a stream the context
+ *    creates).  Host buffers stay owned by the caller.
+ */
+#ifndef DIABLO_B200_H
+#define DIABLO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DB_ABI_VERSION 1
+
+enum db_error {
+  DB_OK = 0,
+  DB_ERR_ARG = 1,          /* bad argument (NULL pointer, bad field id) */
+  DB_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  DB_ERR_SIZE = 3,         /* grid size not supported */
+  DB_ERR_UNSUPPORTED = 4,  /* option the reference supports but not built */
+  DB_ERR_STATE = 5,        /* call out of order (e.g. before db_init) */
+  DB_ERR_NUMERIC = 6,      /* NaN/Inf or dt <= 0 detected on the device */
+  DB_ERR_TIMEOUT = 7       /* a bounded device wait gave up */
+};
+
+/* Status flags reported by db_get_status (bit mask). */
+enum db_flag {
+  DB_FLAG_NONFINITE = 1,   /* NaN/Inf found in the velocity or buoyancy */
+  DB_FLAG_DT_NONPOS = 2,   /* courant found dt <= 0 (reference flow.f90:812) */
+  DB_FLAG_DT_CAPPED = 4,   /* courant capped dt at 1000 (flow.f90:817) */
+  DB_FLAG_DT_TINY = 8      /* next dt < 1e-10 (flow.f90:848) */
+};
+
+/* Field ids for db_upload_field / db_download_field. */
+enum db_field {
+  DB_CU1 = 0, DB_CU2 = 1, DB_CU3 = 2, DB_CP = 3, DB_CTH = 4,
+  DB_CF1 = 5, DB_CF2 = 6, DB_CF3 = 7, DB_CFTH = 8,
+  DB_NU_T = 9, DB_KAPPA_T = 10,   /* physical layout, GY points */
+  DB_NFIELDS = 11
+};
+
+/*
+ * Run parameters: the contents of input.dat / input_chan.dat version 3.4
+ * (for/parameters.f90:84-121, 202-250) plus grid_def, as the Fortran reads
+ * them (before input_chan's thermal-wind compensation, which db_init applies
+ * exactly as for/parameters.f90:255-279 does).
+ */
+typedef struct db_params {
+  /* grid_def: code sizes (for/domain.f90:20-24) */
+  int32_t nx, ny, nz, n_th;
+  /* input.dat */
+  double re, beta, lx, ly, lz, nu_v_scale;
+  double delta_t, cfl;
+  int32_t variable_dt, update_dt;
+  double ri, pr;
+  int32_t use_les, create_new_flow;
+  /* input_chan.dat */
+  int32_t time_ad_meth, les_model_type, ic_type, physical_noise;
+  double kick, ro, delta, grav_x, grav_y, grav_z;
+  int32_t f_type, flavor_front;   /* flavor_front: 1 when FLAVOUR == 'Front' */
+  double ubulk0, px0, omega0, amp_omega0, force_start;
+  int32_t u_bc_ymin, v_bc_ymin, w_bc_ymin, th_bc_ymin;
+  int32_t u_bc_ymax, v_bc_ymax, w_bc_ymax, th_bc_ymax;
+  double u_bc_ymin_c1, v_bc_ymin_c1, w_bc_ymin_c1, th_bc_ymin_c1;
+  double u_bc_ymax_c1, v_bc_ymax_c1, w_bc_ymax_c1, th_bc_ymax_c1;
+  /* Extension (not in the reference): background buoyancy gradient M^2.
+   * NaN keeps the reference tie dTHdX = Ro_inv/delta (infinite front) or
+   * 2/Lx*Ro_inv (finite front), for/parameters.f90:264,274. */
+  double dthdx_override;
+  /* run control used by courant's next-event scheduling (flow.f90:825) */
+  double time_limit, save_stats_dt, save_flow_dt;
+  int32_t precision;               /* 0 = FP64 throughout (plain path) */
+  int32_t reserved_i[7];
+} db_params;
+
+typedef struct db_status {
+  int32_t flags;          /* DB_FLAG_* bits accumulated since last clear */
+  int32_t time_step;      /* driver counter (for/diablo.f90:59) */
+  double time;            /* simulation time */
+  double delta_t;         /* current dt (updated by courant) */
+  double max_div;         /* max |div u| over modes, from db_divergence */
+} db_status;
+
+typedef struct db_ctx db_ctx;
+
+/* ABI version of the loaded library (DB_ABI_VERSION). */
+int db_abi_version(void);
+
+/* Message for the last error on this context (or the last db_init error when
+ * ctx is NULL).  Never NULL. */
+const char* db_last_error(const db_ctx* ctx);
+
+/*
+ * Create a context: allocates the whole state on the current CUDA device,
+ * builds grid metrics and wavenumbers.  gy holds the ny+1 values of
+ * grid.h5:/grids/y, i.e. GY(1:Nyp+1).
+ * Replaces init_parameters' grid/coefficient part + init_fft + allocate_all
+ * (for/parameters.f90:75-188, for/domain.f90:246-374, for/fft.f90:128-236,
+ * for/flow.f90:176-196).
+ */
+int db_init(const db_params* p, const double* gy, void* cuda_stream, db_ctx** out);
+
+/* Release all device memory of the context. */
+int db_finalize(db_ctx* ctx);
+
+/* Copy spectral state from / to host arrays in the reference spectral layout.
+ * Any pointer may be NULL (upload: field set to zero; download: skipped).
+ * Replaces the module-global state of for/flow.f90:12-18. */
+int db_upload_state(db_ctx* ctx, const double* cu1, const double* cu2,
+                    const double* cu3, const double* cp, const double* cth,
+                    const double* cf1, const double* cf2, const double* cf3,
+                    const double* cfth);
+int db_download_state(db_ctx* ctx, double* cu1, double* cu2, double* cu3,
+                      double* cp, double* cth, double* cf1, double* cf2,
+                      double* cf3, double* cfth);
+
+/* One field (enum db_field): spectral fields in the reference spectral
+ * layout, DB_NU_T / DB_KAPPA_T in the reference physical layout. */
+int db_upload_field(db_ctx* ctx, int field, const double* host);
+int db_download_field(db_ctx* ctx, int field, double* host);
+
+/* Driver clock: time, time_step and the next output times used by courant
+ * (for/diablo.f90:59-68, for/flow.f90:825-828). */
+int db_set_clock(db_ctx* ctx, double time, int32_t time_step,
+                 double save_stats_time, double save_flow_time);
+int db_get_status(db_ctx* ctx, db_status* out);
+int db_clear_status(db_ctx* ctx);
+
+/* In-place 2-D transforms of one host array in the reference layout.
+ * fft_xz_to_fourier: physical -> packed, dealiased spectral, forward scaled
+ * by 1/(Nx Nz).  fft_xz_to_physical: inverse, unnormalised.
+ * Replace for/fft.f90:242-307 and 311-374. */
+int db_fft_xz_to_fourier(db_ctx* ctx, double* inout);
+int db_fft_xz_to_physical(db_ctx* ctx, double* inout);
+
+/* RKW3 + Crank-Nicolson substep rk_step in {1,2,3} on the device state.
+ * Replaces rk_chan_1 (for/solver.f90:366-1273). */
+int db_rk_substep(db_ctx* ctx, int rk_step);
+
+/* nsteps full time steps (3 substeps each, then time += delta_t), replayed
+ * from a CUDA graph captured on first use.  Replaces the loop body of
+ * for/diablo.f90:58-69 (without I/O). */
+int db_rk_steps(db_ctx* ctx, int nsteps);
+
+/* Divergence removal on the spectral velocity (projection, phi kept in the
+ * context).  Replaces rem_div_chan (for/solver.f90:1302-1379). */
+int db_rem_div(db_ctx* ctx);
+
+/* Ghost/boundary rows of the spectral velocity after an initial condition.
+ * Replaces apply_BC_vel_mpi_post (for/flow.f90:1161-1360, 1698-1713). */
+int db_apply_bc_vel_post(db_ctx* ctx);
+
+/* CFL time step from the current state (velocity transformed internally),
+ * with courant's limits and next-event scheduling; sets delta_t and the RK
+ * coefficients.  Replaces courant (for/flow.f90:746-857). */
+int db_courant(db_ctx* ctx, double* delta_t_out);
+
+/* max over (kx,kz,j) of |ikx u1 + d(u2)/dy + ikz u3| in spectral space at
+ * GYF points j = 2..Nyp-1, the quantity rem_div_chan drives to zero. */
+int db_divergence(db_ctx* ctx, double* max_div_out);
+
+/* ---- measurement hooks (no counterpart in the reference, which only
+ * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */
+
+/* Stages of one substep, in launch order. */
+enum db_stage {
+  DB_ST_INV_Z = 0,     /* cu -> x-half, 4 fields      (fft.f90:322-337)   */
+  DB_ST_INV_X = 1,     /* x-half -> u, 4 fields       (fft.f90:364-372)   */
+  DB_ST_PRODUCTS = 2,  /* 11 products + x-FFT         (solver.f90:655-964) */
+  DB_ST_ZPASS_RHS = 3, /* z-FFT + spectral RHS + inverse z of cr          */
+  DB_ST_INV_X_R = 4,   /* cr x-half -> r, 4 fields                        */
+  DB_ST_THOMAS = 5,    /* CN explicit + Thomas, 4 eqs (solver.f90:1012-1233) */
+  DB_ST_COURANT = 6,   /* CFL reduction (rk_step 3)   (flow.f90:746-857)  */
+  DB_ST_FWD_X = 7,     /* u -> x-half, 4 fields                           */
+  DB_ST_FWD_Z = 8,     /* x-half -> cu, 4 fields                          */
+  DB_ST_REM_DIV = 9,   /* projection + cp update      (solver.f90:1257-1267) */
+  DB_NSTAGES = 10
+};
+
+/* Record CUDA events between the stages of every substep (the step graph is
+ * re-captured with event nodes).  Off by default. */
+int db_set_timing(db_ctx* ctx, int enable);
+
+/* Device milliseconds per stage of the most recent full step, summed over
+ * its three substeps; ms must hold DB_NSTAGES values. */
+int db_stage_times(db_ctx* ctx, double* ms, int nstages);
+
+/* Number of this library's kernels issued on the context so far. */
+int db_kernel_launches(db_ctx* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIABLO_B200_H */

@@ -1,0 +1,165 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+FP64 tolerances: transforms 1e-13 relative; one substep 1e-12; 20 steps
+1e-10 relative L2 per field (the plain-path bar); divergence after the
+projection <= 1e-12.
+"""
+import numpy as np
+import pytest
+
+from _util import (NAMES, STATE, channel_state, config0_params, grid_for, oracle_state, rel_l2,
+                   seed_pair, significant)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def Channel():
+    from diablo3_b200.channel import Channel
+    return Channel
+
+
+def _cmp(o, ch, p, tol, fields=STATE):
+    so, sg = oracle_state(o, p), channel_state(ch, p)
+    errs = {NAMES[f]: rel_l2(sg[f], so[f]) for f in fields}
+    bad = {k: v for k, v in errs.items() if not (v <= tol)}
+    assert not bad, f"rel L2 above {tol}: {bad} (all: {errs})"
+    return errs
+
+
+@pytest.mark.parametrize("n", [(16, 17, 16), (64, 33, 32), (32, 65, 128)])
+def test_fft_xz_matches_oracle(oracle_mod, Channel, n):
+    nx, ny, nz = n
+    p = config0_params(nx=nx, ny=ny, nz=nz)
+    gy = grid_for(p)
+    o = oracle_mod.Oracle(p, gy)
+    rng = np.random.default_rng(11)
+    phys = rng.standard_normal((p.ny + 2, p.nz + 2, p.nx + 2))
+    a = phys.copy()
+    o.fft_to_fourier(a.reshape(-1))
+    with Channel(p, gy) as ch:
+        b = phys.copy()
+        cb = ch.fft_xz_to_fourier(b)
+        ca = a.reshape(-1).view(np.complex128).reshape(cb.shape)
+        assert rel_l2(significant(p, cb), significant(p, ca)) < 1e-13
+        # inverse on the (dealiased) spectrum
+        a2 = ca.copy()
+        o.fft_to_physical(a2.view(np.float64).reshape(-1))
+        b2 = cb.copy()
+        rb = ch.fft_xz_to_physical(b2)
+        ra = a2.view(np.float64).reshape(rb.shape)
+        assert rel_l2(rb[:, :nz, :nx], ra[:, :nz, :nx]) < 1e-13
+
+
+def test_rem_div_matches_oracle_and_zeroes_divergence(oracle_mod, Channel):
+    p = config0_params(nx=32, ny=33, nz=32)
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=3)
+    # perturb the velocity so it is not divergence free, identically on both
+    rng = np.random.default_rng(5)
+    for fid in (0, 1, 2):
+        c = o.cplx(fid)
+        c[:, : 2 * p.nkz + 1, : p.nkx + 1] += 1e-2 * (rng.standard_normal(c[:, : 2 * p.nkz + 1, : p.nkx + 1].shape)
+                                                      + 1j * rng.standard_normal(c[:, : 2 * p.nkz + 1, : p.nkx + 1].shape))
+        ch.upload_field(fid, c.copy())
+    o.rem_div()
+    ch.rem_div_chan()
+    _cmp(o, ch, p, 1e-12, fields=(0, 1, 2))
+    assert ch.divergence() < 1e-12
+
+
+@pytest.mark.parametrize("rk", [1, 2, 3])
+def test_single_substep_matches_oracle(oracle_mod, Channel, rk):
+    p = config0_params(nx=32, ny=33, nz=32)
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=5)
+    # give cf a non-trivial history so rk > 1 exercises zeta*h*cf
+    o.rk_substep(1)
+    ch.upload_state({fid: o.cplx(fid).copy() for fid in STATE})
+    o.rk_substep(rk)
+    ch.rk_chan_1(rk)
+    _cmp(o, ch, p, 1e-12)
+
+
+def test_config0_20_steps(oracle_mod, Channel):
+    """Config 0 (64x65x64), 20 RKW3 steps at fixed dt: relative L2 <= 1e-10
+    per field, divergence <= 1e-12."""
+    p = config0_params()
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=0)
+    for _ in range(20):
+        o.step()
+    ch.step(20)
+    errs = _cmp(o, ch, p, 1e-10)
+    assert ch.divergence() <= 1e-12, errs
+    t, ts, dt = o.clock()
+    s = ch.status()
+    assert s.time_step == ts == 20
+    assert abs(s.time - t) <= 1e-15 * max(1.0, abs(t))
+
+
+@pytest.mark.parametrize("bcs", [
+    dict(u_bc_ymin=1, w_bc_ymin=1, v_bc_ymin=0, u_bc_ymax=1, w_bc_ymax=1, v_bc_ymax=0,
+         th_bc_ymin=1, th_bc_ymax=1),                       # infinite_front_DNS rows
+    dict(u_bc_ymin=0, w_bc_ymin=0, v_bc_ymin=0, u_bc_ymax=0, w_bc_ymax=0, v_bc_ymax=0,
+         th_bc_ymin=0, th_bc_ymax=0, th_bc_ymin_c1=-1.0, th_bc_ymax_c1=1.0),
+    dict(u_bc_ymin=1, w_bc_ymin=0, v_bc_ymin=1, u_bc_ymax=0, w_bc_ymax=1, v_bc_ymax=1,
+         th_bc_ymin=0, th_bc_ymax=1, u_bc_ymin_c1=0.3, w_bc_ymax_c1=-0.2),
+])
+def test_boundary_variants_5_steps(oracle_mod, Channel, bcs):
+    p = config0_params(nx=32, ny=33, nz=32, **bcs)
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=2)
+    for _ in range(5):
+        o.step()
+    ch.step(5)
+    _cmp(o, ch, p, 1e-11)
+
+
+@pytest.mark.parametrize("extra", [
+    dict(f_type=1, px0=-0.5),
+    dict(f_type=2, px0=0.1, amp_omega0=0.3, omega0=2.0),
+    dict(f_type=4, amp_omega0=0.05, omega0=3.0, w_bc_ymax=1),
+    dict(ic_type=7, ro=1.0, delta=0.5, lx=4.0, ri=1.0),
+    dict(ic_type=2, flavor_front=0, ro=1e30, ri=0.5, th_bc_ymin=1, th_bc_ymax=1),
+    dict(dthdx_override=0.1),
+    dict(grav_x=0.2, grav_z=-0.1, nu_v_scale=2.0, pr=0.7),
+])
+def test_forcing_and_physics_variants(oracle_mod, Channel, extra):
+    p = config0_params(nx=32, ny=33, nz=32, **extra)
+    gy = grid_for(p, grid_type=3 if extra.get("ic_type") == 7 else 1)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=4)
+    for _ in range(4):
+        o.step()
+    ch.step(4)
+    _cmp(o, ch, p, 1e-11)
+
+
+def test_variable_dt_courant(oracle_mod, Channel):
+    p = config0_params(nx=32, ny=33, nz=32, variable_dt=1, cfl=0.5, update_dt=1, kick=0.05,
+                       delta_t=1e-3, time_limit=1e9)
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=9)
+    for _ in range(6):
+        o.step()
+    ch.step(6)
+    t, ts, dt = o.clock()
+    s = ch.status()
+    assert abs(s.delta_t - dt) <= 1e-13 * dt
+    assert abs(s.time - t) <= 1e-13 * max(t, 1e-300)
+    _cmp(o, ch, p, 1e-11)
+
+
+def test_substep_entry_equals_graph_step(oracle_mod, Channel):
+    """db_rk_substep x3 and the captured-graph db_rk_steps give the same state."""
+    p = config0_params(nx=32, ny=33, nz=32)
+    gy = grid_for(p)
+    o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=1)
+    with Channel(p, gy) as ch2:
+        ch2.upload_state({fid: o.cplx(fid).copy() for fid in STATE})
+        for rk in (1, 2, 3):
+            ch2.rk_chan_1(rk)
+        ch.step(1)
+        a, b = channel_state(ch, p), channel_state(ch2, p)
+        for f in STATE:
+            assert rel_l2(a[f], b[f]) < 1e-15
