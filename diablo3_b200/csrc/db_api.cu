@@ -43,7 +43,7 @@ struct db_ctx {
 static std::string g_init_err;
 
 static void mark(db_ctx* c, int rk, int stage) {
-  if (c->timing) cudaEventRecord(c->ev[rk][stage], c->st);
+  if (c->timing) cudaEventRecordWithFlags(c->ev[rk][stage], c->st, cudaEventRecordExternal);
 }
 
 #define CK(call)                                                                         \
@@ -506,6 +506,10 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */) {
   if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st))) return e;
   mark(c, rk, 9);
   if ((e = launch_rem_div(g, s, rk, 1, st))) return e;
+  if (rk == 2 && c->p.variable_dt) {
+    if ((e = launch_apply_dt(s.sc, st))) return e;
+    n += 1;
+  }
   mark(c, rk, 10);
   n += 3;
   c->launches += n;
@@ -619,6 +623,7 @@ extern "C" int db_courant(db_ctx* c, double* delta_t_out) {
   CK(launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2]), fset(s.u1, s.u2, s.u3), 3, c->st));
   CflCtl ctl{c->p.cfl, c->p.time_limit, 1, 1, 1};
   CK(launch_courant(g, c->ph, s, ctl, c->st));
+  CK(launch_apply_dt(s.sc, c->st));
   db_status stt;
   int rc = db_get_status(c, &stt);
   if (rc) return rc;

@@ -70,7 +70,10 @@ struct DevScalars {
   int time_step;
   int flags;                        // DB_FLAG_* bits
   double max_div;
-  double pad[4];
+  double dt_next;                   // courant's new dt, applied after the substep
+  int dt_pending;
+  int pad_i;
+  double pad[2];
 };
 
 // RKW3 constants, for/parameters.f90:179-184

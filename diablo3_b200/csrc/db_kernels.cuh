@@ -66,6 +66,7 @@ struct CflCtl {
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st);
 cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp, cudaStream_t st);
 cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_apply_dt(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_end(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st);

@@ -603,10 +603,21 @@ __global__ void k_courant_final(DevScalars* sc, Phys ph, CflCtl ctl) {
   else if (next < (1. + r_max) * dt) delta_t = 1. / (1. + r_max) * next;
   else delta_t = dt;
   if (delta_t < 1.e-10) sc->flags |= 8;
+  // rk_chan_1 froze temp1..temp5 at its start (solver.f90:385-389): the new
+  // dt takes effect after the substep's projection and pressure update
+  sc->dt_next = delta_t;
+  sc->dt_pending = 1;
+}
+
+// flow.f90:852-854, applied once the substep that called courant is done
+__global__ void k_apply_dt(DevScalars* sc) {
+  if (!sc->dt_pending) return;
+  const double delta_t = sc->dt_next;
   sc->delta_t = delta_t;
   sc->h_bar[0] = delta_t * (8.0 / 15.0);
   sc->h_bar[1] = delta_t * (2.0 / 15.0);
   sc->h_bar[2] = delta_t * (5.0 / 15.0);
+  sc->dt_pending = 0;
 }
 
 __global__ void k_step_begin(DevScalars* sc) { sc->time_step += 1; }
@@ -763,6 +774,10 @@ cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp,
 }
 cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st) {
   k_pfac<<<dim3((g.nkx + 1 + 127) / 128, g.nkzp), 128, 0, st>>>(g, s.pfac);
+  return cudaGetLastError();
+}
+cudaError_t launch_apply_dt(DevScalars* sc, cudaStream_t st) {
+  k_apply_dt<<<1, 1, 0, st>>>(sc);
   return cudaGetLastError();
 }
 cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st) {
