@@ -27,6 +27,7 @@ EXPORTS = (
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
     "db_courant", "db_divergence",
     "db_set_timing", "db_stage_times", "db_kernel_launches",
+    "db_rem_div_static",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -81,6 +82,7 @@ def load(path: str | None = None):
     L.db_set_timing.argtypes = [vp, ctypes.c_int]
     L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
     L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.db_rem_div_static.argtypes = [ctypes.POINTER(DbParams), dp, vp, vp, vp, vp]
     for name in EXPORTS:
         if name not in ("db_abi_version", "db_last_error"):
             getattr(L, name).restype = ctypes.c_int

@@ -181,6 +181,25 @@ int db_courant(db_ctx* ctx, double* delta_t_out);
  * GYF points j = 2..Nyp-1, the quantity rem_div_chan drives to zero. */
 int db_divergence(db_ctx* ctx, double* max_div_out);
 
+/*
+ * Divergence removal that allocates nothing.  No counterpart in the
+ * reference (it follows rem_div_chan's arithmetic, for/solver.f90:1302-1379,
+ * but needs no context).  For callers that cannot allocate device memory:
+ * their device arrays belong to another memory manager (CUDA Fortran or
+ * OpenACC pools), or they must not allocate once their time loop runs.
+ * cu1, cu2, cu3 are DEVICE arrays in the reference spectral layout
+ * (0:Nxp, 0:Nz+1, 0:Nyp+1) complex(8), projected in place; gy is the HOST
+ * grid GY(1:Nyp+1).  Only p->nx, ny, nz, lx, lz are read.  Work is queued on
+ * `stream` and is complete when the stream is.  Working memory is an 8 MiB
+ * static device array held by every GPU that loads the library; it limits
+ * ny to 10697 (DB_ERR_SIZE above that).  The first call on each device looks
+ * up that array's address and should come before any stream capture.  All
+ * calls share the array: calls overlapping on the GPU race, so serialise
+ * them.  Returns DB_ERR_ARG / DB_ERR_SIZE / DB_ERR_CUDA on failure.
+ */
+int db_rem_div_static(const db_params* p, const double* gy, double* cu1,
+                      double* cu2, double* cu3, void* cuda_stream);
+
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */
 
