@@ -40,6 +40,10 @@ def workload_params(name: str):
             u_bc_ymin=0, w_bc_ymin=0, v_bc_ymin=0, th_bc_ymin=1,
             u_bc_ymax=1, w_bc_ymax=1, v_bc_ymax=0, th_bc_ymax=1,
             th_bc_ymin_c1=1.0, th_bc_ymax_c1=1.0)
+    if name == "slab":
+        p = workload_params("config1")
+        p.ny = 65  # 512x65x512: same planes, fields still > L2, for ncu captures
+        return p
     if name == "config0":
         p = workload_params("config1")
         p.nx, p.ny, p.nz, p.re, p.variable_dt = 64, 65, 64, 1000.0, 0
@@ -50,6 +54,7 @@ def workload_params(name: str):
 WORKLOAD_DESC = {
     "config1": "plain FP64 DNS, infinite front, 512x257x512 (x,y,z), Re 5000, Ri 1 (M2=N2=f=1), CFL 0.5",
     "config0": "plain FP64 DNS, infinite front, 64x65x64, Re 1000, fixed dt 1e-3",
+    "slab": "plain FP64 DNS, infinite front, 512x65x512 (profiling case), Re 5000, Ri 1, CFL 0.5",
 }
 
 
@@ -177,7 +182,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--config", default="config1", choices=["config1", "config0", "slab"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()

@@ -1,0 +1,200 @@
+"""Host-side logic and the C-ABI surface (no GPU needed)."""
+import ctypes
+import math
+import os
+import re
+import textwrap
+
+import numpy as np
+import pytest
+
+from diablo3_b200 import roofline
+from diablo3_b200.grid import create_grid, metrics
+from diablo3_b200.params import DbParams, InputError, make_params, read_inputs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "diablo_b200.h")
+
+
+def test_header_symbols_exported_by_library():
+    from diablo3_b200 import lib as L
+    lib = L.load()
+    src = open(HEADER).read()
+    names = set(re.findall(r"^\s*(?:int|const char\*)\s+(db_\w+)\s*\(", src, flags=re.M))
+    assert names, "no declarations parsed"
+    for n in sorted(names):
+        assert hasattr(lib, n), f"{n} declared in the header but not exported"
+    assert set(L.EXPORTS) == names
+    assert lib.db_abi_version() == 1
+
+
+def test_params_struct_layout_matches_header():
+    # every field of the C struct appears in the ctypes mirror, in order
+    src = open(HEADER).read()
+    body = src[src.index("typedef struct db_params"):src.index("} db_params;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    cfields = []
+    for decl in re.findall(r"(?:int32_t|double)\s+([^;]+);", body):
+        for name in decl.split(","):
+            cfields.append(re.sub(r"\[.*\]", "", name).strip())
+    assert [f for f, _ in DbParams._fields_] == cfields
+    assert ctypes.sizeof(DbParams) % 8 == 0
+
+
+def test_init_without_gpu_fails_cleanly():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from diablo3_b200 import lib as L
+    p = make_params(nx=32, ny=33, nz=32)
+    gy = create_grid(p.ny, lz=2.0, grid_type=1)
+    h = ctypes.c_void_p()
+    rc = L.load().db_init(ctypes.byref(p), L.dptr(gy), None, ctypes.byref(h))
+    assert rc == 2 and not h.value
+    assert b"CUDA" in L.load().db_last_error(None)
+
+
+def test_init_rejects_unsupported_options():
+    from diablo3_b200 import lib as L
+    gy = create_grid(33, lz=2.0, grid_type=1)
+    for bad, code in ((dict(nx=48), 3), (dict(n_th=2), 4), (dict(time_ad_meth=2), 4),
+                      (dict(u_bc_ymin=2), 1)):
+        p = make_params(nx=32, ny=33, nz=32)
+        for k, v in bad.items():
+            setattr(p, k, v)
+        h = ctypes.c_void_p()
+        assert L.load().db_init(ctypes.byref(p), L.dptr(gy), None, ctypes.byref(h)) == code
+
+
+@pytest.mark.parametrize("gt", [1, 3])
+def test_create_grid_walls_and_metrics(gt):
+    n = 65
+    g = create_grid(n, lz=2.0 if gt == 1 else 1.0, cs=1.5, grid_type=gt)
+    assert g.shape == (n + 1,)
+    assert np.all(np.diff(g) > 0)
+    m = metrics(g)
+    lo, hi = (-1.0, 1.0) if gt == 1 else (0.0, 1.0)
+    # GF(2) and GF(N+1) are the walls (create_grid.m:60-82)
+    assert abs(m["gyf"][1] - lo) < 1e-14 and abs(m["gyf"][n] - hi) < 1e-14
+    assert np.allclose(m["dy"][1:], np.diff(m["gyf"]))
+    if gt == 1:  # symmetric stretching
+        assert np.allclose(g + g[::-1], 0.0, atol=1e-14)
+
+
+def _write_run(tmp, version="3.4", nth=1):
+    (tmp / "grid_def.all").write_text("# Full Grid Resolution\nNx  = 128\nNy  = 96\nNz  = 33\nNth = 1\n")
+    (tmp / "input.dat").write_text(textwrap.dedent(f"""\
+        C comment
+        C comment
+        C comment
+        C   FLAVOUR       VERSION
+            'Front'       {version}
+        C   USE_MPI       USE_LES
+            .TRUE.        .FALSE.
+        C Parameters:     RE      BETA      LX      LY      LZ
+                          4.D3    1.0       10.0    2.5     1.5
+        C NU_V_SCALE
+                          1.5
+        C Method:         NUM_PER_DIR       CREATE_NEW_FLOW
+                          2                 .TRUE.
+        C Time
+                  1000           500       0.002     .FALSE.     .TRUE.       0.4      2
+        C I/O
+                  2               100            1.0              5.0            1.0 0.0 0.5
+        C Here include 6*N_TH lines
+        C         CREATE_FLOW_TH(1)
+                    .TRUE.
+        C         FILTER_TH(1)      FILTER_INT(1)
+                    .FALSE.           10
+        C         RI(1)       PR(1)
+                  0.7         2.0
+        """))
+    (tmp / "input_chan.dat").write_text(textwrap.dedent(f"""\
+        C comment
+        C comment
+        C comment
+        C VERSION
+           {version}
+        C TIME_AD_METH
+              1
+        C LES:    LES_MODEL_TYPE
+                  5
+        C ICs:	  IC_TYPE,     KICK,     PHYSICAL_NOISE
+                   7           1.D-5      .TRUE.
+        C Rotation
+                     2.0
+        C Aspect Ratio: DELTA
+                        3.0
+        C Upward vertical vector components, GRAV_X, GRAV_Y, GRAV_Z
+                                              0.1     0.2     1.0
+        C Forcing:      F_TYPE,   UBULK0,   PX0,    OMEGA0,   AMP_OMEGA0,  FORCE_START
+                          2         0.5     0.25     3.0        0.125	    0.5
+        C BCs in vertical
+        C     u_BC_Zmin,  u_BC_Zmin_C1
+              0           0.1
+        C     v_BC_Zmin,  v_BC_Zmin_C1
+              1           0.2
+        C     w_BC_Zmin,  w_BC_Zmin_C1
+              0           0.3
+        C     u_BC_Zmax,  u_BC_Zmax_C1
+              1           0.4
+        C     v_BC_Zmax,  v_BC_Zmax_C1
+              0           0.5
+        C     w_BC_Zmax,  w_BC_Zmax_C1
+              1           0.6
+        C Here include 6*N_TH lines
+        C     TH_BC_Zmin(1),  TH_BC_Zmin_C1(1)
+              1               0.7
+        C     TH_BC_Zmax(1),  TH_BC_Zmax_C1(1)
+              0               0.8
+        """))
+
+
+def test_read_inputs_applies_reference_swaps(tmp_path):
+    _write_run(tmp_path)
+    p = read_inputs(str(tmp_path))
+    # grid_def "Ny"/"Nz" -> code NZ/NY (make_headers:17-21)
+    assert (p.nx, p.ny, p.nz) == (128, 33, 96)
+    # LX LY LZ read into Lx, Lz, Ly (parameters.f90:101)
+    assert (p.lx, p.lz, p.ly) == (10.0, 2.5, 1.5)
+    assert p.re == 4000.0 and p.nu_v_scale == 1.5 and p.delta_t == 0.002
+    assert p.variable_dt == 1 and p.cfl == 0.4 and p.update_dt == 2
+    assert p.ri == 0.7 and p.pr == 2.0 and p.flavor_front == 1
+    assert p.ic_type == 7 and p.kick == 1e-5 and p.les_model_type == 5
+    assert p.ro == 2.0 and p.delta == 3.0
+    # GRAV_X, GRAV_Y, GRAV_Z read into grav_x, grav_z, grav_y (parameters.f90:227)
+    assert (p.grav_x, p.grav_z, p.grav_y) == (0.1, 0.2, 1.0)
+    assert (p.f_type, p.px0, p.omega0, p.amp_omega0, p.force_start) == (2, 0.25, 3.0, 0.125, 0.5)
+    # BC lines in the order u, w, v (parameters.f90:232-242)
+    assert (p.u_bc_ymin, p.u_bc_ymin_c1) == (0, 0.1)
+    assert (p.w_bc_ymin, p.w_bc_ymin_c1) == (1, 0.2)
+    assert (p.v_bc_ymin, p.v_bc_ymin_c1) == (0, 0.3)
+    assert (p.u_bc_ymax, p.w_bc_ymax, p.v_bc_ymax) == (1, 0, 1)
+    assert (p.th_bc_ymin, p.th_bc_ymin_c1, p.th_bc_ymax, p.th_bc_ymax_c1) == (1, 0.7, 0, 0.8)
+    assert p.save_stats_dt == 1.0 and p.save_flow_dt == 100.0
+
+
+def test_read_inputs_rejects_old_versions(tmp_path):
+    _write_run(tmp_path, version="3.3")
+    with pytest.raises(InputError):
+        read_inputs(str(tmp_path))
+
+
+def test_reference_setup_parses_when_present():
+    d = "/root/reference/setups/finite_front_LES"
+    if not os.path.isdir(d):
+        pytest.skip("reference tree not mounted")
+    p = read_inputs(d)
+    assert (p.nx, p.ny, p.nz) == (2048, 65, 128)
+    assert p.use_les == 1 and p.les_model_type == 5 and p.ic_type == 7
+
+
+def test_roofline_model_totals():
+    p = make_params(nx=512, ny=257, nz=512, variable_dt=1)
+    b = roofline.stage_bytes(p)
+    u = roofline.units(p)
+    total_p = roofline.substep_bytes(p) / u["P"]
+    assert 60 < total_p < 75
+    per_point = roofline.substep_bytes(p) / (512 * 257 * 512)
+    assert 500 < per_point < 600
+    assert b["thomas"] == 12 * u["P"]
