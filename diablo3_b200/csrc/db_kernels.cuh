@@ -8,6 +8,20 @@
 namespace db {
 
 constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple of 4)
+
+// minimum resident CTAs per SM requested from the compiler (register caps)
+#ifndef DB_LB_FFT
+#define DB_LB_FFT 3
+#endif
+#ifndef DB_LB_ZPASS
+#define DB_LB_ZPASS 2
+#endif
+#ifndef DB_ZPASS_LAZY
+#define DB_ZPASS_LAZY 1
+#endif
+#ifndef DB_LB_PROD
+#define DB_LB_PROD 4
+#endif
 constexpr int MAXF = 12;
 
 struct FieldSet {
@@ -36,9 +50,24 @@ struct TriRow {
   double ap;      // forward-eliminated multiplier a'_j (Thomas)
   double ibp;     // 1 / b'_j
   double cn_lo, cn_hi;  // explicit CN: term = cn_hi*(u_{j+1}-u_j) - cn_lo*(u_j-u_{j-1})
+  double pa;      // prod of a'_i from the start of j's chunk to j (forward carry weight)
+  double pm;      // prod of m_i = -u_i / b'_i from j to the end of its chunk (backward)
   int is_bc, interior;
   int pad[2];
 };
+
+// row chunks of the tiled Thomas solve (k_thomas): nch chunks of len rows
+struct Chunks {
+  int nch, len;
+};
+__host__ __device__ inline Chunks thomas_chunks(int np) {
+  Chunks c;
+  c.nch = np / 2 < 8 ? np / 2 : 8;
+  if (c.nch < 1) c.nch = 1;
+  c.len = (np + c.nch - 1) / c.nch;
+  c.nch = (np + c.len - 1) / c.len;
+  return c;
+}
 
 // Pointers of the full device state for the substep kernels.
 struct State {
@@ -58,6 +87,7 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st);
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st);
+
 struct CflCtl {
   double cfl, time_limit;
   int variable_dt, update_dt;

@@ -11,149 +11,154 @@
 // Inverse: Z_m = A_m + i B_m, Z_{N-m} = conj A_m + i conj B_m, with the
 // imaginary parts of the DC and Nyquist modes dropped as FFTW's c2r does and
 // modes above Nkx zeroed (the 2/3 de-aliasing, fft.f90:259-261, 366-368).
+// All transforms keep their data in registers (fft_reg.cuh).
 #include "db_kernels.cuh"
-#include "fft_smem.cuh"
+#include "fft_reg.cuh"
 
 namespace db {
 
-constexpr int ZPAD = 1;  // double2 padding per shared-memory sequence
-
 // ---------------------------------------------------------------------------
-// physical -> Xh, one CTA = ZP pairs of z-rows (2q, 2q+1) of one plane/field
+// Each group of T = N/E threads (one warp for N <= 512) transforms one
+// sequence; a CTA holds NS = blockDim / T independent sequences.
+
+// physical -> Xh: sequence = rows (2q, 2q+1) of one plane/field
 template <int N>
-__global__ void __launch_bounds__(512) k_fwd_x(FieldSet in, FieldSet out, Geom g, int zp) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet out, Geom g) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int q = blockIdx.x * zp + seq;
+  const int q2 = blockIdx.x * (blockDim.x / T) + seq;
   const int j = blockIdx.y, f = blockIdx.z;
-  const bool active = (seq < zp) && (2 * q + 1 < g.nz);
-  double2* buf = sm + seq * (N + ZPAD);
-  const double* src = (const double*)in.p[f];
-  if (active) {
-    const double* ra = src + (long long)j * g.pp + (long long)(2 * q) * g.nx;
-    const double* rb = ra + g.nx;
+  double2* sq = sm + seq * padded(N);
+  Twiddles<N, E> tw;
+  load_twiddles<N, E>(tw, lane, g.twx);
+  const double* ra = (const double*)in.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
+  const double* rb = ra + g.nx;
+  double2 v[E];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      int e = lane + m * T;
-      buf[e] = make_double2(ra[e], rb[e]);
+  for (int q = 0; q < E; ++q) v[q] = make_double2(__ldg(ra + lane + q * T), __ldg(rb + lane + q * T));
+  fft_reg<N, -1>(v, lane, true, sq, tw);
+  SEQ_SYNC(N);
+#pragma unroll
+  for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
+  SEQ_SYNC(N);
+  double2* oa = (double2*)out.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
+  double2* ob = oa + g.kxs;
+  const double s = 0.5 / (double)N;
+  for (int m = lane; m < g.kxs; m += T) {
+    double2 A = make_double2(0.0, 0.0), B = A;
+    if (m <= g.nkx) {
+      const double2 zm = sq[pidx(m)], zn = cconj(sq[pidx((N - m) & (N - 1))]);
+      A = make_double2((zm.x + zn.x) * s, (zm.y + zn.y) * s);
+      B = make_double2((zm.y - zn.y) * s, -(zm.x - zn.x) * s);  // -i (zm - zn) / 2
     }
-  }
-  __syncthreads();
-  fft_inplace<N, -1>(buf, lane, active, g.twx);
-  if (active) {
-    double2* oa = (double2*)out.p[f] + (long long)j * g.hp + (long long)(2 * q) * g.kxs;
-    double2* ob = oa + g.kxs;
-    const double s = 0.5 / (double)N;
-    for (int m = lane; m < g.kxs; m += T) {
-      double2 A = make_double2(0.0, 0.0), B = A;
-      if (m <= g.nkx) {
-        double2 zm = buf[m], zn = cconj(buf[(N - m) & (N - 1)]);
-        double2 sp = cadd(zm, zn), dm = csub(zm, zn);
-        A = cscale(sp, s);
-        B = make_double2(dm.y * s, -dm.x * s);  // -i (zm - zn) / 2
-      }
-      oa[m] = A;
-      ob[m] = B;
-    }
+    oa[m] = A;
+    ob[m] = B;
   }
 }
 
 // Xh -> physical
 template <int N>
-__global__ void __launch_bounds__(512) k_inv_x(FieldSet in, FieldSet out, Geom g, int zp) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet out, Geom g) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int q = blockIdx.x * zp + seq;
+  const int q2 = blockIdx.x * (blockDim.x / T) + seq;
   const int j = blockIdx.y, f = blockIdx.z;
-  const bool active = (seq < zp) && (2 * q + 1 < g.nz);
-  double2* buf = sm + seq * (N + ZPAD);
-  if (active) {
-    const double2* ia = (const double2*)in.p[f] + (long long)j * g.hp + (long long)(2 * q) * g.kxs;
-    const double2* ib = ia + g.kxs;
-    for (int m = lane; m <= N / 2; m += T) {
-      double2 A = make_double2(0.0, 0.0), B = A;
-      if (m <= g.nkx) {
-        A = ia[m];
-        B = ib[m];
-      }
-      if (m == 0 || m == N / 2) {
-        A.y = 0.0;
-        B.y = 0.0;
-      }
-      buf[m] = make_double2(A.x - B.y, A.y + B.x);                        // A + iB
-      if (m > 0 && m < N / 2) buf[N - m] = make_double2(A.x + B.y, B.x - A.y);  // conj A + i conj B
-    }
-  }
-  __syncthreads();
-  fft_inplace<N, +1>(buf, lane, active, g.twx);
-  if (active) {
-    double* ra = (double*)out.p[f] + (long long)j * g.pp + (long long)(2 * q) * g.nx;
-    double* rb = ra + g.nx;
+  double2* sq = sm + seq * padded(N);
+  Twiddles<N, E> tw;
+  load_twiddles<N, E>(tw, lane, g.twx);
+  const double2* ia = (const double2*)in.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
+  const double2* ib = ia + g.kxs;
+  double2 v[E];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      int e = lane + m * T;
-      double2 v = buf[e];
-      ra[e] = v.x;
-      rb[e] = v.y;
+  for (int q = 0; q < E; ++q) {
+    const int e = lane + q * T;
+    double2 z = make_double2(0.0, 0.0);
+    if (e <= g.nkx) {
+      double2 A = __ldg(ia + e), B = __ldg(ib + e);
+      if (e == 0) { A.y = 0.0; B.y = 0.0; }
+      z = make_double2(A.x - B.y, A.y + B.x);            // A + iB
+    } else if (e >= N - g.nkx) {
+      const double2 A = __ldg(ia + (N - e)), B = __ldg(ib + (N - e));
+      z = make_double2(A.x + B.y, B.x - A.y);            // conj A + i conj B
     }
+    v[q] = z;
+  }
+  fft_reg<N, +1>(v, lane, true, sq, tw);
+  double* ra = (double*)out.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
+  double* rb = ra + g.nx;
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    ra[lane + q * T] = v[q].x;
+    rb[lane + q * T] = v[q].y;
   }
 }
 
-// Xh -> packed spectral, scaled by 1/Nz; one CTA = KT kx columns of a plane
+// Xh -> packed spectral, scaled by 1/Nz; sequence = one kx column of a plane
 template <int N>
-__global__ void __launch_bounds__(512) k_fwd_z(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet out, Geom g) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int kx0 = blockIdx.x * KT, j = blockIdx.y, f = blockIdx.z;
-  const double2* src = (const double2*)in.p[f] + (long long)j * g.hp + kx0;
-  for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-    int z = idx / KT, kl = idx % KT;
-    sm[kl * (N + ZPAD) + z] = src[(long long)z * g.kxs + kl];
-  }
-  __syncthreads();
-  fft_inplace<N, -1>(sm + seq * (N + ZPAD), lane, seq < KT, g.twz);
-  double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx0;
+  const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
+  const bool active = kx < g.kxs;
+  double2* sq = sm + seq * padded(N);
+  Twiddles<N, E> tw;
+  load_twiddles<N, E>(tw, lane, g.twz);
+  const double2* src = (const double2*)in.p[f] + (long long)j * g.hp + kx;
+  double2 v[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : make_double2(0.0, 0.0);
+  fft_reg<N, -1>(v, lane, active, sq, tw);
+  if (!active) return;
+  double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
   const double s = 1.0 / (double)N;
-  for (int idx = threadIdx.x; idx < KT * g.nkzp; idx += blockDim.x) {
-    int kzp = idx / KT, kl = idx % KT;
-    int z = (kzp <= g.nkz) ? kzp : kzp + N - g.nkzp;
-    dst[(long long)kzp * g.kxs + kl] = cscale(sm[kl * (N + ZPAD) + z], s);
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const int z = lane + q * T;
+    const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
+    if (kzp >= 0) dst[(long long)kzp * g.kxs] = cscale(v[q], s);
   }
 }
 
 // packed spectral -> Xh (zero-filled de-aliased rows, unnormalised)
 template <int N>
-__global__ void __launch_bounds__(512) k_inv_z(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet out, Geom g) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int kx0 = blockIdx.x * KT, j = blockIdx.y, f = blockIdx.z;
-  const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx0;
-  for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-    int z = idx / KT, kl = idx % KT;
-    int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
-    sm[kl * (N + ZPAD) + z] = (kzp >= 0) ? src[(long long)kzp * g.kxs + kl] : make_double2(0.0, 0.0);
+  const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
+  const bool active = kx < g.kxs;
+  double2* sq = sm + seq * padded(N);
+  Twiddles<N, E> tw;
+  load_twiddles<N, E>(tw, lane, g.twz);
+  const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx;
+  double2 v[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const int z = lane + q * T;
+    const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
+    v[q] = (active && kzp >= 0) ? __ldg(src + (long long)kzp * g.kxs) : make_double2(0.0, 0.0);
   }
-  __syncthreads();
-  fft_inplace<N, +1>(sm + seq * (N + ZPAD), lane, seq < KT, g.twz);
-  double2* dst = (double2*)out.p[f] + (long long)j * g.hp + kx0;
-  for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-    int z = idx / KT, kl = idx % KT;
-    dst[(long long)z * g.kxs + kl] = sm[kl * (N + ZPAD) + z];
-  }
+  fft_reg<N, +1>(v, lane, active, sq, tw);
+  if (!active) return;
+  double2* dst = (double2*)out.p[f] + (long long)j * g.hp + kx;
+#pragma unroll
+  for (int q = 0; q < E; ++q) dst[(long long)(lane + q * T) * g.kxs] = v[q];
 }
 
 // ---------------------------------------------------------------------------
 // launchers
 
-int x_rows_per_cta(int n, int nz) {
-  int zp = 256 / (n / 8);
-  if (zp < 1) zp = 1;
-  while (zp > 1 && ((nz / 2) % zp) != 0) --zp;
-  return zp;
+// sequences per CTA: 256 threads, or one sequence when it needs more
+template <int N>
+constexpr int seqs_per_cta() {
+  return FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T;
 }
 
 #define DB_DISPATCH_N(n, FN, ...)                                   \
@@ -166,39 +171,47 @@ int x_rows_per_cta(int n, int nz) {
     case 512: FN<512>(__VA_ARGS__); break;                          \
     case 1024: FN<1024>(__VA_ARGS__); break;                        \
     case 2048: FN<2048>(__VA_ARGS__); break;                        \
-    case 4096: FN<4096>(__VA_ARGS__); break;                        \
     default: return cudaErrorInvalidValue;                          \
   }
 
+template <typename K>
+static void smem_attr(K kern, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 template <int N>
 static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  int zp = x_rows_per_cta(N, g.nz);
-  dim3 grid(g.nz / 2 / zp, g.np, nf);
-  size_t smem = (size_t)zp * (N + ZPAD) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_fwd_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_fwd_x<N><<<grid, zp * (N / 8), smem, st>>>(in, out, g, zp);
+  constexpr int ns = seqs_per_cta<N>();
+  int npairs = g.nz / 2;
+  int cps = ns < npairs ? ns : npairs;
+  while (npairs % cps) --cps;
+  size_t smem = (size_t)cps * padded(N) * sizeof(double2);
+  smem_attr(k_fwd_x<N>, smem);
+  k_fwd_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 template <int N>
 static void go_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  int zp = x_rows_per_cta(N, g.nz);
-  dim3 grid(g.nz / 2 / zp, g.np, nf);
-  size_t smem = (size_t)zp * (N + ZPAD) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_inv_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_inv_x<N><<<grid, zp * (N / 8), smem, st>>>(in, out, g, zp);
+  constexpr int ns = seqs_per_cta<N>();
+  int npairs = g.nz / 2;
+  int cps = ns < npairs ? ns : npairs;
+  while (npairs % cps) --cps;
+  size_t smem = (size_t)cps * padded(N) * sizeof(double2);
+  smem_attr(k_inv_x<N>, smem);
+  k_inv_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 template <int N>
 static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  dim3 grid(g.kxs / KT, g.np, nf);
-  size_t smem = (size_t)KT * (N + ZPAD) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_fwd_z<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_fwd_z<N><<<grid, KT * (N / 8), smem, st>>>(in, out, g);
+  constexpr int ns = seqs_per_cta<N>();
+  size_t smem = (size_t)ns * padded(N) * sizeof(double2);
+  smem_attr(k_fwd_z<N>, smem);
+  k_fwd_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 template <int N>
 static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  dim3 grid(g.kxs / KT, g.np, nf);
-  size_t smem = (size_t)KT * (N + ZPAD) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_inv_z<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_inv_z<N><<<grid, KT * (N / 8), smem, st>>>(in, out, g);
+  constexpr int ns = seqs_per_cta<N>();
+  size_t smem = (size_t)ns * padded(N) * sizeof(double2);
+  smem_attr(k_inv_z<N>, smem);
+  k_inv_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {

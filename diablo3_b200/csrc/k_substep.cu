@@ -22,194 +22,209 @@
 #include <math.h>
 
 #include "db_kernels.cuh"
-#include "fft_smem.cuh"
+#include "fft_reg.cuh"
 
 namespace db {
 
-constexpr int ZPAD_S = 1;
 
 __device__ __forceinline__ bool in_rng(int j, int a, int b) { return j >= a && j <= b; }
 
-// X_a (part 0) or X_b (part 1) at mode m of the complex FFT of a + i b
+// ---------------------------------------------------------------------------
+// nonlinear products + forward x-FFT.  One CTA per (z, j) row and group; each
+// complex sequence carries two real products a + i b:
+//  group 0 (u1 and u3 momentum, rows jstart..jend):
+//    s0 = (u1 u1 | Dy u1u2)  s1 = (u1 u3 | Dy u3u2)  s2 = (u3 u3 | 0)
+//  group 1 (u2 momentum rows 2..Nyp; scalar rows jstart_th..jend_th):
+//    s0 = (<u1> u2 | Dy u2u2)  s1 = (th u1 | Dy th u2)  s2 = (<u3> u2 | th u3)
+// Outputs (x-half), o = 0..7 = N1 M1 N3 M3 N2 M2 NT MT with
+//  N = ikx X(a) + X(b) of one sequence, M = one part of a sequence:
+//  N1 = s0(g0)  M1 = s1.a(g0)  N3 = s1(g0)  M3 = s2.a(g0)
+//  N2 = s0(g1)  M2 = s2.a(g1)  NT = s1(g1)  MT = s2.b(g1)
+// so that cf_e -= Z(N_e) + ikz Z(M_e) after the z-pass (solver.f90:655-815,
+// 914-964; <.> is the interpolation to GY points, Dy the conservative
+// y-difference).
 template <int N>
-__device__ __forceinline__ double2 sep(const double2* z, int m, int part) {
-  double2 zm = z[m], zn = cconj(z[(N - m) & (N - 1)]);
+__device__ __forceinline__ double2 sepp(const double2* z, int m, int part) {
+  const double2 zm = z[pidx(m)], zn = cconj(z[pidx((N - m) & (N - 1))]);
   if (part == 0) return make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y + zn.y));
   return make_double2(0.5 * (zm.y - zn.y), -0.5 * (zm.x - zn.x));
 }
 
-// ---------------------------------------------------------------------------
-// nonlinear products + forward x-FFT.  One CTA per (z, j) row, 6 sequences:
-//  seq0 (u1 u3 | u1 u1)        seq1 (u3 u3 | <u1> u2)    seq2 (<u3> u2 | Dy u1u2)
-//  seq3 (Dy u3u2 | Dy u2u2)    seq4 (th u1 | th u3)      seq5 (Dy th u2 | 0)
-// Outputs (x-half), o = 0..7:
-//  N1 = ikx X(u1u1) + X(Dy u1u2)   M1 = X(u1u3)
-//  N3 = ikx X(u1u3) + X(Dy u3u2)   M3 = X(u3u3)
-//  N2 = ikx X(<u1>u2) + X(Dy u2u2) M2 = X(<u3>u2)
-//  NT = ikx X(th u1) + X(Dy th u2) MT = X(th u3)
-// so that cf_e -= Z(N_e) + ikz Z(M_e) after the z-pass.
 template <int N>
-__global__ void __launch_bounds__(6 * (N / 8)) k_products(State s, Geom g) {
+__global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(State s, Geom g) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int z = blockIdx.x, j = blockIdx.y;
+  const int z = blockIdx.x, j = blockIdx.y, grp = blockIdx.z;
   const bool r1 = in_rng(j, g.jstart, g.jend);
   const bool r2 = in_rng(j, 2, g.ny);
   const bool rt = in_rng(j, g.jstart_th, g.jend_th);
   const long long hrow = (long long)j * g.hp + (long long)z * g.kxs;
-  if (!(r1 || r2 || rt)) {
-    for (int idx = threadIdx.x; idx < 8 * g.kxs; idx += blockDim.x)
-      s.xh[idx / g.kxs][hrow + idx % g.kxs] = make_double2(0.0, 0.0);
+  if ((grp == 0 && !r1) || (grp == 1 && !(r2 || rt))) {
+    for (int idx = threadIdx.x; idx < 4 * g.kxs; idx += blockDim.x)
+      s.xh[4 * grp + idx / g.kxs][hrow + idx % g.kxs] = make_double2(0.0, 0.0);
     return;
   }
-  double2* buf = sm + seq * (N + ZPAD_S);
+  double2* sq = sm + seq * padded(N);
+  Twiddles<N, E> tw;
+  load_twiddles<N, E>(tw, lane, g.twx);
   const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
   const long long om = o0 - g.pp, op = o0 + g.pp;
   const double dyj = g.dy[j], dyfj = g.dyf[j];
   const double dyfjm = (j >= 1) ? g.dyf[j - 1] : 0.0;
-#pragma unroll 2
-  for (int m = 0; m < 8; ++m) {
-    const int x = lane + m * T;
+  double2 v[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const int x = lane + q * T;
     double a = 0.0, b = 0.0;
-    switch (seq) {
-      case 0:
-        if (r1) {
-          double u1 = s.u1[o0 + x], u3 = s.u3[o0 + x];
-          a = u3 * u1;
-          b = u1 * u1;
-        }
-        break;
-      case 1:
-        if (r1) {
-          double u3 = s.u3[o0 + x];
-          a = u3 * u3;
-        }
-        if (r2) b = ((dyfj * s.u1[o0 + x] + dyfjm * s.u1[om + x]) / (2. * dyj)) * s.u2[o0 + x];
-        break;
-      case 2:
-        if (r2) a = ((dyfj * s.u3[o0 + x] + dyfjm * s.u3[om + x]) / (2. * dyj)) * s.u2[o0 + x];
-        if (r1) {
-          double u1p = s.u1[op + x], u1 = s.u1[o0 + x], u1m = s.u1[om + x];
-          double u2p = s.u2[op + x], u2 = s.u2[o0 + x];
-          b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (2.0 * dyfj);
-        }
-        break;
-      case 3:
-        if (r1) {
-          double u3p = s.u3[op + x], u3 = s.u3[o0 + x], u3m = s.u3[om + x];
-          double u2p = s.u2[op + x], u2 = s.u2[o0 + x];
-          a = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (2.0 * dyfj);
-        }
-        if (r2) {
-          double u2 = s.u2[o0 + x];
-          double p = u2 + s.u2[op + x], q = u2 + s.u2[om + x];
-          b = (0.25 * (p * p) - 0.25 * (q * q)) / dyj;
-        }
-        break;
-      case 4:
-        if (rt) {
-          double th = s.th[o0 + x];
-          a = th * s.u1[o0 + x];
-          b = th * s.u3[o0 + x];
-        }
-        break;
-      default:
-        if (rt) {
-          double thp = s.th[op + x], th = s.th[o0 + x], thm = s.th[om + x];
-          double u2p = s.u2[op + x], u2 = s.u2[o0 + x];
-          a = (thp * u2p + th * u2p - th * u2 - thm * u2) / (2.0 * dyfj);
-        }
-        break;
-    }
-    buf[x] = make_double2(a, b);
-  }
-  __syncthreads();
-  fft_inplace<N, -1>(buf, lane, true, g.twx);
-  // combine into the 8 x-half outputs, scaled by 1/Nx
-  const double sc = 1.0 / (double)N;
-  const int P = N + ZPAD_S;
-  for (int idx = threadIdx.x; idx < 8 * g.kxs; idx += blockDim.x) {
-    const int o = idx / g.kxs, mm = idx % g.kxs;
-    double2 v = make_double2(0.0, 0.0);
-    if (mm <= g.nkx) {
-      const double k = g.kx[mm];
-      double2 dx = make_double2(0.0, 0.0), pl = make_double2(0.0, 0.0);
-      bool ok = true;
-      switch (o) {
-        case 0: ok = r1; dx = sep<N>(sm + 0 * P, mm, 1); pl = sep<N>(sm + 2 * P, mm, 1); break;
-        case 1: ok = r1; pl = sep<N>(sm + 0 * P, mm, 0); break;
-        case 2: ok = r1; dx = sep<N>(sm + 0 * P, mm, 0); pl = sep<N>(sm + 3 * P, mm, 0); break;
-        case 3: ok = r1; pl = sep<N>(sm + 1 * P, mm, 0); break;
-        case 4: ok = r2; dx = sep<N>(sm + 1 * P, mm, 1); pl = sep<N>(sm + 3 * P, mm, 1); break;
-        case 5: ok = r2; pl = sep<N>(sm + 2 * P, mm, 0); break;
-        case 6: ok = rt; dx = sep<N>(sm + 4 * P, mm, 0); pl = sep<N>(sm + 5 * P, mm, 0); break;
-        default: ok = rt; pl = sep<N>(sm + 4 * P, mm, 1); break;
+    if (grp == 0) {
+      const double u1 = __ldg(s.u1 + o0 + x), u3 = __ldg(s.u3 + o0 + x);
+      if (seq == 0) {
+        const double u1p = __ldg(s.u1 + op + x), u1m = __ldg(s.u1 + om + x);
+        const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
+        a = u1 * u1;
+        b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (2.0 * dyfj);
+      } else if (seq == 1) {
+        const double u3p = __ldg(s.u3 + op + x), u3m = __ldg(s.u3 + om + x);
+        const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
+        a = u3 * u1;
+        b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (2.0 * dyfj);
+      } else {
+        a = u3 * u3;
       }
-      if (ok) v = make_double2((pl.x - k * dx.y) * sc, (pl.y + k * dx.x) * sc);
+    } else {
+      const double u2 = __ldg(s.u2 + o0 + x);
+      if (seq == 0) {
+        if (r2) {
+          const double u1 = __ldg(s.u1 + o0 + x), u1m = __ldg(s.u1 + om + x);
+          const double pp = u2 + __ldg(s.u2 + op + x), qq = u2 + __ldg(s.u2 + om + x);
+          a = ((dyfj * u1 + dyfjm * u1m) / (2. * dyj)) * u2;
+          b = (0.25 * (pp * pp) - 0.25 * (qq * qq)) / dyj;
+        }
+      } else if (seq == 1) {
+        if (rt) {
+          const double th = __ldg(s.th + o0 + x), thp = __ldg(s.th + op + x), thm = __ldg(s.th + om + x);
+          const double u2p = __ldg(s.u2 + op + x);
+          a = th * __ldg(s.u1 + o0 + x);
+          b = (thp * u2p + th * u2p - th * u2 - thm * u2) / (2.0 * dyfj);
+        }
+      } else {
+        if (r2) a = ((dyfj * __ldg(s.u3 + o0 + x) + dyfjm * __ldg(s.u3 + om + x)) / (2. * dyj)) * u2;
+        if (rt) b = __ldg(s.th + o0 + x) * __ldg(s.u3 + o0 + x);
+      }
     }
-    s.xh[o][hrow + mm] = v;
+    v[q] = make_double2(a, b);
+  }
+  fft_reg<N, -1>(v, lane, true, sq, tw);
+  SEQ_SYNC(N);
+#pragma unroll
+  for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
+  SEQ_SYNC(N);
+  // outputs of this sequence, scaled by 1/Nx: an N-type output
+  // ikx X(a) + X(b), and for s1 (group 0) / s2 (both groups) the parts
+  const double sc = 1.0 / (double)N;
+  const bool n_out = (seq < 2) ? ((grp == 0) || (seq == 0 ? r2 : rt)) : false;
+  const int o_n = (grp == 0) ? (seq == 0 ? 0 : 2) : (seq == 0 ? 4 : 6);
+  for (int mm = lane; mm < g.kxs; mm += T) {
+    const bool live = mm <= g.nkx;
+    const double2 A = live ? sepp<N>(sq, mm, 0) : make_double2(0.0, 0.0);
+    const double2 B = live ? sepp<N>(sq, mm, 1) : make_double2(0.0, 0.0);
+    if (seq < 2) {
+      const double k = g.kx[mm];
+      s.xh[o_n][hrow + mm] = n_out ? make_double2((B.x - k * A.y) * sc, (B.y + k * A.x) * sc)
+                                   : make_double2(0.0, 0.0);
+    }
+    if (grp == 0 && seq == 1) s.xh[1][hrow + mm] = make_double2(A.x * sc, A.y * sc);       // M1
+    if (grp == 0 && seq == 2) s.xh[3][hrow + mm] = make_double2(A.x * sc, A.y * sc);       // M3
+    if (grp == 1 && seq == 2) {
+      s.xh[5][hrow + mm] = r2 ? make_double2(A.x * sc, A.y * sc) : make_double2(0.0, 0.0);  // M2
+      s.xh[7][hrow + mm] = rt ? make_double2(B.x * sc, B.y * sc) : make_double2(0.0, 0.0);  // MT
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // z-pass of the nonlinear terms + spectral RHS + inverse z-pass of cr.
-// One CTA = KT kx columns of plane j; 2 KT sequences (N_e, M_e).
-// Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th.  x-half inputs: xh[2e],
-// xh[2e+1]; the inverse-transformed cr_e overwrites xh[2e].
+// One CTA = KT kx columns of plane j; thread t owns column t % KT and the
+// z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
+// x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
 template <int N>
-__global__ void __launch_bounds__(2 * KT * (N / 8)) k_zpass_rhs(State s, Geom g, Phys ph, int rk) {
+__global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1)) k_zpass_rhs(State s, Geom g, Phys ph, int rk) {
   extern __shared__ double2 sm[];
-  constexpr int T = N / 8;
-  constexpr int P = N + ZPAD_S;
-  const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int kx0 = blockIdx.x * KT, j = blockIdx.y;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  // column-fastest mapping: a warp reads KT consecutive kx of 32/KT rows
+  const int seq = threadIdx.x % KT, lane = threadIdx.x / KT;
+  const int j = blockIdx.y, kx = blockIdx.x * KT + seq;
+  const bool active = kx < g.kxs;
+  const int kxc = active ? kx : 0;
+  // per-column buffers, staggered by one element so the KT columns sharing a
+  // warp fall into different shared-memory bank groups
+  double2* sx = sm + seq * (3 * padded(N) + 1);  // exchange buffers (two)
+  double2* sx1 = sx + padded(N);
+  double2* sm_z = sx1 + padded(N);             // Z(M) stash, natural order
+#if DB_ZPASS_LAZY
+#define ZFFT(SIGN_, V_) fft_reg_lazy<N, SIGN_, true>(V_, lane, active, sx, g.twz, sx1)
+#else
+  Twiddles<N, E> twd;
+  load_twiddles<N, E>(twd, lane, g.twz);
+#define ZFFT(SIGN_, V_) fft_reg<N, SIGN_, true>(V_, lane, active, sx, twd, sx1)
+#endif
   const double hb = s.sc->h_bar[rk];
   const double temp3 = zeta_bar(rk) * hb, temp4 = hb, temp5 = beta_bar(rk) * hb;
   const double nu = ph.nu, f = ph.ro_inv / ph.delta;
   const double tw = ph.delta / ph.ro_inv;  // delta / Ro_inv
-  const long long sp0 = (long long)j * g.sp + kx0;
-  constexpr int MAXIT = 3;  // ceil(KT * nkzp / blockDim) <= 3 since nkzp <= 2N/3 + 1
-  for (int e = 0; e < 4; ++e) {
+  const double kxv = g.kx[kxc];
+  const double inz = 1.0 / (double)N;
+  const long long h0 = (long long)j * g.hp + kxc;
+  const long long sp0 = (long long)j * g.sp + kxc;
+  const bool beta1 = (ph.beta == 1.0);
+  {
+    const int e = blockIdx.z;
     const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
     double2* xin_n = s.xh[2 * e];
-    double2* xin_m = s.xh[2 * e + 1];
-    const long long h0 = (long long)j * g.hp + kx0;
+    const double2* xin_m = s.xh[2 * e + 1];
     if (!in_rng(j, jlo, jhi)) {
-      for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x)
-        xin_n[h0 + (long long)(idx / KT) * g.kxs + idx % KT] = make_double2(0.0, 0.0);
-      continue;
-    }
-    for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-      int zz = idx / KT, kl = idx % KT;
-      long long a = h0 + (long long)zz * g.kxs + kl;
-      sm[kl * P + zz] = xin_n[a];
-      sm[(KT + kl) * P + zz] = xin_m[a];
-    }
-    __syncthreads();
-    fft_inplace<N, -1>(sm + seq * P, lane, true, g.twz);
-    // spectral RHS for every packed (kzp, kl) of the tile
-    double2 crv[MAXIT];
-    const double inz = 1.0 / (double)N;
+      if (active)
 #pragma unroll
-    for (int it = 0; it < MAXIT; ++it) {
-      const int idx = threadIdx.x + it * blockDim.x;
-      crv[it] = make_double2(0.0, 0.0);
-      if (idx >= KT * g.nkzp) continue;
-      const int kzp = idx / KT, kl = idx % KT, kx = kx0 + kl;
-      const int zz = (kzp <= g.nkz) ? kzp : kzp + N - g.nkzp;
-      const double kxv = g.kx[kx], kzv = g.kz[kzp];
-      const double2 zn = sm[kl * P + zz], zm = sm[(KT + kl) * P + zz];
+        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = make_double2(0.0, 0.0);
+      return;
+    }
+    double2 vn[E];
+    // Z(M) first, parked in shared memory in natural order
+#pragma unroll
+    for (int q = 0; q < E; ++q)
+      vn[q] = active ? __ldg(xin_m + h0 + (long long)(lane + q * T) * g.kxs) : make_double2(0.0, 0.0);
+    ZFFT(-1, vn);
+#pragma unroll
+    for (int q = 0; q < E; ++q) sm_z[pidx(lane + q * T)] = vn[q];
+#pragma unroll
+    for (int q = 0; q < E; ++q)
+      vn[q] = active ? xin_n[h0 + (long long)(lane + q * T) * g.kxs] : make_double2(0.0, 0.0);
+    __syncthreads();
+    ZFFT(-1, vn);
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int zz = lane + q * T;
+      const int kzp = (zz <= g.nkz) ? zz : (zz >= N - g.nkz ? zz - N + g.nkzp : -1);
+      if (kzp < 0 || !active) {
+        vn[q] = make_double2(0.0, 0.0);
+        continue;
+      }
+      const double kzv = g.kz[kzp];
       // NL = (Z(N) + i kz Z(M)) / Nz
-      const double2 nl = make_double2((zn.x - kzv * zm.y) * inz, (zn.y + kzv * zm.x) * inz);
-      const long long a = sp0 + (long long)kzp * g.kxs + kl;
-      const double kk = pow(kxv * kxv + kzv * kzv, ph.beta);
+      const double2 zmq = sm_z[pidx(zz)];
+      const double2 nl = make_double2((vn[q].x - kzv * zmq.y) * inz, (vn[q].y + kzv * zmq.x) * inz);
+      const long long a = sp0 + (long long)kzp * g.kxs;
+      const double k2 = kxv * kxv + kzv * kzv;
+      const double kk = beta1 ? k2 : pow(k2, ph.beta);
       double2 cf, cr;
       if (e == 0 || e == 1) {
         const double2 cu1 = s.cu1[a], cu3 = s.cu3[a], cth = s.cth[a], cp = s.cp[a];
-        const double2 v2 = make_double2(0.5 * (s.cu2[a].x + s.cu2[a + g.sp].x),
-                                        0.5 * (s.cu2[a].y + s.cu2[a + g.sp].y));
+        const double2 c2a = s.cu2[a], c2b = s.cu2[a + g.sp];
+        const double2 v2 = make_double2(0.5 * (c2a.x + c2b.x), 0.5 * (c2a.y + c2b.y));
         const double2 cu = (e == 0) ? cu1 : cu3;
         cf = cscale(cu, -nu * kk);
         if (e == 0) {
@@ -279,170 +294,240 @@ __global__ void __launch_bounds__(2 * KT * (N / 8)) k_zpass_rhs(State s, Geom g,
         cr = cadd(cr, cscale(cf, temp5));
         s.cfth[a] = cf;
       }
-      crv[it] = cr;
+      vn[q] = cr;
     }
     __syncthreads();
-    // unpack cr into the second half (zero the de-aliased rows) and invert
-    for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-      int zz = idx / KT, kl = idx % KT;
-      int kzp = (zz <= g.nkz) ? zz : (zz >= N - g.nkz ? zz - N + g.nkzp : -1);
-      if (kzp < 0) sm[(KT + kl) * P + zz] = make_double2(0.0, 0.0);
-    }
+    ZFFT(+1, vn);
+    if (active)
 #pragma unroll
-    for (int it = 0; it < MAXIT; ++it) {
-      const int idx = threadIdx.x + it * blockDim.x;
-      if (idx >= KT * g.nkzp) continue;
-      const int kzp = idx / KT, kl = idx % KT;
-      const int zz = (kzp <= g.nkz) ? kzp : kzp + N - g.nkzp;
-      sm[(KT + kl) * P + zz] = crv[it];
-    }
-    __syncthreads();
-    fft_inplace<N, +1>(sm + (KT + seq) * P, lane, seq < KT, g.twz);
-    for (int idx = threadIdx.x; idx < KT * N; idx += blockDim.x) {
-      int zz = idx / KT, kl = idx % KT;
-      xin_n[h0 + (long long)zz * g.kxs + kl] = sm[(KT + kl) * P + zz];
-    }
-    __syncthreads();
+      for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = vn[q];
   }
 }
 
 // ---------------------------------------------------------------------------
-// implicit systems: rows of the four equations (th, u2, u1, u3) -> tri[eq*np + j]
-__global__ void k_tri_coef(Geom g, Phys ph, TriRow* tri, DevScalars* sc, int rk) {
-  const int eq = threadIdx.x;  // 0..3
-  if (eq >= 4) return;
+// implicit systems: rows of the four equations (th, u2, u1, u3) -> tri[eq*np + j].
+// One CTA per equation: rows are filled in parallel in shared memory, the BC
+// rows and the forward elimination (a serial recurrence) by one thread.
+__global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, DevScalars* sc, int rk) {
+  extern __shared__ TriRow Rs[];
+  const int eq = blockIdx.x;  // 0..3
   const int np = g.np, Nyp = g.ny;
-  TriRow* R = tri + eq * np;
   const double temp1 = 0.5 * ph.nu * sc->h_bar[rk];
   const double tv = temp1 * ph.nu_v_scale;
   const double tth = temp1 / ph.pr * ph.nu_v_scale;
-  for (int j = 0; j < np; ++j) {
-    R[j].l = 0.0; R[j].d = 1.0; R[j].u = 0.0; R[j].bc = 0.0;
-    R[j].is_bc = 1; R[j].interior = 0; R[j].cn_lo = 0.0; R[j].cn_hi = 0.0;
-  }
   const double* dy = g.dy;
   const double* dyf = g.dyf;
-  auto setr = [&](int j, double l, double d, double u, double v) {
-    R[j].l = l; R[j].d = d; R[j].u = u; R[j].bc = v; R[j].is_bc = 1; R[j].interior = 0;
-  };
-  if (eq == 0 || eq == 2 || eq == 3) {
-    const int lo = (eq == 0) ? g.jstart_th : g.jstart;
-    const int hi = (eq == 0) ? g.jend_th : g.jend;
-    for (int j = lo; j <= hi; ++j) {
+  const int lo = (eq == 0) ? g.jstart_th : (eq == 1 ? 2 : g.jstart);
+  const int hi = (eq == 0) ? g.jend_th : (eq == 1 ? Nyp : g.jend);
+  for (int j = threadIdx.x; j < np; j += blockDim.x) {
+    TriRow r;
+    r.l = 0.0; r.d = 1.0; r.u = 0.0; r.bc = 0.0; r.ap = 0.0; r.ibp = 1.0;
+    r.cn_lo = 0.0; r.cn_hi = 0.0; r.pa = 1.0; r.pm = 1.0;
+    r.is_bc = 1; r.interior = 0; r.pad[0] = r.pad[1] = 0;
+    if (j >= lo && j <= hi) {
       if (eq == 0) {  // solver.f90:1023-1026
-        R[j].l = -(tth) / (dy[j] * dyf[j]);
-        R[j].d = 1. + (tth) / (dy[j + 1] * dyf[j]) + (tth) / (dy[j] * dyf[j]);
-        R[j].u = -(tth) / (dy[j + 1] * dyf[j]);
-        R[j].cn_hi = (tth) / dyf[j] / dy[j + 1];
-        R[j].cn_lo = (tth) / dyf[j] / dy[j];
+        r.l = -(tth) / (dy[j] * dyf[j]);
+        r.d = 1. + (tth) / (dy[j + 1] * dyf[j]) + (tth) / (dy[j] * dyf[j]);
+        r.u = -(tth) / (dy[j + 1] * dyf[j]);
+        r.cn_hi = (tth) / dyf[j] / dy[j + 1];
+        r.cn_lo = (tth) / dyf[j] / dy[j];
+      } else if (eq == 1) {  // solver.f90:1085-1088
+        r.l = -tv / (dyf[j - 1] * dy[j]);
+        r.d = 1. + tv / (dyf[j] * dy[j]) + tv / (dyf[j - 1] * dy[j]);
+        r.u = -tv / (dyf[j] * dy[j]);
+        r.cn_hi = tv / dy[j] / dyf[j];
+        r.cn_lo = tv / dy[j] / dyf[j - 1];
       } else {        // solver.f90:1140-1143, 1196-1199
-        R[j].l = -tv / (dy[j] * dyf[j]);
-        R[j].d = 1. - tv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
-        R[j].u = -tv / (dy[j + 1] * dyf[j]);
-        R[j].cn_hi = tv / dyf[j] / dy[j + 1];
-        R[j].cn_lo = tv / dyf[j] / dy[j];
+        r.l = -tv / (dy[j] * dyf[j]);
+        r.d = 1. - tv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
+        r.u = -tv / (dy[j + 1] * dyf[j]);
+        r.cn_hi = tv / dyf[j] / dy[j + 1];
+        r.cn_lo = tv / dyf[j] / dy[j];
       }
-      R[j].is_bc = 0; R[j].interior = 1;
+      r.is_bc = 0;
+      r.interior = 1;
     }
-    // apply_BC_th/1/3 lower and upper (solver.f90:1901-1982, 2066-2232)
-    const int bl = (eq == 0) ? BC_TH_MIN : (eq == 2 ? BC_U_MIN : BC_W_MIN);
-    const int bh = (eq == 0) ? BC_TH_MAX : (eq == 2 ? BC_U_MAX : BC_W_MAX);
-    double cmax = ph.bc_c1[bh];
-    if (eq == 3 && ph.bc_type[BC_W_MAX] == 1) {
-      if (ph.f_type == 4)
-        sc->w_bc_ymax_c1_transient = ph.bc_c1[BC_W_MAX] + ph.amp_omega0 *
-            sin(ph.omega0 * (ph.ro_inv / ph.delta * sc->time - ph.force_start));
-      cmax = sc->w_bc_ymax_c1_transient;
-    }
-    if (ph.bc_type[bl] == 0) {
+    Rs[j] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    auto setr = [&](int j, double l, double d, double u, double v) {
+      Rs[j].l = l; Rs[j].d = d; Rs[j].u = u; Rs[j].bc = v; Rs[j].is_bc = 1; Rs[j].interior = 0;
+    };
+    if (eq != 1) {
+      // apply_BC_th/1/3 lower and upper (solver.f90:1901-1982, 2066-2232)
+      const int bl = (eq == 0) ? BC_TH_MIN : (eq == 2 ? BC_U_MIN : BC_W_MIN);
+      const int bh = (eq == 0) ? BC_TH_MAX : (eq == 2 ? BC_U_MAX : BC_W_MAX);
+      double cmax = ph.bc_c1[bh];
+      if (eq == 3 && ph.bc_type[BC_W_MAX] == 1) {
+        if (ph.f_type == 4)
+          sc->w_bc_ymax_c1_transient = ph.bc_c1[BC_W_MAX] + ph.amp_omega0 *
+              sin(ph.omega0 * (ph.ro_inv / ph.delta * sc->time - ph.force_start));
+        cmax = sc->w_bc_ymax_c1_transient;
+      }
+      if (ph.bc_type[bl] == 0) {
+        setr(0, 0., 1., 0., 0.);
+        setr(1, 0., 1., 0., ph.bc_c1[bl]);
+      } else {
+        setr(0, 0., 1., 0., 0.);
+        setr(1, 0., -1., 1., dy[2] * ph.bc_c1[bl]);
+      }
+      if (ph.bc_type[bh] == 0) {
+        setr(Nyp + 1, 0., 1., 0., 0.);
+        setr(Nyp, 0., 1., 0., cmax);
+      } else {
+        setr(Nyp, -1., 1., 0., dy[Nyp] * cmax);
+        setr(Nyp + 1, 0., 1., 0., 0.);
+      }
+    } else {  // apply_BC_2_* (solver.f90:1987-2061)
+      if (ph.bc_type[BC_V_MIN] == 0) {
+        setr(1, 0., 1., 0., ph.bc_c1[BC_V_MIN]);
+        setr(2, 0., 1., 0., ph.bc_c1[BC_V_MIN]);
+      } else {
+        setr(1, 0., -1., 1., dyf[1] * ph.bc_c1[BC_V_MIN]);
+      }
       setr(0, 0., 1., 0., 0.);
-      setr(1, 0., 1., 0., ph.bc_c1[bl]);
-    } else {
-      setr(0, 0., 1., 0., 0.);
-      setr(1, 0., -1., 1., dy[2] * ph.bc_c1[bl]);
+      if (ph.bc_type[BC_V_MAX] == 0) {
+        setr(Nyp + 1, 0., 1., 0., ph.bc_c1[BC_V_MAX]);
+        setr(Nyp, 0., 1., 0., ph.bc_c1[BC_V_MAX]);
+      } else {
+        setr(Nyp + 1, -1., 1., 0., dyf[Nyp] * ph.bc_c1[BC_V_MAX]);
+      }
     }
-    if (ph.bc_type[bh] == 0) {
-      setr(Nyp + 1, 0., 1., 0., 0.);
-      setr(Nyp, 0., 1., 0., cmax);
-    } else {
-      setr(Nyp, -1., 1., 0., dy[Nyp] * cmax);
-      setr(Nyp + 1, 0., 1., 0., 0.);
+    // Thomas forward elimination of the matrix (thomas_forward_real_mpi with
+    // one rank: rows 1..Nyp+1, solver.f90:1731-1757)
+    double bprev = Rs[0].d;
+    Rs[0].ap = 0.0;
+    Rs[0].ibp = 1.0 / bprev;
+    double uprev = Rs[0].u;
+    for (int j = 1; j < np; ++j) {
+      const double a = -Rs[j].l / bprev;
+      const double b = Rs[j].d + a * uprev;
+      Rs[j].ap = a;
+      Rs[j].ibp = 1.0 / b;
+      bprev = b;
+      uprev = Rs[j].u;
     }
-  } else {  // u2, solver.f90:1085-1088 and apply_BC_2_* (1987-2061)
-    for (int j = 2; j <= Nyp; ++j) {
-      R[j].l = -tv / (dyf[j - 1] * dy[j]);
-      R[j].d = 1. + tv / (dyf[j] * dy[j]) + tv / (dyf[j - 1] * dy[j]);
-      R[j].u = -tv / (dyf[j] * dy[j]);
-      R[j].cn_hi = tv / dy[j] / dyf[j];
-      R[j].cn_lo = tv / dy[j] / dyf[j - 1];
-      R[j].is_bc = 0; R[j].interior = 1;
-    }
-    if (ph.bc_type[BC_V_MIN] == 0) {
-      setr(1, 0., 1., 0., ph.bc_c1[BC_V_MIN]);
-      setr(2, 0., 1., 0., ph.bc_c1[BC_V_MIN]);
-    } else {
-      setr(1, 0., -1., 1., dyf[1] * ph.bc_c1[BC_V_MIN]);
-    }
-    setr(0, 0., 1., 0., 0.);
-    if (ph.bc_type[BC_V_MAX] == 0) {
-      setr(Nyp + 1, 0., 1., 0., ph.bc_c1[BC_V_MAX]);
-      setr(Nyp, 0., 1., 0., ph.bc_c1[BC_V_MAX]);
-    } else {
-      setr(Nyp + 1, -1., 1., 0., dyf[Nyp] * ph.bc_c1[BC_V_MAX]);
+    // chunk carry weights of the two recurrences g_j = v_j + a'_j g_{j-1}
+    // and x_j = g_j / b'_j + m_j x_{j+1}, m_j = -u_j / b'_j
+    const Chunks ch = thomas_chunks(np);
+    for (int k = 0; k < ch.nch; ++k) {
+      const int j0 = k * ch.len, j1 = min(np, j0 + ch.len) - 1;
+      double pa = 1.0;
+      for (int j = j0; j <= j1; ++j) { pa *= Rs[j].ap; Rs[j].pa = pa; }
+      double pm = 1.0;
+      for (int j = j1; j >= j0; --j) { pm *= -Rs[j].u * Rs[j].ibp; Rs[j].pm = pm; }
     }
   }
-  // Thomas forward elimination of the matrix (thomas_forward_real_mpi with
-  // one rank: rows 1..Nyp+1, solver.f90:1731-1757)
-  double bprev = R[0].d;
-  R[0].ap = 0.0;
-  R[0].ibp = 1.0 / bprev;
-  for (int j = 1; j < np; ++j) {
-    const double a = -R[j].l / bprev;
-    const double b = R[j].d + a * R[j - 1].u;
-    R[j].ap = a;
-    R[j].ibp = 1.0 / b;
-    bprev = b;
-  }
+  __syncthreads();
+  TriRow* R = tri + eq * np;
+  for (int j = threadIdx.x; j < np; j += blockDim.x) R[j] = Rs[j];
 }
 
-// per-column Thomas for the four equations, one thread per (x, z)
-__global__ void __launch_bounds__(128) k_thomas(State s, Geom g) {
-  const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= g.pp) return;
+// Implicit CN solves of th, u2, u1, u3 (solver.f90:1012-1233) for all (x,z)
+// columns.  One CTA = 32 consecutive x columns at one z; the column tile
+// (all Nyp+2 rows) lives in shared memory.  The shared LU factors (a'_j,
+// 1/b'_j from k_tri_coef) turn the Thomas sweeps into two first-order linear
+// recurrences, solved as a two-level scan: warp k runs its chunk of rows with
+// zero carry-in, one warp propagates the chunk carries, then every row adds
+// its carry times the precomputed chunk products (pa, pm).  HBM sees r and u
+// read once and u written once per equation.
+constexpr int TX = 32;
+
+__global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
+  extern __shared__ double tile[];          // [np][TX]
+  __shared__ double carry[8][TX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int np = g.np, Nyp = g.ny;
+  const Chunks ch = thomas_chunks(np);
+  const int x = blockIdx.x * TX + lane, z = blockIdx.y;
+  const bool xin = x < g.nx;
+  const long long col = (long long)z * g.nx + x;
   const long long pp = g.pp;
+  const int j0 = w * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this warp's rows
+  const bool active = w < ch.nch;
   for (int eq = 0; eq < 4; ++eq) {
     const TriRow* R = s.tri + eq * np;
     double* u = (eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3));
     const double* r = (eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3));
-    u += col;
-    r += col;
     // rows written back (solver.f90:1056, 1115, 1171, 1227)
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    double um = 0.0, uc = u[0], gprev = 0.0, g0 = 0.0, glast = 0.0;
-    for (int j = 0; j < np; ++j) {
-      const double un = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
-      const TriRow row = R[j];
-      double vec;
-      if (row.is_bc) vec = row.bc;
-      else vec = r[(long long)j * pp] + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
-      const double gj = (j == 0) ? vec : vec + row.ap * gprev;
-      if (j >= lo && j <= hi) u[(long long)j * pp] = gj;
-      if (j == 0) g0 = gj;
-      glast = gj;
-      gprev = gj;
-      um = uc;
-      uc = un;
+    // 1. right-hand side (r + explicit CN term, or the BC value) and the
+    //    forward recurrence within the chunk, carry-in zero
+    if (active && xin) {
+      double um = (j0 > 0) ? __ldg(u + (long long)(j0 - 1) * pp + col) : 0.0;
+      double uc = __ldg(u + (long long)j0 * pp + col);
+      double y = 0.0;
+      for (int jb = j0; jb <= j1; jb += 8) {
+        double xr[8], xu[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {   // all loads of the batch first
+          const int j = jb + c;
+          xr[c] = (j <= j1) ? __ldg(r + (long long)j * pp + col) : 0.0;
+          xu[c] = (j <= j1 && j + 1 < np) ? __ldg(u + (long long)(j + 1) * pp + col) : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int j = jb + c;
+          if (j > j1) break;
+          const TriRow* row = R + j;
+          const double un = xu[c];
+          const double v = row->is_bc ? row->bc : xr[c] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+          y = (j == j0) ? v : v + row->ap * y;
+          tile[j * TX + lane] = y;
+          um = uc;
+          uc = un;
+        }
+      }
     }
-    double xn = glast * R[np - 1].ibp;
-    if (np - 1 >= lo && np - 1 <= hi) u[(long long)(np - 1) * pp] = xn;
-    for (int j = np - 2; j >= 0; --j) {
-      const double gj = (j >= lo && j <= hi) ? u[(long long)j * pp] : (j == 0 ? g0 : 0.0);
-      const double x = (gj - R[j].u * xn) * R[j].ibp;
-      if (j >= lo && j <= hi) u[(long long)j * pp] = x;
-      xn = x;
+    __syncthreads();
+    // 2. forward carries: g at the end of chunk k
+    if (w == 0) {
+      double gk = 0.0;
+      for (int k = 0; k < ch.nch; ++k) {
+        const int e = min(np, (k + 1) * ch.len) - 1;
+        gk = tile[e * TX + lane] + (k > 0 ? R[e].pa * gk : 0.0);
+        carry[k][lane] = gk;
+      }
     }
+    __syncthreads();
+    // 3. apply carries, then the backward recurrence within the chunk
+    //    x_j = g_j / b'_j + m_j x_{j+1}, carry-in zero
+    if (active && w > 0) {
+      const double c = carry[w - 1][lane];
+      for (int j = j0; j <= j1; ++j) tile[j * TX + lane] += R[j].pa * c;
+    }
+    __syncthreads();
+    if (active) {
+      double xz = 0.0;
+      for (int j = j1; j >= j0; --j) {
+        const TriRow row = R[j];
+        const double wv = tile[j * TX + lane] * row.ibp;
+        xz = (j == j1) ? wv : wv - row.u * row.ibp * xz;
+        tile[j * TX + lane] = xz;
+      }
+    }
+    __syncthreads();
+    // 4. backward carries: x at the start of chunk k, from the last chunk down
+    if (w == 0) {
+      double xk = 0.0;
+      for (int k = ch.nch - 1; k >= 0; --k) {
+        const int b = k * ch.len;
+        xk = tile[b * TX + lane] + (k < ch.nch - 1 ? R[b].pm * xk : 0.0);
+        carry[k][lane] = xk;
+      }
+    }
+    __syncthreads();
+    // 5. apply carries and write the rows the reference stores
+    if (active && xin) {
+      const double c = (w < ch.nch - 1) ? carry[w + 1][lane] : 0.0;
+      for (int j = j0; j <= j1; ++j) {
+        const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? R[j].pm * c : 0.0);
+        if (j >= lo && j <= hi) u[(long long)j * pp + col] = xv;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -723,15 +808,16 @@ __global__ void k_bc_vel_post(State s, Geom g, Phys ph) {
 
 template <int N>
 static void go_products(const Geom& g, const State& s, cudaStream_t st) {
-  size_t smem = (size_t)6 * (N + ZPAD_S) * sizeof(double2);
+  size_t smem = (size_t)3 * padded(N) * sizeof(double2);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_products<N><<<dim3(g.nz, g.np), 6 * (N / 8), smem, st>>>(s, g);
+  k_products<N><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  size_t smem = (size_t)2 * KT * (N + ZPAD_S) * sizeof(double2);
+  constexpr int T = FftShape<N>::T;
+  size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(double2);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zpass_rhs<N><<<dim3(g.kxs / KT, g.np), 2 * KT * (N / 8), smem, st>>>(s, g, ph, rk);
+  k_zpass_rhs<N><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -755,12 +841,15 @@ cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int 
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  k_tri_coef<<<1, 32, 0, st>>>(g, ph, s.tri, s.sc, rk);
+  const size_t smem = (size_t)g.np * sizeof(TriRow);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_tri_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_tri_coef<<<4, 256, smem, st>>>(g, ph, s.tri, s.sc, rk);
   return cudaGetLastError();
 }
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
-  long long n = g.pp;
-  k_thomas<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(s, g);
+  const size_t smem = (size_t)g.np * TX * sizeof(double);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_thomas<<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {

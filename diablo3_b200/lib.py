@@ -54,7 +54,7 @@ def load(path: str | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("DIABLO_B200_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(f"{path} is missing: run `python -m diablo3_b200.build` (nvcc, sm_100a)")
     L = ctypes.CDLL(path)
