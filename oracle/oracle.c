@@ -50,6 +50,7 @@ struct orc_ctx {
   double time, save_stats_time, save_flow_time;
   int time_step;
   double* arr[16];
+  double* les[30];    /* LES work arrays, indexed by the L_* enum */
   cplx *twx, *twz;
   int *revx, *revz;
 };
@@ -421,6 +422,8 @@ orc_ctx* orc_create(const db_params* p, const double* gy_in) {
   c->zeta_bar[2] = -5.0 / 4.0;
 
   for (int a = 0; a < 16; ++a) c->arr[a] = (double*)calloc((size_t)c->len, sizeof(double));
+  if (p->use_les)
+    for (int a = 0; a < 30; ++a) c->les[a] = (double*)calloc((size_t)c->len, sizeof(double));
   make_fft_tables(Nx, &c->twx, &c->revx);
   make_fft_tables(Nz, &c->twz, &c->revz);
   c->save_stats_time = 1e300;
@@ -431,6 +434,7 @@ orc_ctx* orc_create(const db_params* p, const double* gy_in) {
 void orc_destroy(orc_ctx* c) {
   if (!c) return;
   for (int a = 0; a < 16; ++a) free(c->arr[a]);
+  for (int a = 0; a < 30; ++a) free(c->les[a]);
   free(c->gx); free(c->dx); free(c->gz); free(c->dz);
   free(c->gy); free(c->gyf); free(c->dy); free(c->dyf);
   free(c->kx); free(c->kx2); free(c->cikx);
@@ -745,9 +749,6 @@ double orc_courant_physical(orc_ctx* c) {
   return c->delta_t;
 }
 
-/* ---------------------------------------------------------------------- */
-/* rk_chan_1 (for/solver.f90:366-1273), DNS path                            */
-
 #define LOOP_SPEC(jlo, jhi) \
   for (int j = (jlo); j <= (jhi); ++j) \
     for (int k = 0; k <= c->twoNkz; ++k) \
@@ -757,11 +758,329 @@ double orc_courant_physical(orc_ctx* c) {
     for (int k = 0; k < c->Nzp; ++k) \
       for (int i = 0; i < c->Nx; ++i)
 
+/* ---------------------------------------------------------------------- */
+/* LES, les_model_type 5: anisotropic minimum dissipation, Verstappen form   */
+/* (for/les.f90:3-1068 model-5 branch, 1072-1435, 1443-1746, 1980-2079,      */
+/* 2086-2249; BCs for/flow.f90:1161-1360, 1596-1732).                        */
+
+enum { L_S1 = 0, L_S2, L_S3, L_S4, L_S5, L_S6,          /* Sij (strain)          */
+       L_SI1, L_SI2, L_SI3, L_SI4, L_SI5, L_SI6,        /* SIij (scaled strain)  */
+       L_O4, L_O5, L_O6,                                /* Oij (scaled rotation) */
+       L_DU1DX, L_DU2DY, L_DU3DZ, L_DU2DX, L_DU3DX, L_DU1DZ, L_DU2DZ, L_DU1DY, L_DU3DY,
+       L_DTHX, L_DTHY, L_DTHZ, L_TEMP, L_TEMP_TH, L_S1_TH };
+
+static const double C_AMD = 0.2887;   /* les.f90:25 */
+static const double BETA_SGS = 3.0;   /* les.f90:43 */
+
+/* apply_BC_th_mpi_post (for/flow.f90:1596-1689) */
+static void apply_bc_th_post(orc_ctx* c) {
+  const db_params* p = &c->p;
+  int Nyp = c->Nyp;
+  double* cth = c->arr[DB_CTH];
+  for (int k = 0; k <= c->twoNkz; ++k)
+    for (int i = 0; i < c->Nxp; ++i) {
+      if (p->th_bc_ymin == 0) { CV(c, cth, i, k, 0) = 0.; CV(c, cth, i, k, 1) = 0.; }
+      else { CV(c, cth, i, k, 1) = CV(c, cth, i, k, 2); CV(c, cth, i, k, 0) = CV(c, cth, i, k, 1); }
+    }
+  if (p->th_bc_ymin == 0) { CV(c, cth, 0, 0, 1) = p->th_bc_ymin_c1; CV(c, cth, 0, 0, 0) = p->th_bc_ymin_c1; }
+  else {
+    CV(c, cth, 0, 0, 1) = CV(c, cth, 0, 0, 2) - c->dy[2] * p->th_bc_ymin_c1;
+    CV(c, cth, 0, 0, 0) = CV(c, cth, 0, 0, 1) - c->dy[1] * p->th_bc_ymin_c1;
+  }
+  for (int k = 0; k <= c->twoNkz; ++k)
+    for (int i = 0; i < c->Nxp; ++i) {
+      if (p->th_bc_ymax == 0) { CV(c, cth, i, k, Nyp) = 0.; CV(c, cth, i, k, Nyp + 1) = 0.; }
+      else { CV(c, cth, i, k, Nyp) = CV(c, cth, i, k, Nyp - 1); CV(c, cth, i, k, Nyp + 1) = CV(c, cth, i, k, Nyp); }
+    }
+  if (p->th_bc_ymax == 0) { CV(c, cth, 0, 0, Nyp) = p->th_bc_ymax_c1; CV(c, cth, 0, 0, Nyp + 1) = p->th_bc_ymax_c1; }
+  else {
+    CV(c, cth, 0, 0, Nyp) = CV(c, cth, 0, 0, Nyp - 1) + c->dy[Nyp] * p->th_bc_ymax_c1;
+    CV(c, cth, 0, 0, Nyp + 1) = CV(c, cth, 0, 0, Nyp) + c->dy[Nyp] * p->th_bc_ymax_c1;
+  }
+}
+
+/* apply_BC_les and apply_BC_th_les (for/les.f90:1980-2079) */
+static void apply_bc_les(orc_ctx* c) {
+  const db_params* p = &c->p;
+  int Nyp = c->Nyp;
+  double* cu1 = c->arr[DB_CU1]; double* cu3 = c->arr[DB_CU3]; double* cth = c->arr[DB_CTH];
+  for (int k = 0; k <= c->twoNkz; ++k)
+    for (int i = 0; i < c->Nxp; ++i) {
+      if (p->u_bc_ymax == 1) { CV(c, cu1, i, k, Nyp) = CV(c, cu1, i, k, Nyp - 1); CV(c, cu1, i, k, Nyp + 1) = CV(c, cu1, i, k, Nyp); }
+      if (p->w_bc_ymax == 1) { CV(c, cu3, i, k, Nyp) = CV(c, cu3, i, k, Nyp - 1); CV(c, cu3, i, k, Nyp + 1) = CV(c, cu3, i, k, Nyp); }
+      if (p->u_bc_ymin == 1) { CV(c, cu1, i, k, 1) = CV(c, cu1, i, k, 2); CV(c, cu1, i, k, 0) = CV(c, cu1, i, k, 1); }
+      if (p->w_bc_ymin == 1) { CV(c, cu3, i, k, 1) = CV(c, cu3, i, k, 2); CV(c, cu3, i, k, 0) = CV(c, cu3, i, k, 1); }
+      if (p->th_bc_ymax == 1) { CV(c, cth, i, k, Nyp) = CV(c, cth, i, k, Nyp - 1); CV(c, cth, i, k, Nyp + 1) = CV(c, cth, i, k, Nyp); }
+      if (p->th_bc_ymin == 1) { CV(c, cth, i, k, 1) = CV(c, cth, i, k, 2); CV(c, cth, i, k, 0) = CV(c, cth, i, k, 1); }
+    }
+}
+
+/* the spectral tensors of compute_strain_chan, compute_strain_chan_invariant,
+ * compute_rotation_chan_invariant and compute_all_gradients_chan
+ * (les.f90:1443-1746), then all of them to physical space */
+static void les_tensors(orc_ctx* c) {
+  int Nyp = c->Nyp;
+  double* cu1 = c->arr[DB_CU1]; double* cu2 = c->arr[DB_CU2]; double* cu3 = c->arr[DB_CU3];
+  double* cth = c->arr[DB_CTH];
+  double** L = c->les;
+  const double deltax = c->dx[1] * BETA_SGS, deltaz = c->dz[1] * BETA_SGS;
+  for (int j = 0; j <= Nyp + 1; ++j) {
+    for (int k = 0; k <= c->twoNkz; ++k)
+      for (int i = 0; i < c->Nxp; ++i) {
+        cplx ikx = c->cikx[i], ikz = c->cikz[k];
+        cplx a1 = CV(c, cu1, i, k, j), a2 = CV(c, cu2, i, k, j), a3 = CV(c, cu3, i, k, j);
+        CV(c, L[L_S1], i, k, j) = ikx * a1;
+        CV(c, L[L_S3], i, k, j) = ikz * a3;
+        CV(c, L[L_S5], i, k, j) = 0.5 * (ikz * a1 + ikx * a3);
+        CV(c, L[L_SI1], i, k, j) = ikx * a1;
+        CV(c, L[L_SI3], i, k, j) = ikz * a3;
+        CV(c, L[L_SI5], i, k, j) = 0.5 * (ikz * a1 * (deltaz / deltax) + ikx * a3 * (deltax / deltaz));
+        CV(c, L[L_O5], i, k, j) = 0.5 * (ikz * a1 * (deltaz / deltax) - ikx * a3 * (deltax / deltaz));
+        CV(c, L[L_DU1DX], i, k, j) = ikx * a1;
+        CV(c, L[L_DU1DZ], i, k, j) = ikz * a1;
+        CV(c, L[L_DU2DX], i, k, j) = ikx * a2;
+        CV(c, L[L_DU2DZ], i, k, j) = ikz * a2;
+        CV(c, L[L_DU3DX], i, k, j) = ikx * a3;
+        CV(c, L[L_DU3DZ], i, k, j) = ikz * a3;
+        if (j != Nyp + 1) {
+          cplx d2 = (CV(c, cu2, i, k, j + 1) - a2) / c->dyf[j];
+          CV(c, L[L_S2], i, k, j) = d2;
+          CV(c, L[L_SI2], i, k, j) = d2;
+          CV(c, L[L_DU2DY], i, k, j) = d2;
+        } else {
+          /* ghost_CS2_mpi with one rank (les.f90:2505-2512) */
+          CV(c, L[L_S2], i, k, j) = -10000.0;
+          CV(c, L[L_SI2], i, k, j) = -10000.0;
+          /* the reference reads cu2(Nyp+2), outside its array; the value
+           * only reaches rows the model never uses (les.f90:1679, 1266) */
+          CV(c, L[L_DU2DY], i, k, j) = 0.0;
+        }
+        if (j >= 1) {
+          const double deltay = c->dy[j] * 2.0;
+          cplx d1 = (a1 - CV(c, cu1, i, k, j - 1)) / c->dy[j];
+          cplx d3 = (a3 - CV(c, cu3, i, k, j - 1)) / c->dy[j];
+          CV(c, L[L_S4], i, k, j) = 0.5 * (d1 + ikx * a2);
+          CV(c, L[L_S6], i, k, j) = 0.5 * (ikz * a2 + d3);
+          CV(c, L[L_SI4], i, k, j) = 0.5 * (d1 * (deltay / deltax) + ikx * a2 * (deltax / deltay));
+          CV(c, L[L_SI6], i, k, j) = 0.5 * (ikz * a2 * (deltaz / deltay) + d3 * (deltay / deltaz));
+          CV(c, L[L_O4], i, k, j) = 0.5 * (d1 * (deltay / deltax) - ikx * a2 * (deltax / deltay));
+          CV(c, L[L_O6], i, k, j) = 0.5 * (ikz * a2 * (deltaz / deltay) - d3 * (deltay / deltaz));
+          CV(c, L[L_DU1DY], i, k, j) = d1;
+          CV(c, L[L_DU3DY], i, k, j) = d3;
+          cplx t = CV(c, cth, i, k, j);
+          CV(c, L[L_DTHX], i, k, j) = ikx * t;
+          CV(c, L[L_DTHZ], i, k, j) = ikz * t;
+          CV(c, L[L_DTHY], i, k, j) = (t - CV(c, cth, i, k, j - 1)) / c->dy[j];
+        }
+      }
+  }
+  for (int a = L_S1; a <= L_DTHZ; ++a) orc_fft_xz_to_physical(c, L[a]);
+}
+
+/* AMD eddy viscosity and SGS stress divergence (les.f90:551-900) */
+static void les_chan(orc_ctx* c, int rk_step) {
+  (void)rk_step;
+  int Nyp = c->Nyp, js = c->jstart, je = c->jend;
+  double** L = c->les;
+  double* cu1 = c->arr[DB_CU1]; double* cu2 = c->arr[DB_CU2]; double* cu3 = c->arr[DB_CU3];
+  double* cf1 = c->arr[DB_CF1]; double* cf2 = c->arr[DB_CF2]; double* cf3 = c->arr[DB_CF3];
+  double* nu_t = c->arr[DB_NU_T];
+  double *u1 = cu1, *u2 = cu2, *u3 = cu3;
+  /* j1, j2 with one rank: the "upper wall" branch (les.f90:46-49) */
+  const int j1 = js, j2 = Nyp - 1;
+  orc_apply_bc_vel_post(c);           /* les.f90:63 */
+  apply_bc_th_post(c);                /* les.f90:64 */
+  apply_bc_les(c);                    /* les.f90:74-75 */
+  les_tensors(c);                     /* les.f90:555-564 */
+  orc_fft_xz_to_physical(c, cu1);     /* les.f90:567-569 */
+  orc_fft_xz_to_physical(c, cu2);
+  orc_fft_xz_to_physical(c, cu3);
+#define SI(n, i, k, j) RV(c, L[L_SI##n], i, k, j)
+#define OO(n, i, k, j) RV(c, L[L_O##n], i, k, j)
+  double* s1 = c->arr[A_S1];
+  double* temp = L[L_TEMP];
+  /* max{0, -(I3-I4)}/(I1-I2) at GYF points (les.f90:574-623) */
+  LOOP_PHYS(js, je) {
+    double s4 = 0.5 * (SI(4, i, k, j + 1) + SI(4, i, k, j)), s6 = 0.5 * (SI(6, i, k, j + 1) + SI(6, i, k, j));
+    double o4 = 0.5 * (OO(4, i, k, j + 1) + OO(4, i, k, j)), o6 = 0.5 * (OO(6, i, k, j + 1) + OO(6, i, k, j));
+    double s1v = SI(1, i, k, j), s2v = SI(2, i, k, j), s3v = SI(3, i, k, j), s5 = SI(5, i, k, j), o5 = OO(5, i, k, j);
+    double v = s1v * s1v * s1v + s2v * s2v * s2v + s3v * s3v * s3v
+             + 3.0 * s1v * s4 * s4 + 3.0 * s1v * s5 * s5 + 3.0 * s2v * s4 * s4 + 3.0 * s2v * s6 * s6
+             + 3.0 * s3v * s5 * s5 + 3.0 * s3v * s6 * s6 + 6.0 * s4 * s5 * s6;
+    v = (-v - s1v * o4 * o4 - s1v * o5 * o5 - s2v * o4 * o4 - s2v * o6 * o6 - s3v * o5 * o5 - s3v * o6 * o6
+         - 2.0 * s4 * o5 * o6 + 2.0 * s5 * o4 * o6 - 2.0 * s6 * o4 * o5);
+    if (v <= 0.0) v = 0.0;
+    else v = v / (s1v * s1v + s2v * s2v + s3v * s3v + 2.0 * s4 * s4 + 2.0 * o4 * o4 + 2.0 * s5 * s5
+                  + 2.0 * o5 * o5 + 2.0 * s6 * s6 + 2.0 * o6 * o6);
+    RV(c, s1, i, k, j) = v;
+  }
+  /* the same at GY points (les.f90:628-719) */
+  LOOP_PHYS(2, Nyp) {
+    double w = 1.0 / (2.0 * c->dy[j]);
+#define GI(X) ((X(i, k, j) * c->dyf[j - 1] + X(i, k, j - 1) * c->dyf[j]) * w)
+#define SIA1(i, k, j) SI(1, i, k, j)
+#define SIA2(i, k, j) SI(2, i, k, j)
+#define SIA3(i, k, j) SI(3, i, k, j)
+#define SIA5(i, k, j) SI(5, i, k, j)
+#define OA5(i, k, j) OO(5, i, k, j)
+    double s1v = GI(SIA1), s2v = GI(SIA2), s3v = GI(SIA3), s5 = GI(SIA5), o5 = GI(OA5);
+    double s4 = SI(4, i, k, j), s6 = SI(6, i, k, j), o4 = OO(4, i, k, j), o6 = OO(6, i, k, j);
+    double v = s1v * s1v * s1v + s2v * s2v * s2v + s3v * s3v * s3v
+             + 3.0 * s1v * s4 * s4 + 3.0 * s1v * s5 * s5 + 3.0 * s2v * s4 * s4 + 3.0 * s2v * s6 * s6
+             + 3.0 * s3v * s5 * s5 + 3.0 * s3v * s6 * s6 + 6.0 * s4 * s6 * s5;
+    v = -v - s1v * o4 * o4 - s1v * o5 * o5 - s2v * o4 * o4 - s2v * o6 * o6 - s3v * o5 * o5 - s3v * o6 * o6
+        - 2.0 * s4 * o5 * o6 + 2.0 * s5 * o4 * o6 - 2.0 * s6 * o4 * o5;
+    if (v <= 0.0) v = 0.0;
+    else v = v / (s1v * s1v + s2v * s2v + s3v * s3v + 2.0 * s4 * s4 + 2.0 * o4 * o4 + 2.0 * s5 * s5
+                  + 2.0 * o5 * o5 + 2.0 * s6 * s6 + 2.0 * o6 * o6);
+    RV(c, temp, i, k, j) = v;
+  }
+#undef GI
+  /* les.f90:724-750 */
+  LOOP_PHYS(js, je) {
+    double f = RV(c, s1, i, k, j);
+    RV(c, L[L_S1], i, k, j) = f * RV(c, L[L_S1], i, k, j);
+    RV(c, L[L_S5], i, k, j) = f * RV(c, L[L_S5], i, k, j);
+    RV(c, L[L_S2], i, k, j) = 0.0;
+    RV(c, L[L_S3], i, k, j) = f * RV(c, L[L_S3], i, k, j);
+  }
+  LOOP_PHYS(2, Nyp + 1) {
+    double f = RV(c, temp, i, k, j);
+    RV(c, L[L_S4], i, k, j) = f * (RV(c, L[L_S4], i, k, j) - 0.5 * (RV(c, u1, i, k, j) - RV(c, u1, i, k, j - 1)) / c->dy[j]);
+    RV(c, L[L_S6], i, k, j) = f * (RV(c, L[L_S6], i, k, j) - 0.5 * (RV(c, u3, i, k, j) - RV(c, u3, i, k, j - 1)) / c->dy[j]);
+  }
+  /* filter widths with -2 C^2 absorbed (les.f90:756-780) */
+  double* dyf_w = (double*)calloc(Nyp + 2, sizeof(double));
+  double* dy_w = (double*)calloc(Nyp + 2, sizeof(double));
+  for (int j = 1; j <= Nyp + 1; ++j) {
+    dyf_w[j] = -2.0 * C_AMD * C_AMD * 3.0 /
+        (1.0 / pow(c->dx[1] * BETA_SGS, 2.0) + 1.0 / pow(c->dyf[j] * 2.0, 2.0) + 1.0 / pow(c->dz[1] * BETA_SGS, 2.0));
+    dy_w[j] = -2.0 * C_AMD * C_AMD * 3.0 /
+        (1.0 / pow(c->dx[1] * BETA_SGS, 2.0) + 1.0 / pow(c->dy[j] * 2.0, 2.0) + 1.0 / pow(c->dz[1] * BETA_SGS, 2.0));
+  }
+  LOOP_PHYS(2, Nyp + 1) RV(c, nu_t, i, k, j) = -0.5 * dy_w[j] * RV(c, temp, i, k, j);
+  /* ghost_les_mpi with one rank: nu_t = 0 at both walls (les.f90:2229-2244) */
+  for (int k = 0; k < c->Nzp; ++k)
+    for (int i = 0; i < c->Nx; ++i) {
+      RV(c, nu_t, i, k, 1) = 0.0; RV(c, nu_t, i, k, 2) = 0.0;
+      RV(c, nu_t, i, k, Nyp) = 0.0; RV(c, nu_t, i, k, Nyp + 1) = 0.0;
+    }
+  /* stress to Fourier space and its divergence (les.f90:800-866) */
+  orc_fft_xz_to_fourier(c, L[L_S1]);
+  orc_fft_xz_to_fourier(c, L[L_S3]);
+  orc_fft_xz_to_fourier(c, L[L_S4]);
+  orc_fft_xz_to_fourier(c, L[L_S5]);
+  orc_fft_xz_to_fourier(c, L[L_S6]);
+  LOOP_SPEC(1, Nyp) {
+    CV(c, L[L_S1], i, k, j) = dyf_w[j] * CV(c, L[L_S1], i, k, j);
+    CV(c, L[L_S5], i, k, j) = dyf_w[j] * CV(c, L[L_S5], i, k, j);
+    CV(c, L[L_S3], i, k, j) = dyf_w[j] * CV(c, L[L_S3], i, k, j);
+  }
+  LOOP_SPEC(1, Nyp + 1) {
+    CV(c, L[L_S4], i, k, j) = dy_w[j] * CV(c, L[L_S4], i, k, j);
+    CV(c, L[L_S6], i, k, j) = dy_w[j] * CV(c, L[L_S6], i, k, j);
+  }
+  LOOP_SPEC(j1, j2) {
+    CV(c, cf1, i, k, j) = CV(c, cf1, i, k, j) - c->cikx[i] * CV(c, L[L_S1], i, k, j)
+        - (CV(c, L[L_S4], i, k, j + 1) - CV(c, L[L_S4], i, k, j)) / c->dyf[j] - c->cikz[k] * CV(c, L[L_S5], i, k, j);
+    CV(c, cf3, i, k, j) = CV(c, cf3, i, k, j) - c->cikx[i] * CV(c, L[L_S5], i, k, j)
+        - (CV(c, L[L_S6], i, k, j + 1) - CV(c, L[L_S6], i, k, j)) / c->dyf[j] - c->cikz[k] * CV(c, L[L_S3], i, k, j);
+  }
+  LOOP_SPEC(2, Nyp)
+    CV(c, cf2, i, k, j) = CV(c, cf2, i, k, j) - c->cikx[i] * CV(c, L[L_S4], i, k, j) - c->cikz[k] * CV(c, L[L_S6], i, k, j);
+  /* explicit cross terms nu_t d(u1,u3)/dy (les.f90:871-900) */
+  LOOP_PHYS(2, Nyp) RV(c, temp, i, k, j) = RV(c, nu_t, i, k, j) * (RV(c, u1, i, k, j) - RV(c, u1, i, k, j - 1)) / c->dy[j];
+  orc_fft_xz_to_fourier(c, temp);
+  LOOP_SPEC(2, Nyp) CV(c, cf2, i, k, j) = CV(c, cf2, i, k, j) + c->cikx[i] * CV(c, temp, i, k, j);
+  LOOP_PHYS(2, Nyp) RV(c, temp, i, k, j) = RV(c, nu_t, i, k, j) * (RV(c, u3, i, k, j) - RV(c, u3, i, k, j - 1)) / c->dy[j];
+  orc_fft_xz_to_fourier(c, temp);
+  LOOP_SPEC(2, Nyp) CV(c, cf2, i, k, j) = CV(c, cf2, i, k, j) + c->cikz[k] * CV(c, temp, i, k, j);
+  free(dyf_w);
+  free(dy_w);
+}
+
+/* scalar AMD eddy diffusivity and SGS flux divergence (les.f90:1201-1395) */
+static void les_chan_th(orc_ctx* c) {
+  int Nyp = c->Nyp, jst = c->jstart_th, jet = c->jend_th;
+  double** L = c->les;
+  double* cth = c->arr[DB_CTH];
+  double* cfth = c->arr[DB_CFTH];
+  double* kappa_t = c->arr[DB_KAPPA_T];
+  orc_fft_xz_to_physical(c, cth);
+  const double dxs = c->dx[1] * BETA_SGS, dzs = c->dz[1] * BETA_SGS;
+#define G(a, i, k, j) RV(c, L[a], i, k, j)
+  LOOP_PHYS(jst, jet) {
+    const double dys = c->dyf[j] * 2.0;
+    const double ty = 0.5 * (G(L_DTHY, i, k, j + 1) + G(L_DTHY, i, k, j));
+    const double tx = G(L_DTHX, i, k, j), tz = G(L_DTHZ, i, k, j);
+    double v = -(dxs * dxs * G(L_DU1DX, i, k, j) * tx * tx
+                 + dys * dys * G(L_DU2DY, i, k, j) * ty * ty
+                 + dzs * dzs * G(L_DU3DZ, i, k, j) * tz * tz
+                 + (dys * dys * 0.5 * (G(L_DU1DY, i, k, j + 1) + G(L_DU1DY, i, k, j))
+                    + dxs * dxs * 0.5 * (G(L_DU2DX, i, k, j + 1) + G(L_DU2DX, i, k, j))) * tx * ty
+                 + (dzs * dzs * G(L_DU1DZ, i, k, j) + dxs * dxs * G(L_DU3DX, i, k, j)) * tx * tz
+                 + (dzs * dzs * 0.5 * (G(L_DU2DZ, i, k, j + 1) + G(L_DU2DZ, i, k, j))
+                    + dys * dys * 0.5 * (G(L_DU3DY, i, k, j + 1) + G(L_DU3DY, i, k, j))) * ty * tz);
+    if (v <= 0.0) v = 0.0;
+    else v = v / ((dxs * tx) * (dxs * tx) + (dys * ty) * (dys * ty) + (dzs * tz) * (dzs * tz));
+    RV(c, L[L_S1_TH], i, k, j) = v;
+  }
+  LOOP_PHYS(2, Nyp) {   /* temp_th at GY; row Nyp+1 of the reference is never used */
+    const double dys = c->dy[j] * 2.0, w = 1.0 / (2.0 * c->dy[j]);
+#define GY(a) ((G(a, i, k, j) * c->dyf[j - 1] + G(a, i, k, j - 1) * c->dyf[j]) * w)
+    const double tx = GY(L_DTHX), tz = GY(L_DTHZ), ty = G(L_DTHY, i, k, j);
+    double v = -(dxs * dxs * GY(L_DU1DX) * tx * tx
+                 + dys * dys * GY(L_DU2DY) * ty * ty
+                 + dzs * dzs * GY(L_DU3DZ) * tz * tz
+                 + (dys * dys * G(L_DU1DY, i, k, j) + dxs * dxs * G(L_DU2DX, i, k, j)) * tx * ty
+                 + (dzs * dzs * GY(L_DU1DZ) + dxs * dxs * GY(L_DU3DX)) * tx * tz
+                 + (dzs * dzs * G(L_DU2DZ, i, k, j) + dys * dys * G(L_DU3DY, i, k, j)) * ty * tz);
+#undef GY
+    if (v <= 0.0) v = 0.0;
+    else v = v / ((dxs * tx) * (dxs * tx) + (dys * ty) * (dys * ty) + (dzs * tz) * (dzs * tz));
+    RV(c, L[L_TEMP_TH], i, k, j) = v;
+  }
+  LOOP_PHYS(jst, jet) {
+    RV(c, L[L_DTHX], i, k, j) = RV(c, L[L_S1_TH], i, k, j) * RV(c, L[L_DTHX], i, k, j);
+    RV(c, L[L_DTHZ], i, k, j) = RV(c, L[L_S1_TH], i, k, j) * RV(c, L[L_DTHZ], i, k, j);
+  }
+  double* dyf_w = (double*)calloc(Nyp + 2, sizeof(double));
+  double* dy_w = (double*)calloc(Nyp + 2, sizeof(double));
+  for (int j = 1; j <= Nyp + 1; ++j) {
+    dyf_w[j] = -2.0 * C_AMD * C_AMD * 3.0 /
+        (1.0 / pow(c->dx[1] * BETA_SGS, 2.0) + 1.0 / pow(c->dyf[j] * 2.0, 2.0) + 1.0 / pow(c->dz[1] * BETA_SGS, 2.0));
+    dy_w[j] = -2.0 * C_AMD * C_AMD * 3.0 /
+        (1.0 / pow(c->dx[1] * BETA_SGS, 2.0) + 1.0 / pow(c->dy[j] * 2.0, 2.0) + 1.0 / pow(c->dz[1] * BETA_SGS, 2.0));
+  }
+  LOOP_PHYS(2, Nyp) RV(c, kappa_t, i, k, j) = -0.5 * dy_w[j] * RV(c, L[L_TEMP_TH], i, k, j);
+  /* ghost_les_th_mpi with one rank (les.f90:2396-2411) */
+  for (int k = 0; k < c->Nzp; ++k)
+    for (int i = 0; i < c->Nx; ++i) {
+      RV(c, kappa_t, i, k, 1) = 0.0; RV(c, kappa_t, i, k, 2) = 0.0;
+      RV(c, kappa_t, i, k, Nyp) = 0.0; RV(c, kappa_t, i, k, Nyp + 1) = 0.0;
+    }
+  orc_fft_xz_to_fourier(c, L[L_DTHX]);
+  orc_fft_xz_to_fourier(c, L[L_DTHZ]);
+  LOOP_SPEC(1, Nyp + 1) {
+    CV(c, L[L_DTHX], i, k, j) = 0.5 * dyf_w[j] * CV(c, L[L_DTHX], i, k, j);
+    CV(c, L[L_DTHZ], i, k, j) = 0.5 * dyf_w[j] * CV(c, L[L_DTHZ], i, k, j);
+  }
+  LOOP_SPEC(jst, jet)
+    CV(c, cfth, i, k, j) = CV(c, cfth, i, k, j) - c->cikx[i] * CV(c, L[L_DTHX], i, k, j)
+                           - c->cikz[k] * CV(c, L[L_DTHZ], i, k, j);
+  free(dyf_w);
+  free(dy_w);
+#undef G
+}
+
+/* ---------------------------------------------------------------------- */
+/* rk_chan_1 (for/solver.f90:366-1273), DNS path                            */
+
 int orc_rk_chan_1(orc_ctx* c, int rk_step) {
   const db_params* p = &c->p;
   if (rk_step < 1 || rk_step > 3) return -1;
-  if (p->use_les) {
-    snprintf(g_err, sizeof g_err, "oracle: LES path not in this restatement");
+  if (p->use_les && p->les_model_type != 5) {
+    snprintf(g_err, sizeof g_err, "oracle: only LES model 5 (AMD, Verstappen) is restated");
     return -1;
   }
   int Nyp = c->Nyp, js = c->jstart, je = c->jend, jst = c->jstart_th, jet = c->jend_th;
@@ -782,7 +1101,6 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
   double temp3 = c->zeta_bar[rk] * c->h_bar[rk];
   double temp4 = c->h_bar[rk];
   double temp5 = c->beta_bar[rk] * c->h_bar[rk];
-  (void)temp2;
 
   /* :396-410 */
   LOOP_SPEC(js, je) { CV(c, cr1, i, k, j) = CV(c, cu1, i, k, j); CV(c, cr3, i, k, j) = CV(c, cu3, i, k, j); }
@@ -837,11 +1155,16 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
     CV(c, cfth, i, k, j) = CV(c, cfth, i, k, j) - CV(c, cu1, i, k, j) * c->dTHdX - CV(c, cu3, i, k, j) * c->dTHdZ;
   /* :609 */
   user_rhs_chan_fourier(c);
-  /* :635-643 */
-  orc_fft_xz_to_physical(c, cu1);
-  orc_fft_xz_to_physical(c, cu2);
-  orc_fft_xz_to_physical(c, cu3);
-  orc_fft_xz_to_physical(c, cth);
+  /* :615-645 */
+  if (p->use_les && (!p->create_new_flow || c->time_step > 100)) {
+    les_chan(c, rk_step);
+    les_chan_th(c);
+  } else {
+    orc_fft_xz_to_physical(c, cu1);
+    orc_fft_xz_to_physical(c, cu2);
+    orc_fft_xz_to_physical(c, cu3);
+    orc_fft_xz_to_physical(c, cth);
+  }
 
   /* nonlinear terms :655-815 */
   LOOP_PHYS(js, je) RV(c, s1, i, k, j) = RV(c, u3, i, k, j) * RV(c, u1, i, k, j);
@@ -909,6 +1232,23 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
     RV(c, r2, i, k, j) = RV(c, r2, i, k, j) + temp1 * nvs *
         (((RV(c, u2, i, k, j + 1) - RV(c, u2, i, k, j)) / c->dyf[j] -
           (RV(c, u2, i, k, j) - RV(c, u2, i, k, j - 1)) / c->dyf[j - 1]) / c->dy[j]);
+  if (p->use_les) { /* :875-903, nu_t at GY points */
+    double* nt = c->arr[DB_NU_T];
+    LOOP_PHYS(js, je) {
+      RV(c, r1, i, k, j) = RV(c, r1, i, k, j) + temp2 *
+          ((RV(c, nt, i, k, j + 1) * (RV(c, u1, i, k, j + 1) - RV(c, u1, i, k, j)) / c->dy[j + 1]
+            - RV(c, nt, i, k, j) * (RV(c, u1, i, k, j) - RV(c, u1, i, k, j - 1)) / c->dy[j]) / c->dyf[j]);
+      RV(c, r3, i, k, j) = RV(c, r3, i, k, j) + temp2 *
+          ((RV(c, nt, i, k, j + 1) * (RV(c, u3, i, k, j + 1) - RV(c, u3, i, k, j)) / c->dy[j + 1]
+            - RV(c, nt, i, k, j) * (RV(c, u3, i, k, j) - RV(c, u3, i, k, j - 1)) / c->dy[j]) / c->dyf[j]);
+    }
+    LOOP_PHYS(2, Nyp)
+      RV(c, r2, i, k, j) = RV(c, r2, i, k, j) + temp2 *
+          ((0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j + 1))) * (RV(c, u2, i, k, j + 1) - RV(c, u2, i, k, j))
+               / c->dyf[j]
+           - 0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j - 1)) * (RV(c, u2, i, k, j) - RV(c, u2, i, k, j - 1))
+               / c->dyf[j - 1]) / c->dy[j];
+  }
 
   /* scalar :914-973 */
   LOOP_PHYS(jst, jet) RV(c, s1, i, k, j) = RV(c, th, i, k, j) * RV(c, u1, i, k, j);
@@ -931,6 +1271,13 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
     RV(c, rth, i, k, j) = RV(c, rth, i, k, j) + (temp1 / Pr) * nvs *
         (((RV(c, th, i, k, j + 1) - RV(c, th, i, k, j)) / c->dy[j + 1] -
           (RV(c, th, i, k, j) - RV(c, th, i, k, j - 1)) / c->dy[j]) / c->dyf[j]);
+  if (p->use_les) { /* :992-1002, kappa_t at GY points */
+    double* kt = c->arr[DB_KAPPA_T];
+    LOOP_PHYS(jst, jet)
+      RV(c, rth, i, k, j) = RV(c, rth, i, k, j) + temp2 *
+          ((RV(c, kt, i, k, j + 1) * (RV(c, th, i, k, j + 1) - RV(c, th, i, k, j)) / c->dy[j + 1]
+            - RV(c, kt, i, k, j) * (RV(c, th, i, k, j) - RV(c, th, i, k, j - 1)) / c->dy[j]) / c->dyf[j]);
+  }
 
   /* implicit solves, one z-plane k at a time (every row 0..Nyp+1 of the
    * system is rewritten each k by the interior loop or the BC routines, so
@@ -956,6 +1303,16 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
           TU(t, i, j) = -(tth) / (c->dy[j + 1] * c->dyf[j]);
           TVv(t, i, j) = RV(c, rth, i, k, j);
         }
+      if (p->use_les) { /* :1032-1045 */
+        double* kt = c->arr[DB_KAPPA_T];
+        for (int j = jst; j <= jet; ++j)
+          for (int i = 0; i < Nx; ++i) {
+            TL(t, i, j) = TL(t, i, j) - temp2 * RV(c, kt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TD(t, i, j) = TD(t, i, j) + temp2 * RV(c, kt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j])
+                          + temp2 * RV(c, kt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TU(t, i, j) = TU(t, i, j) - temp2 * RV(c, kt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j]);
+          }
+      }
       bc_horizontal(c, t, p->th_bc_ymin, p->th_bc_ymin_c1, p->th_bc_ymax, p->th_bc_ymax_c1);
       orc_thomas_real(t.l, t.d, t.u, t.v, Nyp, Nx);
       for (int j = jst - 1; j <= jet + 1; ++j)
@@ -969,6 +1326,16 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
           TU(t, i, j) = -tv / (c->dyf[j] * c->dy[j]);
           TVv(t, i, j) = RV(c, r2, i, k, j);
         }
+      if (p->use_les) { /* :1092-1105 */
+        double* nt = c->arr[DB_NU_T];
+        for (int j = 2; j <= Nyp; ++j)
+          for (int i = 0; i < Nx; ++i) {
+            TL(t, i, j) = TL(t, i, j) - temp2 * 0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j - 1)) / (c->dyf[j - 1] * c->dy[j]);
+            TD(t, i, j) = TD(t, i, j) + temp2 * 0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j + 1)) / (c->dyf[j] * c->dy[j])
+                          + temp2 * 0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j - 1)) / (c->dyf[j - 1] * c->dy[j]);
+            TU(t, i, j) = TU(t, i, j) - temp2 * 0.5 * (RV(c, nt, i, k, j) + RV(c, nt, i, k, j + 1)) / (c->dyf[j] * c->dy[j]);
+          }
+      }
       bc_u2(c, t);
       orc_thomas_real(t.l, t.d, t.u, t.v, Nyp, Nx);
       for (int j = 1; j <= Nyp + 1; ++j)
@@ -982,6 +1349,16 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
           TU(t, i, j) = -tv / (c->dy[j + 1] * c->dyf[j]);
           TVv(t, i, j) = RV(c, r1, i, k, j);
         }
+      if (p->use_les) { /* :1148-1161, 1204-1217 */
+        double* nt = c->arr[DB_NU_T];
+        for (int j = js; j <= je; ++j)
+          for (int i = 0; i < Nx; ++i) {
+            TL(t, i, j) = TL(t, i, j) - temp2 * RV(c, nt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TD(t, i, j) = TD(t, i, j) + temp2 * RV(c, nt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j])
+                          + temp2 * RV(c, nt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TU(t, i, j) = TU(t, i, j) - temp2 * RV(c, nt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j]);
+          }
+      }
       bc_horizontal(c, t, p->u_bc_ymin, p->u_bc_ymin_c1, p->u_bc_ymax, p->u_bc_ymax_c1);
       orc_thomas_real(t.l, t.d, t.u, t.v, Nyp, Nx);
       for (int j = js - 1; j <= je + 1; ++j)
@@ -995,6 +1372,16 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step) {
           TU(t, i, j) = -tv / (c->dy[j + 1] * c->dyf[j]);
           TVv(t, i, j) = RV(c, r3, i, k, j);
         }
+      if (p->use_les) { /* :1148-1161, 1204-1217 */
+        double* nt = c->arr[DB_NU_T];
+        for (int j = js; j <= je; ++j)
+          for (int i = 0; i < Nx; ++i) {
+            TL(t, i, j) = TL(t, i, j) - temp2 * RV(c, nt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TD(t, i, j) = TD(t, i, j) + temp2 * RV(c, nt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j])
+                          + temp2 * RV(c, nt, i, k, j) / (c->dy[j] * c->dyf[j]);
+            TU(t, i, j) = TU(t, i, j) - temp2 * RV(c, nt, i, k, j + 1) / (c->dy[j + 1] * c->dyf[j]);
+          }
+      }
       {
         double wmax = c->w_bc_ymax_c1;
         if (p->w_bc_ymax == 1) {

@@ -175,3 +175,131 @@ def test_thermal_wind_rest_state_is_steady(oracle_mod):
     for f in (0, 1, 2):
         assert np.abs(significant(p, o.cplx(f))).max() < 1e-14
     assert rel_l2(significant(p, o.cplx(4)), th0) < 1e-14
+
+
+def _to_phys(p, c):
+    """Packed dealiased spectral planes -> physical planes (numpy irfft2)."""
+    nkx, nkz = p.nkx, p.nkz
+    full = np.zeros((c.shape[0], p.nz, p.nx // 2 + 1), complex)
+    full[:, : nkz + 1, : nkx + 1] = c[:, : nkz + 1, : nkx + 1]
+    full[:, p.nz - nkz:, : nkx + 1] = c[:, nkz + 1: 2 * nkz + 1, : nkx + 1]
+    return np.fft.irfft2(full, s=(p.nz, p.nx), axes=(1, 2)) * (p.nx * p.nz)
+
+
+def _amd_fixture(oracle_mod, **kw):
+    from diablo3_b200.ic import initial_fields
+    p = config0_params(nx=32, ny=33, nz=16, use_les=1, create_new_flow=0, les_model_type=5,
+                       kick=0.05, re=5000.0, **kw)
+    gy = grid_for(p)
+    o = oracle_mod.Oracle(p, gy)
+    o.init_from_physical(*initial_fields(p, gy, seed=11))
+    c = {f: o.cplx(f).copy() for f in (0, 1, 2, 4)}
+    met = {k: o.metric(i, p.ny + 2) for i, k in enumerate(("gy", "gyf", "dy", "dyf"))}
+    kx = o.metric(4, p.nxp)[: p.nkx + 1]
+    kz = o.metric(5, 2 * p.nkz + 1)
+    o.rk_substep(1)
+    return p, o, c, met, kx, kz
+
+
+def _gradients_at_gy(p, c, met, kx, kz, fid_list=(0, 1, 2)):
+    """Velocity gradient G[i][k] = d u_i / d x_k and scalar gradient g[k],
+    physical, at GY rows (x/z derivatives and d u2/dy live at GYF rows and
+    are interpolated to GY with the dyf weights)."""
+    dy, dyf = met["dy"], met["dyf"]
+    ny = p.ny
+    sl = (slice(None), slice(0, 2 * p.nkz + 1), slice(0, p.nkx + 1))
+    ikx = 1j * kx[None, None, :]
+    ikz = 1j * kz[None, :, None]
+    u = [c[f][sl] for f in (0, 1, 2)]
+    th = c[4][sl]
+
+    def ph(a):
+        return _to_phys(p, a)
+
+    def gyf_to_gy(x):  # rows j of result = GY row j, j = 1..ny
+        out = np.zeros_like(x)
+        for j in range(1, ny + 1):
+            out[j] = (x[j] * dyf[j - 1] + x[j - 1] * dyf[j]) / (2 * dy[j])
+        return out
+
+    def ddy_gy(a):  # (a(j) - a(j-1)) / dy(j), GYF field -> GY
+        out = np.zeros_like(a)
+        out[1:] = (a[1:] - a[:-1]) / dy[1:, None, None]
+        return out
+
+    d2dy = np.zeros_like(u[1])
+    d2dy[:-1] = (u[1][1:] - u[1][:-1]) / dyf[:-1, None, None]
+    G = [[None] * 3 for _ in range(3)]
+    G[0][0] = gyf_to_gy(ph(ikx * u[0]))
+    G[0][1] = ph(ddy_gy(u[0]))
+    G[0][2] = gyf_to_gy(ph(ikz * u[0]))
+    G[1][0] = ph(ikx * u[1])
+    G[1][1] = gyf_to_gy(ph(d2dy))
+    G[1][2] = ph(ikz * u[1])
+    G[2][0] = gyf_to_gy(ph(ikx * u[2]))
+    G[2][1] = ph(ddy_gy(u[2]))
+    G[2][2] = gyf_to_gy(ph(ikz * u[2]))
+    g = [gyf_to_gy(ph(ikx * th)), ph(ddy_gy(th)), gyf_to_gy(ph(ikz * th))]
+    return np.array(G), np.array(g)
+
+
+def _filter_widths(p, met):
+    dx, dz = p.lx / p.nx, p.lz / p.nz
+    return 3.0 * dx, 2.0 * met["dy"], 3.0 * dz
+
+
+def test_amd_eddy_viscosity_matches_tensor_form(oracle_mod):
+    """nu_t of the AMD model (les_model_type 5) from the oracle's
+    element-wise restatement equals the closed tensor form
+    C^2 max(0, -tr(S^3) + tr(S W^2)) / |D|^2 * 3 / sum_k delta_k^-2 with
+    D_ij = (delta_j / delta_i) du_i/dx_j, S, W its symmetric and
+    antisymmetric parts, evaluated here with numpy at GY rows."""
+    p, o, c, met, kx, kz = _amd_fixture(oracle_mod)
+    G, _ = _gradients_at_gy(p, c, met, kx, kz)
+    dxs, dys, dzs = _filter_widths(p, met)
+    ny = p.ny
+    rows = range(3, ny)   # rows 1, 2, ny, ny+1 are the zeroed wall rows
+    nut = o.real(9)[:, : p.nz, : p.nx]
+    assert np.all(nut >= 0.0)
+    for j in (1, 2, ny, ny + 1):
+        assert np.all(nut[j] == 0.0)
+    worst = 0.0
+    for j in rows:
+        delta = np.array([dxs, dys[j], dzs])
+        D = G[:, :, j] * (delta[None, :] / delta[:, None])[:, :, None, None]
+        S = 0.5 * (D + D.transpose(1, 0, 2, 3))
+        W = 0.5 * (D - D.transpose(1, 0, 2, 3))
+        S3 = np.einsum("ijzx,jkzx,kizx->zx", S, S, S)
+        SW2 = np.einsum("ijzx,jkzx,kizx->zx", S, W, W)
+        num = -S3 + SW2
+        den = np.einsum("ijzx,ijzx->zx", D, D)
+        v = np.where(num > 0, num / den, 0.0)
+        ref = 0.2887 ** 2 * 3.0 / (1 / dxs ** 2 + 1 / dys[j] ** 2 + 1 / dzs ** 2) * v
+        worst = max(worst, float(np.abs(nut[j] - ref).max()))
+    scale = float(nut.max())
+    assert scale > 0.0
+    assert worst < 1e-11 * scale
+
+
+def test_amd_eddy_diffusivity_matches_tensor_form(oracle_mod):
+    """kappa_t of the scalar AMD model equals
+    C^2 max(0, -g^T G Delta^2 g) / |Delta g|^2 * 3 / sum_k delta_k^-2
+    (G the velocity gradient, g the scalar gradient, Delta = diag(delta))."""
+    p, o, c, met, kx, kz = _amd_fixture(oracle_mod)
+    G, g = _gradients_at_gy(p, c, met, kx, kz)
+    dxs, dys, dzs = _filter_widths(p, met)
+    ny = p.ny
+    kt = o.real(10)[:, : p.nz, : p.nx]
+    assert np.all(kt >= 0.0)
+    worst = 0.0
+    for j in range(3, ny):
+        d2 = np.array([dxs, dys[j], dzs]) ** 2
+        gj = g[:, j]
+        num = -np.einsum("izx,ikzx,k,kzx->zx", gj, G[:, :, j], d2, gj)
+        den = np.einsum("k,kzx->zx", d2, gj * gj)
+        v = np.where(num > 0, num / den, 0.0)
+        ref = 0.2887 ** 2 * 3.0 / (1 / dxs ** 2 + 1 / dys[j] ** 2 + 1 / dzs ** 2) * v
+        worst = max(worst, float(np.abs(kt[j] - ref).max()))
+    scale = float(kt.max())
+    assert scale > 0.0
+    assert worst < 1e-11 * scale
