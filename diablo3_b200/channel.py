@@ -68,6 +68,12 @@ class Channel:
         self._ck(self.L.db_upload_field(self.h, fid, _L.dptr(self._as_d(arr).reshape(-1))))
 
     def download_field(self, fid: int) -> np.ndarray:
+        """Spectral fields as reference complex arrays; nu_t / kappa_t
+        (LES) as reference real arrays."""
+        if fid in (_L.NU_T, _L.KAPPA_T):
+            out = self.new_real()
+            self._ck(self.L.db_download_field(self.h, fid, _L.dptr(out.reshape(-1))))
+            return out
         out = self.new_spectral()
         self._ck(self.L.db_download_field(self.h, fid, _L.dptr(out.view(np.float64).reshape(-1))))
         return out

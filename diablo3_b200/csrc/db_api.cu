@@ -26,7 +26,8 @@ struct db_ctx {
   std::vector<void*> allocs;
   double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [LES model active]
+  int time_step = 0;             // host mirror of the driver's time_step
   std::string err;
   double* h_stage = nullptr;     // pinned staging, one physical field
   size_t stage_doubles = 0;
@@ -37,7 +38,7 @@ struct db_ctx {
   bool timing = false;
   cudaEvent_t ev[3][DB_NSTAGES + 1] = {};
   long long launches = 0;          // kernels issued so far
-  long long graph_kernels = 0;     // kernel nodes in one captured step
+  long long graph_kernels[2] = {0, 0};   // kernel nodes in one captured step
 };
 
 static std::string g_init_err;
@@ -78,7 +79,11 @@ static int validate(const db_params* p, std::string& why) {
   if (p->ny < 4) { why = "ny must be >= 4"; return DB_ERR_SIZE; }
   if (p->n_th != 1) { why = "n_th must be 1 (one scalar)"; return DB_ERR_UNSUPPORTED; }
   if (p->time_ad_meth != 1) { why = "time_ad_meth 2 (rk_chan_2) stops in the reference (solver.f90:1289-1293)"; return DB_ERR_UNSUPPORTED; }
-  if (p->use_les) { why = "LES closure not available in this build"; return DB_ERR_UNSUPPORTED; }
+  if (p->use_les && p->les_model_type != 5) {
+    why = "LES: only les_model_type 5 (AMD) is built";
+    return DB_ERR_UNSUPPORTED;
+  }
+  if (p->use_les && p->ny + 2 > 900) { why = "LES: ny + 2 must be <= 900 (per-column Thomas tile)"; return DB_ERR_SIZE; }
   if (p->precision != 0) { why = "only the FP64 path (precision 0) is available"; return DB_ERR_UNSUPPORTED; }
   const int b[8] = {p->u_bc_ymin, p->v_bc_ymin, p->w_bc_ymin, p->th_bc_ymin,
                     p->u_bc_ymax, p->v_bc_ymax, p->w_bc_ymax, p->th_bc_ymax};
@@ -207,6 +212,14 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
     if ((rc = dalloc(c, &ph_[i], Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   s.u1 = ph_[0]; s.u2 = ph_[1]; s.u3 = ph_[2]; s.th = ph_[3];
   s.r1 = ph_[4]; s.r2 = ph_[5]; s.r3 = ph_[6]; s.rth = ph_[7];
+  if (p->use_les) {
+    double** lf[19] = {&s.gx[0], &s.gx[1], &s.gx[2], &s.gx[3], &s.gz[0], &s.gz[1], &s.gz[2], &s.gz[3],
+                       &s.les[0], &s.les[1], &s.les[2], &s.les[3], &s.les[4], &s.les[5], &s.les[6],
+                       &s.les[7], &s.les[8], &s.nu_t, &s.kappa_t};
+    for (int i = 0; i < 19; ++i)
+      if ((rc = dalloc(c, lf[i], Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  }
   if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
   if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
   size_t ntab = 4 * (size_t)np + g.kxs + g.nkzp;
@@ -266,7 +279,8 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
 
 extern "C" int db_finalize(db_ctx* c) {
   if (!c) return DB_ERR_ARG;
-  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (int i = 0; i < 2; ++i)
+    if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
   if (c->st) cudaStreamSynchronize(c->st);
   for (int r = 0; r < 3; ++r)
     for (int k = 0; k <= DB_NSTAGES; ++k)
@@ -391,17 +405,40 @@ extern "C" int db_download_state(db_ctx* c, double* cu1, double* cu2, double* cu
   return DB_OK;
 }
 
+static double* les_field(db_ctx* c, int id) {
+  if (!c->p.use_les) return nullptr;
+  return id == DB_NU_T ? c->s.nu_t : c->s.kappa_t;
+}
+
 extern "C" int db_upload_field(db_ctx* c, int field, const double* host) {
   if (!c || !host) return DB_ERR_ARG;
   if (field >= DB_CU1 && field <= DB_CFTH) return upload_spec(c, field, host);
-  if (field == DB_NU_T || field == DB_KAPPA_T) return fail(c, DB_ERR_UNSUPPORTED, "LES fields not built");
+  if (field == DB_NU_T || field == DB_KAPPA_T) {
+    double* d = les_field(c, field);
+    if (!d) return fail(c, DB_ERR_STATE, "nu_t / kappa_t exist only with use_les");
+    phys_ref_to_compact(c, host, c->h_stage);
+    CK(cudaMemcpyAsync(d, c->h_stage, (size_t)c->g.np * c->g.pp * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return DB_OK;
+  }
   return fail(c, DB_ERR_ARG, "bad field id");
 }
 
 extern "C" int db_download_field(db_ctx* c, int field, double* host) {
   if (!c || !host) return DB_ERR_ARG;
   if (field >= DB_CU1 && field <= DB_CFTH) return download_spec(c, field, host);
-  if (field == DB_NU_T || field == DB_KAPPA_T) return fail(c, DB_ERR_UNSUPPORTED, "LES fields not built");
+  if (field == DB_NU_T || field == DB_KAPPA_T) {
+    double* d = les_field(c, field);
+    if (!d) return fail(c, DB_ERR_STATE, "nu_t / kappa_t exist only with use_les");
+    const Geom& g = c->g;
+    CK(cudaMemcpyAsync(c->h_stage, d, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    // the reference array's padding (x >= Nx, z >= Nz) reads as zero
+    const int nx2 = c->p.nx + 2, nz2 = c->p.nz + 2;
+    memset(host, 0, sizeof(double) * (size_t)g.np * nz2 * nx2);
+    compact_to_phys_ref(c, c->h_stage, host);
+    return DB_OK;
+  }
   return fail(c, DB_ERR_ARG, "bad field id");
 }
 
@@ -416,6 +453,7 @@ extern "C" int db_set_clock(db_ctx* c, double time, int32_t time_step, double ss
   h.time = time; h.time_step = time_step; h.save_stats_time = sst; h.save_flow_time = sft;
   CK(cudaMemcpyAsync(c->s.sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
+  c->time_step = time_step;
   return DB_OK;
 }
 
@@ -468,20 +506,43 @@ extern "C" int db_fft_xz_to_physical(db_ctx* c, double* buf) {
 // ---------------------------------------------------------------------------
 // the substep
 
-static cudaError_t substep(db_ctx* c, int rk /* 0-based */) {
+// the LES model runs on a substep of driver step time_step (solver.f90:615)
+static bool les_active(const db_ctx* c, int time_step) {
+  return c->p.use_les && (!c->p.create_new_flow || time_step > 100);
+}
+
+static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   const Geom& g = c->g;
   State& s = c->s;
   cudaStream_t st = c->st;
   cudaError_t e;
   long long n = 0;
   mark(c, rk, 0);
-  // velocity and buoyancy to physical space (solver.f90:635-643)
-  if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
-  mark(c, rk, 1);
-  if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.u1, s.u2, s.u3, s.th), 4, st))) return e;
-  mark(c, rk, 2);
-  // nonlinear products + x-FFT, then z-FFT + spectral RHS + inverse z of cr
-  if ((e = launch_products(g, s, st))) return e;
+  if (les) {
+    // les_chan / les_chan_th: ghost rows, then the state and its x and z
+    // derivatives to physical space (les.f90:63-75, 555-569, 1209-1211)
+    if ((e = launch_les_bc(g, c->ph, s, st))) return e;
+    if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth, s.cu1, s.cu2, s.cu3, s.cth),
+                          fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]), 8, st,
+                          0xF0u, s.ghost))) return e;
+    mark(c, rk, 1);
+    FieldSet in = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[0], s.xh[1], s.xh[2], s.xh[3]);
+    FieldSet out = fset(s.u1, s.u2, s.u3, s.th, s.gx[0], s.gx[1], s.gx[2], s.gx[3]);
+    for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
+    if ((e = launch_inv_x(g, in, out, 12, st, 0xF0u))) return e;
+    mark(c, rk, 2);
+    if ((e = launch_les_amd(g, c->ph, s, st))) return e;
+    n += 2;
+  } else {
+    // velocity and buoyancy to physical space (solver.f90:635-643)
+    if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
+    mark(c, rk, 1);
+    if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.u1, s.u2, s.u3, s.th), 4, st))) return e;
+    mark(c, rk, 2);
+  }
+  // nonlinear products (+ SGS forcing) + x-FFT, then z-FFT + spectral RHS +
+  // inverse z of cr
+  if ((e = launch_products(g, s, st, les))) return e;
   mark(c, rk, 3);
   if ((e = launch_zpass_rhs(g, c->ph, s, rk, st))) return e;
   mark(c, rk, 4);
@@ -490,7 +551,11 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */) {
   mark(c, rk, 5);
   // implicit CN solves (solver.f90:1012-1233)
   if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
-  if ((e = launch_thomas(g, s, st))) return e;
+  if (c->p.use_les) {   // eddy terms whether or not the model ran this step
+    if ((e = launch_thomas_les(g, s, rk, st))) return e;
+  } else {
+    if ((e = launch_thomas(g, s, st))) return e;
+  }
   mark(c, rk, 6);
   n += 7;
   // CFL on the last substep (solver.f90:1241-1244)
@@ -521,18 +586,18 @@ extern "C" int db_rk_substep(db_ctx* c, int rk_step) {
   if (rk_step < 1 || rk_step > 3) return fail(c, DB_ERR_ARG, "rk_step must be 1, 2 or 3");
   const bool t = c->timing;
   c->timing = false;  // stage events belong to whole steps
-  cudaError_t e = substep(c, rk_step - 1);
+  cudaError_t e = substep(c, rk_step - 1, les_active(c, c->time_step));
   c->timing = t;
   CK(e);
   CK(cudaStreamSynchronize(c->st));
   return DB_OK;
 }
 
-static cudaError_t one_step(db_ctx* c) {
+static cudaError_t one_step(db_ctx* c, bool les) {
   cudaError_t e;
   if ((e = launch_step_begin(c->s.sc, c->st))) return e;
   for (int rk = 0; rk < 3; ++rk)
-    if ((e = substep(c, rk))) return e;
+    if ((e = substep(c, rk, les))) return e;
   c->launches += 2;
   return launch_step_end(c->s.sc, c->st);
 }
@@ -540,28 +605,33 @@ static cudaError_t one_step(db_ctx* c) {
 extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
   if (!c) return DB_ERR_ARG;
   if (nsteps < 0) return fail(c, DB_ERR_ARG, "nsteps must be >= 0");
-  if (!c->graph) {
-    cudaGraph_t gr;
-    const long long before = c->launches;
-    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
-    cudaError_t e = one_step(c);
-    c->graph_kernels = c->launches - before;
-    c->launches = before;
-    cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-      c->err = std::string("graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2);
-      return DB_ERR_CUDA;
+  for (int i = 0; i < nsteps; ++i) {
+    // time_step is incremented at the start of the step (diablo.f90:58-61)
+    const int m = les_active(c, c->time_step + 1) ? 1 : 0;
+    if (!c->graph[m]) {
+      cudaGraph_t gr;
+      const long long before = c->launches;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+      cudaError_t e = one_step(c, m == 1);
+      c->graph_kernels[m] = c->launches - before;
+      c->launches = before;
+      cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+      if (e != cudaSuccess || e2 != cudaSuccess) {
+        c->err = std::string("graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2);
+        return DB_ERR_CUDA;
+      }
+      e = cudaGraphInstantiate(&c->graph[m], gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) {
+        c->graph[m] = nullptr;
+        c->err = std::string("graph instantiate failed: ") + cudaGetErrorString(e);
+        return DB_ERR_CUDA;
+      }
     }
-    e = cudaGraphInstantiate(&c->graph, gr, 0);
-    cudaGraphDestroy(gr);
-    if (e != cudaSuccess) {
-      c->graph = nullptr;
-      c->err = std::string("graph instantiate failed: ") + cudaGetErrorString(e);
-      return DB_ERR_CUDA;
-    }
+    CK(cudaGraphLaunch(c->graph[m], c->st));
+    c->launches += c->graph_kernels[m];
+    c->time_step += 1;
   }
-  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
-  c->launches += (long long)nsteps * c->graph_kernels;
   CK(cudaStreamSynchronize(c->st));
   return DB_OK;
 }
@@ -571,10 +641,12 @@ extern "C" int db_set_timing(db_ctx* c, int enable) {
   if (enable && !c->ev[0][0])
     for (int r = 0; r < 3; ++r)
       for (int k = 0; k <= DB_NSTAGES; ++k) CK(cudaEventCreate(&c->ev[r][k]));
-  if ((enable != 0) != c->timing && c->graph) {  // re-capture with/without event nodes
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  if ((enable != 0) != c->timing)  // re-capture with/without event nodes
+    for (int i = 0; i < 2; ++i)
+      if (c->graph[i]) {
+        cudaGraphExecDestroy(c->graph[i]);
+        c->graph[i] = nullptr;
+      }
   c->timing = enable != 0;
   return DB_OK;
 }

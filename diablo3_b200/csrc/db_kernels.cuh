@@ -38,9 +38,13 @@ inline FieldSet fset(void* a = nullptr, void* b = nullptr, void* c = nullptr, vo
 
 // k_fft.cu
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
-cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+// dmask: bit f set -> field f is differentiated (x: i kx, z: i kz) on the way
+cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0);
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
-cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+// ghost (optional): rows 0, 1, Nyp, Nyp+1 of field f are read from
+// ghost + (4 (f % 4) + q) sp instead (q = 0..3 for those rows)
+cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0,
+                         const double2* ghost = nullptr);
 
 // Tridiagonal row description of one implicit equation (one per row j of
 // 0..Nyp+1): coefficients l, d, u; is_bc marks rows whose right-hand side
@@ -80,10 +84,16 @@ struct State {
   double2* pfac;                             // rem_div factors (a', 1/b') per (kx,kz,j)
   TriRow* tri;                               // 4 equations x np rows (th, u2, u1, u3)
   DevScalars* sc;
+  // LES (les_model_type 5), physical [j][z][x]; null without use_les
+  double* gx[4];                             // d/dx of u1, u2, u3, th
+  double* gz[4];                             // d/dz of u1, u2, u3, th
+  double* les[9];                            // SGS forcing per product slot (k_les.cu)
+  double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
+  double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
 };
 
-// k_substep.cu
-cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st);
+// k_substep.cu; les: add the SGS forcing fields s.les to the products
+cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les = false);
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st);
@@ -101,5 +111,10 @@ cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_end(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st);
 cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
+
+// k_les.cu
+cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
+cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
+cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st);
 
 }  // namespace db

@@ -58,9 +58,10 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet 
   }
 }
 
-// Xh -> physical
+// Xh -> physical; fields f with bit f of dmask set are differentiated in x
+// (multiplied by i kx before the transform)
 template <int N>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet out, Geom g, unsigned dmask) {
   extern __shared__ double2 sm[];
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -72,6 +73,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet 
   load_twiddles<N, E>(tw, lane, g.twx);
   const double2* ia = (const double2*)in.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
   const double2* ib = ia + g.kxs;
+  const bool dx = (dmask >> f) & 1u;
   double2 v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
@@ -79,10 +81,12 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet 
     double2 z = make_double2(0.0, 0.0);
     if (e <= g.nkx) {
       double2 A = __ldg(ia + e), B = __ldg(ib + e);
+      if (dx) { A = cmul_i(A, g.kx[e]); B = cmul_i(B, g.kx[e]); }
       if (e == 0) { A.y = 0.0; B.y = 0.0; }
       z = make_double2(A.x - B.y, A.y + B.x);            // A + iB
     } else if (e >= N - g.nkx) {
-      const double2 A = __ldg(ia + (N - e)), B = __ldg(ib + (N - e));
+      double2 A = __ldg(ia + (N - e)), B = __ldg(ib + (N - e));
+      if (dx) { A = cmul_i(A, g.kx[N - e]); B = cmul_i(B, g.kx[N - e]); }
       z = make_double2(A.x + B.y, B.x - A.y);            // conj A + i conj B
     }
     v[q] = z;
@@ -125,9 +129,11 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet 
   }
 }
 
-// packed spectral -> Xh (zero-filled de-aliased rows, unnormalised)
+// packed spectral -> Xh (zero-filled de-aliased rows, unnormalised); fields
+// f with bit f of dmask set are differentiated in z (times i kz)
 template <int N>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet out, Geom g, unsigned dmask,
+                                                          const double2* __restrict__ ghost) {
   extern __shared__ double2 sm[];
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -138,12 +144,18 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet 
   Twiddles<N, E> tw;
   load_twiddles<N, E>(tw, lane, g.twz);
   const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx;
+  if (ghost) {   // rows 0, 1, Nyp, Nyp+1 from the overlay
+    const int q = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
+    if (q >= 0) src = ghost + (long long)(4 * (f & 3) + q) * g.sp + kx;
+  }
+  const bool dz = (dmask >> f) & 1u;
   double2 v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     const int z = lane + q * T;
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
     v[q] = (active && kzp >= 0) ? __ldg(src + (long long)kzp * g.kxs) : make_double2(0.0, 0.0);
+    if (dz && kzp >= 0) v[q] = cmul_i(v[q], g.kz[kzp]);
   }
   fft_reg<N, +1>(v, lane, active, sq, tw);
   if (!active) return;
@@ -190,14 +202,14 @@ static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStrea
   k_fwd_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 template <int N>
-static void go_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+static void go_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, cudaStream_t st) {
   constexpr int ns = seqs_per_cta<N>();
   int npairs = g.nz / 2;
   int cps = ns < npairs ? ns : npairs;
   while (npairs % cps) --cps;
   size_t smem = (size_t)cps * padded(N) * sizeof(double2);
   smem_attr(k_inv_x<N>, smem);
-  k_inv_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
+  k_inv_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask);
 }
 template <int N>
 static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
@@ -207,27 +219,31 @@ static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStrea
   k_fwd_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
 }
 template <int N>
-static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
+                     cudaStream_t st) {
   constexpr int ns = seqs_per_cta<N>();
   size_t smem = (size_t)ns * padded(N) * sizeof(double2);
   smem_attr(k_inv_z<N>, smem);
-  k_inv_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
+  k_inv_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);
 }
 
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
   DB_DISPATCH_N(g.nx, go_fwd_x, g, in, out, nf, st);
   return cudaGetLastError();
 }
-cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  DB_DISPATCH_N(g.nx, go_inv_x, g, in, out, nf, st);
+cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask) {
+  if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nx, go_inv_x, g, in, out, nf, dmask, st);
   return cudaGetLastError();
 }
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
   DB_DISPATCH_N(g.nz, go_fwd_z, g, in, out, nf, st);
   return cudaGetLastError();
 }
-cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  DB_DISPATCH_N(g.nz, go_inv_z, g, in, out, nf, st);
+cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask,
+                         const double2* ghost) {
+  if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nz, go_inv_z, g, in, out, nf, dmask, ghost, st);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,331 @@
+// k_les.cu -- LES closure of the channel substep, les_model_type 5:
+// anisotropic minimum dissipation (AMD, Verstappen form) for momentum and
+// scalar (for/les.f90:3-1068 model-5 branch, 1072-1435, 1443-1746).
+//
+// The reference builds 26 spectral tensor fields (Sij, SIij, Oij, all nine
+// velocity gradients, three scalar gradients), transforms them all to
+// physical space, forms the model there and transforms 9 stress/flux fields
+// back.  Every one of those fields is a fixed linear combination of
+//   u_i, th                      (needed by the substep anyway),
+//   d/dx and d/dz of u_i and th  (8 fields),
+//   y-differences of u_i, th     (formed pointwise in physical space),
+// so here only the 8 x/z derivatives are transformed (as extra outputs of
+// the state's inverse transforms, the derivative applied on the way), and
+// the divergence of the model stress is folded into the nonlinear-product
+// fields before their forward transform: the SGS terms cost no forward FFT.
+//
+//  k_les_bc     : apply_BC_vel_mpi_post, apply_BC_th_mpi_post, apply_BC_les,
+//                 apply_BC_th_les on the spectral ghost rows (les.f90:63-75),
+//                 into a side buffer the inverse transforms overlay.
+//  k_les_amd    : one thread per (x, z) column walks j; from the gradients it
+//                 forms the AMD coefficients at GYF and GY rows (les.f90:
+//                 574-719, 1216-1310), nu_t and kappa_t (:783-795, :1347-1358,
+//                 ghost_les_mpi with one rank), and the physical-space parts
+//                 of the SGS forcing per product slot (:800-900, :1360-1391).
+//  k_thomas_les : the CN solves with the eddy viscosity/diffusivity in the
+//                 explicit term and the matrix (solver.f90:872-903, 988-1003,
+//                 1028-1045, 1088-1105, 1144-1161, 1200-1217): the matrix
+//                 differs per (x, z) column, so each thread runs its own
+//                 Thomas sweep, the eliminated upper coefficients in shared
+//                 memory and the eliminated right-hand side in the r array.
+#include <math.h>
+
+#include "db_bc.cuh"
+#include "db_kernels.cuh"
+
+namespace db {
+
+// ---------------------------------------------------------------------------
+// Ghost rows the model sees (les.f90:63-75).  The reference rewrites the
+// state's rows 0, 1, Nyp, Nyp+1 here, after the substep has already formed
+// cr and cf from the unmodified state (solver.f90:396-609), and the rewrite
+// reaches the rest of the substep only through the physical fields.  So the
+// rewritten rows go to a side buffer ghost[f][q] (f = cu1, cu2, cu3, cth;
+// q = rows 0, 1, Nyp, Nyp+1) that the inverse transforms read in place of
+// the state's rows; the final forward transform of the physical fields
+// carries them into the new state exactly as in the reference.
+__global__ void k_les_bc(State s, Geom g, Phys ph) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
+  if (kx >= g.kxs) return;
+  const long long c0 = (long long)kzp * g.kxs + kx, sp = g.sp;
+  const int Nyp = g.ny;
+  GhostCol a, b, c, t;
+  load_col(a, s.cu1 + c0, sp, Nyp);
+  load_col(b, s.cu2 + c0, sp, Nyp);
+  load_col(c, s.cu3 + c0, sp, Nyp);
+  load_col(t, s.cth + c0, sp, Nyp);
+  if (kx <= g.nkx) {
+    const bool m0 = (kx == 0 && kzp == 0);
+    bc_vel_post(a, b, c, g, ph, m0, s.sc->time);
+    bc_th_post(t, g, ph, m0);
+    bc_les(a, c, t, ph);
+  }
+  const GhostCol* f[4] = {&a, &b, &c, &t};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double2* o = s.ghost + (long long)(4 * i) * sp + c0;
+    o[0] = f[i]->v[G_0];
+    o[sp] = f[i]->v[G_1];
+    o[2 * sp] = f[i]->v[G_N];
+    o[3 * sp] = f[i]->v[G_N1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// AMD model
+
+constexpr double C_AMD = 0.2887;     // les.f90:25
+constexpr double BETA_SGS = 3.0;     // les.f90:43
+
+// max{0, -(I3 - I4)} / (I1 - I2) of the scaled strain SI and rotation O
+// tensors (les.f90:578-619): -tr(SI^3) + tr(SI O^2) over |SI|^2 + |O|^2
+__device__ __forceinline__ double amd_ratio(double s1, double s2, double s3, double s4, double s5, double s6,
+                                            double o4, double o5, double o6) {
+  const double i3 = s1 * s1 * s1 + s2 * s2 * s2 + s3 * s3 * s3 + 3.0 * s1 * s4 * s4 + 3.0 * s1 * s5 * s5 +
+                    3.0 * s2 * s4 * s4 + 3.0 * s2 * s6 * s6 + 3.0 * s3 * s5 * s5 + 3.0 * s3 * s6 * s6 +
+                    6.0 * s4 * s5 * s6;
+  const double v = -i3 - s1 * o4 * o4 - s1 * o5 * o5 - s2 * o4 * o4 - s2 * o6 * o6 - s3 * o5 * o5 -
+                   s3 * o6 * o6 - 2.0 * s4 * o5 * o6 + 2.0 * s5 * o4 * o6 - 2.0 * s6 * o4 * o5;
+  if (v <= 0.0) return 0.0;
+  return v / (s1 * s1 + s2 * s2 + s3 * s3 + 2.0 * s4 * s4 + 2.0 * o4 * o4 + 2.0 * s5 * s5 + 2.0 * o5 * o5 +
+              2.0 * s6 * s6 + 2.0 * o6 * o6);
+}
+
+// scalar AMD: max{0, -(delta_k^2 du_i/dx_k dth/dx_k dth/dx_i)} / |delta dth|^2
+// (les.f90:1222-1249, 1265-1305); arguments are the gradient components
+// at one point, dy the y filter width there
+__device__ __forceinline__ double amd_th_ratio(double dxs, double dys, double dzs, double u1x, double u2y,
+                                               double u3z, double u1y, double u2x, double u1z, double u3x,
+                                               double u2z, double u3y, double tx, double ty, double tz) {
+  const double v = -(dxs * dxs * u1x * tx * tx + dys * dys * u2y * ty * ty + dzs * dzs * u3z * tz * tz +
+                     (dys * dys * u1y + dxs * dxs * u2x) * tx * ty + (dzs * dzs * u1z + dxs * dxs * u3x) * tx * tz +
+                     (dzs * dzs * u2z + dys * dys * u3y) * ty * tz);
+  if (v <= 0.0) return 0.0;
+  return v / ((dxs * tx) * (dxs * tx) + (dys * ty) * (dys * ty) + (dzs * tz) * (dzs * tz));
+}
+
+// filter coefficient -2 C^2 Delta^2 at a row of spacing h (les.f90:756-780)
+__device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
+  return -2.0 * C_AMD * C_AMD * 3.0 / (1.0 / (dxs * dxs) + 1.0 / ((h * 2.0) * (h * 2.0)) + 1.0 / (dzs * dzs));
+}
+
+// Outputs, physical [j][z][x], zero outside the rows where the reference
+// applies each term, in the product slots of k_products:
+//  les[0] = dyf-filter * s1 S11            (u1 eq., times i kx)      rows j1..j2
+//  les[1] = Dy(delta_y tau_12)             (u1 eq., no derivative)   rows j1..j2
+//  les[2] = dyf-filter * s1 S13            (u1: i kz, u3: i kx)      rows j1..j2
+//  les[3] = Dy(delta_y tau_23)             (u3 eq., no derivative)   rows j1..j2
+//  les[4] = dyf-filter * s1 S33            (u3 eq., times i kz)      rows j1..j2
+//  les[5] = delta_y tau_12 - nu_t du1/dy   (u2 eq., times i kx)      rows 2..Nyp
+//  les[6] = delta_y tau_23 - nu_t du3/dy   (u2 eq., times i kz)      rows 2..Nyp
+//  les[7] = dyf-filter/2 * s1_th dth/dx    (th eq., times i kx)      rows jst..jet
+//  les[8] = dyf-filter/2 * s1_th dth/dz    (th eq., times i kz)      rows jst..jet
+// with j1 = jstart, j2 = Nyp - 1 (les.f90:46-49, one rank), tau_12 at GY
+// rows = temp (S12 - du1/dy / 2) for j >= 2 and the raw strain at j = 1
+// (les.f90:737-748).
+__global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
+  if (x >= g.nx) return;
+  const long long pp = g.pp;
+  const long long col = (long long)z * g.nx + x;
+  const int Nyp = g.ny;
+  const int jst = g.jstart_th, jet = g.jend_th;
+  const int j1 = g.jstart, j2 = Nyp - 1;
+  const double dxs = ph.dx * BETA_SGS, dzs = ph.dz * BETA_SGS;
+  const double rzx = dzs / dxs, rxz = dxs / dzs;
+  const double* dy = g.dy;
+  const double* dyf = g.dyf;
+  const double* u1 = s.u1 + col;
+  const double* u2 = s.u2 + col;
+  const double* u3 = s.u3 + col;
+  const double* th = s.th + col;
+  const double *g1x = s.gx[0] + col, *g2x = s.gx[1] + col, *g3x = s.gx[2] + col, *gtx = s.gx[3] + col;
+  const double *g1z = s.gz[0] + col, *g2z = s.gz[1] + col, *g3z = s.gz[2] + col, *gtz = s.gz[3] + col;
+  double* o[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) o[i] = s.les[i] + col;
+  double* nut = s.nu_t + col;
+  double* kat = s.kappa_t + col;
+
+  // row 0: GYF values only (GY row 0 does not exist)
+  double u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
+  double f1x = __ldg(g1x), f3z = __ldg(g3z), f1z = __ldg(g1z), f3x = __ldg(g3x);
+  double ftx = __ldg(gtx), ftz = __ldg(gtz);
+  double f2y = (u2c - __ldg(u2)) / dyf[0];
+  // previous GY row (r = j - 1) values
+  double h1y = 0.0, h3y = 0.0, hty = 0.0, h2x = 0.0, h2z = 0.0;
+  double hSI4 = 0.0, hSI6 = 0.0, hO4 = 0.0, hO6 = 0.0, hP4 = 0.0, hP6 = 0.0, hdl = 0.0;
+  nut[0] = 0.0;
+  kat[0] = 0.0;
+  o[5][0] = 0.0;
+  o[6][0] = 0.0;
+
+  for (int j = 1; j <= Nyp + 1; ++j) {
+    const long long oj = (long long)j * pp;
+    const double u1j = __ldg(u1 + oj), u3j = __ldg(u3 + oj), thj = __ldg(th + oj);
+    const double u2n = (j + 1 <= Nyp + 1) ? __ldg(u2 + oj + pp) : 0.0;
+    const double a1x = __ldg(g1x + oj), a2x = __ldg(g2x + oj), a3x = __ldg(g3x + oj), atx = __ldg(gtx + oj);
+    const double a1z = __ldg(g1z + oj), a2z = __ldg(g2z + oj), a3z = __ldg(g3z + oj), atz = __ldg(gtz + oj);
+    const double dyj = dy[j], dyfj = dyf[j], dyfm = dyf[j - 1];
+    // GY row j: y-derivatives and the tensors that live there
+    const double d1y = (u1j - u1m) / dyj, d3y = (u3j - u3m) / dyj, dty = (thj - thm) / dyj;
+    const double dly = dyj * 2.0;
+    const double SI4 = 0.5 * (d1y * (dly / dxs) + a2x * (dxs / dly));
+    const double SI6 = 0.5 * (a2z * (dzs / dly) + d3y * (dly / dzs));
+    const double O4 = 0.5 * (d1y * (dly / dxs) - a2x * (dxs / dly));
+    const double O6 = 0.5 * (a2z * (dzs / dly) - d3y * (dly / dzs));
+    const double S4 = 0.5 * (d1y + a2x), S6 = 0.5 * (a2z + d3y);
+    // GYF row j (d u2/dy there needs u2 at j + 1; row Nyp + 1 is unused)
+    const double c2y = (j <= Nyp) ? (u2n - u2c) / dyfj : 0.0;
+    const double delt = amd_delta(dxs, dzs, dyj);
+    double temp = 0.0, temp_th = 0.0;
+    if (j >= 2 && j <= Nyp) {
+      const double w = 2.0 * dyj;
+#define GYI(A, B) (((A) * dyfm + (B) * dyfj) / w)
+      const double SI5c = 0.5 * (a1z * rzx + a3x * rxz), SI5p = 0.5 * (f1z * rzx + f3x * rxz);
+      const double O5c = 0.5 * (a1z * rzx - a3x * rxz), O5p = 0.5 * (f1z * rzx - f3x * rxz);
+      temp = amd_ratio(GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), SI4, GYI(SI5c, SI5p), SI6, O4,
+                       GYI(O5c, O5p), O6);
+      temp_th = amd_th_ratio(dxs, dly, dzs, GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), d1y, a2x,
+                             GYI(a1z, f1z), GYI(a3x, f3x), a2z, d3y, GYI(atx, ftx), dty, GYI(atz, ftz));
+#undef GYI
+    }
+    const bool wall = (j <= 2 || j >= Nyp);     // ghost_les_mpi / ghost_les_th_mpi
+    const double nu = wall ? 0.0 : -0.5 * delt * temp;
+    const double ka = wall ? 0.0 : -0.5 * delt * temp_th;
+    const double P4 = (j >= 2) ? temp * (S4 - 0.5 * d1y) : S4;
+    const double P6 = (j >= 2) ? temp * (S6 - 0.5 * d3y) : S6;
+    const bool gy2 = (j >= 2 && j <= Nyp);
+    nut[oj] = nu;
+    kat[oj] = ka;
+    o[5][oj] = gy2 ? delt * P4 - nu * d1y : 0.0;
+    o[6][oj] = gy2 ? delt * P6 - nu * d3y : 0.0;
+
+    // GYF row r = j - 1: needs GY rows r and r + 1 = j
+    {
+      const int r = j - 1;
+      const long long orr = (long long)r * pp;
+      const double dyfr = dyfm;
+      const double dlf = amd_delta(dxs, dzs, dyfr);
+      double L0 = 0.0, L1 = 0.0, L2 = 0.0, L3 = 0.0, L4 = 0.0, L7 = 0.0, L8 = 0.0;
+      if (r >= j1 && r <= j2) {
+        const double s4 = 0.5 * (SI4 + hSI4), s6 = 0.5 * (SI6 + hSI6);
+        const double q4 = 0.5 * (O4 + hO4), q6 = 0.5 * (O6 + hO6);
+        const double s5 = 0.5 * (f1z * rzx + f3x * rxz), q5 = 0.5 * (f1z * rzx - f3x * rxz);
+        const double s1 = amd_ratio(f1x, f2y, f3z, s4, s5, s6, q4, q5, q6);
+        L0 = dlf * (s1 * f1x);
+        L2 = dlf * (s1 * (0.5 * (f1z + f3x)));
+        L4 = dlf * (s1 * f3z);
+        L1 = (delt * P4 - hdl * hP4) / dyfr;
+        L3 = (delt * P6 - hdl * hP6) / dyfr;
+      }
+      if (r >= jst && r <= jet) {
+        const double dys = dyfr * 2.0;
+        const double s1t = amd_th_ratio(dxs, dys, dzs, f1x, f2y, f3z, 0.5 * (d1y + h1y), 0.5 * (a2x + h2x), f1z,
+                                        f3x, 0.5 * (a2z + h2z), 0.5 * (d3y + h3y), ftx, 0.5 * (dty + hty), ftz);
+        L7 = 0.5 * dlf * (s1t * ftx);
+        L8 = 0.5 * dlf * (s1t * ftz);
+      }
+      o[0][orr] = L0;
+      o[1][orr] = L1;
+      o[2][orr] = L2;
+      o[3][orr] = L3;
+      o[4][orr] = L4;
+      o[7][orr] = L7;
+      o[8][orr] = L8;
+    }
+    // shift
+    u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
+    f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
+    h1y = d1y; h3y = d3y; hty = dty; h2x = a2x; h2z = a2z;
+    hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
+  }
+  const long long oe = (long long)(Nyp + 1) * pp;
+  o[0][oe] = 0.0; o[1][oe] = 0.0; o[2][oe] = 0.0; o[3][oe] = 0.0; o[4][oe] = 0.0;
+  o[7][oe] = 0.0; o[8][oe] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// CN solves with eddy viscosity (one Thomas sweep per thread and column)
+constexpr int TL = 32;
+
+__global__ void __launch_bounds__(TL) k_thomas_les(State s, Geom g, int rk) {
+  extern __shared__ double cm[];      // [np][TL]: u_j / b'_j
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * TL + lane, z = blockIdx.y;
+  if (x >= g.nx) return;
+  const int np = g.np, Nyp = g.ny;
+  const long long pp = g.pp, col = (long long)z * g.nx + x;
+  const double* dy = g.dy;
+  const double* dyf = g.dyf;
+  const double temp2 = 0.5 * s.sc->h_bar[rk];
+  for (int eq = 0; eq < 4; ++eq) {
+    const TriRow* R = s.tri + eq * np;
+    double* u = ((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
+    double* r = ((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
+    const double* nv = ((eq == 0) ? s.kappa_t : s.nu_t) + col;
+    const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
+    const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
+    double um = 0.0, uc = u[0], nm = 0.0, nc = nv[0];
+    double bprev = 1.0, gprev = 0.0, uprev = 0.0;
+    for (int j = 0; j < np; ++j) {
+      const TriRow row = R[j];
+      const double un = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
+      const double nn = (j + 1 < np) ? nv[(long long)(j + 1) * pp] : 0.0;
+      double l = row.l, d = row.d, uu = row.u, v = row.bc;
+      if (!row.is_bc) {
+        v = r[(long long)j * pp] + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
+        double lo_c, hi_c;
+        if (eq != 1) {    // nu_t / kappa_t at GY rows j, j + 1
+          v += temp2 * ((nn * (un - uc) / dy[j + 1] - nc * (uc - um) / dy[j]) / dyf[j]);
+          lo_c = nc / (dy[j] * dyf[j]);
+          hi_c = nn / (dy[j + 1] * dyf[j]);
+        } else {          // interpolated to the GYF rows around u2's GY row
+          v += temp2 * (((0.5 * (nc + nn)) * (un - uc) / dyf[j] - 0.5 * (nc + nm) * (uc - um) / dyf[j - 1]) / dy[j]);
+          lo_c = 0.5 * (nc + nm) / (dyf[j - 1] * dy[j]);
+          hi_c = 0.5 * (nc + nn) / (dyf[j] * dy[j]);
+        }
+        l = l - temp2 * lo_c;
+        d = d + temp2 * hi_c + temp2 * lo_c;
+        uu = uu - temp2 * hi_c;
+      }
+      double b = d, gg = v;
+      if (j > 0) {
+        const double a = -l / bprev;
+        b = d + a * uprev;
+        gg = v + a * gprev;
+      }
+      const double ib = 1.0 / b;
+      cm[j * TL + lane] = uu * ib;
+      r[(long long)j * pp] = gg * ib;
+      bprev = b; gprev = gg; uprev = uu;
+      um = uc; uc = un; nm = nc; nc = nn;
+    }
+    double xn = 0.0;
+    for (int j = np - 1; j >= 0; --j) {
+      const double xv = r[(long long)j * pp] - cm[j * TL + lane] * xn;
+      if (j >= lo && j <= hi) u[(long long)j * pp] = xv;
+      xn = xv;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStream_t st) {
+  k_les_bc<<<dim3((g.kxs + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, ph);
+  return cudaGetLastError();
+}
+cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st) {
+  const int bx = g.nx < 128 ? g.nx : 128;
+  k_les_amd<<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
+  return cudaGetLastError();
+}
+cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
+  const size_t smem = (size_t)g.np * TL * sizeof(double);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_thomas_les<<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
+  return cudaGetLastError();
+}
+
+}  // namespace db

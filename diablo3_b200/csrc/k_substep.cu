@@ -21,6 +21,7 @@
 //  k_courant    : CFL reduction and dt scheduling (flow.f90:746-857).
 #include <math.h>
 
+#include "db_bc.cuh"
 #include "db_kernels.cuh"
 #include "fft_reg.cuh"
 
@@ -50,7 +51,7 @@ __device__ __forceinline__ double2 sepp(const double2* z, int m, int part) {
   return make_double2(0.5 * (zm.y - zn.y), -0.5 * (zm.x - zn.x));
 }
 
-template <int N>
+template <int N, bool LES>
 __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(State s, Geom g) {
   extern __shared__ double2 sm[];
   using S = FftShape<N>;
@@ -85,13 +86,16 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
         const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
         a = u1 * u1;
         b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (2.0 * dyfj);
+        if (LES) { a += __ldg(s.les[0] + o0 + x); b += __ldg(s.les[1] + o0 + x); }
       } else if (seq == 1) {
         const double u3p = __ldg(s.u3 + op + x), u3m = __ldg(s.u3 + om + x);
         const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
         a = u3 * u1;
         b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (2.0 * dyfj);
+        if (LES) { a += __ldg(s.les[2] + o0 + x); b += __ldg(s.les[3] + o0 + x); }
       } else {
         a = u3 * u3;
+        if (LES) a += __ldg(s.les[4] + o0 + x);
       }
     } else {
       const double u2 = __ldg(s.u2 + o0 + x);
@@ -101,6 +105,7 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
           const double pp = u2 + __ldg(s.u2 + op + x), qq = u2 + __ldg(s.u2 + om + x);
           a = ((dyfj * u1 + dyfjm * u1m) / (2. * dyj)) * u2;
           b = (0.25 * (pp * pp) - 0.25 * (qq * qq)) / dyj;
+          if (LES) a += __ldg(s.les[5] + o0 + x);
         }
       } else if (seq == 1) {
         if (rt) {
@@ -108,10 +113,15 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
           const double u2p = __ldg(s.u2 + op + x);
           a = th * __ldg(s.u1 + o0 + x);
           b = (thp * u2p + th * u2p - th * u2 - thm * u2) / (2.0 * dyfj);
+          if (LES) a += __ldg(s.les[7] + o0 + x);
         }
       } else {
         if (r2) a = ((dyfj * __ldg(s.u3 + o0 + x) + dyfjm * __ldg(s.u3 + om + x)) / (2. * dyj)) * u2;
         if (rt) b = __ldg(s.th + o0 + x) * __ldg(s.u3 + o0 + x);
+        if (LES) {
+          if (r2) a += __ldg(s.les[6] + o0 + x);
+          if (rt) b += __ldg(s.les[8] + o0 + x);
+        }
       }
     }
     v[q] = make_double2(a, b);
@@ -733,84 +743,31 @@ __global__ void k_divergence(State s, Geom g) {
 __global__ void k_bc_vel_post(State s, Geom g, Phys ph) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx > g.nkx) return;
-  const long long c0 = (long long)kzp * g.kxs + kx, sp = g.sp;
-  const int Nyp = g.ny;
-  const bool m0 = (kx == 0 && kzp == 0);
-  const double2 Z = make_double2(0.0, 0.0);
-  auto R = [&](double v) { return make_double2(v, 0.0); };
-  double2 *cu1 = s.cu1 + c0, *cu2 = s.cu2 + c0, *cu3 = s.cu3 + c0;
-  // lower
-  if (ph.bc_type[BC_U_MIN] == 0) {
-    cu1[0] = Z; cu1[sp] = Z;
-    if (m0) { cu1[sp] = R(ph.bc_c1[BC_U_MIN]); cu1[0] = R(ph.bc_c1[BC_U_MIN]); }
-  } else {
-    cu1[sp] = cu1[2 * sp]; cu1[0] = cu1[sp];
-    if (m0) {
-      cu1[sp] = csub(cu1[2 * sp], R(g.dy[2] * ph.bc_c1[BC_U_MIN]));
-      cu1[0] = csub(cu1[sp], R(g.dy[1] * ph.bc_c1[BC_U_MIN]));
-    }
-  }
-  if (ph.bc_type[BC_W_MIN] == 0) {
-    cu3[0] = Z; cu3[sp] = Z;
-    if (m0) { cu3[sp] = R(ph.bc_c1[BC_W_MIN]); cu3[0] = R(ph.bc_c1[BC_W_MIN]); }
-  } else {
-    cu3[sp] = cu3[2 * sp]; cu3[0] = cu3[sp];
-    if (m0) {
-      cu3[sp] = csub(cu3[2 * sp], R(g.dy[2] * ph.bc_c1[BC_W_MIN]));
-      cu3[0] = csub(cu3[sp], R(g.dy[1] * ph.bc_c1[BC_W_MIN]));
-    }
-  }
-  if (ph.bc_type[BC_V_MIN] == 0) {
-    cu2[sp] = csub(R(2.0 * ph.bc_c1[BC_V_MIN]), cu2[2 * sp]);
-    cu2[0] = cu2[sp];
-  } else {
-    cu2[sp] = cu2[2 * sp]; cu2[0] = cu2[sp];
-    if (m0) {
-      cu2[sp] = csub(cu2[2 * sp], R(g.dyf[1] * ph.bc_c1[BC_V_MIN]));
-      cu2[0] = csub(cu2[sp], R(g.dyf[1] * ph.bc_c1[BC_V_MIN]));
-    }
-  }
-  // upper
-  const long long N0 = (long long)Nyp * sp, N1 = (long long)(Nyp + 1) * sp, Nm = (long long)(Nyp - 1) * sp;
-  if (ph.bc_type[BC_U_MAX] == 0) {
-    cu1[N0] = Z; cu1[N1] = Z;
-    if (m0) { cu1[N0] = R(ph.bc_c1[BC_U_MAX]); cu1[N1] = R(ph.bc_c1[BC_U_MAX]); }
-  } else {
-    cu1[N0] = cu1[Nm]; cu1[N1] = cu1[N0];
-    if (m0) {
-      cu1[N0] = cadd(cu1[Nm], R(g.dy[Nyp] * ph.bc_c1[BC_U_MAX]));
-      cu1[N1] = cadd(cu1[N0], R(g.dy[Nyp] * ph.bc_c1[BC_U_MAX]));
-    }
-  }
-  if (ph.bc_type[BC_W_MAX] == 0) {
-    cu3[N0] = Z; cu3[N1] = Z;
-    if (m0) { cu3[N0] = R(ph.bc_c1[BC_W_MAX]); cu3[N1] = Z; }
-  } else {
-    cu3[N0] = cu3[Nm]; cu3[N1] = cu3[N0];
-    if (m0) {
-      double wt = ph.bc_c1[BC_W_MAX];
-      if (ph.f_type == 4)
-        wt = ph.bc_c1[BC_W_MAX] + ph.amp_omega0 * sin(ph.omega0 * (ph.ro_inv / ph.delta * s.sc->time - ph.force_start));
-      cu3[N0] = cadd(cu3[Nm], R(g.dy[Nyp] * wt));
-      cu3[N1] = cadd(cu3[N0], R(g.dy[Nyp] * wt));
-    }
-  }
-  if (ph.bc_type[BC_V_MAX] == 0) {
-    if (m0) cu2[N1] = csub(R(2.0 * ph.bc_c1[BC_V_MAX]), cu2[N0]);
-  } else {
-    cu2[N0] = cu2[Nm]; cu2[N1] = cu2[N0];
-    if (m0) cu2[N1] = cadd(cu2[N0], R(g.dy[Nyp] * ph.bc_c1[BC_V_MAX]));
-  }
+  const long long c0 = (long long)kzp * g.kxs + kx;
+  GhostCol a, b, c;
+  load_col(a, s.cu1 + c0, g.sp, g.ny);
+  load_col(b, s.cu2 + c0, g.sp, g.ny);
+  load_col(c, s.cu3 + c0, g.sp, g.ny);
+  bc_vel_post(a, b, c, g, ph, kx == 0 && kzp == 0, s.sc->time);
+  store_ghosts(a, s.cu1 + c0, g.sp, g.ny);
+  store_ghosts(b, s.cu2 + c0, g.sp, g.ny);
+  store_ghosts(c, s.cu3 + c0, g.sp, g.ny);
 }
 
 // ---------------------------------------------------------------------------
 // launchers
 
 template <int N>
-static void go_products(const Geom& g, const State& s, cudaStream_t st) {
+static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les) {
   size_t smem = (size_t)3 * padded(N) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_products<N><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
+  const dim3 grid(g.nz, g.np, 2);
+  if (les) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<N, true><<<grid, 3 * FftShape<N>::T, smem, st>>>(s, g);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<N, false><<<grid, 3 * FftShape<N>::T, smem, st>>>(s, g);
+  }
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
@@ -832,8 +789,8 @@ static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, cuda
     default: return cudaErrorInvalidValue;          \
   }
 
-cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st) {
-  DB_DISPATCH_N2(g.nx, go_products, g, s, st);
+cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les) {
+  DB_DISPATCH_N2(g.nx, go_products, g, s, st, les);
   return cudaGetLastError();
 }
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
