@@ -58,6 +58,15 @@ WORKLOAD_DESC = {
 }
 
 
+def workload_suffix(args) -> str:
+    s = ""
+    if args.les:
+        s += ", AMD LES (les_model_type 5) on every substep"
+    if args.precision == "mixed":
+        s += ", mixed precision (FP32 transforms/products/SGS; FP64 state, CN and Poisson solves)"
+    return s
+
+
 def measured_peak_hbm():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -185,6 +194,9 @@ def main():
     ap.add_argument("--config", default="config1", choices=["config1", "config0", "slab"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 transforms/products/SGS, FP64 state and solves")
+    ap.add_argument("--les", action="store_true", help="AMD LES closure (les_model_type 5) on")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -211,6 +223,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     p = workload_params(args.config)
+    if args.precision == "mixed":
+        p.precision = 1
+    if args.les:
+        p.use_les, p.les_model_type, p.create_new_flow = 1, 5, 0
     gy = create_grid(p.ny, lz=p.ly, cs=1.5, grid_type=1)
     stream = torch.cuda.Stream()
     ch = Channel(p, gy, stream=stream.cuda_stream)
@@ -304,9 +320,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded infinite-front IC, no dataset)",
-        "config": {"workload": WORKLOAD_DESC[args.config], "grid_xyz": [p.nx, p.ny, p.nz],
+        "config": {"workload": WORKLOAD_DESC[args.config] + workload_suffix(args), "grid_xyz": [p.nx, p.ny, p.nz],
                    "points": npts, "substeps_per_step": 3,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "state ~10 GB resident in HBM, far above the 126 MB L2 (no flush needed)"},

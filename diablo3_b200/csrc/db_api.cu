@@ -26,6 +26,7 @@ struct db_ctx {
   std::vector<void*> allocs;
   double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
+  float2* d_twf = nullptr;       // the same in FP32
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [LES model active]
   int time_step = 0;             // host mirror of the driver's time_step
   std::string err;
@@ -84,7 +85,10 @@ static int validate(const db_params* p, std::string& why) {
     return DB_ERR_UNSUPPORTED;
   }
   if (p->use_les && p->ny + 2 > 900) { why = "LES: ny + 2 must be <= 900 (per-column Thomas tile)"; return DB_ERR_SIZE; }
-  if (p->precision != 0) { why = "only the FP64 path (precision 0) is available"; return DB_ERR_UNSUPPORTED; }
+  if (p->precision != 0 && p->precision != 1) {
+    why = "precision must be 0 (FP64) or 1 (mixed: FP32 transforms, products and SGS)";
+    return DB_ERR_ARG;
+  }
   const int b[8] = {p->u_bc_ymin, p->v_bc_ymin, p->w_bc_ymin, p->th_bc_ymin,
                     p->u_bc_ymax, p->v_bc_ymax, p->w_bc_ymax, p->th_bc_ymax};
   for (int i = 0; i < 8; ++i)
@@ -100,6 +104,27 @@ static void twiddles(int n, std::vector<double2>& out) {
     long double a = 2.0L * PI * (long double)k / (long double)n;
     out.push_back(make_double2((double)cosl(a), -(double)sinl(a)));
   }
+}
+
+static void twiddles_f(int n, std::vector<float2>& out) {
+  const long double PI = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < n; ++k) {
+    long double a = 2.0L * PI * (long double)k / (long double)n;
+    out.push_back(make_float2((float)cosl(a), -(float)sinl(a)));
+  }
+}
+
+// bytes of one physical / x-half element at the context's precision
+static size_t phys_elem(const db_ctx* c) { return c->p.precision ? sizeof(float) : sizeof(double); }
+static size_t xh_elem(const db_ctx* c) { return c->p.precision ? sizeof(float2) : sizeof(double2); }
+
+static int balloc(db_ctx* c, void** ptr, size_t bytes) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, bytes));
+  CK(cudaMemset(q, 0, bytes));
+  c->allocs.push_back(q);
+  *ptr = q;
+  return DB_OK;
 }
 
 template <typename T>
@@ -143,6 +168,7 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   g.jend = (p->u_bc_ymax == 1) ? Nyp : Nyp - 1;
   g.jstart_th = (p->th_bc_ymin == 1) ? 1 : 2;
   g.jend_th = (p->th_bc_ymax == 1) ? Nyp : Nyp - 1;
+  g.prec = p->precision;
 
   // grid metrics, for/domain.f90:276-300, 538-565
   c->gy.assign(np, 0.0); c->gyf.assign(np, 0.0); c->dy.assign(np, 0.0); c->dyf.assign(np, 0.0);
@@ -205,11 +231,12 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
   s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
   s.phi_g = sp[9]; s.pfac = sp[10];
+  const size_t eP = phys_elem(c), eH = xh_elem(c);
   for (int i = 0; i < 8; ++i)
-    if ((rc = dalloc(c, &s.xh[i], H))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = balloc(c, (void**)&s.xh[i], H * eH))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   double* ph_[8];
   for (int i = 0; i < 8; ++i)
-    if ((rc = dalloc(c, &ph_[i], Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = balloc(c, (void**)&ph_[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   s.u1 = ph_[0]; s.u2 = ph_[1]; s.u3 = ph_[2]; s.th = ph_[3];
   s.r1 = ph_[4]; s.r2 = ph_[5]; s.r3 = ph_[6]; s.rth = ph_[7];
   if (p->use_les) {
@@ -217,8 +244,9 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
                        &s.les[0], &s.les[1], &s.les[2], &s.les[3], &s.les[4], &s.les[5], &s.les[6],
                        &s.les[7], &s.les[8], &s.nu_t, &s.kappa_t};
     for (int i = 0; i < 19; ++i)
-      if ((rc = dalloc(c, lf[i], Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+      if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if (p->precision && (rc = dalloc(c, &s.tscr, Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   }
   if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
   if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
@@ -234,9 +262,14 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   std::vector<double2> tw;
   twiddles(Nx, tw);
   twiddles(Nz, tw);
+  std::vector<float2> twf;
+  twiddles_f(Nx, twf);
+  twiddles_f(Nz, twf);
   if ((rc = dalloc(c, &c->d_tw, tw.size()))) { db_finalize(c); g_init_err = c->err; return rc; }
+  if ((rc = dalloc(c, &c->d_twf, twf.size()))) { db_finalize(c); g_init_err = c->err; return rc; }
   if (cudaMemcpy(c->d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaMemcpy(c->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
     db_finalize(c);
     g_init_err = "db_init: table upload failed";
     return DB_ERR_CUDA;
@@ -244,6 +277,7 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   g.gy = c->d_tab; g.gyf = c->d_tab + np; g.dy = c->d_tab + 2 * np; g.dyf = c->d_tab + 3 * np;
   g.kx = c->d_tab + 4 * np; g.kz = c->d_tab + 4 * np + g.kxs;
   g.twx = c->d_tw; g.twz = c->d_tw + Nx;
+  g.twxf = c->d_twf; g.twzf = c->d_twf + Nx;
 
   // run scalars (for/parameters.f90:176-178)
   DevScalars h{};
@@ -358,6 +392,32 @@ static void compact_to_phys_ref(const db_ctx* c, const double* src, double* ref)
              sizeof(double) * g.nx);
 }
 
+// one physical field between the reference layout on the host and the
+// device at the context's precision (FP32 on the mixed path)
+static int phys_upload(db_ctx* c, const double* ref, void* dev) {
+  const size_t n = (size_t)c->g.np * c->g.pp;
+  phys_ref_to_compact(c, ref, c->h_stage);
+  if (c->p.precision) {
+    float* f = (float*)c->h_stage;
+    for (size_t i = 0; i < n; ++i) f[i] = (float)c->h_stage[i];
+  }
+  CK(cudaMemcpyAsync(dev, c->h_stage, n * phys_elem(c), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DB_OK;
+}
+
+static int phys_download(db_ctx* c, const void* dev, double* ref) {
+  const size_t n = (size_t)c->g.np * c->g.pp;
+  CK(cudaMemcpyAsync(c->h_stage, dev, n * phys_elem(c), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (c->p.precision) {
+    const float* f = (const float*)c->h_stage;
+    for (size_t i = n; i-- > 0;) c->h_stage[i] = (double)f[i];
+  }
+  compact_to_phys_ref(c, c->h_stage, ref);
+  return DB_OK;
+}
+
 static int upload_spec(db_ctx* c, int id, const double* ref) {
   double2* d = spec_field(c, id);
   if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
@@ -416,10 +476,7 @@ extern "C" int db_upload_field(db_ctx* c, int field, const double* host) {
   if (field == DB_NU_T || field == DB_KAPPA_T) {
     double* d = les_field(c, field);
     if (!d) return fail(c, DB_ERR_STATE, "nu_t / kappa_t exist only with use_les");
-    phys_ref_to_compact(c, host, c->h_stage);
-    CK(cudaMemcpyAsync(d, c->h_stage, (size_t)c->g.np * c->g.pp * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return DB_OK;
+    return phys_upload(c, host, d);
   }
   return fail(c, DB_ERR_ARG, "bad field id");
 }
@@ -430,14 +487,10 @@ extern "C" int db_download_field(db_ctx* c, int field, double* host) {
   if (field == DB_NU_T || field == DB_KAPPA_T) {
     double* d = les_field(c, field);
     if (!d) return fail(c, DB_ERR_STATE, "nu_t / kappa_t exist only with use_les");
-    const Geom& g = c->g;
-    CK(cudaMemcpyAsync(c->h_stage, d, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
     // the reference array's padding (x >= Nx, z >= Nz) reads as zero
     const int nx2 = c->p.nx + 2, nz2 = c->p.nz + 2;
-    memset(host, 0, sizeof(double) * (size_t)g.np * nz2 * nx2);
-    compact_to_phys_ref(c, c->h_stage, host);
-    return DB_OK;
+    memset(host, 0, sizeof(double) * (size_t)c->g.np * nz2 * nx2);
+    return phys_download(c, d, host);
   }
   return fail(c, DB_ERR_ARG, "bad field id");
 }
@@ -480,8 +533,8 @@ extern "C" int db_clear_status(db_ctx* c) {
 extern "C" int db_fft_xz_to_fourier(db_ctx* c, double* buf) {
   if (!c || !buf) return DB_ERR_ARG;
   const Geom& g = c->g;
-  phys_ref_to_compact(c, buf, c->h_stage);
-  CK(cudaMemcpyAsync(c->s.r1, c->h_stage, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  int rc = phys_upload(c, buf, c->s.r1);
+  if (rc) return rc;
   CK(launch_fwd_x(g, fset(c->s.r1), fset(c->s.xh[0]), 1, c->st));
   CK(launch_fwd_z(g, fset(c->s.xh[0]), fset(c->s.phi_g), 1, c->st));
   CK(cudaMemcpyAsync(c->h_stage, c->s.phi_g, (size_t)g.np * g.sp * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
@@ -497,10 +550,7 @@ extern "C" int db_fft_xz_to_physical(db_ctx* c, double* buf) {
   CK(cudaMemcpyAsync(c->s.phi_g, c->h_stage, (size_t)g.np * g.sp * sizeof(double2), cudaMemcpyHostToDevice, c->st));
   CK(launch_inv_z(g, fset(c->s.phi_g), fset(c->s.xh[0]), 1, c->st));
   CK(launch_inv_x(g, fset(c->s.xh[0]), fset(c->s.r1), 1, c->st));
-  CK(cudaMemcpyAsync(c->h_stage, c->s.r1, (size_t)g.np * g.pp * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  compact_to_phys_ref(c, c->h_stage, buf);
-  return DB_OK;
+  return phys_download(c, c->s.r1, buf);
 }
 
 // ---------------------------------------------------------------------------

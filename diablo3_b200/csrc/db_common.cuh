@@ -1,6 +1,6 @@
 // db_common.cuh -- device-side layout, geometry and run scalars.
 //
-// HBM layout (all FP64):
+// HBM layout (FP64; with prec = 1 the physical and x-half fields are FP32):
 //   spectral field  double2 s[j][kzp][kx]   j in [0, Nyp+2), kzp in [0, 2Nkz],
 //                   kx in [0, kxs) with only kx <= Nkx significant (the rest 0).
 //                   kzp uses the reference's packing: 0..Nkz, then -Nkz..-1
@@ -35,6 +35,9 @@ struct Geom {
   const double* kz;        // nkzp entries, packed order
   const double2* twx;      // FFT twiddles, Nx entries
   const double2* twz;      // Nz entries
+  const float2* twxf;      // the same rounded to FP32 (mixed path)
+  const float2* twzf;
+  int prec;                // 0: FP64 throughout; 1: mixed (FP32 physical / x-half)
 };
 
 // Physics constants of the substep (host-computed once at init).

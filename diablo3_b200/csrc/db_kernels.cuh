@@ -4,8 +4,17 @@
 #include <cuda_runtime.h>
 
 #include "db_common.cuh"
+#include "fft_smem.cuh"
 
 namespace db {
+
+// FFT twiddle tables in the work precision R
+template <typename R> __device__ __forceinline__ const typename CplxOf<R>::type* tw_x(const Geom& g);
+template <> __device__ __forceinline__ const double2* tw_x<double>(const Geom& g) { return g.twx; }
+template <> __device__ __forceinline__ const float2* tw_x<float>(const Geom& g) { return g.twxf; }
+template <typename R> __device__ __forceinline__ const typename CplxOf<R>::type* tw_z(const Geom& g);
+template <> __device__ __forceinline__ const double2* tw_z<double>(const Geom& g) { return g.twz; }
+template <> __device__ __forceinline__ const float2* tw_z<float>(const Geom& g) { return g.twzf; }
 
 constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple of 4)
 
@@ -73,7 +82,9 @@ __host__ __device__ inline Chunks thomas_chunks(int np) {
   return c;
 }
 
-// Pointers of the full device state for the substep kernels.
+// Pointers of the full device state for the substep kernels.  Physical and
+// x-half fields are typed double / double2 here; with Geom::prec = 1 they
+// hold float / float2 and the kernels cast them to their work type.
 struct State {
   double2 *cu1, *cu2, *cu3, *cp, *cth;       // spectral
   double2 *cf1, *cf2, *cf3, *cfth;           // spectral RK history
@@ -90,6 +101,7 @@ struct State {
   double* les[9];                            // SGS forcing per product slot (k_les.cu)
   double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
+  double* tscr;                              // FP64 Thomas scratch, one field (mixed LES only)
 };
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products

@@ -1,4 +1,5 @@
-// fft_reg.cuh -- register-resident FP64 Stockham FFT, E elements per thread,
+// fft_reg.cuh -- register-resident Stockham FFT (FP64 double2 or FP32 float2
+// complex type C), E elements per thread,
 // T = N/E threads per sequence (sm_100a).
 //
 // Thread `lane` of a group holds v[q] = x[lane + q T], q = 0..E-1.  That set
@@ -65,14 +66,14 @@ __device__ __forceinline__ void fft_sync_t(int T) {
 }
 
 // twiddle bases of one thread for every pass p >= 1 and butterfly m
-template <int N, int E>
+template <int N, int E, typename C = double2>
 struct Twiddles {
   static constexpr int MAXB = 8;  // E / R <= 8
-  double2 w[RPlan<N>::npass > 1 ? RPlan<N>::npass - 1 : 1][MAXB];
+  C w[RPlan<N>::npass > 1 ? RPlan<N>::npass - 1 : 1][MAXB];
 };
 
-template <int N, int E>
-__device__ __forceinline__ void load_twiddles(Twiddles<N, E>& tw, int lane, const double2* __restrict__ tab) {
+template <int N, int E, typename C>
+__device__ __forceinline__ void load_twiddles(Twiddles<N, E, C>& tw, int lane, const C* __restrict__ tab) {
   using P = RPlan<N>;
   constexpr int T = N / E;
 #pragma unroll
@@ -87,10 +88,10 @@ __device__ __forceinline__ void load_twiddles(Twiddles<N, E>& tw, int lane, cons
   }
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void twiddle_apply(double2* x, double2 w) {
+template <int R, int SIGN, typename C>
+__device__ __forceinline__ void twiddle_apply(C* x, C w) {
   if (SIGN > 0) w.y = -w.y;
-  double2 wr = w;
+  C wr = w;
 #pragma unroll
   for (int r = 1; r < R; ++r) {
     x[r] = cmul(x[r], wr);
@@ -98,12 +99,12 @@ __device__ __forceinline__ void twiddle_apply(double2* x, double2 w) {
   }
 }
 
-template <int N, int E, int R, int SIGN>
-__device__ __forceinline__ void reg_pass(double2 (&v)[E], const double2* wb) {
+template <int N, int E, int R, int SIGN, typename C>
+__device__ __forceinline__ void reg_pass(C (&v)[E], const C* wb) {
   constexpr int PER = E / R;
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
-    double2 x[R];
+    C x[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) x[r] = v[m + r * PER];
     if (wb) twiddle_apply<R, SIGN>(x, wb[m]);
@@ -115,8 +116,8 @@ __device__ __forceinline__ void reg_pass(double2 (&v)[E], const double2* wb) {
   }
 }
 
-template <int N, int E, int R>
-__device__ __forceinline__ void reg_scatter(const double2 (&v)[E], int lane, int Ns, double2* s) {
+template <int N, int E, int R, typename C>
+__device__ __forceinline__ void reg_scatter(const C (&v)[E], int lane, int Ns, C* s) {
   constexpr int T = N / E;
   constexpr int PER = E / R;
 #pragma unroll
@@ -128,8 +129,8 @@ __device__ __forceinline__ void reg_scatter(const double2 (&v)[E], int lane, int
   }
 }
 
-template <int N, int E>
-__device__ __forceinline__ void reg_gather(double2 (&v)[E], int lane, const double2* s) {
+template <int N, int E, typename C>
+__device__ __forceinline__ void reg_gather(C (&v)[E], int lane, const C* s) {
   constexpr int T = N / E;
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = s[pidx(lane + q * T)];
@@ -144,9 +145,9 @@ __device__ __forceinline__ void reg_gather(double2 (&v)[E], int lane, const doub
 // mapping) and every exchange uses __syncthreads.
 // s1 (optional): a second buffer; exchanges then alternate between s and s1
 // and skip the barrier that protects a single buffer from the next scatter.
-template <int N, int SIGN, bool CTA = false>
-__device__ __forceinline__ void fft_reg(double2 (&v)[FftShape<N>::E], int lane, bool active, double2* s,
-                                        const Twiddles<N, FftShape<N>::E>& tw, double2* s1 = nullptr) {
+template <int N, int SIGN, bool CTA = false, typename C>
+__device__ __forceinline__ void fft_reg(C (&v)[FftShape<N>::E], int lane, bool active, C* s,
+                                        const Twiddles<N, FftShape<N>::E, C>& tw, C* s1 = nullptr) {
   using P = RPlan<N>;
   constexpr int E = FftShape<N>::E;
   constexpr bool W = FftShape<N>::warp;
@@ -155,11 +156,11 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[FftShape<N>::E], int lane, 
     constexpr int dummy = 0;
     (void)dummy;
     const int R = P::radix(p), Ns = P::ns(p);
-    const double2* wb = (p == 0) ? nullptr : tw.w[p > 0 ? p - 1 : 0];
+    const C* wb = (p == 0) ? nullptr : tw.w[p > 0 ? p - 1 : 0];
     if (R == 8) {
       if (active) reg_pass<N, E, 8, SIGN>(v, wb);
       if (p + 1 < P::npass) {
-        double2* sb = (s1 != nullptr && (p & 1)) ? s1 : s;
+        C* sb = (s1 != nullptr && (p & 1)) ? s1 : s;
         if (p > 0 && s1 == nullptr) {
           if (CTA) __syncthreads(); else fft_sync_t<W>(N / E);
         }
@@ -177,9 +178,9 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[FftShape<N>::E], int lane, 
 
 // Same transform with the twiddle base of each pass fetched inside the pass
 // (no twiddle registers held across passes; for register-heavy callers).
-template <int N, int SIGN, bool CTA = false>
-__device__ __forceinline__ void fft_reg_lazy(double2 (&v)[FftShape<N>::E], int lane, bool active, double2* s,
-                                             const double2* __restrict__ tab, double2* s1 = nullptr) {
+template <int N, int SIGN, bool CTA = false, typename C>
+__device__ __forceinline__ void fft_reg_lazy(C (&v)[FftShape<N>::E], int lane, bool active, C* s,
+                                             const C* __restrict__ tab, C* s1 = nullptr) {
   using P = RPlan<N>;
   constexpr int E = FftShape<N>::E;
   constexpr int T = N / E;
@@ -189,18 +190,18 @@ __device__ __forceinline__ void fft_reg_lazy(double2 (&v)[FftShape<N>::E], int l
     constexpr int dummy = 0;
     (void)dummy;
     const int R = P::radix(p), Ns = P::ns(p);
-    double2 wb[8];
+    C wb[8];
     if (p > 0) {
       const int PER = E / R;
 #pragma unroll
       for (int m = 0; m < 8; ++m)
         if (m < PER) wb[m] = __ldg(&tab[((lane + m * T) % Ns) * (N / (Ns * R))]);
     }
-    const double2* wbp = (p == 0) ? nullptr : wb;
+    const C* wbp = (p == 0) ? nullptr : wb;
     if (R == 8) {
       if (active) reg_pass<N, E, 8, SIGN>(v, wbp);
       if (p + 1 < P::npass) {
-        double2* sb = (s1 != nullptr && (p & 1)) ? s1 : s;
+        C* sb = (s1 != nullptr && (p & 1)) ? s1 : s;
         if (p > 0 && s1 == nullptr) {
           if (CTA) __syncthreads(); else fft_sync_t<W>(T);
         }

@@ -12,6 +12,10 @@
 // imaginary parts of the DC and Nyquist modes dropped as FFTW's c2r does and
 // modes above Nkx zeroed (the 2/3 de-aliasing, fft.f90:259-261, 366-368).
 // All transforms keep their data in registers (fft_reg.cuh).
+//
+// R is the real type of the physical and x-half fields: double, or float on
+// the mixed path, where the spectral state stays FP64 and is converted on
+// the z-pass load/store.
 #include "db_kernels.cuh"
 #include "fft_reg.cuh"
 
@@ -22,36 +26,38 @@ namespace db {
 // sequence; a CTA holds NS = blockDim / T independent sequences.
 
 // physical -> Xh: sequence = rows (2q, 2q+1) of one plane/field
-template <int N>
+template <int N, typename R>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet out, Geom g) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
   const int q2 = blockIdx.x * (blockDim.x / T) + seq;
   const int j = blockIdx.y, f = blockIdx.z;
-  double2* sq = sm + seq * padded(N);
-  Twiddles<N, E> tw;
-  load_twiddles<N, E>(tw, lane, g.twx);
-  const double* ra = (const double*)in.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
-  const double* rb = ra + g.nx;
-  double2 v[E];
+  C* sq = sm + seq * padded(N);
+  Twiddles<N, E, C> tw;
+  load_twiddles<N, E>(tw, lane, tw_x<R>(g));
+  const R* ra = (const R*)in.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
+  const R* rb = ra + g.nx;
+  C v[E];
 #pragma unroll
-  for (int q = 0; q < E; ++q) v[q] = make_double2(__ldg(ra + lane + q * T), __ldg(rb + lane + q * T));
+  for (int q = 0; q < E; ++q) v[q] = mkc<C>(__ldg(ra + lane + q * T), __ldg(rb + lane + q * T));
   fft_reg<N, -1>(v, lane, true, sq, tw);
   SEQ_SYNC(N);
 #pragma unroll
   for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
   SEQ_SYNC(N);
-  double2* oa = (double2*)out.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
-  double2* ob = oa + g.kxs;
-  const double s = 0.5 / (double)N;
+  C* oa = (C*)out.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
+  C* ob = oa + g.kxs;
+  const R s = (R)(0.5 / (double)N);
   for (int m = lane; m < g.kxs; m += T) {
-    double2 A = make_double2(0.0, 0.0), B = A;
+    C A = mkc<C>(0, 0), B = A;
     if (m <= g.nkx) {
-      const double2 zm = sq[pidx(m)], zn = cconj(sq[pidx((N - m) & (N - 1))]);
-      A = make_double2((zm.x + zn.x) * s, (zm.y + zn.y) * s);
-      B = make_double2((zm.y - zn.y) * s, -(zm.x - zn.x) * s);  // -i (zm - zn) / 2
+      const C zm = sq[pidx(m)], zn = cconj(sq[pidx((N - m) & (N - 1))]);
+      A = mkc<C>((zm.x + zn.x) * s, (zm.y + zn.y) * s);
+      B = mkc<C>((zm.y - zn.y) * s, -(zm.x - zn.x) * s);  // -i (zm - zn) / 2
     }
     oa[m] = A;
     ob[m] = B;
@@ -60,40 +66,42 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet 
 
 // Xh -> physical; fields f with bit f of dmask set are differentiated in x
 // (multiplied by i kx before the transform)
-template <int N>
+template <int N, typename R>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet out, Geom g, unsigned dmask) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
   const int q2 = blockIdx.x * (blockDim.x / T) + seq;
   const int j = blockIdx.y, f = blockIdx.z;
-  double2* sq = sm + seq * padded(N);
-  Twiddles<N, E> tw;
-  load_twiddles<N, E>(tw, lane, g.twx);
-  const double2* ia = (const double2*)in.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
-  const double2* ib = ia + g.kxs;
+  C* sq = sm + seq * padded(N);
+  Twiddles<N, E, C> tw;
+  load_twiddles<N, E>(tw, lane, tw_x<R>(g));
+  const C* ia = (const C*)in.p[f] + (long long)j * g.hp + (long long)(2 * q2) * g.kxs;
+  const C* ib = ia + g.kxs;
   const bool dx = (dmask >> f) & 1u;
-  double2 v[E];
+  C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     const int e = lane + q * T;
-    double2 z = make_double2(0.0, 0.0);
+    C z = mkc<C>(0, 0);
     if (e <= g.nkx) {
-      double2 A = __ldg(ia + e), B = __ldg(ib + e);
-      if (dx) { A = cmul_i(A, g.kx[e]); B = cmul_i(B, g.kx[e]); }
-      if (e == 0) { A.y = 0.0; B.y = 0.0; }
-      z = make_double2(A.x - B.y, A.y + B.x);            // A + iB
+      C A = __ldg(ia + e), B = __ldg(ib + e);
+      if (dx) { A = cmul_i(A, (R)g.kx[e]); B = cmul_i(B, (R)g.kx[e]); }
+      if (e == 0) { A.y = 0; B.y = 0; }
+      z = mkc<C>(A.x - B.y, A.y + B.x);            // A + iB
     } else if (e >= N - g.nkx) {
-      double2 A = __ldg(ia + (N - e)), B = __ldg(ib + (N - e));
-      if (dx) { A = cmul_i(A, g.kx[N - e]); B = cmul_i(B, g.kx[N - e]); }
-      z = make_double2(A.x + B.y, B.x - A.y);            // conj A + i conj B
+      C A = __ldg(ia + (N - e)), B = __ldg(ib + (N - e));
+      if (dx) { A = cmul_i(A, (R)g.kx[N - e]); B = cmul_i(B, (R)g.kx[N - e]); }
+      z = mkc<C>(A.x + B.y, B.x - A.y);            // conj A + i conj B
     }
     v[q] = z;
   }
   fft_reg<N, +1>(v, lane, true, sq, tw);
-  double* ra = (double*)out.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
-  double* rb = ra + g.nx;
+  R* ra = (R*)out.p[f] + (long long)j * g.pp + (long long)(2 * q2) * g.nx;
+  R* rb = ra + g.nx;
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     ra[lane + q * T] = v[q].x;
@@ -101,22 +109,24 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet 
   }
 }
 
-// Xh -> packed spectral, scaled by 1/Nz; sequence = one kx column of a plane
-template <int N>
+// Xh -> packed spectral (FP64), scaled by 1/Nz; sequence = one kx column of a plane
+template <int N, typename R>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet out, Geom g) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
   const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
-  double2* sq = sm + seq * padded(N);
-  Twiddles<N, E> tw;
-  load_twiddles<N, E>(tw, lane, g.twz);
-  const double2* src = (const double2*)in.p[f] + (long long)j * g.hp + kx;
-  double2 v[E];
+  C* sq = sm + seq * padded(N);
+  Twiddles<N, E, C> tw;
+  load_twiddles<N, E>(tw, lane, tw_z<R>(g));
+  const C* src = (const C*)in.p[f] + (long long)j * g.hp + kx;
+  C v[E];
 #pragma unroll
-  for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : make_double2(0.0, 0.0);
+  for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
   fft_reg<N, -1>(v, lane, active, sq, tw);
   if (!active) return;
   double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
@@ -125,41 +135,44 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet 
   for (int q = 0; q < E; ++q) {
     const int z = lane + q * T;
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
-    if (kzp >= 0) dst[(long long)kzp * g.kxs] = cscale(v[q], s);
+    if (kzp >= 0) dst[(long long)kzp * g.kxs] = cscale(to_d2(v[q]), s);
   }
 }
 
-// packed spectral -> Xh (zero-filled de-aliased rows, unnormalised); fields
-// f with bit f of dmask set are differentiated in z (times i kz)
-template <int N>
+// packed spectral (FP64) -> Xh (zero-filled de-aliased rows, unnormalised);
+// fields f with bit f of dmask set are differentiated in z (times i kz)
+template <int N, typename R>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet out, Geom g, unsigned dmask,
                                                           const double2* __restrict__ ghost) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
   const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
-  double2* sq = sm + seq * padded(N);
-  Twiddles<N, E> tw;
-  load_twiddles<N, E>(tw, lane, g.twz);
+  C* sq = sm + seq * padded(N);
+  Twiddles<N, E, C> tw;
+  load_twiddles<N, E>(tw, lane, tw_z<R>(g));
   const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx;
   if (ghost) {   // rows 0, 1, Nyp, Nyp+1 from the overlay
     const int q = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
     if (q >= 0) src = ghost + (long long)(4 * (f & 3) + q) * g.sp + kx;
   }
   const bool dz = (dmask >> f) & 1u;
-  double2 v[E];
+  C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     const int z = lane + q * T;
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
-    v[q] = (active && kzp >= 0) ? __ldg(src + (long long)kzp * g.kxs) : make_double2(0.0, 0.0);
-    if (dz && kzp >= 0) v[q] = cmul_i(v[q], g.kz[kzp]);
+    double2 a = (active && kzp >= 0) ? __ldg(src + (long long)kzp * g.kxs) : make_double2(0.0, 0.0);
+    if (dz && kzp >= 0) a = cmul_i(a, g.kz[kzp]);
+    v[q] = from_d2<C>(a);
   }
   fft_reg<N, +1>(v, lane, active, sq, tw);
   if (!active) return;
-  double2* dst = (double2*)out.p[f] + (long long)j * g.hp + kx;
+  C* dst = (C*)out.p[f] + (long long)j * g.hp + kx;
 #pragma unroll
   for (int q = 0; q < E; ++q) dst[(long long)(lane + q * T) * g.kxs] = v[q];
 }
@@ -191,43 +204,69 @@ static void smem_attr(K kern, size_t smem) {
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-template <int N>
-static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+template <int N, typename R>
+static void go_fwd_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
   constexpr int ns = seqs_per_cta<N>();
   int npairs = g.nz / 2;
   int cps = ns < npairs ? ns : npairs;
   while (npairs % cps) --cps;
-  size_t smem = (size_t)cps * padded(N) * sizeof(double2);
-  smem_attr(k_fwd_x<N>, smem);
-  k_fwd_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
+  size_t smem = (size_t)cps * padded(N) * sizeof(C);
+  smem_attr(k_fwd_x<N, R>, smem);
+  k_fwd_x<N, R><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
+}
+template <int N, typename R>
+static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  constexpr int ns = seqs_per_cta<N>();
+  int npairs = g.nz / 2;
+  int cps = ns < npairs ? ns : npairs;
+  while (npairs % cps) --cps;
+  size_t smem = (size_t)cps * padded(N) * sizeof(C);
+  smem_attr(k_inv_x<N, R>, smem);
+  k_inv_x<N, R><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask);
+}
+template <int N, typename R>
+static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  constexpr int ns = seqs_per_cta<N>();
+  size_t smem = (size_t)ns * padded(N) * sizeof(C);
+  smem_attr(k_fwd_z<N, R>, smem);
+  k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
+}
+template <int N, typename R>
+static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
+                       cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  constexpr int ns = seqs_per_cta<N>();
+  size_t smem = (size_t)ns * padded(N) * sizeof(C);
+  smem_attr(k_inv_z<N, R>, smem);
+  k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);
+}
+template <int N>
+static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  if (g.prec) go_fwd_x_t<N, float>(g, in, out, nf, st);
+  else go_fwd_x_t<N, double>(g, in, out, nf, st);
 }
 template <int N>
 static void go_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, cudaStream_t st) {
-  constexpr int ns = seqs_per_cta<N>();
-  int npairs = g.nz / 2;
-  int cps = ns < npairs ? ns : npairs;
-  while (npairs % cps) --cps;
-  size_t smem = (size_t)cps * padded(N) * sizeof(double2);
-  smem_attr(k_inv_x<N>, smem);
-  k_inv_x<N><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask);
+  if (g.prec) go_inv_x_t<N, float>(g, in, out, nf, dmask, st);
+  else go_inv_x_t<N, double>(g, in, out, nf, dmask, st);
 }
 template <int N>
 static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  constexpr int ns = seqs_per_cta<N>();
-  size_t smem = (size_t)ns * padded(N) * sizeof(double2);
-  smem_attr(k_fwd_z<N>, smem);
-  k_fwd_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
+  if (g.prec) go_fwd_z_t<N, float>(g, in, out, nf, st);
+  else go_fwd_z_t<N, double>(g, in, out, nf, st);
 }
 template <int N>
 static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
                      cudaStream_t st) {
-  constexpr int ns = seqs_per_cta<N>();
-  size_t smem = (size_t)ns * padded(N) * sizeof(double2);
-  smem_attr(k_inv_z<N>, smem);
-  k_inv_z<N><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);
+  if (g.prec) go_inv_z_t<N, float>(g, in, out, nf, dmask, ghost, st);
+  else go_inv_z_t<N, double>(g, in, out, nf, dmask, ghost, st);
 }
 
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
   DB_DISPATCH_N(g.nx, go_fwd_x, g, in, out, nf, st);
   return cudaGetLastError();
 }
@@ -237,6 +276,7 @@ cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
   return cudaGetLastError();
 }
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
   DB_DISPATCH_N(g.nz, go_fwd_z, g, in, out, nf, st);
   return cudaGetLastError();
 }

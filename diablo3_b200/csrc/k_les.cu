@@ -27,7 +27,8 @@
 //                 1028-1045, 1088-1105, 1144-1161, 1200-1217): the matrix
 //                 differs per (x, z) column, so each thread runs its own
 //                 Thomas sweep, the eliminated upper coefficients in shared
-//                 memory and the eliminated right-hand side in the r array.
+//                 memory and the eliminated right-hand side (FP64) in the r
+//                 array, or in an FP64 scratch when r is FP32.
 #include <math.h>
 
 #include "db_bc.cuh"
@@ -79,28 +80,28 @@ constexpr double BETA_SGS = 3.0;     // les.f90:43
 
 // max{0, -(I3 - I4)} / (I1 - I2) of the scaled strain SI and rotation O
 // tensors (les.f90:578-619): -tr(SI^3) + tr(SI O^2) over |SI|^2 + |O|^2
-__device__ __forceinline__ double amd_ratio(double s1, double s2, double s3, double s4, double s5, double s6,
-                                            double o4, double o5, double o6) {
-  const double i3 = s1 * s1 * s1 + s2 * s2 * s2 + s3 * s3 * s3 + 3.0 * s1 * s4 * s4 + 3.0 * s1 * s5 * s5 +
-                    3.0 * s2 * s4 * s4 + 3.0 * s2 * s6 * s6 + 3.0 * s3 * s5 * s5 + 3.0 * s3 * s6 * s6 +
-                    6.0 * s4 * s5 * s6;
-  const double v = -i3 - s1 * o4 * o4 - s1 * o5 * o5 - s2 * o4 * o4 - s2 * o6 * o6 - s3 * o5 * o5 -
-                   s3 * o6 * o6 - 2.0 * s4 * o5 * o6 + 2.0 * s5 * o4 * o6 - 2.0 * s6 * o4 * o5;
-  if (v <= 0.0) return 0.0;
-  return v / (s1 * s1 + s2 * s2 + s3 * s3 + 2.0 * s4 * s4 + 2.0 * o4 * o4 + 2.0 * s5 * s5 + 2.0 * o5 * o5 +
-              2.0 * s6 * s6 + 2.0 * o6 * o6);
+template <typename R>
+__device__ __forceinline__ R amd_ratio(R s1, R s2, R s3, R s4, R s5, R s6, R o4, R o5, R o6) {
+  const R c2 = 2, c3 = 3, c6 = 6;
+  const R i3 = s1 * s1 * s1 + s2 * s2 * s2 + s3 * s3 * s3 + c3 * s1 * s4 * s4 + c3 * s1 * s5 * s5 +
+               c3 * s2 * s4 * s4 + c3 * s2 * s6 * s6 + c3 * s3 * s5 * s5 + c3 * s3 * s6 * s6 + c6 * s4 * s5 * s6;
+  const R v = -i3 - s1 * o4 * o4 - s1 * o5 * o5 - s2 * o4 * o4 - s2 * o6 * o6 - s3 * o5 * o5 - s3 * o6 * o6 -
+              c2 * s4 * o5 * o6 + c2 * s5 * o4 * o6 - c2 * s6 * o4 * o5;
+  if (v <= (R)0) return (R)0;
+  return v / (s1 * s1 + s2 * s2 + s3 * s3 + c2 * s4 * s4 + c2 * o4 * o4 + c2 * s5 * s5 + c2 * o5 * o5 +
+              c2 * s6 * s6 + c2 * o6 * o6);
 }
 
 // scalar AMD: max{0, -(delta_k^2 du_i/dx_k dth/dx_k dth/dx_i)} / |delta dth|^2
 // (les.f90:1222-1249, 1265-1305); arguments are the gradient components
-// at one point, dy the y filter width there
-__device__ __forceinline__ double amd_th_ratio(double dxs, double dys, double dzs, double u1x, double u2y,
-                                               double u3z, double u1y, double u2x, double u1z, double u3x,
-                                               double u2z, double u3y, double tx, double ty, double tz) {
-  const double v = -(dxs * dxs * u1x * tx * tx + dys * dys * u2y * ty * ty + dzs * dzs * u3z * tz * tz +
-                     (dys * dys * u1y + dxs * dxs * u2x) * tx * ty + (dzs * dzs * u1z + dxs * dxs * u3x) * tx * tz +
-                     (dzs * dzs * u2z + dys * dys * u3y) * ty * tz);
-  if (v <= 0.0) return 0.0;
+// at one point, dys the y filter width there
+template <typename R>
+__device__ __forceinline__ R amd_th_ratio(R dxs, R dys, R dzs, R u1x, R u2y, R u3z, R u1y, R u2x, R u1z, R u3x,
+                                          R u2z, R u3y, R tx, R ty, R tz) {
+  const R v = -(dxs * dxs * u1x * tx * tx + dys * dys * u2y * ty * ty + dzs * dzs * u3z * tz * tz +
+                (dys * dys * u1y + dxs * dxs * u2x) * tx * ty + (dzs * dzs * u1z + dxs * dxs * u3x) * tx * tz +
+                (dzs * dzs * u2z + dys * dys * u3y) * ty * tz);
+  if (v <= (R)0) return (R)0;
   return v / ((dxs * tx) * (dxs * tx) + (dys * ty) * (dys * ty) + (dzs * tz) * (dzs * tz));
 }
 
@@ -122,7 +123,8 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 //  les[8] = dyf-filter/2 * s1_th dth/dz    (th eq., times i kz)      rows jst..jet
 // with j1 = jstart, j2 = Nyp - 1 (les.f90:46-49, one rank), tau_12 at GY
 // rows = temp (S12 - du1/dy / 2) for j >= 2 and the raw strain at j = 1
-// (les.f90:737-748).
+// (les.f90:737-748).  R: arithmetic and storage type (FP32 on the mixed path).
+template <typename R>
 __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
@@ -131,100 +133,104 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
   const int Nyp = g.ny;
   const int jst = g.jstart_th, jet = g.jend_th;
   const int j1 = g.jstart, j2 = Nyp - 1;
-  const double dxs = ph.dx * BETA_SGS, dzs = ph.dz * BETA_SGS;
-  const double rzx = dzs / dxs, rxz = dxs / dzs;
+  const R h = 0.5, two = 2;
+  const double dxs_d = ph.dx * BETA_SGS, dzs_d = ph.dz * BETA_SGS;
+  const R dxs = (R)dxs_d, dzs = (R)dzs_d;
+  const R rzx = (R)(dzs_d / dxs_d), rxz = (R)(dxs_d / dzs_d);
   const double* dy = g.dy;
   const double* dyf = g.dyf;
-  const double* u1 = s.u1 + col;
-  const double* u2 = s.u2 + col;
-  const double* u3 = s.u3 + col;
-  const double* th = s.th + col;
-  const double *g1x = s.gx[0] + col, *g2x = s.gx[1] + col, *g3x = s.gx[2] + col, *gtx = s.gx[3] + col;
-  const double *g1z = s.gz[0] + col, *g2z = s.gz[1] + col, *g3z = s.gz[2] + col, *gtz = s.gz[3] + col;
-  double* o[9];
+  const R* u1 = (const R*)s.u1 + col;
+  const R* u2 = (const R*)s.u2 + col;
+  const R* u3 = (const R*)s.u3 + col;
+  const R* th = (const R*)s.th + col;
+  const R *g1x = (const R*)s.gx[0] + col, *g2x = (const R*)s.gx[1] + col, *g3x = (const R*)s.gx[2] + col,
+          *gtx = (const R*)s.gx[3] + col;
+  const R *g1z = (const R*)s.gz[0] + col, *g2z = (const R*)s.gz[1] + col, *g3z = (const R*)s.gz[2] + col,
+          *gtz = (const R*)s.gz[3] + col;
+  R* o[9];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) o[i] = s.les[i] + col;
-  double* nut = s.nu_t + col;
-  double* kat = s.kappa_t + col;
+  for (int i = 0; i < 9; ++i) o[i] = (R*)s.les[i] + col;
+  R* nut = (R*)s.nu_t + col;
+  R* kat = (R*)s.kappa_t + col;
 
   // row 0: GYF values only (GY row 0 does not exist)
-  double u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
-  double f1x = __ldg(g1x), f3z = __ldg(g3z), f1z = __ldg(g1z), f3x = __ldg(g3x);
-  double ftx = __ldg(gtx), ftz = __ldg(gtz);
-  double f2y = (u2c - __ldg(u2)) / dyf[0];
+  R u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
+  R f1x = __ldg(g1x), f3z = __ldg(g3z), f1z = __ldg(g1z), f3x = __ldg(g3x);
+  R ftx = __ldg(gtx), ftz = __ldg(gtz);
+  R f2y = (u2c - __ldg(u2)) / (R)dyf[0];
   // previous GY row (r = j - 1) values
-  double h1y = 0.0, h3y = 0.0, hty = 0.0, h2x = 0.0, h2z = 0.0;
-  double hSI4 = 0.0, hSI6 = 0.0, hO4 = 0.0, hO6 = 0.0, hP4 = 0.0, hP6 = 0.0, hdl = 0.0;
-  nut[0] = 0.0;
-  kat[0] = 0.0;
-  o[5][0] = 0.0;
-  o[6][0] = 0.0;
+  R h1y = 0, h3y = 0, hty = 0, h2x = 0, h2z = 0;
+  R hSI4 = 0, hSI6 = 0, hO4 = 0, hO6 = 0, hP4 = 0, hP6 = 0, hdl = 0;
+  nut[0] = 0;
+  kat[0] = 0;
+  o[5][0] = 0;
+  o[6][0] = 0;
 
   for (int j = 1; j <= Nyp + 1; ++j) {
     const long long oj = (long long)j * pp;
-    const double u1j = __ldg(u1 + oj), u3j = __ldg(u3 + oj), thj = __ldg(th + oj);
-    const double u2n = (j + 1 <= Nyp + 1) ? __ldg(u2 + oj + pp) : 0.0;
-    const double a1x = __ldg(g1x + oj), a2x = __ldg(g2x + oj), a3x = __ldg(g3x + oj), atx = __ldg(gtx + oj);
-    const double a1z = __ldg(g1z + oj), a2z = __ldg(g2z + oj), a3z = __ldg(g3z + oj), atz = __ldg(gtz + oj);
-    const double dyj = dy[j], dyfj = dyf[j], dyfm = dyf[j - 1];
+    const R u1j = __ldg(u1 + oj), u3j = __ldg(u3 + oj), thj = __ldg(th + oj);
+    const R u2n = (j + 1 <= Nyp + 1) ? __ldg(u2 + oj + pp) : (R)0;
+    const R a1x = __ldg(g1x + oj), a2x = __ldg(g2x + oj), a3x = __ldg(g3x + oj), atx = __ldg(gtx + oj);
+    const R a1z = __ldg(g1z + oj), a2z = __ldg(g2z + oj), a3z = __ldg(g3z + oj), atz = __ldg(gtz + oj);
+    const R dyj = (R)dy[j], dyfj = (R)dyf[j], dyfm = (R)dyf[j - 1];
     // GY row j: y-derivatives and the tensors that live there
-    const double d1y = (u1j - u1m) / dyj, d3y = (u3j - u3m) / dyj, dty = (thj - thm) / dyj;
-    const double dly = dyj * 2.0;
-    const double SI4 = 0.5 * (d1y * (dly / dxs) + a2x * (dxs / dly));
-    const double SI6 = 0.5 * (a2z * (dzs / dly) + d3y * (dly / dzs));
-    const double O4 = 0.5 * (d1y * (dly / dxs) - a2x * (dxs / dly));
-    const double O6 = 0.5 * (a2z * (dzs / dly) - d3y * (dly / dzs));
-    const double S4 = 0.5 * (d1y + a2x), S6 = 0.5 * (a2z + d3y);
+    const R d1y = (u1j - u1m) / dyj, d3y = (u3j - u3m) / dyj, dty = (thj - thm) / dyj;
+    const R dly = dyj * two;
+    const R SI4 = h * (d1y * (dly / dxs) + a2x * (dxs / dly));
+    const R SI6 = h * (a2z * (dzs / dly) + d3y * (dly / dzs));
+    const R O4 = h * (d1y * (dly / dxs) - a2x * (dxs / dly));
+    const R O6 = h * (a2z * (dzs / dly) - d3y * (dly / dzs));
+    const R S4 = h * (d1y + a2x), S6 = h * (a2z + d3y);
     // GYF row j (d u2/dy there needs u2 at j + 1; row Nyp + 1 is unused)
-    const double c2y = (j <= Nyp) ? (u2n - u2c) / dyfj : 0.0;
-    const double delt = amd_delta(dxs, dzs, dyj);
-    double temp = 0.0, temp_th = 0.0;
+    const R c2y = (j <= Nyp) ? (u2n - u2c) / dyfj : (R)0;
+    const R delt = (R)amd_delta(dxs_d, dzs_d, dy[j]);
+    R temp = 0, temp_th = 0;
     if (j >= 2 && j <= Nyp) {
-      const double w = 2.0 * dyj;
+      const R w = two * dyj;
 #define GYI(A, B) (((A) * dyfm + (B) * dyfj) / w)
-      const double SI5c = 0.5 * (a1z * rzx + a3x * rxz), SI5p = 0.5 * (f1z * rzx + f3x * rxz);
-      const double O5c = 0.5 * (a1z * rzx - a3x * rxz), O5p = 0.5 * (f1z * rzx - f3x * rxz);
-      temp = amd_ratio(GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), SI4, GYI(SI5c, SI5p), SI6, O4,
-                       GYI(O5c, O5p), O6);
-      temp_th = amd_th_ratio(dxs, dly, dzs, GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), d1y, a2x,
-                             GYI(a1z, f1z), GYI(a3x, f3x), a2z, d3y, GYI(atx, ftx), dty, GYI(atz, ftz));
+      const R SI5c = h * (a1z * rzx + a3x * rxz), SI5p = h * (f1z * rzx + f3x * rxz);
+      const R O5c = h * (a1z * rzx - a3x * rxz), O5p = h * (f1z * rzx - f3x * rxz);
+      temp = amd_ratio<R>(GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), SI4, GYI(SI5c, SI5p), SI6, O4,
+                          GYI(O5c, O5p), O6);
+      temp_th = amd_th_ratio<R>(dxs, dly, dzs, GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), d1y, a2x,
+                                GYI(a1z, f1z), GYI(a3x, f3x), a2z, d3y, GYI(atx, ftx), dty, GYI(atz, ftz));
 #undef GYI
     }
     const bool wall = (j <= 2 || j >= Nyp);     // ghost_les_mpi / ghost_les_th_mpi
-    const double nu = wall ? 0.0 : -0.5 * delt * temp;
-    const double ka = wall ? 0.0 : -0.5 * delt * temp_th;
-    const double P4 = (j >= 2) ? temp * (S4 - 0.5 * d1y) : S4;
-    const double P6 = (j >= 2) ? temp * (S6 - 0.5 * d3y) : S6;
+    const R nu = wall ? (R)0 : -h * delt * temp;
+    const R ka = wall ? (R)0 : -h * delt * temp_th;
+    const R P4 = (j >= 2) ? temp * (S4 - h * d1y) : S4;
+    const R P6 = (j >= 2) ? temp * (S6 - h * d3y) : S6;
     const bool gy2 = (j >= 2 && j <= Nyp);
     nut[oj] = nu;
     kat[oj] = ka;
-    o[5][oj] = gy2 ? delt * P4 - nu * d1y : 0.0;
-    o[6][oj] = gy2 ? delt * P6 - nu * d3y : 0.0;
+    o[5][oj] = gy2 ? delt * P4 - nu * d1y : (R)0;
+    o[6][oj] = gy2 ? delt * P6 - nu * d3y : (R)0;
 
     // GYF row r = j - 1: needs GY rows r and r + 1 = j
     {
       const int r = j - 1;
       const long long orr = (long long)r * pp;
-      const double dyfr = dyfm;
-      const double dlf = amd_delta(dxs, dzs, dyfr);
-      double L0 = 0.0, L1 = 0.0, L2 = 0.0, L3 = 0.0, L4 = 0.0, L7 = 0.0, L8 = 0.0;
+      const R dyfr = dyfm;
+      const R dlf = (R)amd_delta(dxs_d, dzs_d, dyf[r]);
+      R L0 = 0, L1 = 0, L2 = 0, L3 = 0, L4 = 0, L7 = 0, L8 = 0;
       if (r >= j1 && r <= j2) {
-        const double s4 = 0.5 * (SI4 + hSI4), s6 = 0.5 * (SI6 + hSI6);
-        const double q4 = 0.5 * (O4 + hO4), q6 = 0.5 * (O6 + hO6);
-        const double s5 = 0.5 * (f1z * rzx + f3x * rxz), q5 = 0.5 * (f1z * rzx - f3x * rxz);
-        const double s1 = amd_ratio(f1x, f2y, f3z, s4, s5, s6, q4, q5, q6);
+        const R s4 = h * (SI4 + hSI4), s6 = h * (SI6 + hSI6);
+        const R q4 = h * (O4 + hO4), q6 = h * (O6 + hO6);
+        const R s5 = h * (f1z * rzx + f3x * rxz), q5 = h * (f1z * rzx - f3x * rxz);
+        const R s1 = amd_ratio<R>(f1x, f2y, f3z, s4, s5, s6, q4, q5, q6);
         L0 = dlf * (s1 * f1x);
-        L2 = dlf * (s1 * (0.5 * (f1z + f3x)));
+        L2 = dlf * (s1 * (h * (f1z + f3x)));
         L4 = dlf * (s1 * f3z);
         L1 = (delt * P4 - hdl * hP4) / dyfr;
         L3 = (delt * P6 - hdl * hP6) / dyfr;
       }
       if (r >= jst && r <= jet) {
-        const double dys = dyfr * 2.0;
-        const double s1t = amd_th_ratio(dxs, dys, dzs, f1x, f2y, f3z, 0.5 * (d1y + h1y), 0.5 * (a2x + h2x), f1z,
-                                        f3x, 0.5 * (a2z + h2z), 0.5 * (d3y + h3y), ftx, 0.5 * (dty + hty), ftz);
-        L7 = 0.5 * dlf * (s1t * ftx);
-        L8 = 0.5 * dlf * (s1t * ftz);
+        const R dys = dyfr * two;
+        const R s1t = amd_th_ratio<R>(dxs, dys, dzs, f1x, f2y, f3z, h * (d1y + h1y), h * (a2x + h2x), f1z, f3x,
+                                      h * (a2z + h2z), h * (d3y + h3y), ftx, h * (dty + hty), ftz);
+        L7 = h * dlf * (s1t * ftx);
+        L8 = h * dlf * (s1t * ftz);
       }
       o[0][orr] = L0;
       o[1][orr] = L1;
@@ -241,14 +247,16 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
     hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
   }
   const long long oe = (long long)(Nyp + 1) * pp;
-  o[0][oe] = 0.0; o[1][oe] = 0.0; o[2][oe] = 0.0; o[3][oe] = 0.0; o[4][oe] = 0.0;
-  o[7][oe] = 0.0; o[8][oe] = 0.0;
+  o[0][oe] = 0; o[1][oe] = 0; o[2][oe] = 0; o[3][oe] = 0; o[4][oe] = 0;
+  o[7][oe] = 0; o[8][oe] = 0;
 }
 
 // ---------------------------------------------------------------------------
-// CN solves with eddy viscosity (one Thomas sweep per thread and column)
+// CN solves with eddy viscosity (one Thomas sweep per thread and column);
+// FP64 arithmetic, fields stored as R
 constexpr int TL = 32;
 
+template <typename R>
 __global__ void __launch_bounds__(TL) k_thomas_les(State s, Geom g, int rk) {
   extern __shared__ double cm[];      // [np][TL]: u_j / b'_j
   const int lane = threadIdx.x;
@@ -260,21 +268,24 @@ __global__ void __launch_bounds__(TL) k_thomas_les(State s, Geom g, int rk) {
   const double* dyf = g.dyf;
   const double temp2 = 0.5 * s.sc->h_bar[rk];
   for (int eq = 0; eq < 4; ++eq) {
-    const TriRow* R = s.tri + eq * np;
-    double* u = ((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
-    double* r = ((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
-    const double* nv = ((eq == 0) ? s.kappa_t : s.nu_t) + col;
+    const TriRow* Rw = s.tri + eq * np;
+    R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
+    R* r = (R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
+    const R* nv = (const R*)((eq == 0) ? s.kappa_t : s.nu_t) + col;
+    // eliminated right-hand side, FP64: in r itself, or in the FP64 scratch
+    // when r is FP32
+    double* gs = (sizeof(R) == sizeof(double)) ? reinterpret_cast<double*>(r) : s.tscr + col;
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    double um = 0.0, uc = u[0], nm = 0.0, nc = nv[0];
+    double um = 0.0, uc = (double)u[0], nm = 0.0, nc = (double)nv[0];
     double bprev = 1.0, gprev = 0.0, uprev = 0.0;
     for (int j = 0; j < np; ++j) {
-      const TriRow row = R[j];
-      const double un = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
-      const double nn = (j + 1 < np) ? nv[(long long)(j + 1) * pp] : 0.0;
+      const TriRow row = Rw[j];
+      const double un = (j + 1 < np) ? (double)u[(long long)(j + 1) * pp] : 0.0;
+      const double nn = (j + 1 < np) ? (double)nv[(long long)(j + 1) * pp] : 0.0;
       double l = row.l, d = row.d, uu = row.u, v = row.bc;
       if (!row.is_bc) {
-        v = r[(long long)j * pp] + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
+        v = (double)r[(long long)j * pp] + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
         double lo_c, hi_c;
         if (eq != 1) {    // nu_t / kappa_t at GY rows j, j + 1
           v += temp2 * ((nn * (un - uc) / dy[j + 1] - nc * (uc - um) / dy[j]) / dyf[j]);
@@ -297,14 +308,14 @@ __global__ void __launch_bounds__(TL) k_thomas_les(State s, Geom g, int rk) {
       }
       const double ib = 1.0 / b;
       cm[j * TL + lane] = uu * ib;
-      r[(long long)j * pp] = gg * ib;
+      gs[(long long)j * pp] = gg * ib;
       bprev = b; gprev = gg; uprev = uu;
       um = uc; uc = un; nm = nc; nc = nn;
     }
     double xn = 0.0;
     for (int j = np - 1; j >= 0; --j) {
-      const double xv = r[(long long)j * pp] - cm[j * TL + lane] * xn;
-      if (j >= lo && j <= hi) u[(long long)j * pp] = xv;
+      const double xv = gs[(long long)j * pp] - cm[j * TL + lane] * xn;
+      if (j >= lo && j <= hi) u[(long long)j * pp] = (R)xv;
       xn = xv;
     }
   }
@@ -317,14 +328,20 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
 }
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st) {
   const int bx = g.nx < 128 ? g.nx : 128;
-  k_les_amd<<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
+  if (g.prec) k_les_amd<float><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
+  else k_les_amd<double><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
   return cudaGetLastError();
 }
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
   const size_t smem = (size_t)g.np * TL * sizeof(double);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_thomas_les<<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
+  if (g.prec) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_thomas_les<float><<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_thomas_les<double><<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
+  }
   return cudaGetLastError();
 }
 

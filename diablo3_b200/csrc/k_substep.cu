@@ -44,16 +44,19 @@ __device__ __forceinline__ bool in_rng(int j, int a, int b) { return j >= a && j
 // so that cf_e -= Z(N_e) + ikz Z(M_e) after the z-pass (solver.f90:655-815,
 // 914-964; <.> is the interpolation to GY points, Dy the conservative
 // y-difference).
-template <int N>
-__device__ __forceinline__ double2 sepp(const double2* z, int m, int part) {
-  const double2 zm = z[pidx(m)], zn = cconj(z[pidx((N - m) & (N - 1))]);
-  if (part == 0) return make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y + zn.y));
-  return make_double2(0.5 * (zm.y - zn.y), -0.5 * (zm.x - zn.x));
+template <int N, typename C>
+__device__ __forceinline__ C sepp(const C* z, int m, int part) {
+  using R = typename RealOf<C>::type;
+  const C zm = z[pidx(m)], zn = cconj(z[pidx((N - m) & (N - 1))]);
+  if (part == 0) return mkc<C>((R)0.5 * (zm.x + zn.x), (R)0.5 * (zm.y + zn.y));
+  return mkc<C>((R)0.5 * (zm.y - zn.y), (R)-0.5 * (zm.x - zn.x));
 }
 
-template <int N, bool LES>
+template <int N, bool LES, typename R>
 __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(State s, Geom g) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   const int seq = threadIdx.x / T, lane = threadIdx.x % T;
@@ -62,69 +65,76 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
   const bool r2 = in_rng(j, 2, g.ny);
   const bool rt = in_rng(j, g.jstart_th, g.jend_th);
   const long long hrow = (long long)j * g.hp + (long long)z * g.kxs;
+  C* const* xh = reinterpret_cast<C* const*>(s.xh);
   if ((grp == 0 && !r1) || (grp == 1 && !(r2 || rt))) {
     for (int idx = threadIdx.x; idx < 4 * g.kxs; idx += blockDim.x)
-      s.xh[4 * grp + idx / g.kxs][hrow + idx % g.kxs] = make_double2(0.0, 0.0);
+      xh[4 * grp + idx / g.kxs][hrow + idx % g.kxs] = mkc<C>(0, 0);
     return;
   }
-  double2* sq = sm + seq * padded(N);
-  Twiddles<N, E> tw;
-  load_twiddles<N, E>(tw, lane, g.twx);
+  C* sq = sm + seq * padded(N);
+  Twiddles<N, E, C> tw;
+  load_twiddles<N, E>(tw, lane, tw_x<R>(g));
+  const R* U1 = (const R*)s.u1;
+  const R* U2 = (const R*)s.u2;
+  const R* U3 = (const R*)s.u3;
+  const R* TH = (const R*)s.th;
+  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
   const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
   const long long om = o0 - g.pp, op = o0 + g.pp;
-  const double dyj = g.dy[j], dyfj = g.dyf[j];
-  const double dyfjm = (j >= 1) ? g.dyf[j - 1] : 0.0;
-  double2 v[E];
+  const R dyj = (R)g.dy[j], dyfj = (R)g.dyf[j];
+  const R dyfjm = (j >= 1) ? (R)g.dyf[j - 1] : (R)0;
+  const R two = 2, qrt = 0.25;
+  C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     const int x = lane + q * T;
-    double a = 0.0, b = 0.0;
+    R a = 0, b = 0;
     if (grp == 0) {
-      const double u1 = __ldg(s.u1 + o0 + x), u3 = __ldg(s.u3 + o0 + x);
+      const R u1 = __ldg(U1 + o0 + x), u3 = __ldg(U3 + o0 + x);
       if (seq == 0) {
-        const double u1p = __ldg(s.u1 + op + x), u1m = __ldg(s.u1 + om + x);
-        const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
+        const R u1p = __ldg(U1 + op + x), u1m = __ldg(U1 + om + x);
+        const R u2p = __ldg(U2 + op + x), u2 = __ldg(U2 + o0 + x);
         a = u1 * u1;
-        b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (2.0 * dyfj);
-        if (LES) { a += __ldg(s.les[0] + o0 + x); b += __ldg(s.les[1] + o0 + x); }
+        b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (two * dyfj);
+        if (LES) { a += __ldg(LS[0] + o0 + x); b += __ldg(LS[1] + o0 + x); }
       } else if (seq == 1) {
-        const double u3p = __ldg(s.u3 + op + x), u3m = __ldg(s.u3 + om + x);
-        const double u2p = __ldg(s.u2 + op + x), u2 = __ldg(s.u2 + o0 + x);
+        const R u3p = __ldg(U3 + op + x), u3m = __ldg(U3 + om + x);
+        const R u2p = __ldg(U2 + op + x), u2 = __ldg(U2 + o0 + x);
         a = u3 * u1;
-        b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (2.0 * dyfj);
-        if (LES) { a += __ldg(s.les[2] + o0 + x); b += __ldg(s.les[3] + o0 + x); }
+        b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (two * dyfj);
+        if (LES) { a += __ldg(LS[2] + o0 + x); b += __ldg(LS[3] + o0 + x); }
       } else {
         a = u3 * u3;
-        if (LES) a += __ldg(s.les[4] + o0 + x);
+        if (LES) a += __ldg(LS[4] + o0 + x);
       }
     } else {
-      const double u2 = __ldg(s.u2 + o0 + x);
+      const R u2 = __ldg(U2 + o0 + x);
       if (seq == 0) {
         if (r2) {
-          const double u1 = __ldg(s.u1 + o0 + x), u1m = __ldg(s.u1 + om + x);
-          const double pp = u2 + __ldg(s.u2 + op + x), qq = u2 + __ldg(s.u2 + om + x);
-          a = ((dyfj * u1 + dyfjm * u1m) / (2. * dyj)) * u2;
-          b = (0.25 * (pp * pp) - 0.25 * (qq * qq)) / dyj;
-          if (LES) a += __ldg(s.les[5] + o0 + x);
+          const R u1 = __ldg(U1 + o0 + x), u1m = __ldg(U1 + om + x);
+          const R pp = u2 + __ldg(U2 + op + x), qq = u2 + __ldg(U2 + om + x);
+          a = ((dyfj * u1 + dyfjm * u1m) / (two * dyj)) * u2;
+          b = (qrt * (pp * pp) - qrt * (qq * qq)) / dyj;
+          if (LES) a += __ldg(LS[5] + o0 + x);
         }
       } else if (seq == 1) {
         if (rt) {
-          const double th = __ldg(s.th + o0 + x), thp = __ldg(s.th + op + x), thm = __ldg(s.th + om + x);
-          const double u2p = __ldg(s.u2 + op + x);
-          a = th * __ldg(s.u1 + o0 + x);
-          b = (thp * u2p + th * u2p - th * u2 - thm * u2) / (2.0 * dyfj);
-          if (LES) a += __ldg(s.les[7] + o0 + x);
+          const R th = __ldg(TH + o0 + x), thp = __ldg(TH + op + x), thm = __ldg(TH + om + x);
+          const R u2p = __ldg(U2 + op + x);
+          a = th * __ldg(U1 + o0 + x);
+          b = (thp * u2p + th * u2p - th * u2 - thm * u2) / (two * dyfj);
+          if (LES) a += __ldg(LS[7] + o0 + x);
         }
       } else {
-        if (r2) a = ((dyfj * __ldg(s.u3 + o0 + x) + dyfjm * __ldg(s.u3 + om + x)) / (2. * dyj)) * u2;
-        if (rt) b = __ldg(s.th + o0 + x) * __ldg(s.u3 + o0 + x);
+        if (r2) a = ((dyfj * __ldg(U3 + o0 + x) + dyfjm * __ldg(U3 + om + x)) / (two * dyj)) * u2;
+        if (rt) b = __ldg(TH + o0 + x) * __ldg(U3 + o0 + x);
         if (LES) {
-          if (r2) a += __ldg(s.les[6] + o0 + x);
-          if (rt) b += __ldg(s.les[8] + o0 + x);
+          if (r2) a += __ldg(LS[6] + o0 + x);
+          if (rt) b += __ldg(LS[8] + o0 + x);
         }
       }
     }
-    v[q] = make_double2(a, b);
+    v[q] = mkc<C>(a, b);
   }
   fft_reg<N, -1>(v, lane, true, sq, tw);
   SEQ_SYNC(N);
@@ -133,23 +143,23 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
   SEQ_SYNC(N);
   // outputs of this sequence, scaled by 1/Nx: an N-type output
   // ikx X(a) + X(b), and for s1 (group 0) / s2 (both groups) the parts
-  const double sc = 1.0 / (double)N;
+  const R sc = (R)(1.0 / (double)N);
   const bool n_out = (seq < 2) ? ((grp == 0) || (seq == 0 ? r2 : rt)) : false;
   const int o_n = (grp == 0) ? (seq == 0 ? 0 : 2) : (seq == 0 ? 4 : 6);
+  const C Z = mkc<C>(0, 0);
   for (int mm = lane; mm < g.kxs; mm += T) {
     const bool live = mm <= g.nkx;
-    const double2 A = live ? sepp<N>(sq, mm, 0) : make_double2(0.0, 0.0);
-    const double2 B = live ? sepp<N>(sq, mm, 1) : make_double2(0.0, 0.0);
+    const C A = live ? sepp<N>(sq, mm, 0) : Z;
+    const C B = live ? sepp<N>(sq, mm, 1) : Z;
     if (seq < 2) {
-      const double k = g.kx[mm];
-      s.xh[o_n][hrow + mm] = n_out ? make_double2((B.x - k * A.y) * sc, (B.y + k * A.x) * sc)
-                                   : make_double2(0.0, 0.0);
+      const R k = (R)g.kx[mm];
+      xh[o_n][hrow + mm] = n_out ? mkc<C>((B.x - k * A.y) * sc, (B.y + k * A.x) * sc) : Z;
     }
-    if (grp == 0 && seq == 1) s.xh[1][hrow + mm] = make_double2(A.x * sc, A.y * sc);       // M1
-    if (grp == 0 && seq == 2) s.xh[3][hrow + mm] = make_double2(A.x * sc, A.y * sc);       // M3
+    if (grp == 0 && seq == 1) xh[1][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M1
+    if (grp == 0 && seq == 2) xh[3][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M3
     if (grp == 1 && seq == 2) {
-      s.xh[5][hrow + mm] = r2 ? make_double2(A.x * sc, A.y * sc) : make_double2(0.0, 0.0);  // M2
-      s.xh[7][hrow + mm] = rt ? make_double2(B.x * sc, B.y * sc) : make_double2(0.0, 0.0);  // MT
+      xh[5][hrow + mm] = r2 ? mkc<C>(A.x * sc, A.y * sc) : Z;  // M2
+      xh[7][hrow + mm] = rt ? mkc<C>(B.x * sc, B.y * sc) : Z;  // MT
     }
   }
 }
@@ -159,9 +169,11 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
-template <int N>
+template <int N, typename R>
 __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1)) k_zpass_rhs(State s, Geom g, Phys ph, int rk) {
-  extern __shared__ double2 sm[];
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
   // column-fastest mapping: a warp reads KT consecutive kx of 32/KT rows
@@ -171,14 +183,14 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   const int kxc = active ? kx : 0;
   // per-column buffers, staggered by one element so the KT columns sharing a
   // warp fall into different shared-memory bank groups
-  double2* sx = sm + seq * (3 * padded(N) + 1);  // exchange buffers (two)
-  double2* sx1 = sx + padded(N);
-  double2* sm_z = sx1 + padded(N);             // Z(M) stash, natural order
+  C* sx = sm + seq * (3 * padded(N) + 1);  // exchange buffers (two)
+  C* sx1 = sx + padded(N);
+  C* sm_z = sx1 + padded(N);             // Z(M) stash, natural order
 #if DB_ZPASS_LAZY
-#define ZFFT(SIGN_, V_) fft_reg_lazy<N, SIGN_, true>(V_, lane, active, sx, g.twz, sx1)
+#define ZFFT(SIGN_, V_) fft_reg_lazy<N, SIGN_, true>(V_, lane, active, sx, tw_z<R>(g), sx1)
 #else
-  Twiddles<N, E> twd;
-  load_twiddles<N, E>(twd, lane, g.twz);
+  Twiddles<N, E, C> twd;
+  load_twiddles<N, E>(twd, lane, tw_z<R>(g));
 #define ZFFT(SIGN_, V_) fft_reg<N, SIGN_, true>(V_, lane, active, sx, twd, sx1)
 #endif
   const double hb = s.sc->h_bar[rk];
@@ -194,25 +206,25 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
     const int e = blockIdx.z;
     const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
-    double2* xin_n = s.xh[2 * e];
-    const double2* xin_m = s.xh[2 * e + 1];
+    C* xin_n = (C*)s.xh[2 * e];
+    const C* xin_m = (const C*)s.xh[2 * e + 1];
     if (!in_rng(j, jlo, jhi)) {
       if (active)
 #pragma unroll
-        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = make_double2(0.0, 0.0);
+        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
       return;
     }
-    double2 vn[E];
+    C vn[E];
     // Z(M) first, parked in shared memory in natural order
 #pragma unroll
     for (int q = 0; q < E; ++q)
-      vn[q] = active ? __ldg(xin_m + h0 + (long long)(lane + q * T) * g.kxs) : make_double2(0.0, 0.0);
+      vn[q] = active ? __ldg(xin_m + h0 + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
     ZFFT(-1, vn);
 #pragma unroll
     for (int q = 0; q < E; ++q) sm_z[pidx(lane + q * T)] = vn[q];
 #pragma unroll
     for (int q = 0; q < E; ++q)
-      vn[q] = active ? xin_n[h0 + (long long)(lane + q * T) * g.kxs] : make_double2(0.0, 0.0);
+      vn[q] = active ? xin_n[h0 + (long long)(lane + q * T) * g.kxs] : mkc<C>(0, 0);
     __syncthreads();
     ZFFT(-1, vn);
 #pragma unroll
@@ -220,13 +232,13 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       const int zz = lane + q * T;
       const int kzp = (zz <= g.nkz) ? zz : (zz >= N - g.nkz ? zz - N + g.nkzp : -1);
       if (kzp < 0 || !active) {
-        vn[q] = make_double2(0.0, 0.0);
+        vn[q] = mkc<C>(0, 0);
         continue;
       }
       const double kzv = g.kz[kzp];
-      // NL = (Z(N) + i kz Z(M)) / Nz
-      const double2 zmq = sm_z[pidx(zz)];
-      const double2 nl = make_double2((vn[q].x - kzv * zmq.y) * inz, (vn[q].y + kzv * zmq.x) * inz);
+      // NL = (Z(N) + i kz Z(M)) / Nz, formed in FP64
+      const double2 zmq = to_d2(sm_z[pidx(zz)]), zn = to_d2(vn[q]);
+      const double2 nl = make_double2((zn.x - kzv * zmq.y) * inz, (zn.y + kzv * zmq.x) * inz);
       const long long a = sp0 + (long long)kzp * g.kxs;
       const double k2 = kxv * kxv + kzv * kzv;
       const double kk = beta1 ? k2 : pow(k2, ph.beta);
@@ -304,7 +316,7 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
         cr = cadd(cr, cscale(cf, temp5));
         s.cfth[a] = cf;
       }
-      vn[q] = cr;
+      vn[q] = from_d2<C>(cr);
     }
     __syncthreads();
     ZFFT(+1, vn);
@@ -444,6 +456,7 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // read once and u written once per equation.
 constexpr int TX = 32;
 
+template <typename R>
 __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
   extern __shared__ double tile[];          // [np][TX]
   __shared__ double carry[8][TX];
@@ -457,31 +470,31 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
   const int j0 = w * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this warp's rows
   const bool active = w < ch.nch;
   for (int eq = 0; eq < 4; ++eq) {
-    const TriRow* R = s.tri + eq * np;
-    double* u = (eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3));
-    const double* r = (eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3));
+    const TriRow* Rw = s.tri + eq * np;
+    R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3)));
+    const R* r = (const R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3)));
     // rows written back (solver.f90:1056, 1115, 1171, 1227)
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
     // 1. right-hand side (r + explicit CN term, or the BC value) and the
     //    forward recurrence within the chunk, carry-in zero
     if (active && xin) {
-      double um = (j0 > 0) ? __ldg(u + (long long)(j0 - 1) * pp + col) : 0.0;
-      double uc = __ldg(u + (long long)j0 * pp + col);
+      double um = (j0 > 0) ? (double)__ldg(u + (long long)(j0 - 1) * pp + col) : 0.0;
+      double uc = (double)__ldg(u + (long long)j0 * pp + col);
       double y = 0.0;
       for (int jb = j0; jb <= j1; jb += 8) {
         double xr[8], xu[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {   // all loads of the batch first
           const int j = jb + c;
-          xr[c] = (j <= j1) ? __ldg(r + (long long)j * pp + col) : 0.0;
-          xu[c] = (j <= j1 && j + 1 < np) ? __ldg(u + (long long)(j + 1) * pp + col) : 0.0;
+          xr[c] = (j <= j1) ? (double)__ldg(r + (long long)j * pp + col) : 0.0;
+          xu[c] = (j <= j1 && j + 1 < np) ? (double)__ldg(u + (long long)(j + 1) * pp + col) : 0.0;
         }
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
           const int j = jb + c;
           if (j > j1) break;
-          const TriRow* row = R + j;
+          const TriRow* row = Rw + j;
           const double un = xu[c];
           const double v = row->is_bc ? row->bc : xr[c] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
           y = (j == j0) ? v : v + row->ap * y;
@@ -497,7 +510,7 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
       double gk = 0.0;
       for (int k = 0; k < ch.nch; ++k) {
         const int e = min(np, (k + 1) * ch.len) - 1;
-        gk = tile[e * TX + lane] + (k > 0 ? R[e].pa * gk : 0.0);
+        gk = tile[e * TX + lane] + (k > 0 ? Rw[e].pa * gk : 0.0);
         carry[k][lane] = gk;
       }
     }
@@ -506,13 +519,13 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
     //    x_j = g_j / b'_j + m_j x_{j+1}, carry-in zero
     if (active && w > 0) {
       const double c = carry[w - 1][lane];
-      for (int j = j0; j <= j1; ++j) tile[j * TX + lane] += R[j].pa * c;
+      for (int j = j0; j <= j1; ++j) tile[j * TX + lane] += Rw[j].pa * c;
     }
     __syncthreads();
     if (active) {
       double xz = 0.0;
       for (int j = j1; j >= j0; --j) {
-        const TriRow row = R[j];
+        const TriRow row = Rw[j];
         const double wv = tile[j * TX + lane] * row.ibp;
         xz = (j == j1) ? wv : wv - row.u * row.ibp * xz;
         tile[j * TX + lane] = xz;
@@ -524,7 +537,7 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
       double xk = 0.0;
       for (int k = ch.nch - 1; k >= 0; --k) {
         const int b = k * ch.len;
-        xk = tile[b * TX + lane] + (k < ch.nch - 1 ? R[b].pm * xk : 0.0);
+        xk = tile[b * TX + lane] + (k < ch.nch - 1 ? Rw[b].pm * xk : 0.0);
         carry[k][lane] = xk;
       }
     }
@@ -533,8 +546,8 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
     if (active && xin) {
       const double c = (w < ch.nch - 1) ? carry[w + 1][lane] : 0.0;
       for (int j = j0; j <= j1; ++j) {
-        const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? R[j].pm * c : 0.0);
-        if (j >= lo && j <= hi) u[(long long)j * pp + col] = xv;
+        const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
+        if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
       }
     }
     __syncthreads();
@@ -638,8 +651,12 @@ __global__ void __launch_bounds__(128) k_rem_div(State s, Geom g, int rk, int up
 // courant: CFL minimum over the physical velocity (flow.f90:781-808)
 __device__ __forceinline__ unsigned long long dbits(double v) { return (unsigned long long)__double_as_longlong(v); }
 
+template <typename R>
 __global__ void __launch_bounds__(256) k_courant_reduce(State s, Geom g, Phys ph, CflCtl ctl) {
   DevScalars* sc = s.sc;
+  const R* U1 = (const R*)s.u1;
+  const R* U2 = (const R*)s.u2;
+  const R* U3 = (const R*)s.u3;
   if (!ctl.force && !(ctl.variable_dt && (sc->time_step % ctl.update_dt) == 0)) return;
   const long long n = (long long)g.pp;
   const int jlo = ph.front ? g.jstart : 1, jhi = ph.front ? g.jend : g.ny;
@@ -650,18 +667,19 @@ __global__ void __launch_bounds__(256) k_courant_reduce(State s, Geom g, Phys ph
        idx += (long long)gridDim.x * blockDim.x) {
     const int j = jlo + (int)(idx / n);
     const long long p = (long long)j * n + idx % n;
+    const double v1 = (double)U1[p], v2 = (double)U2[p], v3 = (double)U3[p];
     double dx, dyv, dz;
     if (ph.front) {
-      dx = ctl.cfl * ph.dx / fabs(s.u1[p] - ph.dthdz * g.gyf[j] / f);
-      dyv = ctl.cfl * g.dy[j] / fabs(s.u2[p]);
-      dz = ctl.cfl * ph.dz / fabs(s.u3[p] + (1.0 / f) * ph.dthdx * (g.gyf[j] - 0.5 * ph.ly));
+      dx = ctl.cfl * ph.dx / fabs(v1 - ph.dthdz * g.gyf[j] / f);
+      dyv = ctl.cfl * g.dy[j] / fabs(v2);
+      dz = ctl.cfl * ph.dz / fabs(v3 + (1.0 / f) * ph.dthdx * (g.gyf[j] - 0.5 * ph.ly));
     } else {
-      dx = ctl.cfl * ph.dx / fabs(s.u1[p]);
-      dyv = ctl.cfl * g.dy[j] / fabs(s.u2[p]);
-      dz = ctl.cfl * ph.dz / fabs(s.u3[p]);
+      dx = ctl.cfl * ph.dx / fabs(v1);
+      dyv = ctl.cfl * g.dy[j] / fabs(v2);
+      dz = ctl.cfl * ph.dz / fabs(v3);
     }
     dmin = fmin(dmin, fmin(dx, fmin(dyv, dz)));
-    if (!isfinite(s.u1[p]) || !isfinite(s.u2[p]) || !isfinite(s.u3[p])) atomicOr(&sc->flags, 1);
+    if (!isfinite(v1) || !isfinite(v2) || !isfinite(v3)) atomicOr(&sc->flags, 1);
   }
   for (int o = 16; o > 0; o >>= 1) dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
   __shared__ double red[8];
@@ -757,24 +775,31 @@ __global__ void k_bc_vel_post(State s, Geom g, Phys ph) {
 // ---------------------------------------------------------------------------
 // launchers
 
+template <int N, bool LES, typename R>
+static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
+  size_t smem = (size_t)3 * padded(N) * sizeof(typename CplxOf<R>::type);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_products<N, LES, R><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
+}
 template <int N>
 static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les) {
-  size_t smem = (size_t)3 * padded(N) * sizeof(double2);
-  const dim3 grid(g.nz, g.np, 2);
-  if (les) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<N, true><<<grid, 3 * FftShape<N>::T, smem, st>>>(s, g);
+  if (g.prec) {
+    if (les) go_products_t<N, true, float>(g, s, st); else go_products_t<N, false, float>(g, s, st);
   } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<N, false><<<grid, 3 * FftShape<N>::T, smem, st>>>(s, g);
+    if (les) go_products_t<N, true, double>(g, s, st); else go_products_t<N, false, double>(g, s, st);
   }
+}
+template <int N, typename R>
+static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  constexpr int T = FftShape<N>::T;
+  size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zpass_rhs<N, R><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk);
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  constexpr int T = FftShape<N>::T;
-  size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(double2);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zpass_rhs<N><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk);
+  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, st);
+  else go_zpass_t<N, double>(g, ph, s, rk, st);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -805,12 +830,18 @@ cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int r
 }
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
   const size_t smem = (size_t)g.np * TX * sizeof(double);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_thomas<<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
+  if (g.prec) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_thomas<double><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
+  }
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
-  k_courant_reduce<<<148 * 8, 256, 0, st>>>(s, g, ph, ctl);
+  if (g.prec) k_courant_reduce<float><<<148 * 8, 256, 0, st>>>(s, g, ph, ctl);
+  else k_courant_reduce<double><<<148 * 8, 256, 0, st>>>(s, g, ph, ctl);
   k_courant_final<<<1, 1, 0, st>>>(s.sc, ph, ctl);
   return cudaGetLastError();
 }

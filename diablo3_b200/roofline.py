@@ -1,9 +1,10 @@
-"""Algorithmic HBM bytes of the FP64 substep, per stage (one place).
+"""Algorithmic HBM bytes of the substep, per stage (one place).
 
 Units per wall-normal plane set (Nyp+2 planes, ghosts included):
-  P  = Nx * Nz * 8 B             one physical field
+  P  = Nx * Nz * 8 B             one physical field (4 B on the mixed path)
   Xh = (Nkx+1) * Nz * 16 B       one x-transformed, not z-transformed field
-  S  = (Nkx+1) * (2Nkz+1) * 16 B one dealiased packed spectral field
+                                 (8 B per complex on the mixed path)
+  S  = (Nkx+1) * (2Nkz+1) * 16 B one dealiased packed spectral field (always FP64)
 Each stage counts the bytes it must read and write once when everything
 inside it is fused (neighbour planes in y are L2 hits):
 
@@ -19,6 +20,13 @@ inside it is fused (neighbour planes in y are L2 hits):
   fwd_z      4 Xh -> 4 S
   rem_div    4 S  -> 4 S            cu1, cu2, cu3, cp in and out
 At 512x257x512 this is ~67 P, i.e. ~540 B per grid point and substep.
+
+With the LES model (les_model_type 5) the stages change to
+  inv_z      4 S  -> 8 Xh           state and its z-derivatives
+  inv_x      8 Xh -> 12 P           state, x- and z-derivatives
+  products   12 P -> 11 P (AMD: nu_t, kappa_t, 9 SGS forcing fields),
+             then 4 P + 9 P -> 8 Xh
+  thomas     per equation r, u, nu in, u out: 16 P
 """
 from __future__ import annotations
 
@@ -29,9 +37,10 @@ import re
 def units(p) -> dict:
     nplanes = p.ny + 2
     nkx, nkz = p.nx // 3, p.nz // 3
+    w = 4 if getattr(p, "precision", 0) else 8
     return {
-        "P": p.nx * p.nz * 8 * nplanes,
-        "Xh": (nkx + 1) * p.nz * 16 * nplanes,
+        "P": p.nx * p.nz * w * nplanes,
+        "Xh": (nkx + 1) * p.nz * 2 * w * nplanes,
         "S": (nkx + 1) * (2 * nkz + 1) * 16 * nplanes,
     }
 
@@ -40,13 +49,14 @@ def stage_bytes(p) -> dict:
     u = units(p)
     P, X, S = u["P"], u["Xh"], u["S"]
     cour = (3 * P / 3.0) if p.variable_dt else 0.0
+    les = bool(getattr(p, "use_les", 0))
     return {
-        "inv_z": 4 * S + 4 * X,
-        "inv_x": 4 * X + 4 * P,
-        "products": 4 * P + 8 * X,
+        "inv_z": 4 * S + (8 if les else 4) * X,
+        "inv_x": (8 * X + 12 * P) if les else (4 * X + 4 * P),
+        "products": (23 * P + 13 * P + 8 * X) if les else (4 * P + 8 * X),
         "zpass_rhs": 8 * X + 9 * S + 4 * S + 4 * X,
         "inv_x_r": 4 * X + 4 * P,
-        "thomas": 12 * P,
+        "thomas": 16 * P if les else 12 * P,
         "courant": cour,
         "fwd_x": 4 * P + 4 * X,
         "fwd_z": 4 * X + 4 * S,

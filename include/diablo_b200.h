@@ -91,7 +91,11 @@ typedef struct db_params {
   double dthdx_override;
   /* run control used by courant's next-event scheduling (flow.f90:825) */
   double time_limit, save_stats_dt, save_flow_dt;
-  int32_t precision;               /* 0 = FP64 throughout (plain path) */
+  /* 0 = FP64 throughout (plain path); 1 = mixed: transforms, nonlinear
+   * products and the SGS model in FP32 (physical and x-half fields stored
+   * FP32), the spectral state, the CN tridiagonal solves, the Poisson solve /
+   * divergence removal and diagnostics in FP64 */
+  int32_t precision;
   int32_t reserved_i[7];
 } db_params;
 
