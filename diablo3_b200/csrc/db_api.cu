@@ -84,7 +84,6 @@ static int validate(const db_params* p, std::string& why) {
     why = "LES: only les_model_type 5 (AMD) is built";
     return DB_ERR_UNSUPPORTED;
   }
-  if (p->use_les && p->ny + 2 > 900) { why = "LES: ny + 2 must be <= 900 (per-column Thomas tile)"; return DB_ERR_SIZE; }
   if (p->precision != 0 && p->precision != 1) {
     why = "precision must be 0 (FP64) or 1 (mixed: FP32 transforms, products and SGS)";
     return DB_ERR_ARG;
@@ -246,7 +245,7 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
     for (int i = 0; i < 19; ++i)
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
-    if (p->precision && (rc = dalloc(c, &s.tscr, Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = dalloc(c, &s.tscr, 2 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   }
   if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
   if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
@@ -594,7 +593,8 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   // inverse z of cr
   if ((e = launch_products(g, s, st, les))) return e;
   mark(c, rk, 3);
-  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st))) return e;
+  const double2* ov = les ? s.ghost : nullptr;   // ghost rows the transforms saw
+  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov))) return e;
   mark(c, rk, 4);
   // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
   if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
@@ -616,9 +616,14 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   }
   mark(c, rk, 7);
   // back to Fourier space (solver.f90:1247-1252) and projection
-  if ((e = launch_fwd_x(g, fset(s.u1, s.u2, s.u3, s.th), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
+  // mixed path: the solve left u's increment in r; transform it and add it
+  // to the state the substep started from
+  const bool inc = c->p.precision != 0;
+  const FieldSet src = inc ? fset(s.r1, s.r2, s.r3, s.rth) : fset(s.u1, s.u2, s.u3, s.th);
+  if ((e = launch_fwd_x(g, src, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
   mark(c, rk, 8);
-  if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st))) return e;
+  if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st,
+                        inc ? 1 : 0, ov))) return e;
   mark(c, rk, 9);
   if ((e = launch_rem_div(g, s, rk, 1, st))) return e;
   if (rk == 2 && c->p.variable_dt) {

@@ -49,7 +49,10 @@ inline FieldSet fset(void* a = nullptr, void* b = nullptr, void* c = nullptr, vo
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
 // dmask: bit f set -> field f is differentiated (x: i kx, z: i kz) on the way
 cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0);
-cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st);
+// accumulate: out += transform, with rows 0, 1, Nyp, Nyp+1 based on ghost
+// (when given) instead of out
+cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, int accumulate = 0,
+                         const double2* ghost = nullptr);
 // ghost (optional): rows 0, 1, Nyp, Nyp+1 of field f are read from
 // ghost + (4 (f % 4) + q) sp instead (q = 0..3 for those rows)
 cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0,
@@ -101,12 +104,14 @@ struct State {
   double* les[9];                            // SGS forcing per product slot (k_les.cu)
   double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
-  double* tscr;                              // FP64 Thomas scratch, one field (mixed LES only)
+  double* tscr;                              // FP64 Thomas scratch, two fields (LES)
 };
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
 cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les = false);
-cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
+// ghost: the LES overlay, when the inverse transforms of this substep used it
+cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
+                             const double2* ghost = nullptr);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st);
 

@@ -109,9 +109,12 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet 
   }
 }
 
-// Xh -> packed spectral (FP64), scaled by 1/Nz; sequence = one kx column of a plane
+// Xh -> packed spectral (FP64), scaled by 1/Nz; sequence = one kx column of a plane.
+// accumulate: out = base + transform, base = out itself, or for rows 0, 1,
+// Nyp, Nyp+1 the ghost overlay (field f % 4) when one is given
 template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet out, Geom g, int accumulate,
+                                                          const double2* __restrict__ ghost) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -130,12 +133,21 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet 
   fft_reg<N, -1>(v, lane, active, sq, tw);
   if (!active) return;
   double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
+  const double2* base = dst;
+  if (accumulate && ghost) {
+    const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
+    if (qg >= 0) base = ghost + (long long)(4 * (f & 3) + qg) * g.sp + kx;
+  }
   const double s = 1.0 / (double)N;
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     const int z = lane + q * T;
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
-    if (kzp >= 0) dst[(long long)kzp * g.kxs] = cscale(to_d2(v[q]), s);
+    if (kzp >= 0) {
+      double2 w = cscale(to_d2(v[q]), s);
+      if (accumulate) w = cadd(base[(long long)kzp * g.kxs], w);
+      dst[(long long)kzp * g.kxs] = w;
+    }
   }
 }
 
@@ -227,12 +239,13 @@ static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   k_inv_x<N, R><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask);
 }
 template <int N, typename R>
-static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, const double2* ghost,
+                       cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   constexpr int ns = seqs_per_cta<N>();
   size_t smem = (size_t)ns * padded(N) * sizeof(C);
   smem_attr(k_fwd_z<N, R>, smem);
-  k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g);
+  k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, acc, ghost);
 }
 template <int N, typename R>
 static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
@@ -254,9 +267,10 @@ static void go_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned 
   else go_inv_x_t<N, double>(g, in, out, nf, dmask, st);
 }
 template <int N>
-static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  if (g.prec) go_fwd_z_t<N, float>(g, in, out, nf, st);
-  else go_fwd_z_t<N, double>(g, in, out, nf, st);
+static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, const double2* ghost,
+                     cudaStream_t st) {
+  if (g.prec) go_fwd_z_t<N, float>(g, in, out, nf, acc, ghost, st);
+  else go_fwd_z_t<N, double>(g, in, out, nf, acc, ghost, st);
 }
 template <int N>
 static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
@@ -275,9 +289,10 @@ cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
   DB_DISPATCH_N(g.nx, go_inv_x, g, in, out, nf, dmask, st);
   return cudaGetLastError();
 }
-cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, int accumulate,
+                         const double2* ghost) {
   if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
-  DB_DISPATCH_N(g.nz, go_fwd_z, g, in, out, nf, st);
+  DB_DISPATCH_N(g.nz, go_fwd_z, g, in, out, nf, accumulate, ghost, st);
   return cudaGetLastError();
 }
 cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask,

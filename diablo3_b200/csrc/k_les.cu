@@ -26,9 +26,8 @@
 //                 explicit term and the matrix (solver.f90:872-903, 988-1003,
 //                 1028-1045, 1088-1105, 1144-1161, 1200-1217): the matrix
 //                 differs per (x, z) column, so each thread runs its own
-//                 Thomas sweep, the eliminated upper coefficients in shared
-//                 memory and the eliminated right-hand side (FP64) in the r
-//                 array, or in an FP64 scratch when r is FP32.
+//                 Thomas sweep, with an FP64 scratch for the eliminated
+//                 coefficients and batched row loads.
 #include <math.h>
 
 #include "db_bc.cuh"
@@ -252,71 +251,101 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
 }
 
 // ---------------------------------------------------------------------------
-// CN solves with eddy viscosity (one Thomas sweep per thread and column);
-// FP64 arithmetic, fields stored as R
-constexpr int TL = 32;
+// CN solves with eddy viscosity: one thread per (x, z) column runs the
+// Thomas sweeps of the four equations (FP64 arithmetic, fields stored as R).
+// The matrix differs per column, so nothing is shared: the eliminated upper
+// coefficients u_j / b'_j and right-hand side g_j / b'_j go to an FP64
+// scratch (2 fields) and come back in the backward sweep.  Rows are handled
+// in batches of TB whose loads are all issued first, so each thread keeps
+// 3 TB loads in flight instead of waiting on every row.
+constexpr int TB = 8;
 
 template <typename R>
-__global__ void __launch_bounds__(TL) k_thomas_les(State s, Geom g, int rk) {
-  extern __shared__ double cm[];      // [np][TL]: u_j / b'_j
-  const int lane = threadIdx.x;
-  const int x = blockIdx.x * TL + lane, z = blockIdx.y;
+__global__ void __launch_bounds__(128) k_thomas_les(State s, Geom g, int rk) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
   const int np = g.np, Nyp = g.ny;
   const long long pp = g.pp, col = (long long)z * g.nx + x;
   const double* dy = g.dy;
   const double* dyf = g.dyf;
   const double temp2 = 0.5 * s.sc->h_bar[rk];
+  double* cmv = s.tscr + col;                        // u_j / b'_j
+  double* gsv = s.tscr + (long long)np * pp + col;   // g_j / b'_j
+  constexpr bool INC = sizeof(R) == sizeof(float);   // r holds increments over u
   for (int eq = 0; eq < 4; ++eq) {
     const TriRow* Rw = s.tri + eq * np;
     R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
     R* r = (R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
     const R* nv = (const R*)((eq == 0) ? s.kappa_t : s.nu_t) + col;
-    // eliminated right-hand side, FP64: in r itself, or in the FP64 scratch
-    // when r is FP32
-    double* gs = (sizeof(R) == sizeof(double)) ? reinterpret_cast<double*>(r) : s.tscr + col;
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
     double um = 0.0, uc = (double)u[0], nm = 0.0, nc = (double)nv[0];
     double bprev = 1.0, gprev = 0.0, uprev = 0.0;
-    for (int j = 0; j < np; ++j) {
-      const TriRow row = Rw[j];
-      const double un = (j + 1 < np) ? (double)u[(long long)(j + 1) * pp] : 0.0;
-      const double nn = (j + 1 < np) ? (double)nv[(long long)(j + 1) * pp] : 0.0;
-      double l = row.l, d = row.d, uu = row.u, v = row.bc;
-      if (!row.is_bc) {
-        v = (double)r[(long long)j * pp] + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
-        double lo_c, hi_c;
-        if (eq != 1) {    // nu_t / kappa_t at GY rows j, j + 1
-          v += temp2 * ((nn * (un - uc) / dy[j + 1] - nc * (uc - um) / dy[j]) / dyf[j]);
-          lo_c = nc / (dy[j] * dyf[j]);
-          hi_c = nn / (dy[j + 1] * dyf[j]);
-        } else {          // interpolated to the GYF rows around u2's GY row
-          v += temp2 * (((0.5 * (nc + nn)) * (un - uc) / dyf[j] - 0.5 * (nc + nm) * (uc - um) / dyf[j - 1]) / dy[j]);
-          lo_c = 0.5 * (nc + nm) / (dyf[j - 1] * dy[j]);
-          hi_c = 0.5 * (nc + nn) / (dyf[j] * dy[j]);
+    for (int jb = 0; jb < np; jb += TB) {
+      double xr[TB], xu[TB], xn[TB];
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jb + c;
+        xr[c] = (j < np) ? (double)r[(long long)j * pp] : 0.0;
+        xu[c] = (j + 1 < np) ? (double)u[(long long)(j + 1) * pp] : 0.0;
+        xn[c] = (j + 1 < np) ? (double)nv[(long long)(j + 1) * pp] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jb + c;
+        if (j >= np) break;
+        const TriRow row = Rw[j];
+        const double un = xu[c], nn = xn[c];
+        double l = row.l, d = row.d, uu = row.u, v = row.bc;
+        if (!row.is_bc) {
+          v = (INC ? xr[c] + uc : xr[c]) + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
+          double lo_c, hi_c;
+          if (eq != 1) {    // nu_t / kappa_t at GY rows j, j + 1
+            v += temp2 * ((nn * (un - uc) / dy[j + 1] - nc * (uc - um) / dy[j]) / dyf[j]);
+            lo_c = nc / (dy[j] * dyf[j]);
+            hi_c = nn / (dy[j + 1] * dyf[j]);
+          } else {          // interpolated to the GYF rows around u2's GY row
+            v += temp2 * (((0.5 * (nc + nn)) * (un - uc) / dyf[j] - 0.5 * (nc + nm) * (uc - um) / dyf[j - 1]) / dy[j]);
+            lo_c = 0.5 * (nc + nm) / (dyf[j - 1] * dy[j]);
+            hi_c = 0.5 * (nc + nn) / (dyf[j] * dy[j]);
+          }
+          l = l - temp2 * lo_c;
+          d = d + temp2 * hi_c + temp2 * lo_c;
+          uu = uu - temp2 * hi_c;
         }
-        l = l - temp2 * lo_c;
-        d = d + temp2 * hi_c + temp2 * lo_c;
-        uu = uu - temp2 * hi_c;
+        double b = d, gg = v;
+        if (j > 0) {
+          const double a = -l / bprev;
+          b = d + a * uprev;
+          gg = v + a * gprev;
+        }
+        const double ib = 1.0 / b;
+        cmv[(long long)j * pp] = uu * ib;
+        gsv[(long long)j * pp] = gg * ib;
+        bprev = b; gprev = gg; uprev = uu;
+        um = uc; uc = un; nm = nc; nc = nn;
       }
-      double b = d, gg = v;
-      if (j > 0) {
-        const double a = -l / bprev;
-        b = d + a * uprev;
-        gg = v + a * gprev;
-      }
-      const double ib = 1.0 / b;
-      cm[j * TL + lane] = uu * ib;
-      gs[(long long)j * pp] = gg * ib;
-      bprev = b; gprev = gg; uprev = uu;
-      um = uc; uc = un; nm = nc; nc = nn;
     }
-    double xn = 0.0;
-    for (int j = np - 1; j >= 0; --j) {
-      const double xv = gs[(long long)j * pp] - cm[j * TL + lane] * xn;
-      if (j >= lo && j <= hi) u[(long long)j * pp] = (R)xv;
-      xn = xv;
+    double xnext = 0.0;
+    for (int jt = np - 1; jt >= 0; jt -= TB) {
+      double xc[TB], xg[TB], xo[TB];
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jt - c;
+        xc[c] = (j >= 0) ? cmv[(long long)j * pp] : 0.0;
+        xg[c] = (j >= 0) ? gsv[(long long)j * pp] : 0.0;
+        xo[c] = (INC && j >= 0) ? (double)u[(long long)j * pp] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jt - c;
+        if (j < 0) break;
+        const double xv = xg[c] - xc[c] * xnext;
+        const bool stored = (j >= lo && j <= hi);
+        if (stored) u[(long long)j * pp] = (R)xv;
+        if (INC) r[(long long)j * pp] = stored ? (R)(xv - xo[c]) : (R)0;   // increment for the transform
+        xnext = xv;
+      }
     }
   }
 }
@@ -333,15 +362,9 @@ cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaSt
   return cudaGetLastError();
 }
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
-  const size_t smem = (size_t)g.np * TL * sizeof(double);
-  if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  if (g.prec) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_thomas_les<float><<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
-  } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas_les<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_thomas_les<double><<<dim3((g.nx + TL - 1) / TL, g.nz), TL, smem, st>>>(s, g, rk);
-  }
+  const int bx = g.nx < 128 ? g.nx : 128;
+  if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
+  else k_thomas_les<double><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
   return cudaGetLastError();
 }
 

@@ -170,7 +170,12 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
 template <int N, typename R>
-__global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1)) k_zpass_rhs(State s, Geom g, Phys ph, int rk) {
+__global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1))
+    k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost) {
+  // FP32 work type: write the increment cr - base (base = the state as the
+  // inverse transforms saw it), so FP32 rounding scales with the substep's
+  // change, not with the field
+  constexpr bool INC = sizeof(R) == sizeof(float);
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       const long long a = sp0 + (long long)kzp * g.kxs;
       const double k2 = kxv * kxv + kzv * kzv;
       const double kk = beta1 ? k2 : pow(k2, ph.beta);
-      double2 cf, cr;
+      double2 cf, cr, cuf;
       if (e == 0 || e == 1) {
         const double2 cu1 = s.cu1[a], cu3 = s.cu3[a], cth = s.cth[a], cp = s.cp[a];
         const double2 c2a = s.cu2[a], c2b = s.cu2[a + g.sp];
@@ -268,7 +273,8 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
         }
         cf = csub(cf, nl);
         const double kd = (e == 0) ? kxv : kzv;
-        cr = cu;
+        cuf = cu;
+        cr = INC ? make_double2(0.0, 0.0) : cu;
         if (rk > 0) cr = cadd(cr, cscale((e == 0) ? s.cf1[a] : s.cf3[a], temp3));
         cr = csub(cr, cscale(cmul_i(cp, 1.0), temp4 * kd));
         if (e == 0 && kx == 0 && kzp == 0) {
@@ -293,7 +299,8 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
           cf = csub(cf, cscale(t1, -1.0 * ph.dthdz * y * tw * kxv));
         }
         cf = csub(cf, nl);
-        cr = cu2;
+        cuf = cu2;
+        cr = INC ? make_double2(0.0, 0.0) : cu2;
         if (rk > 0) cr = cadd(cr, cscale(s.cf2[a], temp3));
         const double2 dp = csub(s.cp[a], s.cp[a - g.sp]);
         cr = csub(cr, cscale(dp, temp4 / g.dy[j]));
@@ -311,10 +318,19 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
           cf = csub(cf, cscale(t1, tw * (-1.0) * ph.dthdz * y * kxv));
         }
         cf = csub(cf, nl);
-        cr = cth;
+        cuf = cth;
+        cr = INC ? make_double2(0.0, 0.0) : cth;
         if (rk > 0) cr = cadd(cr, cscale(s.cfth[a], temp3));
         cr = cadd(cr, cscale(cf, temp5));
         s.cfth[a] = cf;
+      }
+      if (INC && ghost) {   // ghost rows: base is the overlay, cr - base = (cu - base) + increment
+        const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
+        if (qg >= 0) {
+          const int gf = (e == 0) ? 0 : (e == 1 ? 2 : (e == 2 ? 1 : 3));
+          const double2 base = ghost[(long long)(4 * gf + qg) * g.sp + (long long)kzp * g.kxs + kxc];
+          cr = cadd(cr, csub(cuf, base));
+        }
       }
       vn[q] = from_d2<C>(cr);
     }
@@ -496,7 +512,9 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
           if (j > j1) break;
           const TriRow* row = Rw + j;
           const double un = xu[c];
-          const double v = row->is_bc ? row->bc : xr[c] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+          // FP32 work type: r holds the increment over u (k_zpass_rhs)
+          const double rj = (sizeof(R) == sizeof(float)) ? xr[c] + uc : xr[c];
+          const double v = row->is_bc ? row->bc : rj + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
           y = (j == j0) ? v : v + row->ap * y;
           tile[j * TX + lane] = y;
           um = uc;
@@ -545,9 +563,36 @@ __global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
     // 5. apply carries and write the rows the reference stores
     if (active && xin) {
       const double c = (w < ch.nch - 1) ? carry[w + 1][lane] : 0.0;
-      for (int j = j0; j <= j1; ++j) {
-        const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
-        if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
+      if (sizeof(R) == sizeof(float)) {
+        // new u for courant, and its increment (into r) for the forward
+        // transform; rows the solve does not store keep u, increment 0.
+        // The old u of a batch of rows is loaded before any of them is written.
+        R* rr = const_cast<R*>(r);
+        for (int jb = j0; jb <= j1; jb += 8) {
+          R uo[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int j = jb + q;
+            uo[q] = (j <= j1) ? u[(long long)j * pp + col] : (R)0;
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int j = jb + q;
+            if (j > j1) break;
+            const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
+            if (j >= lo && j <= hi) {
+              u[(long long)j * pp + col] = (R)xv;
+              rr[(long long)j * pp + col] = (R)(xv - (double)uo[q]);
+            } else {
+              rr[(long long)j * pp + col] = (R)0;
+            }
+          }
+        }
+      } else {
+        for (int j = j0; j <= j1; ++j) {
+          const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
+          if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
+        }
       }
     }
     __syncthreads();
@@ -790,16 +835,16 @@ static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les
   }
 }
 template <int N, typename R>
-static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
   constexpr int T = FftShape<N>::T;
   size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zpass_rhs<N, R><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk);
+  k_zpass_rhs<N, R><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk, ghost);
 }
 template <int N>
-static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, st);
-  else go_zpass_t<N, double>(g, ph, s, rk, st);
+static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
+  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, st);
+  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, st);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -818,8 +863,9 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
   DB_DISPATCH_N2(g.nx, go_products, g, s, st, les);
   return cudaGetLastError();
 }
-cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, st);
+cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
+                             const double2* ghost) {
+  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, st);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
