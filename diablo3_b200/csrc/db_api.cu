@@ -246,6 +246,9 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.tscr, 2 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    LesRow* lr = nullptr;
+    if ((rc = dalloc(c, &lr, (size_t)np))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    s.lrow = lr;
   }
   if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
   if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
@@ -274,6 +277,34 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
     return DB_ERR_CUDA;
   }
   g.gy = c->d_tab; g.gyf = c->d_tab + np; g.dy = c->d_tab + 2 * np; g.dyf = c->d_tab + 3 * np;
+  if (p->use_les) {   // AMD per-row constants (les.f90:756-780, 1213-1222)
+    const double dxs = ph.dx * 3.0, dzs = ph.dz * 3.0, C = 0.2887;
+    auto dcoef = [&](double h) {
+      return -2.0 * C * C * 3.0 / (1.0 / (dxs * dxs) + 1.0 / ((h * 2.0) * (h * 2.0)) + 1.0 / (dzs * dzs));
+    };
+    std::vector<LesRow> rows(np);
+    for (int j = 0; j < np; ++j) {
+      LesRow& r = rows[j];
+      memset(&r, 0, sizeof(r));
+      const double dyj = c->dy[j], dyfj = c->dyf[j];
+      r.idy = dyj != 0.0 ? 1.0 / dyj : 0.0;
+      r.idyf = dyfj != 0.0 ? 1.0 / dyfj : 0.0;
+      r.dgy = dyj != 0.0 ? dcoef(dyj) : 0.0;
+      r.dgyf = dcoef(dyfj);
+      const double dly = 2.0 * dyj;
+      r.ryx = dly / dxs; r.rxy = dly != 0.0 ? dxs / dly : 0.0;
+      r.rzy = dly != 0.0 ? dzs / dly : 0.0; r.ryz = dly / dzs;
+      r.wa = (j >= 1 && dyj != 0.0) ? c->dyf[j - 1] / (2.0 * dyj) : 0.0;
+      r.wb = dyj != 0.0 ? dyfj / (2.0 * dyj) : 0.0;
+      r.dys_f = 2.0 * dyfj;
+      r.dys_y = dly;
+    }
+    if (cudaMemcpy((void*)s.lrow, rows.data(), np * sizeof(LesRow), cudaMemcpyHostToDevice) != cudaSuccess) {
+      db_finalize(c);
+      g_init_err = "db_init: LES table upload failed";
+      return DB_ERR_CUDA;
+    }
+  }
   g.kx = c->d_tab + 4 * np; g.kz = c->d_tab + 4 * np + g.kxs;
   g.twx = c->d_tw; g.twz = c->d_tw + Nx;
   g.twxf = c->d_twf; g.twzf = c->d_twf + Nx;

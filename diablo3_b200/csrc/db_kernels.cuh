@@ -68,8 +68,26 @@ struct TriRow {
   double cn_lo, cn_hi;  // explicit CN: term = cn_hi*(u_{j+1}-u_j) - cn_lo*(u_j-u_{j-1})
   double pa;      // prod of a'_i from the start of j's chunk to j (forward carry weight)
   double pm;      // prod of m_i = -u_i / b'_i from j to the end of its chunk (backward)
+  // eddy-viscosity metric factors of the row (LES): the lower / upper
+  // coupling is nu_lo * ef_lo, nu_hi * ef_hi (per-column nu), with
+  // ef = 1/(dy dyf) at the neighbouring GY / GYF spacing
+  double ef_lo, ef_hi;
   int is_bc, interior;
   int pad[2];
+};
+
+// Per-row constants of the AMD model (k_les_amd), host-computed once:
+// reciprocals of the spacings, the filter coefficients -2 C^2 Delta^2 at GY
+// and GYF rows, the filter-width ratios at GY rows and the GYF -> GY
+// interpolation weights (A(j) dyf(j-1) + A(j-1) dyf(j)) / (2 dy(j)).
+struct LesRow {
+  double idy, idyf;        // 1/dy(j), 1/dyf(j)
+  double dgy, dgyf;        // filter coefficient at GY row j, GYF row j
+  double ryx, rxy;         // (2 dy(j)) / (3 dx), (3 dx) / (2 dy(j))
+  double rzy, ryz;         // (3 dz) / (2 dy(j)), (2 dy(j)) / (3 dz)
+  double wa, wb;           // dyf(j-1) / (2 dy(j)), dyf(j) / (2 dy(j))
+  double dys_f;            // 2 dyf(j)  (GYF-row y filter width)
+  double dys_y;            // 2 dy(j)   (GY-row y filter width)
 };
 
 // row chunks of the tiled Thomas solve (k_thomas): nch chunks of len rows
@@ -105,6 +123,7 @@ struct State {
   double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
   double* tscr;                              // FP64 Thomas scratch, two fields (LES)
+  const LesRow* lrow;                        // np rows (LES)
 };
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products

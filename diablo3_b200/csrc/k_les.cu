@@ -124,7 +124,7 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 // rows = temp (S12 - du1/dy / 2) for j >= 2 and the raw strain at j = 1
 // (les.f90:737-748).  R: arithmetic and storage type (FP32 on the mixed path).
 template <typename R>
-__global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
+__global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
   const long long pp = g.pp;
@@ -132,12 +132,11 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
   const int Nyp = g.ny;
   const int jst = g.jstart_th, jet = g.jend_th;
   const int j1 = g.jstart, j2 = Nyp - 1;
-  const R h = 0.5, two = 2;
+  const R h = 0.5;
   const double dxs_d = ph.dx * BETA_SGS, dzs_d = ph.dz * BETA_SGS;
   const R dxs = (R)dxs_d, dzs = (R)dzs_d;
   const R rzx = (R)(dzs_d / dxs_d), rxz = (R)(dxs_d / dzs_d);
-  const double* dy = g.dy;
-  const double* dyf = g.dyf;
+  const LesRow* LR = s.lrow;
   const R* u1 = (const R*)s.u1 + col;
   const R* u2 = (const R*)s.u2 + col;
   const R* u3 = (const R*)s.u3 + col;
@@ -156,7 +155,7 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
   R u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
   R f1x = __ldg(g1x), f3z = __ldg(g3z), f1z = __ldg(g1z), f3x = __ldg(g3x);
   R ftx = __ldg(gtx), ftz = __ldg(gtz);
-  R f2y = (u2c - __ldg(u2)) / (R)dyf[0];
+  R f2y = (u2c - __ldg(u2)) * (R)LR[0].idyf;
   // previous GY row (r = j - 1) values
   R h1y = 0, h3y = 0, hty = 0, h2x = 0, h2z = 0;
   R hSI4 = 0, hSI6 = 0, hO4 = 0, hO6 = 0, hP4 = 0, hP6 = 0, hdl = 0;
@@ -171,22 +170,24 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
     const R u2n = (j + 1 <= Nyp + 1) ? __ldg(u2 + oj + pp) : (R)0;
     const R a1x = __ldg(g1x + oj), a2x = __ldg(g2x + oj), a3x = __ldg(g3x + oj), atx = __ldg(gtx + oj);
     const R a1z = __ldg(g1z + oj), a2z = __ldg(g2z + oj), a3z = __ldg(g3z + oj), atz = __ldg(gtz + oj);
-    const R dyj = (R)dy[j], dyfj = (R)dyf[j], dyfm = (R)dyf[j - 1];
+    const LesRow lr = LR[j];
+    const R idy = (R)lr.idy;
     // GY row j: y-derivatives and the tensors that live there
-    const R d1y = (u1j - u1m) / dyj, d3y = (u3j - u3m) / dyj, dty = (thj - thm) / dyj;
-    const R dly = dyj * two;
-    const R SI4 = h * (d1y * (dly / dxs) + a2x * (dxs / dly));
-    const R SI6 = h * (a2z * (dzs / dly) + d3y * (dly / dzs));
-    const R O4 = h * (d1y * (dly / dxs) - a2x * (dxs / dly));
-    const R O6 = h * (a2z * (dzs / dly) - d3y * (dly / dzs));
+    const R d1y = (u1j - u1m) * idy, d3y = (u3j - u3m) * idy, dty = (thj - thm) * idy;
+    const R dly = (R)lr.dys_y;
+    const R ryx = (R)lr.ryx, rxy = (R)lr.rxy, rzy = (R)lr.rzy, ryz = (R)lr.ryz;
+    const R SI4 = h * (d1y * ryx + a2x * rxy);
+    const R SI6 = h * (a2z * rzy + d3y * ryz);
+    const R O4 = h * (d1y * ryx - a2x * rxy);
+    const R O6 = h * (a2z * rzy - d3y * ryz);
     const R S4 = h * (d1y + a2x), S6 = h * (a2z + d3y);
     // GYF row j (d u2/dy there needs u2 at j + 1; row Nyp + 1 is unused)
-    const R c2y = (j <= Nyp) ? (u2n - u2c) / dyfj : (R)0;
-    const R delt = (R)amd_delta(dxs_d, dzs_d, dy[j]);
+    const R c2y = (j <= Nyp) ? (u2n - u2c) * (R)lr.idyf : (R)0;
+    const R delt = (R)lr.dgy;
     R temp = 0, temp_th = 0;
     if (j >= 2 && j <= Nyp) {
-      const R w = two * dyj;
-#define GYI(A, B) (((A) * dyfm + (B) * dyfj) / w)
+      const R wa = (R)lr.wa, wb = (R)lr.wb;
+#define GYI(A, B) ((A) * wa + (B) * wb)
       const R SI5c = h * (a1z * rzx + a3x * rxz), SI5p = h * (f1z * rzx + f3x * rxz);
       const R O5c = h * (a1z * rzx - a3x * rxz), O5p = h * (f1z * rzx - f3x * rxz);
       temp = amd_ratio<R>(GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), SI4, GYI(SI5c, SI5p), SI6, O4,
@@ -210,8 +211,8 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
     {
       const int r = j - 1;
       const long long orr = (long long)r * pp;
-      const R dyfr = dyfm;
-      const R dlf = (R)amd_delta(dxs_d, dzs_d, dyf[r]);
+      const LesRow lf = LR[r];
+      const R dlf = (R)lf.dgyf, idyfr = (R)lf.idyf;
       R L0 = 0, L1 = 0, L2 = 0, L3 = 0, L4 = 0, L7 = 0, L8 = 0;
       if (r >= j1 && r <= j2) {
         const R s4 = h * (SI4 + hSI4), s6 = h * (SI6 + hSI6);
@@ -221,11 +222,11 @@ __global__ void __launch_bounds__(128) k_les_amd(State s, Geom g, Phys ph) {
         L0 = dlf * (s1 * f1x);
         L2 = dlf * (s1 * (h * (f1z + f3x)));
         L4 = dlf * (s1 * f3z);
-        L1 = (delt * P4 - hdl * hP4) / dyfr;
-        L3 = (delt * P6 - hdl * hP6) / dyfr;
+        L1 = (delt * P4 - hdl * hP4) * idyfr;
+        L3 = (delt * P6 - hdl * hP6) * idyfr;
       }
       if (r >= jst && r <= jet) {
-        const R dys = dyfr * two;
+        const R dys = (R)lf.dys_f;
         const R s1t = amd_th_ratio<R>(dxs, dys, dzs, f1x, f2y, f3z, h * (d1y + h1y), h * (a2x + h2x), f1z, f3x,
                                       h * (a2z + h2z), h * (d3y + h3y), ftx, h * (dty + hty), ftz);
         L7 = h * dlf * (s1t * ftx);
@@ -266,8 +267,6 @@ __global__ void __launch_bounds__(128) k_thomas_les(State s, Geom g, int rk) {
   if (x >= g.nx) return;
   const int np = g.np, Nyp = g.ny;
   const long long pp = g.pp, col = (long long)z * g.nx + x;
-  const double* dy = g.dy;
-  const double* dyf = g.dyf;
   const double temp2 = 0.5 * s.sc->h_bar[rk];
   double* cmv = s.tscr + col;                        // u_j / b'_j
   double* gsv = s.tscr + (long long)np * pp + col;   // g_j / b'_j
@@ -280,7 +279,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(State s, Geom g, int rk) {
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
     double um = 0.0, uc = (double)u[0], nm = 0.0, nc = (double)nv[0];
-    double bprev = 1.0, gprev = 0.0, uprev = 0.0;
+    double ibprev = 1.0, gprev = 0.0, uprev = 0.0;
     for (int jb = 0; jb < np; jb += TB) {
       double xr[TB], xu[TB], xn[TB];
 #pragma unroll
@@ -298,31 +297,26 @@ __global__ void __launch_bounds__(128) k_thomas_les(State s, Geom g, int rk) {
         const double un = xu[c], nn = xn[c];
         double l = row.l, d = row.d, uu = row.u, v = row.bc;
         if (!row.is_bc) {
-          v = (INC ? xr[c] + uc : xr[c]) + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um));
-          double lo_c, hi_c;
-          if (eq != 1) {    // nu_t / kappa_t at GY rows j, j + 1
-            v += temp2 * ((nn * (un - uc) / dy[j + 1] - nc * (uc - um) / dy[j]) / dyf[j]);
-            lo_c = nc / (dy[j] * dyf[j]);
-            hi_c = nn / (dy[j + 1] * dyf[j]);
-          } else {          // interpolated to the GYF rows around u2's GY row
-            v += temp2 * (((0.5 * (nc + nn)) * (un - uc) / dyf[j] - 0.5 * (nc + nm) * (uc - um) / dyf[j - 1]) / dy[j]);
-            lo_c = 0.5 * (nc + nm) / (dyf[j - 1] * dy[j]);
-            hi_c = 0.5 * (nc + nn) / (dyf[j] * dy[j]);
-          }
+          // eddy coupling to the rows below / above: nu_t (kappa_t) at GY
+          // rows j, j+1, or for u2 averaged to the GYF rows around GY row j
+          const double lo_c = (eq != 1 ? nc : nc + nm) * row.ef_lo;
+          const double hi_c = (eq != 1 ? nn : nc + nn) * row.ef_hi;
+          v = (INC ? xr[c] + uc : xr[c]) + (row.cn_hi * (un - uc) - row.cn_lo * (uc - um)) +
+              temp2 * (hi_c * (un - uc) - lo_c * (uc - um));
           l = l - temp2 * lo_c;
           d = d + temp2 * hi_c + temp2 * lo_c;
           uu = uu - temp2 * hi_c;
         }
         double b = d, gg = v;
         if (j > 0) {
-          const double a = -l / bprev;
+          const double a = -l * ibprev;
           b = d + a * uprev;
           gg = v + a * gprev;
         }
         const double ib = 1.0 / b;
         cmv[(long long)j * pp] = uu * ib;
         gsv[(long long)j * pp] = gg * ib;
-        bprev = b; gprev = gg; uprev = uu;
+        ibprev = ib; gprev = gg; uprev = uu;
         um = uc; uc = un; nm = nc; nc = nn;
       }
     }

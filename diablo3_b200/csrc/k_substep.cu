@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
   for (int j = threadIdx.x; j < np; j += blockDim.x) {
     TriRow r;
     r.l = 0.0; r.d = 1.0; r.u = 0.0; r.bc = 0.0; r.ap = 0.0; r.ibp = 1.0;
-    r.cn_lo = 0.0; r.cn_hi = 0.0; r.pa = 1.0; r.pm = 1.0;
+    r.cn_lo = 0.0; r.cn_hi = 0.0; r.pa = 1.0; r.pm = 1.0; r.ef_lo = 0.0; r.ef_hi = 0.0;
     r.is_bc = 1; r.interior = 0; r.pad[0] = r.pad[1] = 0;
     if (j >= lo && j <= hi) {
       if (eq == 0) {  // solver.f90:1023-1026
@@ -369,18 +369,24 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
         r.u = -(tth) / (dy[j + 1] * dyf[j]);
         r.cn_hi = (tth) / dyf[j] / dy[j + 1];
         r.cn_lo = (tth) / dyf[j] / dy[j];
+        r.ef_lo = 1.0 / (dy[j] * dyf[j]);
+        r.ef_hi = 1.0 / (dy[j + 1] * dyf[j]);
       } else if (eq == 1) {  // solver.f90:1085-1088
         r.l = -tv / (dyf[j - 1] * dy[j]);
         r.d = 1. + tv / (dyf[j] * dy[j]) + tv / (dyf[j - 1] * dy[j]);
         r.u = -tv / (dyf[j] * dy[j]);
         r.cn_hi = tv / dy[j] / dyf[j];
         r.cn_lo = tv / dy[j] / dyf[j - 1];
+        r.ef_lo = 0.5 / (dyf[j - 1] * dy[j]);   // times nu(j) + nu(j-1)
+        r.ef_hi = 0.5 / (dyf[j] * dy[j]);       // times nu(j) + nu(j+1)
       } else {        // solver.f90:1140-1143, 1196-1199
         r.l = -tv / (dy[j] * dyf[j]);
         r.d = 1. - tv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
         r.u = -tv / (dy[j + 1] * dyf[j]);
         r.cn_hi = tv / dyf[j] / dy[j + 1];
         r.cn_lo = tv / dyf[j] / dy[j];
+        r.ef_lo = 1.0 / (dy[j] * dyf[j]);
+        r.ef_hi = 1.0 / (dy[j + 1] * dyf[j]);
       }
       r.is_bc = 0;
       r.interior = 1;
