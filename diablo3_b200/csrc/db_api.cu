@@ -17,6 +17,7 @@ using namespace db;
 
 struct db_ctx {
   db_params p;
+  db_sgs_net* sgs = nullptr;     // learned closure (les_model_type 6)
   Geom g;
   Phys ph;
   State s;
@@ -750,6 +751,12 @@ extern "C" int db_stage_times(db_ctx* c, double* ms, int nstages) {
     }
     ms[k] = t;
   }
+  return DB_OK;
+}
+
+extern "C" int db_set_sgs_net(db_ctx* c, db_sgs_net* net) {
+  if (!c) return DB_ERR_ARG;
+  c->sgs = net;
   return DB_OK;
 }
 

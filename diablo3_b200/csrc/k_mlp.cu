@@ -1,0 +1,517 @@
+// k_mlp.cu -- learned SGS closure: a 16 -> 64 -> 64 -> 64 -> 2 MLP (GELU
+// hidden layers, softplus outputs nu_t, kappa_t >= 0) on the 5th-generation
+// tensor cores.  BF16 weights and activations, FP32 accumulation in tensor
+// memory (umma.cuh), FP32 master weights and Adam.
+//
+// One CTA of 128 threads works on tiles of 128 points; thread t owns point
+// (row) t of the tile and reads row t of every accumulator from tensor
+// memory.
+//   forward   X W1^T -> z1 -> h1 = gelu(z1) -> h1 W2^T -> z2 -> ... -> h3,
+//             y = W4 h3 + b4 on CUDA cores (N = 2), out = softplus(y) * scale
+//   backward  (training) dy = dL/dy; dh3 = dy W4, dz3 = dh3 gelu'(z3);
+//             [dW3 | db3] += dz3^T [h2 | 1]   (tensor core, M padded to 128)
+//             dh2 = dz3 W3                     (tensor core)
+//             z2 is recomputed by the tensor core instead of being stored;
+//             likewise down to [dW1 | db1] += dz1^T [x | 1].
+//             dW4, db4 by warp reductions.  The loss is the mean square error
+//             of the scaled outputs against the targets.
+// Gradients are summed over the CTA's tiles in tensor memory and added to a
+// global FP32 buffer once per CTA.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "../../include/diablo_b200.h"
+#include "mlp.cuh"
+#include "umma.cuh"
+
+namespace db {
+
+constexpr int NF = 16, NH = 64, NO = 2, TILE = 128;
+// parameter packing (FP32): W1[64][16] b1 W2[64][64] b2 W3[64][64] b3 W4[2][64] b4
+constexpr int P_W1 = 0, P_B1 = 1024, P_W2 = 1088, P_B2 = 5184, P_W3 = 5248, P_B3 = 9344, P_W4 = 9408,
+              P_B4 = 9536, P_TOTAL = 9538;
+static_assert(P_TOTAL == DB_SGS_NPARAMS, "parameter count");
+
+
+
+// GELU with the exact erf form and its derivative
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+__device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : log1pf(expf(y)); }
+__device__ __forceinline__ float sigm(float y) { return 1.0f / (1.0f + expf(-y)); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat16 x = __float2bfloat16_rn(a), y = __float2bfloat16_rn(b);
+  return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+}
+
+// 8 consecutive K values of one row into a K-major tile (one 16-byte store)
+__device__ __forceinline__ void put8(unsigned char* tile, int row, int k0, int K, const float* v) {
+  uint4 q;
+  q.x = pack_bf16(v[0], v[1]);
+  q.y = pack_bf16(v[2], v[3]);
+  q.z = pack_bf16(v[4], v[5]);
+  q.w = pack_bf16(v[6], v[7]);
+  *reinterpret_cast<uint4*>(tile + kmajor_offset(row, k0, K)) = q;
+}
+__device__ __forceinline__ void put1(unsigned char* tile, int row, int k, int K, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(tile + kmajor_offset(row, k, K)) = __float2bfloat16_rn(v);
+}
+
+// shared-memory plan (bytes); training needs the transposed tiles and the
+// gradient operands, inference only X, H1, H2 and the weights
+template <bool TRAIN>
+struct Plan {
+  static constexpr uint32_t X = 0;                                     // [128][16]
+  static constexpr uint32_t H1 = X + TILE * NF * 2;                    // [128][64]
+  static constexpr uint32_t H2 = H1 + TILE * NH * 2;                   // [128][64]
+  static constexpr uint32_t W1 = H2 + TILE * NH * 2;                   // [64][16]
+  static constexpr uint32_t W2 = W1 + NH * NF * 2;                     // [64][64]
+  static constexpr uint32_t W3 = W2 + NH * NH * 2;                     // [64][64]
+  static constexpr uint32_t XT = W3 + NH * NH * 2;                     // [32][128]: x^T, ones row, zeros
+  static constexpr uint32_t H1T = XT + (TRAIN ? 32 * TILE * 2 : 0);    // [80][128]: h1^T, ones, zeros
+  static constexpr uint32_t H2T = H1T + (TRAIN ? 80 * TILE * 2 : 0);   // [80][128]
+  static constexpr uint32_t DZ = H2T + (TRAIN ? 80 * TILE * 2 : 0);    // [128][64] dz
+  static constexpr uint32_t DZT = DZ + (TRAIN ? TILE * NH * 2 : 0);    // [128][128] dz^T (rows >= 64 zero)
+  static constexpr uint32_t W2T = DZT + (TRAIN ? TILE * TILE * 2 : 0); // [64][64] W2^T
+  static constexpr uint32_t W3T = W2T + (TRAIN ? NH * NH * 2 : 0);     // [64][64] W3^T
+  static constexpr uint32_t RED = W3T + (TRAIN ? NH * NH * 2 : 0);     // dW4, db4 partial sums (floats)
+  static constexpr uint32_t MBAR = RED + (TRAIN ? 136 * 4 : 0);
+  static constexpr uint32_t SLOT = MBAR + 8;
+  static constexpr uint32_t BYTES = SLOT + 8;
+  static constexpr uint32_t TMEM_COLS = TRAIN ? 512 : 64;
+  // tensor-memory columns: z accumulator, dh accumulator, [dW3|db3], [dW2|db2], [dW1|db1]
+  static constexpr uint32_t C_Z = 0, C_H = 64, C_G3 = 128, C_G2 = 256, C_G1 = 384;
+};
+
+constexpr uint32_t WAIT_ITERS = 1u << 22;   // bounded mbarrier waits
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
+  using PL = Plan<TRAIN>;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + PL::MBAR);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + PL::SLOT);
+  const float* P = a.params;
+
+  // ---- weights to shared memory (BF16, K-major), once per CTA
+  for (int r = t; r < NH; r += TILE) {
+    float v[8];
+    for (int k0 = 0; k0 < NF; k0 += 8) {
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W1 + r * NF + k0 + i];
+      put8(sm + PL::W1, r, k0, NF, v);
+    }
+    for (int k0 = 0; k0 < NH; k0 += 8) {
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W2 + r * NH + k0 + i];
+      put8(sm + PL::W2, r, k0, NH, v);
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + r * NH + k0 + i];
+      put8(sm + PL::W3, r, k0, NH, v);
+      if (TRAIN) {   // transposes: row r = input index, K = output index
+        for (int i = 0; i < 8; ++i) v[i] = P[P_W2 + (k0 + i) * NH + r];
+        put8(sm + PL::W2T, r, k0, NH, v);
+        for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + (k0 + i) * NH + r];
+        put8(sm + PL::W3T, r, k0, NH, v);
+      }
+    }
+  }
+  if (TRAIN) {
+    // constant rows of the transposed operands: ones row (bias gradients),
+    // zero padding, and the zero upper half of dz^T
+    for (int m = t; m < TILE; m += TILE) {
+      put1(sm + PL::XT, NF, m, TILE, 1.0f);
+      for (int r = NF + 1; r < 32; ++r) put1(sm + PL::XT, r, m, TILE, 0.0f);
+      put1(sm + PL::H1T, NH, m, TILE, 1.0f);
+      put1(sm + PL::H2T, NH, m, TILE, 1.0f);
+      for (int r = NH + 1; r < 80; ++r) {
+        put1(sm + PL::H1T, r, m, TILE, 0.0f);
+        put1(sm + PL::H2T, r, m, TILE, 0.0f);
+      }
+      for (int r = NH; r < TILE; ++r) put1(sm + PL::DZT, r, m, TILE, 0.0f);
+    }
+    float* red = reinterpret_cast<float*>(sm + PL::RED);
+    for (int i = t; i < 136; i += TILE) red[i] = 0.0f;
+  }
+  if (t == 0) mbar_init(mbar, 1);
+  if (warp == 0) {
+    tmem_alloc(slot, PL::TMEM_COLS);
+    tmem_relinquish();
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);   // this warp's lanes
+  uint32_t phase = 0;
+  bool ok = true;
+
+  const float* mu = a.norm;
+  const float* isd = a.norm + NF;
+  const float osc0 = a.norm[2 * NF], osc1 = a.norm[2 * NF + 1];
+  const uint32_t id64 = umma_idesc_bf16(128, NH), id80 = umma_idesc_bf16(128, 80), id32 = umma_idesc_bf16(128, 32);
+  const uint32_t aX = smem_u32(sm + PL::X), aH1 = smem_u32(sm + PL::H1), aH2 = smem_u32(sm + PL::H2);
+  const uint32_t aW1 = smem_u32(sm + PL::W1), aW2 = smem_u32(sm + PL::W2), aW3 = smem_u32(sm + PL::W3);
+
+  // issue a GEMM D (+)= A B^T over K (steps of 16) by thread 0
+  auto gemm = [&](uint32_t dcol, uint32_t a_addr, uint32_t a_sbo, uint32_t b_addr, uint32_t b_sbo, int K,
+                  uint32_t idesc, bool acc) {
+    for (int s = 0; s < K / 16; ++s)
+      umma_bf16(tbase + dcol, umma_desc(a_addr + 256 * s, 128, a_sbo), umma_desc(b_addr + 256 * s, 128, b_sbo),
+                idesc, acc || s > 0);
+  };
+  // commit, wait, and agree on the outcome
+  auto sync_mma = [&]() -> bool {
+    if (t == 0) umma_commit(mbar);
+    const bool w = mbar_wait(mbar, phase, WAIT_ITERS);
+    phase ^= 1u;
+    tc_fence_after();
+    return __syncthreads_and(w ? 1 : 0) != 0;
+  };
+  // epilogue of a hidden layer: row of z from tensor memory -> h = gelu(z)
+  // into the next A tile (and its transpose when training)
+  auto hidden_out = [&](const float* bias, unsigned char* tileA, unsigned char* tileT) {
+    for (int c = 0; c < NH; c += 16) {
+      float z[16];
+      tmem_ld16(trow + PL::C_Z + c, z);
+      tmem_wait_ld();
+      float h[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) h[i] = gelu(z[i] + bias[c + i]);
+      put8(tileA, t, c, NH, h);
+      put8(tileA, t, c + 8, NH, h + 8);
+      if (TRAIN && tileT) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) put1(tileT, c + i, t, TILE, h[i]);
+      }
+    }
+  };
+
+  __shared__ float sb[3 * NH + NO + NO * NH];   // b1 b2 b3 b4 W4 (FP32)
+  for (int i = t; i < NH; i += TILE) {
+    sb[i] = P[P_B1 + i];
+    sb[NH + i] = P[P_B2 + i];
+    sb[2 * NH + i] = P[P_B3 + i];
+  }
+  for (int i = t; i < NO * NH; i += TILE) sb[3 * NH + NO + i] = P[P_W4 + i];
+  if (t < NO) sb[3 * NH + t] = P[P_B4 + t];
+  __syncthreads();
+  const float* b1 = sb;
+  const float* b2 = sb + NH;
+  const float* b3 = sb + 2 * NH;
+  const float* b4 = sb + 3 * NH;
+  const float* W4 = sb + 3 * NH + NO;
+
+  float lsum = 0.0f;
+  bool first = true;
+  const int ntiles = (a.n + TILE - 1) / TILE;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int p = tile * TILE + t;
+    const bool live = p < a.n;
+    // ---- features, normalised, to BF16
+    float x[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) x[f] = live ? (a.feat[(long long)p * NF + f] - mu[f]) * isd[f] : 0.0f;
+    put8(sm + PL::X, t, 0, NF, x);
+    put8(sm + PL::X, t, 8, NF, x + 8);
+    if (TRAIN) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) put1(sm + PL::XT, f, t, TILE, x[f]);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // ---- layer 1..3
+    if (t == 0) gemm(PL::C_Z, aX, NF * 16, aW1, NF * 16, NF, id64, false);
+    if (!(ok = sync_mma())) break;
+    hidden_out(b1, sm + PL::H1, TRAIN ? sm + PL::H1T : nullptr);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t == 0) gemm(PL::C_Z, aH1, NH * 16, aW2, NH * 16, NH, id64, false);
+    if (!(ok = sync_mma())) break;
+    hidden_out(b2, sm + PL::H2, TRAIN ? sm + PL::H2T : nullptr);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t == 0) gemm(PL::C_Z, aH2, NH * 16, aW3, NH * 16, NH, id64, false);
+    if (!(ok = sync_mma())) break;
+    // ---- output layer on CUDA cores (z3 stays in tensor memory)
+    float y0 = b4[0], y1 = b4[1];
+    for (int c = 0; c < NH; c += 16) {
+      float z[16];
+      tmem_ld16(trow + PL::C_Z + c, z);
+      tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float h = gelu(z[i] + b3[c + i]);
+        y0 += W4[c + i] * h;
+        y1 += W4[NH + c + i] * h;
+      }
+    }
+    const float s0 = softplus(y0) * osc0, s1 = softplus(y1) * osc1;
+    if (!TRAIN) {
+      if (live) {
+        a.out[(long long)p * 2] = s0;
+        a.out[(long long)p * 2 + 1] = s1;
+      }
+      tc_fence_before();
+      __syncthreads();   // X, H tiles are rewritten by the next tile
+      tc_fence_after();
+      continue;
+    }
+    // ---- loss and dL/dy (mean over the batch of the squared error)
+    float dy0 = 0.0f, dy1 = 0.0f;
+    if (live) {
+      const float e0 = s0 - a.target[(long long)p * 2], e1 = s1 - a.target[(long long)p * 2 + 1];
+      lsum += e0 * e0 + e1 * e1;
+      const float g = 2.0f / (float)a.n;
+      dy0 = g * e0 * osc0 * sigm(y0);
+      dy1 = g * e1 * osc1 * sigm(y1);
+    }
+    float* red = reinterpret_cast<float*>(sm + PL::RED);
+    {   // db4
+      float r0 = dy0, r1 = dy1;
+      for (int o = 16; o > 0; o >>= 1) {
+        r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+        r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&red[128], r0);
+        atomicAdd(&red[129], r1);
+      }
+    }
+    // dh3 = dy W4, dz3 = dh3 gelu'(z3); dW4 += dy h3 (warp sums)
+    for (int c = 0; c < NH; c += 16) {
+      float z[16];
+      tmem_ld16(trow + PL::C_Z + c, z);
+      tmem_wait_ld();
+      float dz[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float zz = z[i] + b3[c + i];
+        const float h = gelu(zz);
+        float g0 = dy0 * h, g1 = dy1 * h;
+        for (int o = 16; o > 0; o >>= 1) {
+          g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+          g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+        }
+        if (lane == 0) {
+          atomicAdd(&red[c + i], g0);
+          atomicAdd(&red[NH + c + i], g1);
+        }
+        dz[i] = (dy0 * W4[c + i] + dy1 * W4[NH + c + i]) * gelu_d(zz);
+      }
+      put8(sm + PL::DZ, t, c, NH, dz);
+      put8(sm + PL::DZ, t, c + 8, NH, dz + 8);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) put1(sm + PL::DZT, c + i, t, TILE, dz[i]);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t aDZ = smem_u32(sm + PL::DZ), aDZT = smem_u32(sm + PL::DZT);
+    if (t == 0) {
+      gemm(PL::C_G3, aDZT, TILE * 16, smem_u32(sm + PL::H2T), TILE * 16, TILE, id80, !first);   // [dW3|db3]
+      gemm(PL::C_H, aDZ, NH * 16, smem_u32(sm + PL::W3T), NH * 16, NH, id64, false);           // dh2
+      gemm(PL::C_Z, aH1, NH * 16, aW2, NH * 16, NH, id64, false);                               // z2 again
+    }
+    if (!(ok = sync_mma())) break;
+    // dz2 = dh2 gelu'(z2)
+    for (int c = 0; c < NH; c += 16) {
+      float z[16], dh[16];
+      tmem_ld16(trow + PL::C_Z + c, z);
+      tmem_ld16(trow + PL::C_H + c, dh);
+      tmem_wait_ld();
+      float dz[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) dz[i] = dh[i] * gelu_d(z[i] + b2[c + i]);
+      put8(sm + PL::DZ, t, c, NH, dz);
+      put8(sm + PL::DZ, t, c + 8, NH, dz + 8);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) put1(sm + PL::DZT, c + i, t, TILE, dz[i]);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t == 0) {
+      gemm(PL::C_G2, aDZT, TILE * 16, smem_u32(sm + PL::H1T), TILE * 16, TILE, id80, !first);   // [dW2|db2]
+      gemm(PL::C_H, aDZ, NH * 16, smem_u32(sm + PL::W2T), NH * 16, NH, id64, false);           // dh1
+      gemm(PL::C_Z, aX, NF * 16, aW1, NF * 16, NF, id64, false);                                // z1 again
+    }
+    if (!(ok = sync_mma())) break;
+    // dz1 = dh1 gelu'(z1) -> dz1^T only
+    for (int c = 0; c < NH; c += 16) {
+      float z[16], dh[16];
+      tmem_ld16(trow + PL::C_Z + c, z);
+      tmem_ld16(trow + PL::C_H + c, dh);
+      tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) put1(sm + PL::DZT, c + i, t, TILE, dh[i] * gelu_d(z[i] + b1[c + i]));
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t == 0) gemm(PL::C_G1, aDZT, TILE * 16, smem_u32(sm + PL::XT), TILE * 16, TILE, id32, !first);  // [dW1|db1]
+    if (!(ok = sync_mma())) break;
+    first = false;
+  }
+
+  if (TRAIN && ok && !first) {
+    // gradients of this CTA: rows 0..63 of the accumulators are lanes 0..63
+    if (warp < 2) {
+      const int o = t;   // output unit
+      float v[16];
+      for (int c = 0; c < 80; c += 16) {
+        tmem_ld16(trow + PL::C_G3 + c, v);
+        tmem_wait_ld();
+        for (int i = 0; i < 16; ++i) {
+          const int col = c + i;
+          if (col < NH) atomicAdd(&a.grads[P_W3 + o * NH + col], v[i]);
+          else if (col == NH) atomicAdd(&a.grads[P_B3 + o], v[i]);
+        }
+        tmem_ld16(trow + PL::C_G2 + c, v);
+        tmem_wait_ld();
+        for (int i = 0; i < 16; ++i) {
+          const int col = c + i;
+          if (col < NH) atomicAdd(&a.grads[P_W2 + o * NH + col], v[i]);
+          else if (col == NH) atomicAdd(&a.grads[P_B2 + o], v[i]);
+        }
+      }
+      for (int c = 0; c < 32; c += 16) {
+        tmem_ld16(trow + PL::C_G1 + c, v);
+        tmem_wait_ld();
+        for (int i = 0; i < 16; ++i) {
+          const int col = c + i;
+          if (col < NF) atomicAdd(&a.grads[P_W1 + o * NF + col], v[i]);
+          else if (col == NF) atomicAdd(&a.grads[P_B1 + o], v[i]);
+        }
+      }
+    }
+    __syncthreads();
+    const float* red = reinterpret_cast<const float*>(sm + PL::RED);
+    for (int i = t; i < NO * NH; i += TILE) atomicAdd(&a.grads[P_W4 + i], red[i]);
+    if (t < NO) atomicAdd(&a.grads[P_B4 + t], red[128 + t]);
+  }
+  if (TRAIN) {
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if (lane == 0 && lsum != 0.0f) atomicAdd(a.loss, lsum);
+  }
+  if (!ok && t == 0) atomicExch(a.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tbase, PL::TMEM_COLS);
+}
+
+// Adam (bias-corrected) on the FP32 master weights; grads are consumed and zeroed
+__global__ void k_adam(float* params, float* grads, float* m1, float* m2, int n, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = grads[i];
+  const float m = b1 * m1[i] + (1.0f - b1) * g;
+  const float v = b2 * m2[i] + (1.0f - b2) * g * g;
+  m1[i] = m;
+  m2[i] = v;
+  params[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+  grads[i] = 0.0f;
+}
+
+// single-tile BF16 GEMM D[128][N] = A[128][K] B[N][K]^T through the same
+// tensor-core path (a check of the operand layouts and descriptors)
+__global__ void __launch_bounds__(128, 1) k_umma_gemm(const uint16_t* A, const uint16_t* B, float* D, int K, int N,
+                                                      int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int t = threadIdx.x, warp = t >> 5;
+  unsigned char* sA = sm;
+  unsigned char* sB = sm + 128 * K * 2;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + N * K * 2);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  for (int i = t; i < 128 * K; i += 128) {
+    const int r = i / K, k = i % K;
+    *reinterpret_cast<uint16_t*>(sA + kmajor_offset(r, k, K)) = A[i];
+  }
+  for (int i = t; i < N * K; i += 128) {
+    const int r = i / K, k = i % K;
+    *reinterpret_cast<uint16_t*>(sB + kmajor_offset(r, k, K)) = B[i];
+  }
+  if (t == 0) mbar_init(mbar, 1);
+  if (warp == 0) {
+    tmem_alloc(slot, 256);
+    tmem_relinquish();
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *slot;
+  if (t == 0) {
+    const uint32_t idesc = umma_idesc_bf16(128, N);
+    for (int s = 0; s < K / 16; ++s)
+      umma_bf16(tbase, umma_desc(smem_u32(sA) + 256 * s, 128, K * 16), umma_desc(smem_u32(sB) + 256 * s, 128, K * 16),
+                idesc, s > 0);
+    umma_commit(mbar);
+  }
+  const bool w = mbar_wait(mbar, 0, WAIT_ITERS);
+  tc_fence_after();
+  const bool ok = __syncthreads_and(w ? 1 : 0) != 0;
+  if (ok) {
+    for (int c = 0; c < N; c += 16) {
+      float v[16];
+      tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + c, v);
+      tmem_wait_ld();
+      for (int i = 0; i < 16; ++i) D[(long long)t * N + c + i] = v[i];
+    }
+  } else if (t == 0) {
+    atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tbase, 256);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+cudaError_t launch_mlp(const MlpArgs& a, bool train, int max_ctas, cudaStream_t st) {
+  const int ntiles = (a.n + TILE - 1) / TILE;
+  if (ntiles == 0) return cudaSuccess;
+  int ctas = ntiles < max_ctas ? ntiles : max_ctas;
+  if (train) {
+    const size_t smem = Plan<true>::BYTES;
+    cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mlp<true><<<ctas, TILE, smem, st>>>(a);
+  } else {
+    const size_t smem = Plan<false>::BYTES;
+    cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mlp<false><<<ctas, TILE, smem, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* params, float* grads, float* m1, float* m2, int n, float lr, int step,
+                        cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  k_adam<<<(n + 255) / 256, 256, 0, st>>>(params, grads, m1, m2, n, lr, b1, b2, 1e-8f, c1, c2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_umma_gemm(const uint16_t* A, const uint16_t* B, float* D, int K, int N, int* err,
+                             cudaStream_t st) {
+  const size_t smem = (size_t)(128 + N) * K * 2 + 16;
+  cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_umma_gemm<<<1, 128, smem, st>>>(A, B, D, K, N, err);
+  return cudaGetLastError();
+}
+
+size_t mlp_smem_bytes(bool train) { return train ? Plan<true>::BYTES : Plan<false>::BYTES; }
+
+}  // namespace db

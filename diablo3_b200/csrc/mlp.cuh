@@ -1,0 +1,27 @@
+// mlp.cuh -- interface of the learned-closure kernels (k_mlp.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace db {
+
+struct MlpArgs {
+  const float* feat;      // [n][16] raw features
+  const float* target;    // [n][2] (training)
+  float* out;             // [n][2] (inference)
+  const float* params;    // DB_SGS_NPARAMS FP32
+  const float* norm;      // mean[16], 1/std[16], out_scale[2]
+  float* grads;           // DB_SGS_NPARAMS (training, accumulated)
+  float* loss;            // sum of squared errors (training, accumulated)
+  int n;                  // points (any count; the last tile is padded)
+  int* err;               // set when a tensor-core wait gave up
+};
+
+cudaError_t launch_mlp(const MlpArgs& a, bool train, int max_ctas, cudaStream_t st);
+cudaError_t launch_adam(float* params, float* grads, float* m1, float* m2, int n, float lr, int step,
+                        cudaStream_t st);
+cudaError_t launch_umma_gemm(const uint16_t* A, const uint16_t* B, float* D, int K, int N, int* err,
+                             cudaStream_t st);
+
+}  // namespace db

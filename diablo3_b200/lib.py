@@ -28,6 +28,8 @@ EXPORTS = (
     "db_courant", "db_divergence",
     "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
+    "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_forward",
+    "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -83,6 +85,16 @@ def load(path: str | None = None):
     L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
     L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.db_rem_div_static.argtypes = [ctypes.POINTER(DbParams), dp, vp, vp, vp, vp]
+    fp, ll = ctypes.POINTER(ctypes.c_float), ctypes.c_longlong
+    L.db_sgs_create.argtypes = [vp, ctypes.POINTER(vp)]
+    L.db_sgs_destroy.argtypes = [vp]
+    L.db_sgs_set.argtypes = [vp, fp, fp, fp, fp]
+    L.db_sgs_get.argtypes = [vp, fp]
+    L.db_sgs_forward.argtypes = [vp, vp, vp, ll]
+    L.db_sgs_gradient.argtypes = [vp, vp, vp, ll, fp, dp]
+    L.db_sgs_train_step.argtypes = [vp, vp, vp, ll, ctypes.c_float, dp]
+    L.db_sgs_gemm_check.argtypes = [vp, vp, fp, ctypes.c_int, ctypes.c_int]
+    L.db_set_sgs_net.argtypes = [vp, vp]
     for name in EXPORTS:
         if name not in ("db_abi_version", "db_last_error"):
             getattr(L, name).restype = ctypes.c_int
@@ -96,6 +108,14 @@ def dptr(a: np.ndarray | None):
     if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
         raise ValueError("arrays must be C-contiguous float64")
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    if a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("arrays must be C-contiguous float32")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
 def check(rc: int, handle=None):

@@ -204,6 +204,53 @@ int db_divergence(db_ctx* ctx, double* max_div_out);
 int db_rem_div_static(const db_params* p, const double* gy, double* cu1,
                       double* cu2, double* cu3, void* cuda_stream);
 
+/* ---- learned SGS closure (no counterpart in the reference, whose les.f90
+ * offers Smagorinsky, dynamic and AMD closures).  A 16 -> 64 -> 64 -> 64 -> 2
+ * MLP (GELU, softplus outputs) maps point features to nu_t and kappa_t; its
+ * hidden layers run on the tensor cores in BF16 with FP32 accumulation,
+ * forward and backward.  Features of a point, in this order: the nine
+ * velocity gradients du_i/dx_j (i-major: du1/dx, du1/dy, du1/dz, du2/dx,
+ * ...), dth/dx, dth/dy, dth/dz, the filter widths 3 dx, 2 dy(j), 3 dz, and
+ * the local N^2 = dth/dy (for/les.f90:1213-1222, 1661-1746). ---- */
+#define DB_SGS_NFEAT 16
+#define DB_SGS_NPARAMS 9538   /* W1[64][16] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[2][64] b4[2] */
+
+typedef struct db_sgs_net db_sgs_net;
+
+/* Create / destroy a network (device parameters, Adam moments, gradient
+ * buffer) on the current device; work goes to cuda_stream (NULL: default). */
+int db_sgs_create(void* cuda_stream, db_sgs_net** out);
+int db_sgs_destroy(db_sgs_net* net);
+
+/* Parameters (FP32, DB_SGS_NPARAMS in the order above), the input
+ * normalisation (feature f enters as (x_f - mean_f) / std_f) and the output
+ * units (nu_t = out_scale[0] softplus(y0), kappa_t = out_scale[1]
+ * softplus(y1)).  Setting resets the Adam state. */
+int db_sgs_set(db_sgs_net* net, const float* params, const float* feat_mean, const float* feat_std,
+               const float* out_scale);
+int db_sgs_get(db_sgs_net* net, float* params);
+
+/* Inference on device arrays: feat[n][16] -> out[n][2] = (nu_t, kappa_t). */
+int db_sgs_forward(db_sgs_net* net, const float* d_feat, float* d_out, long long n);
+
+/* Mean squared error of out against d_target[n][2] and its gradient with
+ * respect to the parameters (copied to grads, DB_SGS_NPARAMS floats). */
+int db_sgs_gradient(db_sgs_net* net, const float* d_feat, const float* d_target, long long n,
+                    float* grads, double* loss);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) of learning rate lr on the
+ * batch; loss is the batch's mean squared error before the step. */
+int db_sgs_train_step(db_sgs_net* net, const float* d_feat, const float* d_target, long long n, float lr,
+                      double* loss);
+
+/* Check of the tensor-core path: D[128][N] = A[128][K] B[N][K]^T with A, B
+ * given as BF16 bit patterns (host arrays), K a multiple of 16 up to 256,
+ * N a multiple of 16 up to 256. */
+int db_sgs_gemm_check(const uint16_t* A, const uint16_t* B, float* D, int K, int N);
+
+/* Use net for les_model_type 6 on this context (the net must outlive it). */
+int db_set_sgs_net(db_ctx* ctx, db_sgs_net* net);
+
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */
 

@@ -303,3 +303,30 @@ def test_amd_eddy_diffusivity_matches_tensor_form(oracle_mod):
     scale = float(kt.max())
     assert scale > 0.0
     assert worst < 1e-11 * scale
+
+
+def test_mlp_oracle_gradient_matches_central_differences():
+    """The FP64 (unrounded) MLP oracle's analytic gradient against central
+    differences of its loss, on a few parameters of every block."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+    import mlp_oracle as mo
+    rng = np.random.default_rng(0)
+    n = 64
+    feat = rng.standard_normal((n, 16))
+    tgt = rng.random((n, 2)) * 1e-3
+    mean, std, scale = np.zeros(16), np.ones(16), np.array([1e-3, 1e-3])
+    params = rng.standard_normal(mo.NPARAMS) * 0.2
+    _, g = mo.loss_and_grad(params, feat, tgt, mean, std, scale, quantized=False)
+    for k, (o, sh) in mo.OFF.items():
+        for idx in rng.choice(int(np.prod(sh)), min(3, int(np.prod(sh))), replace=False):
+            i = o + int(idx)
+            h = 1e-6
+            pp, pm = params.copy(), params.copy()
+            pp[i] += h
+            pm[i] -= h
+            lp, _ = mo.loss_and_grad(pp, feat, tgt, mean, std, scale, quantized=False)
+            lm, _ = mo.loss_and_grad(pm, feat, tgt, mean, std, scale, quantized=False)
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - g[i]) <= 1e-6 * max(1e-8, abs(g[i])) + 1e-12, (k, i, fd, g[i])
