@@ -125,6 +125,21 @@ class Channel:
         self._ck(self.L.db_divergence(self.h, ctypes.byref(d)))
         return d.value
 
+    def set_sgs_net(self, net):
+        """Learned closure for les_model_type 6 (a SgsNet that outlives this channel)."""
+        self._sgs = net
+        self._ck(self.L.db_set_sgs_net(self.h, net.h if net is not None else None))
+
+    def les_eval(self, model: int = 5, features: bool = False):
+        """The SGS model on the current state: (nu_t, kappa_t) in the
+        reference physical layout, and the closure features
+        [Nyp+2][Nz][Nx][16] when asked."""
+        nu, ka = self.new_real(), self.new_real()
+        f = np.zeros((self.p.ny + 2, self.p.nz, self.p.nx, 16), np.float32) if features else None
+        self._ck(self.L.db_les_eval(self.h, model, _L.dptr(nu.reshape(-1)), _L.dptr(ka.reshape(-1)),
+                                    _L.fptr(f.reshape(-1)) if f is not None else None))
+        return (nu, ka, f) if features else (nu, ka)
+
     def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
         self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
 

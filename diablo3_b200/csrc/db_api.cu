@@ -12,6 +12,7 @@
 
 #include "../../include/diablo_b200.h"
 #include "db_kernels.cuh"
+#include "mlp.cuh"
 
 using namespace db;
 
@@ -81,8 +82,8 @@ static int validate(const db_params* p, std::string& why) {
   if (p->ny < 4) { why = "ny must be >= 4"; return DB_ERR_SIZE; }
   if (p->n_th != 1) { why = "n_th must be 1 (one scalar)"; return DB_ERR_UNSUPPORTED; }
   if (p->time_ad_meth != 1) { why = "time_ad_meth 2 (rk_chan_2) stops in the reference (solver.f90:1289-1293)"; return DB_ERR_UNSUPPORTED; }
-  if (p->use_les && p->les_model_type != 5) {
-    why = "LES: only les_model_type 5 (AMD) is built";
+  if (p->use_les && p->les_model_type != 5 && p->les_model_type != 6) {
+    why = "LES: les_model_type 5 (AMD) and 6 (learned closure) are built";
     return DB_ERR_UNSUPPORTED;
   }
   if (p->precision != 0 && p->precision != 1) {
@@ -247,6 +248,10 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.tscr, 2 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = balloc(c, (void**)&s.sgs_feat, Pn * 16 * sizeof(float))) ||
+        (rc = balloc(c, (void**)&s.sgs_out, Pn * 2 * sizeof(float)))) {
+      db_finalize(c); g_init_err = "db_init: out of device memory"; return rc;
+    }
     LesRow* lr = nullptr;
     if ((rc = dalloc(c, &lr, (size_t)np))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     s.lrow = lr;
@@ -612,7 +617,14 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
     for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
     if ((e = launch_inv_x(g, in, out, 12, st, 0xF0u))) return e;
     mark(c, rk, 2);
-    if ((e = launch_les_amd(g, c->ph, s, st))) return e;
+    if (c->p.les_model_type == 6) {   // learned closure, AMD outside its range
+      if ((e = launch_les_amd(g, c->ph, s, st, 1))) return e;
+      if (sgs_forward_async(c->sgs, s.sgs_feat, s.sgs_out, (long long)g.np * g.pp, st)) return cudaErrorLaunchFailure;
+      if ((e = launch_les_amd(g, c->ph, s, st, 2))) return e;
+      n += 2;
+    } else {
+      if ((e = launch_les_amd(g, c->ph, s, st))) return e;
+    }
     n += 2;
   } else {
     // velocity and buoyancy to physical space (solver.f90:635-643)
@@ -668,8 +680,11 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   return cudaSuccess;
 }
 
+static int need_net(db_ctx* c);
+
 extern "C" int db_rk_substep(db_ctx* c, int rk_step) {
   if (!c) return DB_ERR_ARG;
+  if (need_net(c)) return DB_ERR_STATE;
   if (rk_step < 1 || rk_step > 3) return fail(c, DB_ERR_ARG, "rk_step must be 1, 2 or 3");
   const bool t = c->timing;
   c->timing = false;  // stage events belong to whole steps
@@ -692,6 +707,7 @@ static cudaError_t one_step(db_ctx* c, bool les) {
 extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
   if (!c) return DB_ERR_ARG;
   if (nsteps < 0) return fail(c, DB_ERR_ARG, "nsteps must be >= 0");
+  if (need_net(c)) return DB_ERR_STATE;
   for (int i = 0; i < nsteps; ++i) {
     // time_step is incremented at the start of the step (diablo.f90:58-61)
     const int m = les_active(c, c->time_step + 1) ? 1 : 0;
@@ -757,6 +773,61 @@ extern "C" int db_stage_times(db_ctx* c, double* ms, int nstages) {
 extern "C" int db_set_sgs_net(db_ctx* c, db_sgs_net* net) {
   if (!c) return DB_ERR_ARG;
   c->sgs = net;
+  c->s.sgs_range = net ? sgs_range_dev(net) : nullptr;
+  for (int i = 0; i < 2; ++i)   // captured steps hold the old state pointers
+    if (c->graph[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph[i] = nullptr;
+    }
+  return DB_OK;
+}
+
+extern "C" int db_les_eval(db_ctx* c, int model, double* nu_t, double* kappa_t, float* feat) {
+  if (!c) return DB_ERR_ARG;
+  if (!c->p.use_les) return fail(c, DB_ERR_STATE, "db_les_eval needs a context created with use_les");
+  if (model != 5 && model != 6) return fail(c, DB_ERR_ARG, "model must be 5 (AMD) or 6 (learned closure)");
+  if (model == 6 && !c->sgs) return fail(c, DB_ERR_STATE, "model 6 needs a network (db_set_sgs_net)");
+  const Geom& g = c->g;
+  State& s = c->s;
+  cudaStream_t st = c->st;
+  CK(launch_les_bc(g, c->ph, s, st));
+  CK(launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth, s.cu1, s.cu2, s.cu3, s.cth),
+                  fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]), 8, st, 0xF0u,
+                  s.ghost));
+  FieldSet in = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[0], s.xh[1], s.xh[2], s.xh[3]);
+  FieldSet out = fset(s.u1, s.u2, s.u3, s.th, s.gx[0], s.gx[1], s.gx[2], s.gx[3]);
+  for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
+  CK(launch_inv_x(g, in, out, 12, st, 0xF0u));
+  if (model == 6 || feat) CK(launch_les_amd(g, c->ph, s, st, 1));
+  if (model == 6) {
+    if (sgs_forward_async(c->sgs, s.sgs_feat, s.sgs_out, (long long)g.np * g.pp, st))
+      return fail(c, DB_ERR_CUDA, "closure inference failed");
+  }
+  CK(launch_les_amd(g, c->ph, s, st, model == 6 ? 2 : 0));
+  c->launches += (model == 6 ? 7 : 5) + (feat && model != 6 ? 1 : 0);
+  const size_t np_ = (size_t)g.np * g.pp;
+  if (feat) {
+    CK(cudaMemcpyAsync(feat, s.sgs_feat, np_ * 16 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  const int nx2 = c->p.nx + 2, nz2 = c->p.nz + 2;
+  if (nu_t) {
+    memset(nu_t, 0, sizeof(double) * np_ / ((size_t)g.nx * g.nz) * nz2 * nx2);
+    int rc = phys_download(c, s.nu_t, nu_t);
+    if (rc) return rc;
+  }
+  if (kappa_t) {
+    memset(kappa_t, 0, sizeof(double) * np_ / ((size_t)g.nx * g.nz) * nz2 * nx2);
+    int rc = phys_download(c, s.kappa_t, kappa_t);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(st));
+  return DB_OK;
+}
+
+static int need_net(db_ctx* c) {
+  if (c->p.use_les && c->p.les_model_type == 6 && !c->sgs)
+    return fail(c, DB_ERR_STATE, "les_model_type 6 needs a network (db_set_sgs_net)");
   return DB_OK;
 }
 

@@ -124,6 +124,11 @@ struct State {
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
   double* tscr;                              // FP64 Thomas scratch, two fields (LES)
   const LesRow* lrow;                        // np rows (LES)
+  // learned closure (les_model_type 6): features [point][16], outputs
+  // [point][2] (nu_t, kappa_t), training range lo[16], hi[16]
+  float* sgs_feat;
+  float* sgs_out;
+  const float* sgs_range;
 };
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
@@ -150,7 +155,8 @@ cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cu
 
 // k_les.cu
 cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
-cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
+// mode 0: AMD; 1: closure features only; 2: closure nu_t, kappa_t with AMD fallback
+cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode = 0);
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st);
 
 }  // namespace db

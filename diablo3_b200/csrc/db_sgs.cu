@@ -18,6 +18,7 @@ struct db_sgs_net {
   float* m2 = nullptr;
   float* norm = nullptr;     // mean[16], 1/std[16], out_scale[2]
   float* loss = nullptr;
+  float* range = nullptr;    // lo[16], hi[16] of the training features
   int* err = nullptr;
   int step = 0;
   int sms = 148;
@@ -42,7 +43,7 @@ extern "C" int db_sgs_create(void* stream, db_sgs_net** out) {
   if (cudaMalloc(&n->params, P) != cudaSuccess || cudaMalloc(&n->grads, P) != cudaSuccess ||
       cudaMalloc(&n->m1, P) != cudaSuccess || cudaMalloc(&n->m2, P) != cudaSuccess ||
       cudaMalloc(&n->norm, 64 * sizeof(float)) != cudaSuccess || cudaMalloc(&n->loss, sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&n->err, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&n->err, sizeof(int)) != cudaSuccess || cudaMalloc(&n->range, 32 * sizeof(float)) != cudaSuccess) {
     db_sgs_destroy(n);
     return DB_ERR_CUDA;
   }
@@ -52,6 +53,11 @@ extern "C" int db_sgs_create(void* stream, db_sgs_net** out) {
   cudaMemset(n->m2, 0, P);
   cudaMemset(n->norm, 0, 64 * sizeof(float));
   cudaMemset(n->err, 0, sizeof(int));
+  {
+    float r[32];
+    for (int f = 0; f < 16; ++f) { r[f] = -3.0e38f; r[16 + f] = 3.0e38f; }   // no fallback until set
+    cudaMemcpy(n->range, r, sizeof(r), cudaMemcpyHostToDevice);
+  }
   *out = n;
   return DB_OK;
 }
@@ -66,6 +72,7 @@ extern "C" int db_sgs_destroy(db_sgs_net* n) {
   cudaFree(n->norm);
   cudaFree(n->loss);
   cudaFree(n->err);
+  cudaFree(n->range);
   delete n;
   return DB_OK;
 }
@@ -91,6 +98,21 @@ extern "C" int db_sgs_set(db_sgs_net* n, const float* params, const float* mean,
   n->step = 0;
   return DB_OK;
 }
+
+extern "C" int db_sgs_set_range(db_sgs_net* n, const float* lo, const float* hi) {
+  if (!n || !lo || !hi) return DB_ERR_ARG;
+  float r[32];
+  for (int f = 0; f < 16; ++f) {
+    if (!(lo[f] <= hi[f])) return DB_ERR_ARG;
+    r[f] = lo[f];
+    r[16 + f] = hi[f];
+  }
+  SCK(cudaMemcpyAsync(n->range, r, sizeof(r), cudaMemcpyHostToDevice, n->st));
+  SCK(cudaStreamSynchronize(n->st));
+  return DB_OK;
+}
+
+const float* sgs_range_dev(const db_sgs_net* n) { return n->range; }
 
 extern "C" int db_sgs_get(db_sgs_net* n, float* params) {
   if (!n || !params) return DB_ERR_ARG;

@@ -123,7 +123,14 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 // with j1 = jstart, j2 = Nyp - 1 (les.f90:46-49, one rank), tau_12 at GY
 // rows = temp (S12 - du1/dy / 2) for j >= 2 and the raw strain at j = 1
 // (les.f90:737-748).  R: arithmetic and storage type (FP32 on the mixed path).
-template <typename R>
+// MODE 0: AMD.  MODE 1: only the learned closure's 16 features at every GY
+// row (include/diablo_b200.h order) into s.sgs_feat[point][16].  MODE 2:
+// the closure's nu_t, kappa_t (s.sgs_out[point][2], at GY rows) take the
+// place of the AMD coefficients, temp = -2 nu / filter at GY rows and
+// s1 = -2 nu_GYF / filter at GYF rows with nu_GYF the mean of the two GY
+// neighbours; a point whose features leave the training range
+// (s.sgs_range: lo[16], hi[16]) keeps its AMD value.
+template <typename R, int MODE>
 __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
@@ -150,6 +157,15 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
   for (int i = 0; i < 9; ++i) o[i] = (R*)s.les[i] + col;
   R* nut = (R*)s.nu_t + col;
   R* kat = (R*)s.kappa_t + col;
+  float* fo = s.sgs_feat;
+  const float* mo = s.sgs_out;
+  const float* rng = s.sgs_range;
+  if (MODE == 1) {
+#pragma unroll
+    for (int f = 0; f < 16; ++f) fo[col * 16 + f] = 0.0f;
+  }
+  R hnu = 0, hka = 0;     // closure values at the previous GY row
+  bool hval = false;
 
   // row 0: GYF values only (GY row 0 does not exist)
   R u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
@@ -185,6 +201,33 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
     const R c2y = (j <= Nyp) ? (u2n - u2c) * (R)lr.idyf : (R)0;
     const R delt = (R)lr.dgy;
     R temp = 0, temp_th = 0;
+    R nu_m = 0, ka_m = 0;
+    bool val = false;
+    if (MODE != 0) {
+      const R wa = (R)lr.wa, wb = (R)lr.wb;
+      float fv[16];
+      fv[0] = (float)(a1x * wa + f1x * wb); fv[1] = (float)d1y; fv[2] = (float)(a1z * wa + f1z * wb);
+      fv[3] = (float)a2x; fv[4] = (float)(c2y * wa + f2y * wb); fv[5] = (float)a2z;
+      fv[6] = (float)(a3x * wa + f3x * wb); fv[7] = (float)d3y; fv[8] = (float)(a3z * wa + f3z * wb);
+      fv[9] = (float)(atx * wa + ftx * wb); fv[10] = (float)dty; fv[11] = (float)(atz * wa + ftz * wb);
+      fv[12] = (float)dxs; fv[13] = (float)dly; fv[14] = (float)dzs; fv[15] = (float)dty;
+      const long long pt = (oj + col) * 16;
+      if (MODE == 1) {
+#pragma unroll
+        for (int f = 0; f < 16; ++f) fo[pt + f] = fv[f];
+      } else {
+        val = true;
+#pragma unroll
+        for (int f = 0; f < 16; ++f) val = val && (fv[f] >= rng[f]) && (fv[f] <= rng[16 + f]);
+        nu_m = (R)mo[(oj + col) * 2];
+        ka_m = (R)mo[(oj + col) * 2 + 1];
+      }
+    }
+    if (MODE == 1) {
+      u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
+      f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
+      continue;
+    }
     if (j >= 2 && j <= Nyp) {
       const R wa = (R)lr.wa, wb = (R)lr.wb;
 #define GYI(A, B) ((A) * wa + (B) * wb)
@@ -195,6 +238,10 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
       temp_th = amd_th_ratio<R>(dxs, dly, dzs, GYI(a1x, f1x), GYI(c2y, f2y), GYI(a3z, f3z), d1y, a2x,
                                 GYI(a1z, f1z), GYI(a3x, f3x), a2z, d3y, GYI(atx, ftx), dty, GYI(atz, ftz));
 #undef GYI
+      if (MODE == 2 && val) {
+        temp = (R)-2 * nu_m / delt;
+        temp_th = (R)-2 * ka_m / delt;
+      }
     }
     const bool wall = (j <= 2 || j >= Nyp);     // ghost_les_mpi / ghost_les_th_mpi
     const R nu = wall ? (R)0 : -h * delt * temp;
@@ -218,7 +265,8 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
         const R s4 = h * (SI4 + hSI4), s6 = h * (SI6 + hSI6);
         const R q4 = h * (O4 + hO4), q6 = h * (O6 + hO6);
         const R s5 = h * (f1z * rzx + f3x * rxz), q5 = h * (f1z * rzx - f3x * rxz);
-        const R s1 = amd_ratio<R>(f1x, f2y, f3z, s4, s5, s6, q4, q5, q6);
+        R s1 = amd_ratio<R>(f1x, f2y, f3z, s4, s5, s6, q4, q5, q6);
+        if (MODE == 2 && val && hval) s1 = -(hnu + nu_m) / dlf;
         L0 = dlf * (s1 * f1x);
         L2 = dlf * (s1 * (h * (f1z + f3x)));
         L4 = dlf * (s1 * f3z);
@@ -227,8 +275,9 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
       }
       if (r >= jst && r <= jet) {
         const R dys = (R)lf.dys_f;
-        const R s1t = amd_th_ratio<R>(dxs, dys, dzs, f1x, f2y, f3z, h * (d1y + h1y), h * (a2x + h2x), f1z, f3x,
-                                      h * (a2z + h2z), h * (d3y + h3y), ftx, h * (dty + hty), ftz);
+        R s1t = amd_th_ratio<R>(dxs, dys, dzs, f1x, f2y, f3z, h * (d1y + h1y), h * (a2x + h2x), f1z, f3x,
+                                h * (a2z + h2z), h * (d3y + h3y), ftx, h * (dty + hty), ftz);
+        if (MODE == 2 && val && hval) s1t = -(hka + ka_m) / dlf;
         L7 = h * dlf * (s1t * ftx);
         L8 = h * dlf * (s1t * ftz);
       }
@@ -245,7 +294,9 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
     f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
     h1y = d1y; h3y = d3y; hty = dty; h2x = a2x; h2z = a2z;
     hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
+    hnu = nu_m; hka = ka_m; hval = val;
   }
+  if (MODE == 1) return;
   const long long oe = (long long)(Nyp + 1) * pp;
   o[0][oe] = 0; o[1][oe] = 0; o[2][oe] = 0; o[3][oe] = 0; o[4][oe] = 0;
   o[7][oe] = 0; o[8][oe] = 0;
@@ -349,10 +400,18 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
   k_les_bc<<<dim3((g.kxs + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, ph);
   return cudaGetLastError();
 }
-cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st) {
+cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode) {
   const int bx = g.nx < 128 ? g.nx : 128;
-  if (g.prec) k_les_amd<float><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
-  else k_les_amd<double><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, ph);
+  const dim3 grid(g.nx / bx, g.nz);
+  if (g.prec) {
+    if (mode == 1) k_les_amd<float, 1><<<grid, bx, 0, st>>>(s, g, ph);
+    else if (mode == 2) k_les_amd<float, 2><<<grid, bx, 0, st>>>(s, g, ph);
+    else k_les_amd<float, 0><<<grid, bx, 0, st>>>(s, g, ph);
+  } else {
+    if (mode == 1) k_les_amd<double, 1><<<grid, bx, 0, st>>>(s, g, ph);
+    else if (mode == 2) k_les_amd<double, 2><<<grid, bx, 0, st>>>(s, g, ph);
+    else k_les_amd<double, 0><<<grid, bx, 0, st>>>(s, g, ph);
+  }
   return cudaGetLastError();
 }
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {

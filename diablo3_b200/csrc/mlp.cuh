@@ -25,3 +25,9 @@ cudaError_t launch_umma_gemm(const uint16_t* A, const uint16_t* B, float* D, int
                              cudaStream_t st);
 
 }  // namespace db
+
+struct db_sgs_net;
+// closure inference on a stream (no synchronisation), and the device
+// training-range bounds lo[16], hi[16] of a network
+int sgs_forward_async(db_sgs_net* n, const float* d_feat, float* d_out, long long npts, cudaStream_t st);
+const float* sgs_range_dev(const db_sgs_net* n);

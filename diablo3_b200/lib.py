@@ -28,8 +28,8 @@ EXPORTS = (
     "db_courant", "db_divergence",
     "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
-    "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_forward",
-    "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net",
+    "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
+    "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -90,11 +90,13 @@ def load(path: str | None = None):
     L.db_sgs_destroy.argtypes = [vp]
     L.db_sgs_set.argtypes = [vp, fp, fp, fp, fp]
     L.db_sgs_get.argtypes = [vp, fp]
+    L.db_sgs_set_range.argtypes = [vp, fp, fp]
     L.db_sgs_forward.argtypes = [vp, vp, vp, ll]
     L.db_sgs_gradient.argtypes = [vp, vp, vp, ll, fp, dp]
     L.db_sgs_train_step.argtypes = [vp, vp, vp, ll, ctypes.c_float, dp]
     L.db_sgs_gemm_check.argtypes = [vp, vp, fp, ctypes.c_int, ctypes.c_int]
     L.db_set_sgs_net.argtypes = [vp, vp]
+    L.db_les_eval.argtypes = [vp, ctypes.c_int, dp, dp, fp]
     for name in EXPORTS:
         if name not in ("db_abi_version", "db_last_error"):
             getattr(L, name).restype = ctypes.c_int

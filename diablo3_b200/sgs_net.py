@@ -75,6 +75,13 @@ class SgsNet:
         assert p.shape == (NPARAMS,) and m.shape == (NFEAT,) and sd.shape == (NFEAT,) and os_.shape == (NOUT,)
         _L.check(self.L.db_sgs_set(self.h, _L.fptr(p), _L.fptr(m), _L.fptr(sd), _L.fptr(os_)))
 
+    def set_range(self, lo, hi):
+        """Training range of the raw features; outside it the channel step
+        keeps AMD's coefficients."""
+        a = np.ascontiguousarray(lo, np.float32)
+        b = np.ascontiguousarray(hi, np.float32)
+        _L.check(self.L.db_sgs_set_range(self.h, _L.fptr(a), _L.fptr(b)))
+
     def get(self) -> np.ndarray:
         p = np.zeros(NPARAMS, np.float32)
         _L.check(self.L.db_sgs_get(self.h, _L.fptr(p)))

@@ -230,6 +230,11 @@ int db_sgs_set(db_sgs_net* net, const float* params, const float* feat_mean, con
                const float* out_scale);
 int db_sgs_get(db_sgs_net* net, float* params);
 
+/* Training range of the features (raw units): inside a channel step, a GY
+ * point whose features leave [lo, hi] keeps the AMD eddy viscosity and
+ * diffusivity (model 5) instead of the network's.  Default: no bounds. */
+int db_sgs_set_range(db_sgs_net* net, const float* lo, const float* hi);
+
 /* Inference on device arrays: feat[n][16] -> out[n][2] = (nu_t, kappa_t). */
 int db_sgs_forward(db_sgs_net* net, const float* d_feat, float* d_out, long long n);
 
@@ -248,8 +253,19 @@ int db_sgs_train_step(db_sgs_net* net, const float* d_feat, const float* d_targe
  * N a multiple of 16 up to 256. */
 int db_sgs_gemm_check(const uint16_t* A, const uint16_t* B, float* D, int K, int N);
 
-/* Use net for les_model_type 6 on this context (the net must outlive it). */
+/* Use net for les_model_type 6 on this context (the net must outlive it).
+ * With use_les and les_model_type 6 the substep evaluates the network at
+ * every GY point in place of AMD's coefficients (AMD where the features
+ * leave the training range); stepping without a net is DB_ERR_STATE. */
 int db_set_sgs_net(db_ctx* ctx, db_sgs_net* net);
+
+/* The SGS model on the current state without stepping: les_chan's ghost
+ * rows, gradients and eddy coefficients (for/les.f90:551-795, 1201-1358)
+ * for model 5 (AMD) or 6 (the attached network, AMD outside its range).
+ * nu_t, kappa_t (reference physical layout, GY points) and feat (FP32
+ * [Nyp+2][Nz][Nx][16], the closure's features at GY rows) may be NULL.  The
+ * context's nu_t / kappa_t are overwritten, as a substep with LES would. */
+int db_les_eval(db_ctx* ctx, int model, double* nu_t, double* kappa_t, float* feat);
 
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */

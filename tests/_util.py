@@ -60,3 +60,54 @@ def seed_pair(oracle_cls, channel_cls, p, gy, seed=7, noise="gaussian"):
     ch = channel_cls(p, gy)
     ch.upload_state({fid: o.cplx(fid).copy() for fid in STATE})
     return o, ch
+
+
+def to_phys(p, c):
+    """Packed dealiased spectral planes -> physical planes (numpy irfft2)."""
+    nkx, nkz = p.nkx, p.nkz
+    full = np.zeros((c.shape[0], p.nz, p.nx // 2 + 1), complex)
+    full[:, : nkz + 1, : nkx + 1] = c[:, : nkz + 1, : nkx + 1]
+    full[:, p.nz - nkz:, : nkx + 1] = c[:, nkz + 1: 2 * nkz + 1, : nkx + 1]
+    return np.fft.irfft2(full, s=(p.nz, p.nx), axes=(1, 2)) * (p.nx * p.nz)
+
+
+def gradients_at_gy(p, c, met, kx, kz, fid_list=(0, 1, 2)):
+    """Velocity gradient G[i][k] = d u_i / d x_k and scalar gradient g[k],
+    physical, at GY rows (x/z derivatives and d u2/dy live at GYF rows and
+    are interpolated to GY with the dyf weights)."""
+    dy, dyf = met["dy"], met["dyf"]
+    ny = p.ny
+    sl = (slice(None), slice(0, 2 * p.nkz + 1), slice(0, p.nkx + 1))
+    ikx = 1j * kx[None, None, :]
+    ikz = 1j * kz[None, :, None]
+    u = [c[f][sl] for f in (0, 1, 2)]
+    th = c[4][sl]
+
+    def ph(a):
+        return to_phys(p, a)
+
+    def gyf_to_gy(x):  # rows j of result = GY row j, j = 1..ny
+        out = np.zeros_like(x)
+        for j in range(1, ny + 1):
+            out[j] = (x[j] * dyf[j - 1] + x[j - 1] * dyf[j]) / (2 * dy[j])
+        return out
+
+    def ddy_gy(a):  # (a(j) - a(j-1)) / dy(j), GYF field -> GY
+        out = np.zeros_like(a)
+        out[1:] = (a[1:] - a[:-1]) / dy[1:, None, None]
+        return out
+
+    d2dy = np.zeros_like(u[1])
+    d2dy[:-1] = (u[1][1:] - u[1][:-1]) / dyf[:-1, None, None]
+    G = [[None] * 3 for _ in range(3)]
+    G[0][0] = gyf_to_gy(ph(ikx * u[0]))
+    G[0][1] = ph(ddy_gy(u[0]))
+    G[0][2] = gyf_to_gy(ph(ikz * u[0]))
+    G[1][0] = ph(ikx * u[1])
+    G[1][1] = gyf_to_gy(ph(d2dy))
+    G[1][2] = ph(ikz * u[1])
+    G[2][0] = gyf_to_gy(ph(ikx * u[2]))
+    G[2][1] = ph(ddy_gy(u[2]))
+    G[2][2] = gyf_to_gy(ph(ikz * u[2]))
+    g = [gyf_to_gy(ph(ikx * th)), ph(ddy_gy(th)), gyf_to_gy(ph(ikz * th))]
+    return np.array(G), np.array(g)

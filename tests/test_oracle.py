@@ -5,7 +5,7 @@ import math
 import numpy as np
 import pytest
 
-from _util import config0_params, grid_for, rel_l2, significant
+from _util import config0_params, gradients_at_gy, grid_for, rel_l2, significant
 
 
 @pytest.mark.parametrize("n", [8, 16, 64, 512])
@@ -177,15 +177,6 @@ def test_thermal_wind_rest_state_is_steady(oracle_mod):
     assert rel_l2(significant(p, o.cplx(4)), th0) < 1e-14
 
 
-def _to_phys(p, c):
-    """Packed dealiased spectral planes -> physical planes (numpy irfft2)."""
-    nkx, nkz = p.nkx, p.nkz
-    full = np.zeros((c.shape[0], p.nz, p.nx // 2 + 1), complex)
-    full[:, : nkz + 1, : nkx + 1] = c[:, : nkz + 1, : nkx + 1]
-    full[:, p.nz - nkz:, : nkx + 1] = c[:, nkz + 1: 2 * nkz + 1, : nkx + 1]
-    return np.fft.irfft2(full, s=(p.nz, p.nx), axes=(1, 2)) * (p.nx * p.nz)
-
-
 def _amd_fixture(oracle_mod, **kw):
     from diablo3_b200.ic import initial_fields
     p = config0_params(nx=32, ny=33, nz=16, use_les=1, create_new_flow=0, les_model_type=5,
@@ -201,48 +192,6 @@ def _amd_fixture(oracle_mod, **kw):
     return p, o, c, met, kx, kz
 
 
-def _gradients_at_gy(p, c, met, kx, kz, fid_list=(0, 1, 2)):
-    """Velocity gradient G[i][k] = d u_i / d x_k and scalar gradient g[k],
-    physical, at GY rows (x/z derivatives and d u2/dy live at GYF rows and
-    are interpolated to GY with the dyf weights)."""
-    dy, dyf = met["dy"], met["dyf"]
-    ny = p.ny
-    sl = (slice(None), slice(0, 2 * p.nkz + 1), slice(0, p.nkx + 1))
-    ikx = 1j * kx[None, None, :]
-    ikz = 1j * kz[None, :, None]
-    u = [c[f][sl] for f in (0, 1, 2)]
-    th = c[4][sl]
-
-    def ph(a):
-        return _to_phys(p, a)
-
-    def gyf_to_gy(x):  # rows j of result = GY row j, j = 1..ny
-        out = np.zeros_like(x)
-        for j in range(1, ny + 1):
-            out[j] = (x[j] * dyf[j - 1] + x[j - 1] * dyf[j]) / (2 * dy[j])
-        return out
-
-    def ddy_gy(a):  # (a(j) - a(j-1)) / dy(j), GYF field -> GY
-        out = np.zeros_like(a)
-        out[1:] = (a[1:] - a[:-1]) / dy[1:, None, None]
-        return out
-
-    d2dy = np.zeros_like(u[1])
-    d2dy[:-1] = (u[1][1:] - u[1][:-1]) / dyf[:-1, None, None]
-    G = [[None] * 3 for _ in range(3)]
-    G[0][0] = gyf_to_gy(ph(ikx * u[0]))
-    G[0][1] = ph(ddy_gy(u[0]))
-    G[0][2] = gyf_to_gy(ph(ikz * u[0]))
-    G[1][0] = ph(ikx * u[1])
-    G[1][1] = gyf_to_gy(ph(d2dy))
-    G[1][2] = ph(ikz * u[1])
-    G[2][0] = gyf_to_gy(ph(ikx * u[2]))
-    G[2][1] = ph(ddy_gy(u[2]))
-    G[2][2] = gyf_to_gy(ph(ikz * u[2]))
-    g = [gyf_to_gy(ph(ikx * th)), ph(ddy_gy(th)), gyf_to_gy(ph(ikz * th))]
-    return np.array(G), np.array(g)
-
-
 def _filter_widths(p, met):
     dx, dz = p.lx / p.nx, p.lz / p.nz
     return 3.0 * dx, 2.0 * met["dy"], 3.0 * dz
@@ -255,7 +204,7 @@ def test_amd_eddy_viscosity_matches_tensor_form(oracle_mod):
     D_ij = (delta_j / delta_i) du_i/dx_j, S, W its symmetric and
     antisymmetric parts, evaluated here with numpy at GY rows."""
     p, o, c, met, kx, kz = _amd_fixture(oracle_mod)
-    G, _ = _gradients_at_gy(p, c, met, kx, kz)
+    G, _ = gradients_at_gy(p, c, met, kx, kz)
     dxs, dys, dzs = _filter_widths(p, met)
     ny = p.ny
     rows = range(3, ny)   # rows 1, 2, ny, ny+1 are the zeroed wall rows
@@ -286,7 +235,7 @@ def test_amd_eddy_diffusivity_matches_tensor_form(oracle_mod):
     C^2 max(0, -g^T G Delta^2 g) / |Delta g|^2 * 3 / sum_k delta_k^-2
     (G the velocity gradient, g the scalar gradient, Delta = diag(delta))."""
     p, o, c, met, kx, kz = _amd_fixture(oracle_mod)
-    G, g = _gradients_at_gy(p, c, met, kx, kz)
+    G, g = gradients_at_gy(p, c, met, kx, kz)
     dxs, dys, dzs = _filter_widths(p, met)
     ny = p.ny
     kt = o.real(10)[:, : p.nz, : p.nx]
