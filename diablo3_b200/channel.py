@@ -140,6 +140,19 @@ class Channel:
                                     _L.fptr(f.reshape(-1)) if f is not None else None))
         return (nu, ka, f) if features else (nu, ka)
 
+    def sgs_targets(self, gy_coarse, fx: int = 4, fy: int = 4, fz: int = 4):
+        """Box-filtered training data of the learned closure from this
+        (resolved) state: CUDA tensors (features [n][16], targets [n][2])."""
+        import torch
+        g = np.ascontiguousarray(gy_coarse, np.float64)
+        n = ctypes.c_longlong()
+        self._ck(self.L.db_sgs_targets(self.h, fx, fy, fz, _L.dptr(g), None, None, ctypes.byref(n)))
+        feat = torch.empty((n.value, 16), dtype=torch.float32, device="cuda")
+        tgt = torch.empty((n.value, 2), dtype=torch.float32, device="cuda")
+        self._ck(self.L.db_sgs_targets(self.h, fx, fy, fz, _L.dptr(g), ctypes.c_void_p(feat.data_ptr()),
+                                       ctypes.c_void_p(tgt.data_ptr()), ctypes.byref(n)))
+        return feat, tgt
+
     def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
         self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
 

@@ -825,6 +825,60 @@ extern "C" int db_les_eval(db_ctx* c, int model, double* nu_t, double* kappa_t, 
   return DB_OK;
 }
 
+namespace db {
+struct SgsData {
+  int fx, fy, fz;
+  int nxc, nzc, nyc;
+  int kmin, kmax;
+  double dxc3, dzc3;
+  const double* dyc2;
+  float* feat;
+  float* target;
+};
+cudaError_t launch_sgs_targets(const Geom& g, const State& s, const SgsData& d, cudaStream_t st);
+}  // namespace db
+
+extern "C" int db_sgs_targets(db_ctx* c, int fx, int fy, int fz, const double* gy_coarse, float* d_feat,
+                              float* d_target, long long* npts) {
+  if (!c || !gy_coarse || !npts) return DB_ERR_ARG;
+  if (!c->p.use_les) return fail(c, DB_ERR_STATE, "db_sgs_targets needs a context created with use_les");
+  const Geom& g = c->g;
+  if (fx < 1 || fz < 1 || fy < 2 || (fy & 1) || g.nx % fx || g.nz % fz || (g.ny - 1) % fy)
+    return fail(c, DB_ERR_ARG, "filter factors must divide nx, nz and ny - 1 (fy even)");
+  const int nxc = g.nx / fx, nzc = g.nz / fz, nyc = (g.ny - 1) / fy + 1;
+  if (nyc < 5) return fail(c, DB_ERR_SIZE, "coarse grid needs at least 5 wall-normal points");
+  const long long n = (long long)nxc * nzc * (nyc - 3);
+  *npts = n;
+  if (!d_feat || !d_target) return DB_OK;   // size query
+  // coarse metrics (same construction as db_init)
+  std::vector<double> cgy(nyc + 2, 0.0), cgyf(nyc + 2, 0.0), c2dy(nyc + 2, 0.0);
+  for (int j = 1; j <= nyc + 1; ++j) cgy[j] = gy_coarse[j - 1];
+  for (int j = 1; j <= nyc; ++j) cgyf[j] = 0.5 * (cgy[j] + cgy[j + 1]);
+  cgyf[0] = 2.0 * cgyf[1] - cgyf[2];
+  cgyf[nyc + 1] = 2.0 * cgyf[nyc] - cgyf[nyc - 1];
+  for (int j = 1; j <= nyc + 1; ++j) c2dy[j] = 2.0 * (cgyf[j] - cgyf[j - 1]);
+  double* d_dy = nullptr;
+  CK(cudaMalloc(&d_dy, c2dy.size() * sizeof(double)));
+  CK(cudaMemcpy(d_dy, c2dy.data(), c2dy.size() * sizeof(double), cudaMemcpyHostToDevice));
+  State& s = c->s;
+  cudaStream_t st = c->st;
+  // the state and its x and z derivatives in physical space (no ghost overlay)
+  CK(launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth, s.cu1, s.cu2, s.cu3, s.cth),
+                  fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]), 8, st, 0xF0u));
+  FieldSet in = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[0], s.xh[1], s.xh[2], s.xh[3]);
+  FieldSet out = fset(s.u1, s.u2, s.u3, s.th, s.gx[0], s.gx[1], s.gx[2], s.gx[3]);
+  for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
+  CK(launch_inv_x(g, in, out, 12, st, 0xF0u));
+  SgsData d{fx, fy, fz, nxc, nzc, nyc, 3, nyc - 1, 3.0 * c->p.lx / nxc, 3.0 * c->p.lz / nzc, d_dy, d_feat, d_target};
+  cudaError_t e = launch_sgs_targets(g, s, d, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaFree(d_dy);
+  c->launches += 3;
+  CK(e);
+  CK(e2);
+  return DB_OK;
+}
+
 static int need_net(db_ctx* c) {
   if (c->p.use_les && c->p.les_model_type == 6 && !c->sgs)
     return fail(c, DB_ERR_STATE, "les_model_type 6 needs a network (db_set_sgs_net)");

@@ -30,6 +30,7 @@ EXPORTS = (
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
+    "db_sgs_targets",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -97,6 +98,8 @@ def load(path: str | None = None):
     L.db_sgs_gemm_check.argtypes = [vp, vp, fp, ctypes.c_int, ctypes.c_int]
     L.db_set_sgs_net.argtypes = [vp, vp]
     L.db_les_eval.argtypes = [vp, ctypes.c_int, dp, dp, fp]
+    L.db_sgs_targets.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, vp, vp,
+                                 ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:
         if name not in ("db_abi_version", "db_last_error"):
             getattr(L, name).restype = ctypes.c_int

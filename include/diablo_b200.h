@@ -267,6 +267,18 @@ int db_set_sgs_net(db_ctx* ctx, db_sgs_net* net);
  * context's nu_t / kappa_t are overwritten, as a substep with LES would. */
 int db_les_eval(db_ctx* ctx, int model, double* nu_t, double* kappa_t, float* feat);
 
+/* Training data of the closure from the context's (resolved) state: a box
+ * filter of fx x fy x fz fine cells around every GY point of the coarse
+ * grid gy_coarse (its GY(1:NYc+1), NYc = (ny - 1) / fy + 1, the same
+ * stretching), the exact subgrid stress and buoyancy flux of that filter,
+ * and nu_t, kappa_t fitted to them by least squares
+ * (nu_t = max(0, -tau^d:S / 2 S:S), kappa_t = max(0, -q.grad th / |grad th|^2)).
+ * Writes DEVICE arrays d_feat[n][16] (closure features of the filtered
+ * field) and d_target[n][2] for the n = nx/fx * nz/fz * (NYc - 3) points of
+ * coarse rows 3..NYc-1; with d_feat or d_target NULL only n is returned. */
+int db_sgs_targets(db_ctx* ctx, int fx, int fy, int fz, const double* gy_coarse, float* d_feat,
+                   float* d_target, long long* npts);
+
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */
 
