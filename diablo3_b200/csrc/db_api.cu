@@ -841,8 +841,14 @@ cudaError_t launch_sgs_targets(const Geom& g, const State& s, const SgsData& d, 
 extern "C" int db_sgs_targets(db_ctx* c, int fx, int fy, int fz, const double* gy_coarse, float* d_feat,
                               float* d_target, long long* npts) {
   if (!c || !gy_coarse || !npts) return DB_ERR_ARG;
-  if (!c->p.use_les) return fail(c, DB_ERR_STATE, "db_sgs_targets needs a context created with use_les");
   const Geom& g = c->g;
+  if (!c->s.gx[0]) {   // a DNS context: gradient fields on first use
+    const size_t bytes = (size_t)g.np * g.pp * phys_elem(c);
+    for (int i = 0; i < 4; ++i) {
+      int rc;
+      if ((rc = balloc(c, (void**)&c->s.gx[i], bytes)) || (rc = balloc(c, (void**)&c->s.gz[i], bytes))) return rc;
+    }
+  }
   if (fx < 1 || fz < 1 || fy < 2 || (fy & 1) || g.nx % fx || g.nz % fz || (g.ny - 1) % fy)
     return fail(c, DB_ERR_ARG, "filter factors must divide nx, nz and ny - 1 (fy even)");
   const int nxc = g.nx / fx, nzc = g.nz / fz, nyc = (g.ny - 1) / fy + 1;

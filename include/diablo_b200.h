@@ -275,7 +275,8 @@ int db_les_eval(db_ctx* ctx, int model, double* nu_t, double* kappa_t, float* fe
  * (nu_t = max(0, -tau^d:S / 2 S:S), kappa_t = max(0, -q.grad th / |grad th|^2)).
  * Writes DEVICE arrays d_feat[n][16] (closure features of the filtered
  * field) and d_target[n][2] for the n = nx/fx * nz/fz * (NYc - 3) points of
- * coarse rows 3..NYc-1; with d_feat or d_target NULL only n is returned. */
+ * coarse rows 3..NYc-1; with d_feat or d_target NULL only n is returned.
+ * A context without use_les allocates its 8 gradient fields on first use. */
 int db_sgs_targets(db_ctx* ctx, int fx, int fy, int fz, const double* gy_coarse, float* d_feat,
                    float* d_target, long long* npts);
 

@@ -279,3 +279,26 @@ def test_mlp_oracle_gradient_matches_central_differences():
             lm, _ = mo.loss_and_grad(pm, feat, tgt, mean, std, scale, quantized=False)
             fd = (lp - lm) / (2 * h)
             assert abs(fd - g[i]) <= 1e-6 * max(1e-8, abs(g[i])) + 1e-12, (k, i, fd, g[i])
+
+
+def test_amd_from_features_is_model_5(oracle_mod):
+    """The yardstick of the learned closure, AMD evaluated on closure
+    features (diablo3_b200.sgs_train), gives the oracle's model-5 nu_t and
+    kappa_t at the interior GY rows."""
+    from diablo3_b200.sgs_train import amd_from_features
+    p, o, c, met, kx, kz = _amd_fixture(oracle_mod)
+    G, g = gradients_at_gy(p, c, met, kx, kz)
+    dxs, dys, dzs = _filter_widths(p, met)
+    for j in range(3, p.ny):
+        f = np.empty((p.nz * p.nx, 16))
+        for i in range(3):
+            for k in range(3):
+                f[:, 3 * i + k] = G[i, k, j].reshape(-1)
+        f[:, 9:12] = g[:, j].reshape(3, -1).T
+        f[:, 12], f[:, 13], f[:, 14] = dxs, dys[j], dzs
+        f[:, 15] = g[1, j].reshape(-1)
+        nu, ka = amd_from_features(f)
+        ref_nu = o.real(9)[j, : p.nz, : p.nx].reshape(-1)
+        ref_ka = o.real(10)[j, : p.nz, : p.nx].reshape(-1)
+        assert np.abs(nu - ref_nu).max() <= 1e-11 * max(ref_nu.max(), 1e-30)
+        assert np.abs(ka - ref_ka).max() <= 1e-11 * max(ref_ka.max(), 1e-30)
