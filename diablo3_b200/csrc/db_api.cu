@@ -739,6 +739,131 @@ extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
   return DB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// ensembles: one CUDA graph per time step that forks into every member's
+// stream, runs its step there and joins back
+
+struct db_ensemble {
+  std::vector<db_ctx*> members;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [LES model active]
+  std::vector<cudaEvent_t> ev;                     // fork event + one join event per member
+  long long kernels[2] = {0, 0};
+  std::string err;
+};
+
+extern "C" int db_ensemble_create(db_ctx** members, int n, void* stream, db_ensemble** out) {
+  if (!members || n < 1 || !out) return DB_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return DB_ERR_ARG;
+    const db_params& a = members[0]->p;
+    const db_params& b = members[i]->p;
+    if (a.use_les != b.use_les || a.les_model_type != b.les_model_type || a.create_new_flow != b.create_new_flow ||
+        a.precision != b.precision || members[i]->time_step != members[0]->time_step || members[i]->timing) {
+      g_init_err = "db_ensemble_create: members must share use_les, les_model_type, create_new_flow, precision, "
+                   "time_step, and have stage timing off";
+      return DB_ERR_ARG;
+    }
+    for (int k = 0; k < i; ++k)
+      if (members[k] == members[i] || members[k]->st == members[i]->st) {
+        g_init_err = "db_ensemble_create: members must be distinct contexts on distinct streams";
+        return DB_ERR_ARG;
+      }
+  }
+  db_ensemble* e = new db_ensemble();
+  e->members.assign(members, members + n);
+  if (stream) e->st = (cudaStream_t)stream;
+  else {
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+      delete e;
+      g_init_err = "db_ensemble_create: stream creation failed";
+      return DB_ERR_CUDA;
+    }
+    e->own_stream = true;
+  }
+  e->ev.resize(n + 1, nullptr);
+  for (auto& v : e->ev)
+    if (cudaEventCreateWithFlags(&v, cudaEventDisableTiming) != cudaSuccess) {
+      db_ensemble_destroy(e);
+      g_init_err = "db_ensemble_create: event creation failed";
+      return DB_ERR_CUDA;
+    }
+  *out = e;
+  return DB_OK;
+}
+
+extern "C" int db_ensemble_destroy(db_ensemble* e) {
+  if (!e) return DB_ERR_ARG;
+  if (e->st) cudaStreamSynchronize(e->st);
+  for (int i = 0; i < 2; ++i)
+    if (e->graph[i]) cudaGraphExecDestroy(e->graph[i]);
+  for (auto v : e->ev)
+    if (v) cudaEventDestroy(v);
+  if (e->own_stream && e->st) cudaStreamDestroy(e->st);
+  delete e;
+  return DB_OK;
+}
+
+extern "C" const char* db_ensemble_error(const db_ensemble* e) { return e ? e->err.c_str() : g_init_err.c_str(); }
+
+extern "C" int db_ensemble_steps(db_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return DB_ERR_ARG;
+  db_ctx* c0 = e->members[0];
+  for (db_ctx* c : e->members)
+    if (need_net(c)) { e->err = c->err; return DB_ERR_STATE; }
+  const int n = (int)e->members.size();
+  for (int it = 0; it < nsteps; ++it) {
+    const int m = les_active(c0, c0->time_step + 1) ? 1 : 0;
+    if (!e->graph[m]) {
+      cudaGraph_t gr;
+      if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        e->err = "ensemble capture could not start";
+        return DB_ERR_CUDA;
+      }
+      cudaError_t er = cudaEventRecord(e->ev[0], e->st);
+      long long k0 = 0;
+      for (int i = 0; i < n && er == cudaSuccess; ++i) {
+        db_ctx* c = e->members[i];
+        er = cudaStreamWaitEvent(c->st, e->ev[0], 0);   // fork: the member's stream joins the capture
+        const long long before = c->launches;
+        if (er == cudaSuccess) er = one_step(c, m == 1);
+        k0 += c->launches - before;
+        c->launches = before;
+        if (er == cudaSuccess) er = cudaEventRecord(e->ev[1 + i], c->st);
+        if (er == cudaSuccess) er = cudaStreamWaitEvent(e->st, e->ev[1 + i], 0);   // join
+      }
+      cudaError_t er2 = cudaStreamEndCapture(e->st, &gr);
+      if (er != cudaSuccess || er2 != cudaSuccess) {
+        e->err = std::string("ensemble capture failed: ") + cudaGetErrorString(er != cudaSuccess ? er : er2);
+        return DB_ERR_CUDA;
+      }
+      er = cudaGraphInstantiate(&e->graph[m], gr, 0);
+      cudaGraphDestroy(gr);
+      if (er != cudaSuccess) {
+        e->graph[m] = nullptr;
+        e->err = std::string("ensemble graph instantiate failed: ") + cudaGetErrorString(er);
+        return DB_ERR_CUDA;
+      }
+      e->kernels[m] = k0;
+    }
+    if (cudaGraphLaunch(e->graph[m], e->st) != cudaSuccess) {
+      e->err = "ensemble graph launch failed";
+      return DB_ERR_CUDA;
+    }
+    for (db_ctx* c : e->members) {
+      c->time_step += 1;
+      c->launches += e->kernels[m] / n;
+    }
+  }
+  if (cudaStreamSynchronize(e->st) != cudaSuccess) {
+    e->err = std::string("ensemble step failed: ") + cudaGetErrorString(cudaGetLastError());
+    return DB_ERR_CUDA;
+  }
+  return DB_OK;
+}
+
 extern "C" int db_set_timing(db_ctx* c, int enable) {
   if (!c) return DB_ERR_ARG;
   if (enable && !c->ev[0][0])

@@ -31,6 +31,7 @@ EXPORTS = (
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
     "db_sgs_targets",
+    "db_ensemble_create", "db_ensemble_steps", "db_ensemble_destroy", "db_ensemble_error",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -98,10 +99,15 @@ def load(path: str | None = None):
     L.db_sgs_gemm_check.argtypes = [vp, vp, fp, ctypes.c_int, ctypes.c_int]
     L.db_set_sgs_net.argtypes = [vp, vp]
     L.db_les_eval.argtypes = [vp, ctypes.c_int, dp, dp, fp]
+    L.db_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp, ctypes.POINTER(vp)]
+    L.db_ensemble_steps.argtypes = [vp, ctypes.c_int]
+    L.db_ensemble_destroy.argtypes = [vp]
+    L.db_ensemble_error.argtypes = [vp]
+    L.db_ensemble_error.restype = ctypes.c_char_p
     L.db_sgs_targets.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, vp, vp,
                                  ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:
-        if name not in ("db_abi_version", "db_last_error"):
+        if name not in ("db_abi_version", "db_last_error", "db_ensemble_error"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -280,6 +280,21 @@ int db_les_eval(db_ctx* ctx, int model, double* nu_t, double* kappa_t, float* fe
 int db_sgs_targets(db_ctx* ctx, int fx, int fy, int fz, const double* gy_coarse, float* d_feat,
                    float* d_target, long long* npts);
 
+/* ---- ensembles (no counterpart in the reference, which runs one channel
+ * per MPI job): independent channels advanced together.  Each member is a
+ * context of its own (own stream, own parameters: seeds, Ri, ...); one CUDA
+ * graph per time step forks into every member's stream, runs that member's
+ * step (time_step += 1, three substeps, time += dt) and joins back, so one
+ * graph launch advances the whole ensemble and the members' kernels run
+ * concurrently.  Members must share use_les, les_model_type,
+ * create_new_flow, precision and time_step; they stay usable on their own
+ * (db_download_state etc.) between ensemble steps. ---- */
+typedef struct db_ensemble db_ensemble;
+int db_ensemble_create(db_ctx** members, int n, void* cuda_stream, db_ensemble** out);
+int db_ensemble_steps(db_ensemble* ens, int nsteps);
+int db_ensemble_destroy(db_ensemble* ens);
+const char* db_ensemble_error(const db_ensemble* ens);
+
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */
 
