@@ -258,6 +258,7 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   }
   if ((rc = dalloc(c, &s.tri, (size_t)4 * np))) { db_finalize(c); g_init_err = c->err; return rc; }
   if ((rc = dalloc(c, &s.sc, 1))) { db_finalize(c); g_init_err = c->err; return rc; }
+  g.flags = &s.sc->flags;
   size_t ntab = 4 * (size_t)np + g.kxs + g.nkzp;
   if ((rc = dalloc(c, &c->d_tab, ntab))) { db_finalize(c); g_init_err = c->err; return rc; }
   std::vector<double> tab;

@@ -38,6 +38,7 @@ struct Geom {
   const float2* twxf;      // the same rounded to FP32 (mixed path)
   const float2* twzf;
   int prec;                // 0: FP64 throughout; 1: mixed (FP32 physical / x-half)
+  int* flags;              // DevScalars::flags, for bounded waits that gave up
 };
 
 // Physics constants of the substep (host-computed once at init).

@@ -18,6 +18,7 @@
 // the z-pass load/store.
 #include "db_kernels.cuh"
 #include "fft_reg.cuh"
+#include "umma.cuh"
 
 namespace db {
 
@@ -27,7 +28,7 @@ namespace db {
 
 // physical -> Xh: sequence = rows (2q, 2q+1) of one plane/field
 template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet out, Geom g) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_x(FieldSet in, FieldSet 
 // Xh -> physical; fields f with bit f of dmask set are differentiated in x
 // (multiplied by i kx before the transform)
 template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet out, Geom g, unsigned dmask) {
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, unsigned dmask) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(FieldSet in, FieldSet 
 // accumulate: out = base + transform, base = out itself, or for rows 0, 1,
 // Nyp, Nyp+1 the ghost overlay (field f % 4) when one is given
 template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet out, Geom g, int accumulate,
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int accumulate,
                                                           const double2* __restrict__ ghost) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -124,13 +125,12 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet 
   const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
   C* sq = sm + seq * padded(N);
-  Twiddles<N, E, C> tw;
-  load_twiddles<N, E>(tw, lane, tw_z<R>(g));
+  const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
   const C* src = (const C*)in.p[f] + (long long)j * g.hp + kx;
   C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
-  fft_reg<N, -1>(v, lane, active, sq, tw);
+  fft_reg_lazy<N, -1>(v, lane, active, sq, twt);
   if (!active) return;
   double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
   const double2* base = dst;
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(FieldSet in, FieldSet 
 // packed spectral (FP64) -> Xh (zero-filled de-aliased rows, unnormalised);
 // fields f with bit f of dmask set are differentiated in z (times i kz)
 template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet out, Geom g, unsigned dmask,
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, unsigned dmask,
                                                           const double2* __restrict__ ghost) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -165,8 +165,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet 
   const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
   C* sq = sm + seq * padded(N);
-  Twiddles<N, E, C> tw;
-  load_twiddles<N, E>(tw, lane, tw_z<R>(g));
+  const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
   const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx;
   if (ghost) {   // rows 0, 1, Nyp, Nyp+1 from the overlay
     const int q = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
@@ -182,11 +181,174 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(FieldSet in, FieldSet 
     if (dz && kzp >= 0) a = cmul_i(a, g.kz[kzp]);
     v[q] = from_d2<C>(a);
   }
-  fft_reg<N, +1>(v, lane, active, sq, tw);
+  fft_reg_lazy<N, +1>(v, lane, active, sq, twt);
   if (!active) return;
   C* dst = (C*)out.p[f] + (long long)j * g.hp + kx;
 #pragma unroll
   for (int q = 0; q < E; ++q) dst[(long long)(lane + q * T) * g.kxs] = v[q];
+}
+
+// ---------------------------------------------------------------------------
+// x-pass kernels with TMA-staged input.  A CTA of NS sequences is persistent
+// over items (field, plane, block of NS row pairs); the rows of one item are
+// contiguous, so one thread brings the NEXT item's rows into the other half
+// of a double buffer with a single cp.async.bulk while the CTA transforms the
+// current item from shared memory: the load latency hides behind the FFT.
+constexpr uint32_t STAGE_WAIT = 1u << 24;
+
+template <int N, typename R>
+__global__ void __launch_bounds__(256, 2) k_fwd_x_st(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int nblk,
+                                                     int nitems) {
+  using C = typename CplxOf<R>::type;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int ns = blockDim.x / T;                       // sequences (row pairs) per item
+  const uint32_t row_bytes = N * sizeof(R);
+  const uint32_t item_bytes = 2u * ns * row_bytes;
+  R* stage0 = reinterpret_cast<R*>(sm_raw);
+  C* xbuf = reinterpret_cast<C*>(sm_raw + 2 * item_bytes);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm_raw + 2 * item_bytes + (size_t)ns * padded(N) * sizeof(C));
+  const int seq = threadIdx.x / T, lane = threadIdx.x % T;
+  C* sq = xbuf + seq * padded(N);
+  const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
+  auto src = [&](int it) -> const R* {
+    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    return (const R*)in.p[f] + (long long)j * g.pp + (long long)(2 * ns * b) * g.nx;
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (int)blockIdx.x < nitems) {
+    mbar_expect_tx(&mbar[0], item_bytes);
+    bulk_g2s(stage0, src(blockIdx.x), item_bytes, &mbar[0]);
+  }
+  int k = 0;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++k) {
+    const int s = k & 1;
+    const int nxt = it + gridDim.x;
+    if (threadIdx.x == 0 && nxt < nitems) {   // prefetch the next item into the other buffer
+      fence_async_smem();
+      mbar_expect_tx(&mbar[s ^ 1], item_bytes);
+      bulk_g2s(reinterpret_cast<unsigned char*>(stage0) + (s ^ 1) * item_bytes, src(nxt), item_bytes, &mbar[s ^ 1]);
+    }
+    const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
+    if (!got) {   // record it, let the prefetch in flight land (bounded), leave
+      if (threadIdx.x == 0) {
+        atomicOr(g.flags, 16);
+        if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
+      }
+      return;
+    }
+    const R* ra = reinterpret_cast<const R*>(reinterpret_cast<const unsigned char*>(stage0) + s * item_bytes) +
+                  (2 * seq) * N;
+    const R* rb = ra + N;
+    C v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) v[q] = mkc<C>(ra[lane + q * T], rb[lane + q * T]);
+    fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
+    SEQ_SYNC(N);
+#pragma unroll
+    for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
+    SEQ_SYNC(N);
+    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    C* oa = (C*)out.p[f] + (long long)j * g.hp + (long long)(2 * (ns * b + seq)) * g.kxs;
+    C* ob = oa + g.kxs;
+    const R sc = (R)(0.5 / (double)N);
+    for (int m = lane; m < g.kxs; m += T) {
+      C A = mkc<C>(0, 0), B = A;
+      if (m <= g.nkx) {
+        const C zm = sq[pidx(m)], zn = cconj(sq[pidx((N - m) & (N - 1))]);
+        A = mkc<C>((zm.x + zn.x) * sc, (zm.y + zn.y) * sc);
+        B = mkc<C>((zm.y - zn.y) * sc, -(zm.x - zn.x) * sc);
+      }
+      oa[m] = A;
+      ob[m] = B;
+    }
+    __syncthreads();   // stage s and the exchange buffers are free again
+  }
+}
+
+template <int N, typename R>
+__global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g,
+                                                      unsigned dmask, int nblk, int nitems) {
+  using C = typename CplxOf<R>::type;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int ns = blockDim.x / T;
+  const uint32_t row_bytes = (uint32_t)g.kxs * sizeof(C);
+  const uint32_t item_bytes = 2u * ns * row_bytes;
+  C* stage0 = reinterpret_cast<C*>(sm_raw);
+  C* xbuf = reinterpret_cast<C*>(sm_raw + 2 * item_bytes);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm_raw + 2 * item_bytes + (size_t)ns * padded(N) * sizeof(C));
+  const int seq = threadIdx.x / T, lane = threadIdx.x % T;
+  C* sq = xbuf + seq * padded(N);
+  const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
+  auto src = [&](int it) -> const C* {
+    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    return (const C*)in.p[f] + (long long)j * g.hp + (long long)(2 * ns * b) * g.kxs;
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (int)blockIdx.x < nitems) {
+    mbar_expect_tx(&mbar[0], item_bytes);
+    bulk_g2s(stage0, src(blockIdx.x), item_bytes, &mbar[0]);
+  }
+  int k = 0;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++k) {
+    const int s = k & 1;
+    const int nxt = it + gridDim.x;
+    if (threadIdx.x == 0 && nxt < nitems) {
+      fence_async_smem();
+      mbar_expect_tx(&mbar[s ^ 1], item_bytes);
+      bulk_g2s(reinterpret_cast<unsigned char*>(stage0) + (s ^ 1) * item_bytes, src(nxt), item_bytes, &mbar[s ^ 1]);
+    }
+    const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
+    if (!got) {   // record it, let the prefetch in flight land (bounded), leave
+      if (threadIdx.x == 0) {
+        atomicOr(g.flags, 16);
+        if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
+      }
+      return;
+    }
+    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    const C* ia = reinterpret_cast<const C*>(reinterpret_cast<const unsigned char*>(stage0) + s * item_bytes) +
+                  (2 * seq) * g.kxs;
+    const C* ib = ia + g.kxs;
+    const bool dx = (dmask >> f) & 1u;
+    C v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int e = lane + q * T;
+      C z = mkc<C>(0, 0);
+      if (e <= g.nkx) {
+        C A = ia[e], B = ib[e];
+        if (dx) { A = cmul_i(A, (R)g.kx[e]); B = cmul_i(B, (R)g.kx[e]); }
+        if (e == 0) { A.y = 0; B.y = 0; }
+        z = mkc<C>(A.x - B.y, A.y + B.x);
+      } else if (e >= N - g.nkx) {
+        C A = ia[N - e], B = ib[N - e];
+        if (dx) { A = cmul_i(A, (R)g.kx[N - e]); B = cmul_i(B, (R)g.kx[N - e]); }
+        z = mkc<C>(A.x + B.y, B.x - A.y);
+      }
+      v[q] = z;
+    }
+    fft_reg_lazy<N, +1>(v, lane, true, sq, twt);
+    R* ra = (R*)out.p[f] + (long long)j * g.pp + (long long)(2 * (ns * b + seq)) * g.nx;
+    R* rb = ra + g.nx;
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      ra[lane + q * T] = v[q].x;
+      rb[lane + q * T] = v[q].y;
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -216,27 +378,45 @@ static void smem_attr(K kern, size_t smem) {
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-template <int N, typename R>
-static void go_fwd_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
-  using C = typename CplxOf<R>::type;
+// sequences per item of the staged x-pass: cps (<= seqs_per_cta, divides nz/2)
+template <int N>
+static int xpass_cps(const Geom& g) {
   constexpr int ns = seqs_per_cta<N>();
   int npairs = g.nz / 2;
   int cps = ns < npairs ? ns : npairs;
   while (npairs % cps) --cps;
-  size_t smem = (size_t)cps * padded(N) * sizeof(C);
-  smem_attr(k_fwd_x<N, R>, smem);
-  k_fwd_x<N, R><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g);
+  return cps;
+}
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int N, typename R>
+static void go_fwd_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int cps = xpass_cps<N>(g);
+  const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * nf;
+  const size_t smem = 2 * (size_t)(2 * cps * N * sizeof(R)) + (size_t)cps * padded(N) * sizeof(C) + 16;
+  smem_attr(k_fwd_x_st<N, R>, smem);
+  const int grid = nitems < 2 * sm_count() ? nitems : 2 * sm_count();
+  k_fwd_x_st<N, R><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, nblk, nitems);
 }
 template <int N, typename R>
 static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, cudaStream_t st) {
   using C = typename CplxOf<R>::type;
-  constexpr int ns = seqs_per_cta<N>();
-  int npairs = g.nz / 2;
-  int cps = ns < npairs ? ns : npairs;
-  while (npairs % cps) --cps;
-  size_t smem = (size_t)cps * padded(N) * sizeof(C);
-  smem_attr(k_inv_x<N, R>, smem);
-  k_inv_x<N, R><<<dim3(npairs / cps, g.np, nf), cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask);
+  const int cps = xpass_cps<N>(g);
+  const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * nf;
+  const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
+  smem_attr(k_inv_x_st<N, R>, smem);
+  const int grid = nitems < 2 * sm_count() ? nitems : 2 * sm_count();
+  k_inv_x_st<N, R><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems);
 }
 template <int N, typename R>
 static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, const double2* ghost,

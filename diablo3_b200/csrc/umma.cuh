@@ -111,6 +111,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
   return false;
 }
 
+// arm the mbarrier's current phase with one arrival and `bytes` of expected
+// asynchronous transactions
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+
+// TMA bulk copy global -> shared of `bytes` (multiple of 16, both addresses
+// 16-byte aligned), completing on the mbarrier; no multicast
+__device__ __forceinline__ void bulk_g2s(void* smem, const void* gmem, uint32_t bytes, uint64_t* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(smem)),
+               "l"(gmem), "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+
 // 16 consecutive FP32 columns of this thread's tensor-memory lane
 // (warp w reads lanes 32 (w % 4) .. 32 (w % 4) + 31)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {

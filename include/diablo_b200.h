@@ -50,7 +50,8 @@ enum db_flag {
   DB_FLAG_NONFINITE = 1,   /* NaN/Inf found in the velocity or buoyancy */
   DB_FLAG_DT_NONPOS = 2,   /* courant found dt <= 0 (reference flow.f90:812) */
   DB_FLAG_DT_CAPPED = 4,   /* courant capped dt at 1000 (flow.f90:817) */
-  DB_FLAG_DT_TINY = 8      /* next dt < 1e-10 (flow.f90:848) */
+  DB_FLAG_DT_TINY = 8,     /* next dt < 1e-10 (flow.f90:848) */
+  DB_FLAG_WAIT_TIMEOUT = 16 /* a bounded device wait gave up (data of that step invalid) */
 };
 
 /* Field ids for db_upload_field / db_download_field. */
