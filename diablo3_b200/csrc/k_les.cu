@@ -44,7 +44,7 @@ namespace db {
 // q = rows 0, 1, Nyp, Nyp+1) that the inverse transforms read in place of
 // the state's rows; the final forward transform of the physical fields
 // carries them into the new state exactly as in the reference.
-__global__ void k_les_bc(State s, Geom g, Phys ph) {
+__global__ void k_les_bc(const __grid_constant__ State s, Geom g, Phys ph) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx >= g.kxs) return;
   const long long c0 = (long long)kzp * g.kxs + kx, sp = g.sp;
@@ -131,7 +131,7 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 // neighbours; a point whose features leave the training range
 // (s.sgs_range: lo[16], hi[16]) keeps its AMD value.
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
+__global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ State s, Geom g, Phys ph) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
   const long long pp = g.pp;
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(State s, Geom g, Phys ph) {
 constexpr int TB = 8;
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_thomas_les(State s, Geom g, int rk) {
+__global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ State s, Geom g, int rk) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= g.nx) return;
   const int np = g.np, Nyp = g.ny;

@@ -33,7 +33,7 @@ struct SgsData {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_sgs_targets(State s, Geom g, SgsData d) {
+__global__ void __launch_bounds__(128) k_sgs_targets(const __grid_constant__ State s, Geom g, SgsData d) {
   const int xc = blockIdx.x * blockDim.x + threadIdx.x;
   const int zc = blockIdx.y;
   const int k = d.kmin + blockIdx.z;

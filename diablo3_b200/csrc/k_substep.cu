@@ -53,7 +53,7 @@ __device__ __forceinline__ C sepp(const C* z, int m, int part) {
 }
 
 template <int N, bool LES, typename R>
-__global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(State s, Geom g) {
+__global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(const __grid_constant__ State s, Geom g) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -72,8 +72,7 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
     return;
   }
   C* sq = sm + seq * padded(N);
-  Twiddles<N, E, C> tw;
-  load_twiddles<N, E>(tw, lane, tw_x<R>(g));
+  const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
   const R* U1 = (const R*)s.u1;
   const R* U2 = (const R*)s.u2;
   const R* U3 = (const R*)s.u3;
@@ -136,7 +135,7 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(Sta
     }
     v[q] = mkc<C>(a, b);
   }
-  fft_reg<N, -1>(v, lane, true, sq, tw);
+  fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
   SEQ_SYNC(N);
 #pragma unroll
   for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
@@ -479,7 +478,7 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 constexpr int TX = 32;
 
 template <typename R>
-__global__ void __launch_bounds__(256, 3) k_thomas(State s, Geom g) {
+__global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g) {
   extern __shared__ double tile[];          // [np][TX]
   __shared__ double carry[8][TX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -637,7 +636,7 @@ __global__ void k_pfac(Geom g, double2* pfac) {
 }
 
 // divergence removal + pressure update, one thread per (kx, kzp) column
-__global__ void __launch_bounds__(128) k_rem_div(State s, Geom g, int rk, int update_cp) {
+__global__ void __launch_bounds__(128) k_rem_div(const __grid_constant__ State s, Geom g, int rk, int update_cp) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx > g.nkx) return;
   const int Nyp = g.ny;
@@ -703,7 +702,7 @@ __global__ void __launch_bounds__(128) k_rem_div(State s, Geom g, int rk, int up
 __device__ __forceinline__ unsigned long long dbits(double v) { return (unsigned long long)__double_as_longlong(v); }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_courant_reduce(State s, Geom g, Phys ph, CflCtl ctl) {
+__global__ void __launch_bounds__(256) k_courant_reduce(const __grid_constant__ State s, Geom g, Phys ph, CflCtl ctl) {
   DevScalars* sc = s.sc;
   const R* U1 = (const R*)s.u1;
   const R* U2 = (const R*)s.u2;
@@ -788,7 +787,7 @@ __global__ void k_step_begin(DevScalars* sc) { sc->time_step += 1; }
 __global__ void k_step_end(DevScalars* sc) { sc->time += sc->delta_t; }
 
 // max |div| at GYF rows 2..Nyp-1 (the rows rem_div zeroes)
-__global__ void k_divergence(State s, Geom g) {
+__global__ void k_divergence(const __grid_constant__ State s, Geom g) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   double m = 0.0;
   if (kx <= g.nkx) {
@@ -809,7 +808,7 @@ __global__ void k_divergence(State s, Geom g) {
 }
 
 // apply_BC_vel_mpi_post on the spectral velocity (flow.f90:1161-1360)
-__global__ void k_bc_vel_post(State s, Geom g, Phys ph) {
+__global__ void k_bc_vel_post(const __grid_constant__ State s, Geom g, Phys ph) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx > g.nkx) return;
   const long long c0 = (long long)kzp * g.kxs + kx;
