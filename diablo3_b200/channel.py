@@ -153,6 +153,12 @@ class Channel:
                                        ctypes.c_void_p(tgt.data_ptr()), ctypes.byref(n)))
         return feat, tgt
 
+    def autotune(self) -> str:
+        """Pick launch shapes by timing them on this context; returns the report."""
+        buf = ctypes.create_string_buffer(4096)
+        self._ck(self.L.db_autotune(self.h, buf, len(buf)))
+        return buf.value.decode()
+
     def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
         self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
 

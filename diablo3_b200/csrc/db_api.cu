@@ -865,6 +865,115 @@ extern "C" int db_ensemble_steps(db_ensemble* e, int nsteps) {
   return DB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// autotuner: launch shapes timed on the context's own scratch buffers
+
+template <typename F>
+static float time_ms(db_ctx* c, F&& launch, int reps = 3) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  launch();   // warm-up (also sets kernel attributes)
+  cudaEventRecord(a, c->st);
+  for (int i = 0; i < reps; ++i) launch();
+  cudaEventRecord(b, c->st);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / reps;
+}
+
+extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
+  if (!c) return DB_ERR_ARG;
+  if (c->timing) return fail(c, DB_ERR_STATE, "turn stage timing off before db_autotune");
+  Geom& g = c->g;
+  State& s = c->s;
+  std::string rep;
+  char buf[160];
+  const int T = g.nx / 8 > 0 ? g.nx / 8 : 1;     // threads per x sequence
+  const int Tz = g.nz / 8 > 0 ? g.nz / 8 : 1;    // threads per z sequence
+  // x-pass: sequences per staged item x persistent CTAs per SM (inverse x of 4 fields)
+  {
+    float best = 1e30f;
+    int bc = 0, bg = 0;
+    for (int cps = T >= 32 ? 1 : 32 / T; cps * T <= 256; cps *= 2)   // whole warps
+      for (int gsm = 1; gsm <= 4; ++gsm) {
+        g.tune_xcps = cps;
+        g.tune_xgrid = gsm;
+        const float ms = time_ms(c, [&] {
+          launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.r1, s.r2, s.r3, s.rth), 4, c->st);
+        });
+        if (cudaGetLastError() != cudaSuccess) continue;
+        snprintf(buf, sizeof buf, "x-pass cps %d ctas/SM %d: %.3f ms\n", cps, gsm, ms);
+        rep += buf;
+        if (ms < best) { best = ms; bc = cps; bg = gsm; }
+      }
+    g.tune_xcps = bc;
+    g.tune_xgrid = bg;
+  }
+  // z-pass: sequences per CTA (inverse z of 4 fields)
+  {
+    float best = 1e30f;
+    int bn = 0;
+    for (int ns = Tz >= 32 ? 1 : 32 / Tz; ns * Tz <= 256; ns *= 2) {
+      g.tune_zns = ns;
+      const float ms = time_ms(c, [&] {
+        launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, c->st);
+      });
+      if (cudaGetLastError() != cudaSuccess) continue;
+      snprintf(buf, sizeof buf, "z-pass seqs/CTA %d: %.3f ms\n", ns, ms);
+      rep += buf;
+      if (ms < best) { best = ms; bn = ns; }
+    }
+    g.tune_zns = bn;
+  }
+  // products: persistent CTAs per SM (physical u in, x-half products out)
+  {
+    float best = 1e30f;
+    int bg = 0;
+    for (int gsm = 1; gsm <= 4; ++gsm) {
+      g.tune_pgrid = gsm;
+      const float ms = time_ms(c, [&] { launch_products(g, s, c->st, false); });
+      if (cudaGetLastError() != cudaSuccess) continue;
+      snprintf(buf, sizeof buf, "products ctas/SM %d: %.3f ms\n", gsm, ms);
+      rep += buf;
+      if (ms < best) { best = ms; bg = gsm; }
+    }
+    g.tune_pgrid = bg;
+  }
+  // LES Thomas: threads per CTA (matrices from the current dt)
+  if (c->p.use_les) {
+    CK(launch_tri_coef(g, c->ph, s, 0, c->st));
+    float best = 1e30f;
+    int bt = 0;
+    for (int tb = 32; tb <= 128; tb *= 2) {   // kernel bound: 128 threads
+      g.tune_les_tb = tb;
+      const float ms = time_ms(c, [&] { launch_thomas_les(g, s, 0, c->st); });
+      if (cudaGetLastError() != cudaSuccess) continue;
+      snprintf(buf, sizeof buf, "LES Thomas threads/CTA %d: %.3f ms\n", tb, ms);
+      rep += buf;
+      if (ms < best) { best = ms; bt = tb; }
+    }
+    g.tune_les_tb = bt;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  snprintf(buf, sizeof buf, "chosen: x-pass cps %d ctas/SM %d, z-pass seqs/CTA %d, products ctas/SM %d, LES Thomas %d\n",
+           g.tune_xcps, g.tune_xgrid, g.tune_zns, g.tune_pgrid, g.tune_les_tb);
+  rep += buf;
+  for (int i = 0; i < 2; ++i)   // captured steps hold the old launch shapes
+    if (c->graph[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph[i] = nullptr;
+    }
+  if (report && report_len > 0) {
+    strncpy(report, rep.c_str(), (size_t)report_len - 1);
+    report[report_len - 1] = 0;
+  }
+  return DB_OK;
+}
+
 extern "C" int db_set_timing(db_ctx* c, int enable) {
   if (!c) return DB_ERR_ARG;
   if (enable && !c->ev[0][0])

@@ -39,6 +39,12 @@ struct Geom {
   const float2* twzf;
   int prec;                // 0: FP64 throughout; 1: mixed (FP32 physical / x-half)
   int* flags;              // DevScalars::flags, for bounded waits that gave up
+  // launch shapes picked by db_autotune (0 = built-in default)
+  int tune_xcps;           // x-pass: sequences (row pairs) per staged item
+  int tune_xgrid;          // x-pass: persistent CTAs per SM
+  int tune_zns;            // z-pass: sequences (kx columns) per CTA
+  int tune_les_tb;         // LES Thomas: threads per CTA
+  int tune_pgrid;          // products: persistent CTAs per SM
 };
 
 // Physics constants of the substep (host-computed once at init).

@@ -132,6 +132,7 @@ struct State {
 };
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
+int sm_count();   // SMs of the current device (cached)
 cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les = false);
 // ghost: the LES overlay, when the inverse transforms of this substep used it
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,

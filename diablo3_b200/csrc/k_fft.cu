@@ -16,6 +16,7 @@
 // R is the real type of the physical and x-half fields: double, or float on
 // the mixed path, where the spectral state stays FP64 and is converted on
 // the z-pass load/store.
+#include "../../include/diablo_b200.h"
 #include "db_kernels.cuh"
 #include "fft_reg.cuh"
 #include "umma.cuh"
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_x_st(const __grid_constant__ Fie
     const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
     if (!got) {   // record it, let the prefetch in flight land (bounded), leave
       if (threadIdx.x == 0) {
-        atomicOr(g.flags, 16);
+        atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
         if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
       }
       return;
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
     const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
     if (!got) {   // record it, let the prefetch in flight land (bounded), leave
       if (threadIdx.x == 0) {
-        atomicOr(g.flags, 16);
+        atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
         if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
       }
       return;
@@ -383,11 +384,18 @@ template <int N>
 static int xpass_cps(const Geom& g) {
   constexpr int ns = seqs_per_cta<N>();
   int npairs = g.nz / 2;
-  int cps = ns < npairs ? ns : npairs;
+  int want = (g.tune_xcps > 0 && g.tune_xcps <= ns) ? g.tune_xcps : ns;
+  int cps = want < npairs ? want : npairs;
   while (npairs % cps) --cps;
   return cps;
 }
-static int sm_count() {
+static int xpass_ctas_per_sm(const Geom& g) { return g.tune_xgrid > 0 ? g.tune_xgrid : 2; }
+template <int N>
+static int zpass_ns(const Geom& g) {
+  constexpr int ns = seqs_per_cta<N>();
+  return (g.tune_zns > 0 && g.tune_zns <= ns) ? g.tune_zns : ns;
+}
+int sm_count() {
   static int n = 0;
   if (!n) {
     int dev = 0;
@@ -405,7 +413,8 @@ static void go_fwd_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStr
   const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * nf;
   const size_t smem = 2 * (size_t)(2 * cps * N * sizeof(R)) + (size_t)cps * padded(N) * sizeof(C) + 16;
   smem_attr(k_fwd_x_st<N, R>, smem);
-  const int grid = nitems < 2 * sm_count() ? nitems : 2 * sm_count();
+  const int gmax = xpass_ctas_per_sm(g) * sm_count();
+  const int grid = nitems < gmax ? nitems : gmax;
   k_fwd_x_st<N, R><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, nblk, nitems);
 }
 template <int N, typename R>
@@ -415,14 +424,15 @@ static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * nf;
   const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
   smem_attr(k_inv_x_st<N, R>, smem);
-  const int grid = nitems < 2 * sm_count() ? nitems : 2 * sm_count();
+  const int gmax = xpass_ctas_per_sm(g) * sm_count();
+  const int grid = nitems < gmax ? nitems : gmax;
   k_inv_x_st<N, R><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems);
 }
 template <int N, typename R>
 static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, const double2* ghost,
                        cudaStream_t st) {
   using C = typename CplxOf<R>::type;
-  constexpr int ns = seqs_per_cta<N>();
+  const int ns = zpass_ns<N>(g);
   size_t smem = (size_t)ns * padded(N) * sizeof(C);
   smem_attr(k_fwd_z<N, R>, smem);
   k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, acc, ghost);
@@ -431,7 +441,7 @@ template <int N, typename R>
 static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
                        cudaStream_t st) {
   using C = typename CplxOf<R>::type;
-  constexpr int ns = seqs_per_cta<N>();
+  const int ns = zpass_ns<N>(g);
   size_t smem = (size_t)ns * padded(N) * sizeof(C);
   smem_attr(k_inv_z<N, R>, smem);
   k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);

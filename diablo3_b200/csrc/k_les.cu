@@ -415,7 +415,8 @@ cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaSt
   return cudaGetLastError();
 }
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
-  const int bx = g.nx < 128 ? g.nx : 128;
+  const int want = (g.tune_les_tb > 0 && g.tune_les_tb <= 128) ? g.tune_les_tb : 128;   // powers of two
+  const int bx = g.nx < want ? g.nx : want;
   if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
   else k_thomas_les<double><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
   return cudaGetLastError();

@@ -21,9 +21,11 @@
 //  k_courant    : CFL reduction and dt scheduling (flow.f90:746-857).
 #include <math.h>
 
+#include "../../include/diablo_b200.h"
 #include "db_bc.cuh"
 #include "db_kernels.cuh"
 #include "fft_reg.cuh"
+#include "umma.cuh"
 
 namespace db {
 
@@ -52,6 +54,111 @@ __device__ __forceinline__ C sepp(const C* z, int m, int part) {
   return mkc<C>((R)0.5 * (zm.y - zn.y), (R)-0.5 * (zm.x - zn.x));
 }
 
+// rows j-1 (m), j, j+1 (p) of u1, u2, u3, th
+template <typename R>
+struct ProdRows {
+  const R *u1m, *u1, *u1p, *u2m, *u2, *u2p, *u3m, *u3, *u3p, *thm, *th, *thp;
+};
+
+// per-plane metric factors: 1 / (2 dyf_j), 1 / dy_j, dyf_j / (2 dy_j),
+// dyf_{j-1} / (2 dy_j) (the y-differences and GY interpolations below
+// multiply by these instead of dividing per point)
+template <typename R>
+struct ProdY {
+  R i2dyf, idy, wj, wjm;
+  __device__ ProdY(const Geom& g, int j) {
+    const double dyj = g.dy[j], dyfj = g.dyf[j], dyfjm = (j >= 1) ? g.dyf[j - 1] : 0.0;
+    i2dyf = (R)(1.0 / (2.0 * dyfj));
+    idy = (R)(1.0 / dyj);
+    wj = (R)(dyfj / (2.0 * dyj));
+    wjm = (R)(dyfjm / (2.0 * dyj));
+  }
+};
+
+// the real pair (a, b) sequence `seq` of group `grp` carries at point x
+template <bool LES, typename R>
+__device__ __forceinline__ void prod_ab(const ProdRows<R>& P, const R* const* LS, long long o0, int grp, int seq, int x,
+                                        bool r2, bool rt, const ProdY<R>& y, R& a, R& b) {
+  const R qrt = 0.25;
+  a = 0;
+  b = 0;
+  if (grp == 0) {
+    const R u1 = P.u1[x], u3 = P.u3[x];
+    if (seq == 0) {
+      const R u1p = P.u1p[x], u1m = P.u1m[x];
+      const R u2p = P.u2p[x], u2 = P.u2[x];
+      a = u1 * u1;
+      b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) * y.i2dyf;
+      if (LES) { a += __ldg(LS[0] + o0 + x); b += __ldg(LS[1] + o0 + x); }
+    } else if (seq == 1) {
+      const R u3p = P.u3p[x], u3m = P.u3m[x];
+      const R u2p = P.u2p[x], u2 = P.u2[x];
+      a = u3 * u1;
+      b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) * y.i2dyf;
+      if (LES) { a += __ldg(LS[2] + o0 + x); b += __ldg(LS[3] + o0 + x); }
+    } else {
+      a = u3 * u3;
+      if (LES) a += __ldg(LS[4] + o0 + x);
+    }
+  } else {
+    const R u2 = P.u2[x];
+    if (seq == 0) {
+      if (r2) {
+        const R u1 = P.u1[x], u1m = P.u1m[x];
+        const R pp = u2 + P.u2p[x], qq = u2 + P.u2m[x];
+        a = (y.wj * u1 + y.wjm * u1m) * u2;
+        b = (qrt * (pp * pp) - qrt * (qq * qq)) * y.idy;
+        if (LES) a += __ldg(LS[5] + o0 + x);
+      }
+    } else if (seq == 1) {
+      if (rt) {
+        const R th = P.th[x], thp = P.thp[x], thm = P.thm[x];
+        const R u2p = P.u2p[x];
+        a = th * P.u1[x];
+        b = (thp * u2p + th * u2p - th * u2 - thm * u2) * y.i2dyf;
+        if (LES) a += __ldg(LS[7] + o0 + x);
+      }
+    } else {
+      if (r2) a = (y.wj * P.u3[x] + y.wjm * P.u3m[x]) * u2;
+      if (rt) b = P.th[x] * P.u3[x];
+      if (LES) {
+        if (r2) a += __ldg(LS[6] + o0 + x);
+        if (rt) b += __ldg(LS[8] + o0 + x);
+      }
+    }
+  }
+}
+
+// outputs of one transformed sequence (in sq, natural order), scaled by
+// 1/Nx: an N-type output ikx X(a) + X(b), and for s1 (group 0) / s2 (both
+// groups) the parts
+template <int N, typename C>
+__device__ __forceinline__ void prod_out(C* const* xh, const C* sq, const Geom& g, long long hrow, int grp, int seq,
+                                         int lane, bool r2, bool rt) {
+  using R = typename RealOf<C>::type;
+  constexpr int T = FftShape<N>::T;
+  const R sc = (R)(1.0 / (double)N);
+  const bool n_out = (seq < 2) ? ((grp == 0) || (seq == 0 ? r2 : rt)) : false;
+  const int o_n = (grp == 0) ? (seq == 0 ? 0 : 2) : (seq == 0 ? 4 : 6);
+  const C Z = mkc<C>(0, 0);
+  for (int mm = lane; mm < g.kxs; mm += T) {
+    const bool live = mm <= g.nkx;
+    const C A = live ? sepp<N>(sq, mm, 0) : Z;
+    const C B = live ? sepp<N>(sq, mm, 1) : Z;
+    if (seq < 2) {
+      const R k = (R)g.kx[mm];
+      xh[o_n][hrow + mm] = n_out ? mkc<C>((B.x - k * A.y) * sc, (B.y + k * A.x) * sc) : Z;
+    }
+    if (grp == 0 && seq == 1) xh[1][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M1
+    if (grp == 0 && seq == 2) xh[3][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M3
+    if (grp == 1 && seq == 2) {
+      xh[5][hrow + mm] = r2 ? mkc<C>(A.x * sc, A.y * sc) : Z;  // M2
+      xh[7][hrow + mm] = rt ? mkc<C>(B.x * sc, B.y * sc) : Z;  // MT
+    }
+  }
+}
+
+// One CTA per (z, j, group), rows read from global memory (Nx > 512).
 template <int N, bool LES, typename R>
 __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(const __grid_constant__ State s, Geom g) {
   using C = typename CplxOf<R>::type;
@@ -73,66 +180,21 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(con
   }
   C* sq = sm + seq * padded(N);
   const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
+  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
+  const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
+  const long long om = o0 - g.pp, op = o0 + g.pp;
   const R* U1 = (const R*)s.u1;
   const R* U2 = (const R*)s.u2;
   const R* U3 = (const R*)s.u3;
   const R* TH = (const R*)s.th;
-  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
-  const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
-  const long long om = o0 - g.pp, op = o0 + g.pp;
-  const R dyj = (R)g.dy[j], dyfj = (R)g.dyf[j];
-  const R dyfjm = (j >= 1) ? (R)g.dyf[j - 1] : (R)0;
-  const R two = 2, qrt = 0.25;
+  const ProdRows<R> P{U1 + om, U1 + o0, U1 + op, U2 + om, U2 + o0, U2 + op,
+                      U3 + om, U3 + o0, U3 + op, TH + om, TH + o0, TH + op};
+  const ProdY<R> y(g, j);
   C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) {
-    const int x = lane + q * T;
-    R a = 0, b = 0;
-    if (grp == 0) {
-      const R u1 = __ldg(U1 + o0 + x), u3 = __ldg(U3 + o0 + x);
-      if (seq == 0) {
-        const R u1p = __ldg(U1 + op + x), u1m = __ldg(U1 + om + x);
-        const R u2p = __ldg(U2 + op + x), u2 = __ldg(U2 + o0 + x);
-        a = u1 * u1;
-        b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) / (two * dyfj);
-        if (LES) { a += __ldg(LS[0] + o0 + x); b += __ldg(LS[1] + o0 + x); }
-      } else if (seq == 1) {
-        const R u3p = __ldg(U3 + op + x), u3m = __ldg(U3 + om + x);
-        const R u2p = __ldg(U2 + op + x), u2 = __ldg(U2 + o0 + x);
-        a = u3 * u1;
-        b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) / (two * dyfj);
-        if (LES) { a += __ldg(LS[2] + o0 + x); b += __ldg(LS[3] + o0 + x); }
-      } else {
-        a = u3 * u3;
-        if (LES) a += __ldg(LS[4] + o0 + x);
-      }
-    } else {
-      const R u2 = __ldg(U2 + o0 + x);
-      if (seq == 0) {
-        if (r2) {
-          const R u1 = __ldg(U1 + o0 + x), u1m = __ldg(U1 + om + x);
-          const R pp = u2 + __ldg(U2 + op + x), qq = u2 + __ldg(U2 + om + x);
-          a = ((dyfj * u1 + dyfjm * u1m) / (two * dyj)) * u2;
-          b = (qrt * (pp * pp) - qrt * (qq * qq)) / dyj;
-          if (LES) a += __ldg(LS[5] + o0 + x);
-        }
-      } else if (seq == 1) {
-        if (rt) {
-          const R th = __ldg(TH + o0 + x), thp = __ldg(TH + op + x), thm = __ldg(TH + om + x);
-          const R u2p = __ldg(U2 + op + x);
-          a = th * __ldg(U1 + o0 + x);
-          b = (thp * u2p + th * u2p - th * u2 - thm * u2) / (two * dyfj);
-          if (LES) a += __ldg(LS[7] + o0 + x);
-        }
-      } else {
-        if (r2) a = ((dyfj * __ldg(U3 + o0 + x) + dyfjm * __ldg(U3 + om + x)) / (two * dyj)) * u2;
-        if (rt) b = __ldg(TH + o0 + x) * __ldg(U3 + o0 + x);
-        if (LES) {
-          if (r2) a += __ldg(LS[6] + o0 + x);
-          if (rt) b += __ldg(LS[8] + o0 + x);
-        }
-      }
-    }
+    R a, b;
+    prod_ab<LES>(P, LS, o0, grp, seq, lane + q * T, r2, rt, y, a, b);
     v[q] = mkc<C>(a, b);
   }
   fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
@@ -140,25 +202,123 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(con
 #pragma unroll
   for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
   SEQ_SYNC(N);
-  // outputs of this sequence, scaled by 1/Nx: an N-type output
-  // ikx X(a) + X(b), and for s1 (group 0) / s2 (both groups) the parts
-  const R sc = (R)(1.0 / (double)N);
-  const bool n_out = (seq < 2) ? ((grp == 0) || (seq == 0 ? r2 : rt)) : false;
-  const int o_n = (grp == 0) ? (seq == 0 ? 0 : 2) : (seq == 0 ? 4 : 6);
-  const C Z = mkc<C>(0, 0);
-  for (int mm = lane; mm < g.kxs; mm += T) {
-    const bool live = mm <= g.nkx;
-    const C A = live ? sepp<N>(sq, mm, 0) : Z;
-    const C B = live ? sepp<N>(sq, mm, 1) : Z;
-    if (seq < 2) {
-      const R k = (R)g.kx[mm];
-      xh[o_n][hrow + mm] = n_out ? mkc<C>((B.x - k * A.y) * sc, (B.y + k * A.x) * sc) : Z;
+  prod_out<N>(xh, sq, g, hrow, grp, seq, lane, r2, rt);
+}
+
+// Persistent y-marching form (Nx <= 512).  A work item is a block of zr
+// consecutive z rows and a range of planes j; the CTA walks the planes in
+// order, keeping the rows j-1, j, j+1 of u1, u2, u3, th in a ring of four
+// shared-memory slots.  While plane j is transformed, a TMA bulk copy brings
+// plane j+2 into the slot plane j-2 occupied, so the loads overlap the
+// FFTs.  Thread layout: sequence (zi, seq) = (sidx / 3, sidx % 3).
+constexpr int PROD_SLOTS = 4;
+constexpr uint32_t PROD_WAIT = 1u << 24;
+
+template <int N>
+constexpr int prod_zr() { return FftShape<N>::T >= 64 ? 1 : 64 / FftShape<N>::T; }
+
+template <int N, bool LES, typename R>
+__global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ State s, Geom g, int zr, int nzb,
+                                                        int jlen, int nitems) {
+  using C = typename CplxOf<R>::type;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const uint32_t fbytes = (uint32_t)zr * N * sizeof(R);   // one field, zr rows of one plane
+  const uint32_t slot_bytes = 4u * fbytes;
+  C* xbuf = reinterpret_cast<C*>(sm_raw + PROD_SLOTS * slot_bytes);
+  uint64_t* mbar =
+      reinterpret_cast<uint64_t*>(sm_raw + PROD_SLOTS * slot_bytes + (size_t)3 * zr * padded(N) * sizeof(C));
+  const int sidx = threadIdx.x / T, lane = threadIdx.x % T;
+  const int zi = sidx / 3, seq = sidx % 3;
+  C* sq = xbuf + sidx * padded(N);
+  const C* twt = tw_x<R>(g);
+  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
+  C* const* xh = reinterpret_cast<C* const*>(s.xh);
+  const int np = g.np;
+  if (threadIdx.x < PROD_SLOTS) mbar_init(&mbar[threadIdx.x], 1);
+  __syncthreads();
+  uint32_t par = 0;    // parity of the next completion of each slot
+  uint32_t pend = 0;   // slots with a copy issued and not yet waited for
+  auto issue = [&](int jr, int z0) {   // plane jr of the four fields into its slot
+    const int sl = jr & (PROD_SLOTS - 1);
+    if (threadIdx.x == 0) {
+      fence_async_smem();
+      unsigned char* dst = sm_raw + sl * slot_bytes;
+      const long long off = (long long)jr * g.pp + (long long)z0 * g.nx;
+      mbar_expect_tx(&mbar[sl], slot_bytes);
+      bulk_g2s(dst, (const R*)s.u1 + off, fbytes, &mbar[sl]);
+      bulk_g2s(dst + fbytes, (const R*)s.u2 + off, fbytes, &mbar[sl]);
+      bulk_g2s(dst + 2 * fbytes, (const R*)s.u3 + off, fbytes, &mbar[sl]);
+      bulk_g2s(dst + 3 * fbytes, (const R*)s.th + off, fbytes, &mbar[sl]);
     }
-    if (grp == 0 && seq == 1) xh[1][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M1
-    if (grp == 0 && seq == 2) xh[3][hrow + mm] = mkc<C>(A.x * sc, A.y * sc);       // M3
-    if (grp == 1 && seq == 2) {
-      xh[5][hrow + mm] = r2 ? mkc<C>(A.x * sc, A.y * sc) : Z;  // M2
-      xh[7][hrow + mm] = rt ? mkc<C>(B.x * sc, B.y * sc) : Z;  // MT
+    pend |= 1u << sl;
+  };
+  auto wait_row = [&](int jr) -> bool {
+    const int sl = jr & (PROD_SLOTS - 1);
+    const bool ok = mbar_wait(&mbar[sl], (par >> sl) & 1u, PROD_WAIT);
+    par ^= 1u << sl;
+    pend &= ~(1u << sl);
+    return ok;
+  };
+  auto row = [&](int jr, int f) -> const R* {
+    return reinterpret_cast<const R*>(sm_raw + (jr & (PROD_SLOTS - 1)) * slot_bytes + f * fbytes) + zi * N;
+  };
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int zb = it % nzb, jc = it / nzb;
+    const int z0 = zb * zr, z = z0 + zi;
+    const int jlo = jc * jlen, jhi = min(np - 1, jlo + jlen - 1);
+    const int jtop = min(np - 1, jhi + 1);
+    __syncthreads();   // every slot is free
+    for (int jr = max(0, jlo - 1); jr <= min(jtop, jlo + 1); ++jr) issue(jr, z0);
+    for (int j = jlo; j <= jhi; ++j) {
+      bool ok = true;
+      if (j == jlo) {
+        for (int jr = max(0, jlo - 1); jr <= min(jtop, jlo + 1); ++jr) ok = wait_row(jr) && ok;
+      } else if (j + 1 <= jtop) {
+        ok = wait_row(j + 1);
+      }
+      if (__syncthreads_and(ok ? 1 : 0) == 0) {   // a copy never landed: record, drain (bounded), leave
+        if (threadIdx.x == 0) {
+          atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
+          for (int sl = 0; sl < PROD_SLOTS; ++sl)
+            if (pend >> sl & 1u) mbar_wait(&mbar[sl], (par >> sl) & 1u, PROD_WAIT);
+        }
+        return;
+      }
+      if (j + 2 <= jtop) issue(j + 2, z0);   // into the slot of plane j - 2
+      const bool r1 = in_rng(j, g.jstart, g.jend);
+      const bool r2 = in_rng(j, 2, g.ny);
+      const bool rt = in_rng(j, g.jstart_th, g.jend_th);
+      const ProdY<R> y(g, j);
+      const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
+      const long long hrow = (long long)j * g.hp + (long long)z * g.kxs;
+      for (int grp = 0; grp < 2; ++grp) {
+        if ((grp == 0 && !r1) || (grp == 1 && !(r2 || rt))) {   // uniform over the CTA
+          const long long hrow0 = (long long)j * g.hp + (long long)z0 * g.kxs;
+          const int w = zr * g.kxs;
+          for (int idx = threadIdx.x; idx < 4 * w; idx += blockDim.x)
+            xh[4 * grp + idx / w][hrow0 + idx % w] = mkc<C>(0, 0);
+          continue;
+        }
+        const int jm = j >= 1 ? j - 1 : j, jp = j + 1 <= np - 1 ? j + 1 : j;
+        const ProdRows<R> P{row(jm, 0), row(j, 0), row(jp, 0), row(jm, 1), row(j, 1), row(jp, 1),
+                            row(jm, 2), row(j, 2), row(jp, 2), row(jm, 3), row(j, 3), row(jp, 3)};
+        C v[E];
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+          R a, b;
+          prod_ab<LES>(P, LS, o0, grp, seq, lane + q * T, r2, rt, y, a, b);
+          v[q] = mkc<C>(a, b);
+        }
+        fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
+        SEQ_SYNC(N);
+#pragma unroll
+        for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
+        SEQ_SYNC(N);
+        prod_out<N>(xh, sq, g, hrow, grp, seq, lane, r2, rt);
+        SEQ_SYNC(N);   // sq is the next group's exchange buffer
+      }
     }
   }
 }
@@ -182,7 +342,9 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   constexpr int E = S::E, T = S::T;
   // column-fastest mapping: a warp reads KT consecutive kx of 32/KT rows
   const int seq = threadIdx.x % KT, lane = threadIdx.x / KT;
-  const int j = blockIdx.y, kx = blockIdx.x * KT + seq;
+  // equation fastest in the grid: the four CTAs of one column block share
+  // their spectral reads (cu, cp, cth) through L2
+  const int j = blockIdx.z, kx = blockIdx.y * KT + seq;
   const bool active = kx < g.kxs;
   const int kxc = active ? kx : 0;
   // per-column buffers, staggered by one element so the KT columns sharing a
@@ -207,7 +369,7 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   const long long sp0 = (long long)j * g.sp + kxc;
   const bool beta1 = (ph.beta == 1.0);
   {
-    const int e = blockIdx.z;
+    const int e = blockIdx.x;
     const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
     C* xin_n = (C*)s.xh[2 * e];
@@ -827,9 +989,28 @@ __global__ void k_bc_vel_post(const __grid_constant__ State s, Geom g, Phys ph) 
 
 template <int N, bool LES, typename R>
 static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
-  size_t smem = (size_t)3 * padded(N) * sizeof(typename CplxOf<R>::type);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_products<N, LES, R><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
+  using C = typename CplxOf<R>::type;
+  if constexpr (N <= 512) {
+    const int zr = prod_zr<N>() < g.nz ? prod_zr<N>() : g.nz;
+    const size_t smem = (size_t)PROD_SLOTS * 4 * zr * N * sizeof(R) + (size_t)3 * zr * padded(N) * sizeof(C) +
+                        PROD_SLOTS * sizeof(uint64_t);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_products_st<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nzb = g.nz / zr;
+    const int gmax = (g.tune_pgrid > 0 ? g.tune_pgrid : 2) * sm_count();
+    // plane ranges: about four items per CTA, at least four planes each
+    int nch = (4 * gmax + nzb - 1) / nzb;
+    nch = nch < 1 ? 1 : (nch > g.np / 4 ? (g.np / 4 > 0 ? g.np / 4 : 1) : nch);
+    const int jlen = (g.np + nch - 1) / nch;
+    nch = (g.np + jlen - 1) / jlen;
+    const int nitems = nzb * nch;
+    const int grid = nitems < gmax ? nitems : gmax;
+    k_products_st<N, LES, R><<<grid, 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr, nzb, jlen, nitems);
+  } else {
+    const size_t smem = (size_t)3 * padded(N) * sizeof(C);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<N, LES, R><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
+  }
 }
 template <int N>
 static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les) {
@@ -844,7 +1025,7 @@ static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, co
   constexpr int T = FftShape<N>::T;
   size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zpass_rhs<N, R><<<dim3(g.kxs / KT, g.np, 4), KT * T, smem, st>>>(s, g, ph, rk, ghost);
+  k_zpass_rhs<N, R><<<dim3(4, g.kxs / KT, g.np), KT * T, smem, st>>>(s, g, ph, rk, ghost);
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {

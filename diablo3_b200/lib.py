@@ -26,7 +26,7 @@ EXPORTS = (
     "db_fft_xz_to_fourier", "db_fft_xz_to_physical",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
     "db_courant", "db_divergence",
-    "db_set_timing", "db_stage_times", "db_kernel_launches",
+    "db_autotune", "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
@@ -83,6 +83,7 @@ def load(path: str | None = None):
     L.db_apply_bc_vel_post.argtypes = [vp]
     L.db_courant.argtypes = [vp, dp]
     L.db_divergence.argtypes = [vp, dp]
+    L.db_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.db_set_timing.argtypes = [vp, ctypes.c_int]
     L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
     L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]

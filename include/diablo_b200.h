@@ -314,6 +314,15 @@ enum db_stage {
   DB_NSTAGES = 10
 };
 
+/* Autotuner (no counterpart in the reference): times candidate launch shapes
+ * of the x-pass (row pairs per TMA-staged item, persistent CTAs per SM), the
+ * z-pass (kx columns per CTA) and, with LES, the per-column Thomas (threads
+ * per CTA) on this context's scratch buffers, keeps the fastest, and writes
+ * the timings and choices as text into report (may be NULL).  Call between
+ * steps; it overwrites only scratch fields (the next substep recomputes
+ * them). */
+int db_autotune(db_ctx* ctx, char* report, int report_len);
+
 /* Record CUDA events between the stages of every substep (the step graph is
  * re-captured with event nodes).  Off by default. */
 int db_set_timing(db_ctx* ctx, int enable);
