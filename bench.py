@@ -48,6 +48,16 @@ def workload_params(name: str):
         p = workload_params("config1")
         p.nx, p.ny, p.nz, p.re, p.variable_dt = 64, 65, 64, 1000.0, 0
         return p
+    if name in ("config2", "config3"):
+        # finite front (IC_type 6, front width 0.5), AMD LES, CFL-limited dt
+        p = workload_params("config1")
+        p.ic_type, p.delta = 6, 0.5
+        p.use_les, p.les_model_type, p.create_new_flow = 1, 5, 0
+        if name == "config2":
+            p.nx, p.ny, p.nz, p.re = 256, 129, 256, 1e5
+        else:
+            p.nx, p.ny, p.nz, p.re = 128, 65, 128, 1e4
+        return p
     raise ValueError(name)
 
 
@@ -55,6 +65,8 @@ WORKLOAD_DESC = {
     "config1": "plain FP64 DNS, infinite front, 512x257x512 (x,y,z), Re 5000, Ri 1 (M2=N2=f=1), CFL 0.5",
     "config0": "plain FP64 DNS, infinite front, 64x65x64, Re 1000, fixed dt 1e-3",
     "slab": "plain FP64 DNS, infinite front, 512x65x512 (profiling case), Re 5000, Ri 1, CFL 0.5",
+    "config2": "LES, finite front (IC 6, width 0.5), 256x129x256, Re 1e5, AMD closure, CFL 0.5",
+    "config3": "LES, finite front (IC 6, width 0.5), 128x65x128, Re 1e4, CFL 0.5",
 }
 
 
@@ -235,13 +247,100 @@ def run_ensemble(args) -> None:
     ens.close()
 
 
+def _timed_run(ch, stream, steps, warmup):
+    """Warm-up, then `steps` steps timed with CUDA events; returns
+    (ms per step, simulated time advanced per wall second)."""
+    import torch
+    for _ in range(warmup):
+        ch.step(1)
+    torch.cuda.synchronize()
+    t0 = ch.status().time
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ch.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = ch.status()
+    if st.flags & 1:
+        raise SystemExit("non-finite values in the flow: run rejected")
+    return ms / steps, (st.time - t0) / (ms / 1e3)
+
+
+def run_les_compare(args) -> None:
+    """Config 2 (256x129x256): FP64 AMD LES against the mixed-precision AMD
+    LES.  Config 3 (128x65x128): FP64 AMD LES against the mixed-precision
+    LES with the learned closure (les_model_type 6).  Both arms run the same
+    IC with CFL-limited dt; the comparison is simulated time per wall second.
+    The network of config 3 is fitted (tensor-core Adam) to AMD's eddy
+    coefficients on the FP64 run's own closure features: its weights do not
+    change its cost, and its accuracy against filtered DNS is what the
+    closure tests establish."""
+    import numpy as np
+    import torch
+    from diablo3_b200 import sgs_train
+    from diablo3_b200.channel import Channel
+    from diablo3_b200.grid import create_grid
+    p64 = workload_params(args.config)
+    gy = create_grid(p64.ny, lz=p64.ly, cs=1.5, grid_type=1)
+    stream = torch.cuda.Stream()
+    npts = p64.nx * p64.ny * p64.nz
+    a = Channel(p64, gy, stream=stream.cuda_stream)
+    a.init_flow(seed=0)
+    if not args.no_autotune:
+        a.autotune()
+    ms_a, rate_a = _timed_run(a, stream, args.steps, args.warmup)
+    net = None
+    if args.config == "config3":
+        nu, ka, feat = a.les_eval(5, features=True)
+        rows = slice(3, p64.ny)
+        f = torch.from_numpy(np.ascontiguousarray(feat[rows].reshape(-1, 16))).cuda()
+        t = torch.from_numpy(np.stack([nu[rows, : p64.nz, : p64.nx].reshape(-1),
+                                       ka[rows, : p64.nz, : p64.nx].reshape(-1)], 1).astype(np.float32)).cuda()
+        net, _ = sgs_train.train(f, t, steps=300, batch=65536, lr=1e-3, seed=0)
+    a.close()
+    pm = workload_params(args.config)
+    pm.precision = 1
+    if net is not None:
+        pm.les_model_type = 6
+    b = Channel(pm, gy, stream=stream.cuda_stream)
+    if net is not None:
+        b.set_sgs_net(net)
+    b.init_flow(seed=0)
+    if not args.no_autotune:
+        b.autotune()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    time.sleep(0.5)
+    ms_b, rate_b = _timed_run(b, stream, args.steps, args.warmup)
+    clk = clocks.stop()
+    b.close()
+    arm_b = "mixed precision, learned closure (les_model_type 6)" if net is not None else "mixed precision, AMD"
+    line = {
+        "metric": METRIC, "value": npts * 3 / (ms_b / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded finite-front IC, no dataset)",
+        "config": {"workload": WORKLOAD_DESC[args.config] + "; " + arm_b + " vs FP64 AMD",
+                   "grid_xyz": [p64.nx, p64.ny, p64.nz], "points": npts, "parallelism": "single GPU"},
+        "les_compare": {
+            "fp64_amd": {"ms_per_step": ms_a, "sim_time_per_wall_s": rate_a,
+                         "grid_pt_substeps_per_s": npts * 3 / (ms_a / 1e3)},
+            "candidate": {"arm": arm_b, "ms_per_step": ms_b, "sim_time_per_wall_s": rate_b,
+                          "grid_pt_substeps_per_s": npts * 3 / (ms_b / 1e3)},
+            "speedup_per_unit_sim_time": rate_b / rate_a},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config1", choices=["config1", "config0", "slab", "config4"])
+    ap.add_argument("--config", default="config1", choices=["config1", "config0", "slab", "config2", "config3", "config4"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
@@ -255,6 +354,8 @@ def main():
         raise SystemExit("--warmup must be >= 3")
     if args.config == "config4":
         return run_ensemble(args)
+    if args.config in ("config2", "config3"):
+        return run_les_compare(args)
 
     import ctypes
 

@@ -72,8 +72,10 @@ struct TriRow {
   // coupling is nu_lo * ef_lo, nu_hi * ef_hi (per-column nu), with
   // ef = 1/(dy dyf) at the neighbouring GY / GYF spacing
   double ef_lo, ef_hi;
+  // weight of the chunk's carry-in g in the zero-carry backward sweep:
+  // qa_j = pa_j / b'_j + m_j qa_{j+1}, zero past the chunk's end
+  double qa;
   int is_bc, interior;
-  int pad[2];
 };
 
 // Per-row constants of the AMD model (k_les_amd), host-computed once:

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
-template <int N, typename R>
+template <int N, typename R, bool EFAST>
 __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1))
     k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost) {
   // FP32 work type: write the increment cr - base (base = the state as the
@@ -342,9 +342,12 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   constexpr int E = S::E, T = S::T;
   // column-fastest mapping: a warp reads KT consecutive kx of 32/KT rows
   const int seq = threadIdx.x % KT, lane = threadIdx.x / KT;
-  // equation fastest in the grid: the four CTAs of one column block share
-  // their spectral reads (cu, cp, cth) through L2
-  const int j = blockIdx.z, kx = blockIdx.y * KT + seq;
+  // EFAST: equation fastest in the grid, so the four CTAs of one column
+  // block share their spectral reads (cu, cp, cth) through L2 (faster for
+  // the FP64 work type; the FP32 one runs faster with the equation slowest).
+  // A compile-time choice: a run-time one cost the FP32 kernel 40%.
+  const int j = EFAST ? blockIdx.z : blockIdx.y;
+  const int kx = (EFAST ? blockIdx.y : blockIdx.x) * KT + seq;
   const bool active = kx < g.kxs;
   const int kxc = active ? kx : 0;
   // per-column buffers, staggered by one element so the KT columns sharing a
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   const long long sp0 = (long long)j * g.sp + kxc;
   const bool beta1 = (ph.beta == 1.0);
   {
-    const int e = blockIdx.x;
+    const int e = EFAST ? blockIdx.x : blockIdx.z;
     const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
     C* xin_n = (C*)s.xh[2 * e];
@@ -522,7 +525,7 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
     TriRow r;
     r.l = 0.0; r.d = 1.0; r.u = 0.0; r.bc = 0.0; r.ap = 0.0; r.ibp = 1.0;
     r.cn_lo = 0.0; r.cn_hi = 0.0; r.pa = 1.0; r.pm = 1.0; r.ef_lo = 0.0; r.ef_hi = 0.0;
-    r.is_bc = 1; r.interior = 0; r.pad[0] = r.pad[1] = 0;
+    r.is_bc = 1; r.interior = 0; r.qa = 0.0;
     if (j >= lo && j <= hi) {
       if (eq == 0) {  // solver.f90:1023-1026
         r.l = -(tth) / (dy[j] * dyf[j]);
@@ -622,6 +625,11 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
       for (int j = j0; j <= j1; ++j) { pa *= Rs[j].ap; Rs[j].pa = pa; }
       double pm = 1.0;
       for (int j = j1; j >= j0; --j) { pm *= -Rs[j].u * Rs[j].ibp; Rs[j].pm = pm; }
+      double qa = 0.0;
+      for (int j = j1; j >= j0; --j) {
+        qa = Rs[j].pa * Rs[j].ibp + (j < j1 ? -Rs[j].u * Rs[j].ibp * qa : 0.0);
+        Rs[j].qa = qa;
+      }
     }
   }
   __syncthreads();
@@ -630,38 +638,45 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 }
 
 // Implicit CN solves of th, u2, u1, u3 (solver.f90:1012-1233) for all (x,z)
-// columns.  One CTA = 32 consecutive x columns at one z; the column tile
-// (all Nyp+2 rows) lives in shared memory.  The shared LU factors (a'_j,
-// 1/b'_j from k_tri_coef) turn the Thomas sweeps into two first-order linear
-// recurrences, solved as a two-level scan: warp k runs its chunk of rows with
-// zero carry-in, one warp propagates the chunk carries, then every row adds
-// its carry times the precomputed chunk products (pa, pm).  HBM sees r and u
-// read once and u written once per equation.
+// columns.  One CTA = 32 consecutive x columns at one z; warp k owns chunk k
+// of the rows.  The shared LU factors (a'_j, 1/b'_j from k_tri_coef) turn
+// the Thomas sweeps into two first-order linear recurrences
+//   g_j = v_j + a'_j g_{j-1},   x_j = g_j / b'_j + m_j x_{j+1}.
+// Each warp runs both over its chunk with zero carries (y, then z = B(y)),
+// so by linearity  x_j = z_j + G_{k-1} qa_j + X_{k+1} pm_j  with
+// G_{k-1} = g at the end of the previous chunk, X_{k+1} = x at the start of
+// the next one and the per-row weights qa = B(pa), pm from k_tri_coef.  The
+// chunk end values (y at the end, z at the start) cross warps through
+// shared memory; every warp scans them itself, so one barrier per equation
+// suffices.  HBM sees r and u read once and u written once per equation.
 constexpr int TX = 32;
+constexpr int TCH = 8;   // chunks (warps) per column tile
 
 template <typename R>
 __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g) {
   extern __shared__ double tile[];          // [np][TX]
-  __shared__ double carry[8][TX];
+  __shared__ double ye[2][TCH][TX], zs[2][TCH][TX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int np = g.np, Nyp = g.ny;
   const Chunks ch = thomas_chunks(np);
   const int x = blockIdx.x * TX + lane, z = blockIdx.y;
   const bool xin = x < g.nx;
-  const long long col = (long long)z * g.nx + x;
+  const long long col = (long long)z * g.nx + (xin ? x : 0);
   const long long pp = g.pp;
   const int j0 = w * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this warp's rows
   const bool active = w < ch.nch;
+  constexpr bool INC = sizeof(R) == sizeof(float);   // r holds the increment over u (k_zpass_rhs)
   for (int eq = 0; eq < 4; ++eq) {
+    const int par = eq & 1;
     const TriRow* Rw = s.tri + eq * np;
     R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3)));
-    const R* r = (const R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3)));
+    R* r = (R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3)));
     // rows written back (solver.f90:1056, 1115, 1171, 1227)
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    // 1. right-hand side (r + explicit CN term, or the BC value) and the
-    //    forward recurrence within the chunk, carry-in zero
-    if (active && xin) {
+    if (active) {
+      // right-hand side (r + explicit CN term, or the BC value), forward
+      // recurrence with carry-in zero
       double um = (j0 > 0) ? (double)__ldg(u + (long long)(j0 - 1) * pp + col) : 0.0;
       double uc = (double)__ldg(u + (long long)j0 * pp + col);
       double y = 0.0;
@@ -679,8 +694,7 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
           if (j > j1) break;
           const TriRow* row = Rw + j;
           const double un = xu[c];
-          // FP32 work type: r holds the increment over u (k_zpass_rhs)
-          const double rj = (sizeof(R) == sizeof(float)) ? xr[c] + uc : xr[c];
+          const double rj = INC ? xr[c] + uc : xr[c];
           const double v = row->is_bc ? row->bc : rj + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
           y = (j == j0) ? v : v + row->ap * y;
           tile[j * TX + lane] = y;
@@ -688,81 +702,74 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
           uc = un;
         }
       }
-    }
-    __syncthreads();
-    // 2. forward carries: g at the end of chunk k
-    if (w == 0) {
-      double gk = 0.0;
-      for (int k = 0; k < ch.nch; ++k) {
-        const int e = min(np, (k + 1) * ch.len) - 1;
-        gk = tile[e * TX + lane] + (k > 0 ? Rw[e].pa * gk : 0.0);
-        carry[k][lane] = gk;
+      ye[par][w][lane] = y;
+      // backward recurrence of the chunk's y, carry-in zero
+      double zz = 0.0;
+      for (int j = j1; j >= j0; --j) {
+        const double ib = Rw[j].ibp;
+        const double wv = tile[j * TX + lane] * ib;
+        zz = (j == j1) ? wv : wv - Rw[j].u * ib * zz;
+        tile[j * TX + lane] = zz;
       }
-    }
-    __syncthreads();
-    // 3. apply carries, then the backward recurrence within the chunk
-    //    x_j = g_j / b'_j + m_j x_{j+1}, carry-in zero
-    if (active && w > 0) {
-      const double c = carry[w - 1][lane];
-      for (int j = j0; j <= j1; ++j) tile[j * TX + lane] += Rw[j].pa * c;
+      zs[par][w][lane] = zz;
     }
     __syncthreads();
     if (active) {
-      double xz = 0.0;
-      for (int j = j1; j >= j0; --j) {
-        const TriRow row = Rw[j];
-        const double wv = tile[j * TX + lane] * row.ibp;
-        xz = (j == j1) ? wv : wv - row.u * row.ibp * xz;
-        tile[j * TX + lane] = xz;
-      }
-    }
-    __syncthreads();
-    // 4. backward carries: x at the start of chunk k, from the last chunk down
-    if (w == 0) {
-      double xk = 0.0;
-      for (int k = ch.nch - 1; k >= 0; --k) {
-        const int b = k * ch.len;
-        xk = tile[b * TX + lane] + (k < ch.nch - 1 ? Rw[b].pm * xk : 0.0);
-        carry[k][lane] = xk;
-      }
-    }
-    __syncthreads();
-    // 5. apply carries and write the rows the reference stores
-    if (active && xin) {
-      const double c = (w < ch.nch - 1) ? carry[w + 1][lane] : 0.0;
-      if (sizeof(R) == sizeof(float)) {
-        // new u for courant, and its increment (into r) for the forward
-        // transform; rows the solve does not store keep u, increment 0.
-        // The old u of a batch of rows is loaded before any of them is written.
-        R* rr = const_cast<R*>(r);
-        for (int jb = j0; jb <= j1; jb += 8) {
-          R uo[8];
+      // chunk carries: G_k = y_end(k) + pa_end(k) G_{k-1};
+      // X_k = z_start(k) + G_{k-1} qa_start(k) + pm_start(k) X_{k+1}
+      double G[TCH];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int j = jb + q;
-            uo[q] = (j <= j1) ? u[(long long)j * pp + col] : (R)0;
-          }
+      for (int k = 0; k < TCH; ++k) {
+        if (k < ch.nch) {
+          const int e = min(np, (k + 1) * ch.len) - 1;
+          G[k] = ye[par][k][lane] + (k > 0 ? Rw[e].pa * G[k - 1] : 0.0);
+        } else {
+          G[k] = 0.0;
+        }
+      }
+      double X = 0.0, Gm = 0.0;
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int j = jb + q;
-            if (j > j1) break;
-            const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
-            if (j >= lo && j <= hi) {
-              u[(long long)j * pp + col] = (R)xv;
-              rr[(long long)j * pp + col] = (R)(xv - (double)uo[q]);
-            } else {
-              rr[(long long)j * pp + col] = (R)0;
+      for (int k = TCH - 1; k >= 1; --k) {
+        if (k < ch.nch && k > w) {
+          const int b = k * ch.len;
+          X = zs[par][k][lane] + G[k - 1] * Rw[b].qa + (k < ch.nch - 1 ? Rw[b].pm * X : 0.0);
+        }
+        if (k == w) Gm = G[k - 1];
+      }
+      // final values and the rows the reference stores
+      if (xin) {
+        if (INC) {
+          // new u for courant, and its increment (into r) for the forward
+          // transform; rows the solve does not store keep u, increment 0.
+          // The old u of a batch of rows is loaded before any of them is written.
+          for (int jb = j0; jb <= j1; jb += 8) {
+            R uo[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int j = jb + q;
+              uo[q] = (j <= j1) ? u[(long long)j * pp + col] : (R)0;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int j = jb + q;
+              if (j > j1) break;
+              const double xv = tile[j * TX + lane] + Gm * Rw[j].qa + X * Rw[j].pm;
+              if (j >= lo && j <= hi) {
+                u[(long long)j * pp + col] = (R)xv;
+                r[(long long)j * pp + col] = (R)(xv - (double)uo[q]);
+              } else {
+                r[(long long)j * pp + col] = (R)0;
+              }
             }
           }
-        }
-      } else {
-        for (int j = j0; j <= j1; ++j) {
-          const double xv = tile[j * TX + lane] + (w < ch.nch - 1 ? Rw[j].pm * c : 0.0);
-          if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
+        } else {
+          for (int j = j0; j <= j1; ++j) {
+            const double xv = tile[j * TX + lane] + Gm * Rw[j].qa + X * Rw[j].pm;
+            if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
+          }
         }
       }
     }
-    __syncthreads();
   }
 }
 
@@ -799,6 +806,9 @@ __global__ void k_pfac(Geom g, double2* pfac) {
 
 // divergence removal + pressure update, one thread per (kx, kzp) column
 __global__ void __launch_bounds__(128) k_rem_div(const __grid_constant__ State s, Geom g, int rk, int update_cp) {
+  // the rows of both sweeps are handled in batches of RB whose loads are all
+  // issued first (each thread keeps several rows in flight)
+  constexpr int RB = 4;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx > g.nkx) return;
   const int Nyp = g.ny;
@@ -809,53 +819,81 @@ __global__ void __launch_bounds__(128) k_rem_div(const __grid_constant__ State s
   double2 gp = make_double2(0.0, 0.0);
   s.phi_g[1 * sp + c0] = gp;
   double2 u2c = s.cu2[2 * sp + c0];
-  for (int j = 2; j <= Nyp; ++j) {
-    const double2 pf = s.pfac[j * sp + c0];
-    double2 rhs = make_double2(0.0, 0.0);
-    const double2 u2n = s.cu2[(long long)(j + 1) * sp + c0];
-    if (j < Nyp) {
-      const double2 a1 = s.cu1[j * sp + c0], a3 = s.cu3[j * sp + c0];
-      const double idf = 1.0 / g.dyf[j];
-      rhs = make_double2(-kxv * a1.y + (u2n.x - u2c.x) * idf - kzv * a3.y,
-                         kxv * a1.x + (u2n.y - u2c.y) * idf + kzv * a3.x);
+  for (int jb = 2; jb <= Nyp; jb += RB) {
+    double2 pf[RB], u2n[RB], a1[RB], a3[RB];
+#pragma unroll
+    for (int c = 0; c < RB; ++c) {
+      const int j = jb + c;
+      const long long a = (long long)j * sp + c0;
+      const bool in = j <= Nyp, mid = j < Nyp;
+      pf[c] = in ? s.pfac[a] : make_double2(0.0, 0.0);
+      u2n[c] = in ? s.cu2[a + sp] : make_double2(0.0, 0.0);
+      a1[c] = mid ? s.cu1[a] : make_double2(0.0, 0.0);
+      a3[c] = mid ? s.cu3[a] : make_double2(0.0, 0.0);
     }
-    gp = make_double2(rhs.x + pf.x * gp.x, rhs.y + pf.x * gp.y);
-    s.phi_g[j * sp + c0] = gp;
-    u2c = u2n;
+#pragma unroll
+    for (int c = 0; c < RB; ++c) {
+      const int j = jb + c;
+      if (j > Nyp) break;
+      double2 rhs = make_double2(0.0, 0.0);
+      if (j < Nyp) {
+        const double idf = 1.0 / g.dyf[j];
+        rhs = make_double2(-kxv * a1[c].y + (u2n[c].x - u2c.x) * idf - kzv * a3[c].y,
+                           kxv * a1[c].x + (u2n[c].y - u2c.y) * idf + kzv * a3[c].x);
+      }
+      gp = make_double2(rhs.x + pf[c].x * gp.x, rhs.y + pf[c].x * gp.y);
+      s.phi_g[(long long)j * sp + c0] = gp;
+      u2c = u2n[c];
+    }
   }
   // backward sweep with the projection (solver.f90:1361-1376) and cp update
   const double itemp4 = 1.0 / s.sc->h_bar[rk];
   double2 phin = make_double2(0.0, 0.0);
-  for (int j = Nyp; j >= 1; --j) {
-    const double2 pf = s.pfac[j * sp + c0];
-    const double2 gj = s.phi_g[j * sp + c0];
-    double cj;
-    if (j == Nyp) cj = 0.0;
-    else if (j == 1) cj = zero_mode ? 0.0 : -1.0;
-    else cj = 1.0 / (g.dy[j + 1] * g.dyf[j]);
-    const double2 phi = (j == Nyp) ? make_double2(gj.x * pf.y, gj.y * pf.y)
-                                   : make_double2((gj.x - cj * phin.x) * pf.y, (gj.y - cj * phin.y) * pf.y);
-    const long long a = j * sp + c0;
-    double2 v1 = s.cu1[a], v3 = s.cu3[a];
-    v1.x += kxv * phi.y; v1.y -= kxv * phi.x;   // cu1 -= i kx phi
-    v3.x += kzv * phi.y; v3.y -= kzv * phi.x;   // cu3 -= i kz phi
-    s.cu1[a] = v1;
-    s.cu3[a] = v3;
-    if (j + 1 <= Nyp) {  // cu2(j+1) -= (phi(j+1) - phi(j)) / dy(j+1)
-      const long long b = (long long)(j + 1) * sp + c0;
-      const double w = 1.0 / g.dy[j + 1];
-      double2 v2 = s.cu2[b];
-      v2.x -= (phin.x - phi.x) * w;
-      v2.y -= (phin.y - phi.y) * w;
-      s.cu2[b] = v2;
+  for (int jt = Nyp; jt >= 1; jt -= RB) {
+    double2 pf[RB], gj[RB], v1[RB], v3[RB], v2[RB], pc[RB];
+#pragma unroll
+    for (int c = 0; c < RB; ++c) {
+      const int j = jt - c;
+      const long long a = (long long)j * sp + c0;
+      const bool in = j >= 1;
+      pf[c] = in ? s.pfac[a] : make_double2(0.0, 0.0);
+      gj[c] = in ? s.phi_g[a] : make_double2(0.0, 0.0);
+      v1[c] = in ? s.cu1[a] : make_double2(0.0, 0.0);
+      v3[c] = in ? s.cu3[a] : make_double2(0.0, 0.0);
+      v2[c] = (in && j + 1 <= Nyp) ? s.cu2[a + sp] : make_double2(0.0, 0.0);
+      pc[c] = (in && update_cp && j >= g.jstart && j <= g.jend) ? s.cp[a] : make_double2(0.0, 0.0);
     }
-    if (update_cp && j >= g.jstart && j <= g.jend) {
-      double2 p = s.cp[a];
-      p.x += phi.x * itemp4;
-      p.y += phi.y * itemp4;
-      s.cp[a] = p;
+#pragma unroll
+    for (int c = 0; c < RB; ++c) {
+      const int j = jt - c;
+      if (j < 1) break;
+      double cj;
+      if (j == Nyp) cj = 0.0;
+      else if (j == 1) cj = zero_mode ? 0.0 : -1.0;
+      else cj = 1.0 / (g.dy[j + 1] * g.dyf[j]);
+      const double2 phi = (j == Nyp) ? make_double2(gj[c].x * pf[c].y, gj[c].y * pf[c].y)
+                                     : make_double2((gj[c].x - cj * phin.x) * pf[c].y, (gj[c].y - cj * phin.y) * pf[c].y);
+      const long long a = (long long)j * sp + c0;
+      double2 w1 = v1[c], w3 = v3[c];
+      w1.x += kxv * phi.y; w1.y -= kxv * phi.x;   // cu1 -= i kx phi
+      w3.x += kzv * phi.y; w3.y -= kzv * phi.x;   // cu3 -= i kz phi
+      s.cu1[a] = w1;
+      s.cu3[a] = w3;
+      if (j + 1 <= Nyp) {  // cu2(j+1) -= (phi(j+1) - phi(j)) / dy(j+1)
+        const double w = 1.0 / g.dy[j + 1];
+        double2 w2 = v2[c];
+        w2.x -= (phin.x - phi.x) * w;
+        w2.y -= (phin.y - phi.y) * w;
+        s.cu2[a + sp] = w2;
+      }
+      if (update_cp && j >= g.jstart && j <= g.jend) {
+        double2 p = pc[c];
+        p.x += phi.x * itemp4;
+        p.y += phi.y * itemp4;
+        s.cp[a] = p;
+      }
+      phin = phi;
     }
-    phin = phi;
   }
 }
 
@@ -1023,9 +1061,12 @@ static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les
 template <int N, typename R>
 static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
   constexpr int T = FftShape<N>::T;
+  constexpr bool EFAST = sizeof(R) == sizeof(double);
   size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zpass_rhs<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zpass_rhs<N, R><<<dim3(4, g.kxs / KT, g.np), KT * T, smem, st>>>(s, g, ph, rk, ghost);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_zpass_rhs<N, R, EFAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
+  k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost);
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {

@@ -207,7 +207,7 @@ int db_rem_div_static(const db_params* p, const double* gy, double* cu1,
 
 /* ---- learned SGS closure (no counterpart in the reference, whose les.f90
  * offers Smagorinsky, dynamic and AMD closures).  A 16 -> 64 -> 64 -> 64 -> 2
- * MLP (GELU, softplus outputs) maps point features to nu_t and kappa_t; its
+ * MLP (GELU in its tanh form, softplus outputs) maps point features to nu_t and kappa_t; its
  * hidden layers run on the tensor cores in BF16 with FP32 accumulation,
  * forward and backward.  Features of a point, in this order: the nine
  * velocity gradients du_i/dx_j (i-major: du1/dx, du1/dy, du1/dz, du2/dx,

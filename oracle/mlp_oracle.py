@@ -9,7 +9,6 @@ plain FP64 network for finite-difference checks.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 OFF = {"W1": (0, (64, 16)), "b1": (1024, (64,)), "W2": (1088, (64, 64)), "b2": (5184, (64,)),
        "W3": (5248, (64, 64)), "b3": (9344, (64,)), "W4": (9408, (2, 64)), "b4": (9536, (2,))}
@@ -28,12 +27,18 @@ def unpack(p):
     return {k: p[o:o + int(np.prod(sh))].reshape(sh) for k, (o, sh) in OFF.items()}
 
 
+GELU_K = np.sqrt(2.0 / np.pi)
+GELU_C = 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016), as the closure kernels use it."""
+    return 0.5 * x * (1.0 + np.tanh(GELU_K * (x + GELU_C * x ** 3)))
 
 
 def gelu_d(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_K * (x + GELU_C * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_K * (1.0 + 3.0 * GELU_C * x * x)
 
 
 def softplus(y):
