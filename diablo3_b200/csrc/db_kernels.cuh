@@ -92,13 +92,15 @@ struct LesRow {
   double dys_y;            // 2 dy(j)   (GY-row y filter width)
 };
 
-// row chunks of the tiled Thomas solve (k_thomas): nch chunks of len rows
+// row chunks of the tiled Thomas solve (k_thomas): nch <= THOMAS_MAXCH
+// chunks of len rows
+constexpr int THOMAS_MAXCH = 16;
 struct Chunks {
   int nch, len;
 };
 __host__ __device__ inline Chunks thomas_chunks(int np) {
   Chunks c;
-  c.nch = np / 2 < 8 ? np / 2 : 8;
+  c.nch = np / 2 < THOMAS_MAXCH ? np / 2 : THOMAS_MAXCH;
   if (c.nch < 1) c.nch = 1;
   c.len = (np + c.nch - 1) / c.nch;
   c.nch = (np + c.len - 1) / c.len;

@@ -638,34 +638,53 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 }
 
 // Implicit CN solves of th, u2, u1, u3 (solver.f90:1012-1233) for all (x,z)
-// columns.  One CTA = 32 consecutive x columns at one z; warp k owns chunk k
-// of the rows.  The shared LU factors (a'_j, 1/b'_j from k_tri_coef) turn
+// columns.  One CTA = TX consecutive x columns at one z; half-warp k owns
+// row chunk k.  The shared LU factors (a'_j, 1/b'_j from k_tri_coef) turn
 // the Thomas sweeps into two first-order linear recurrences
 //   g_j = v_j + a'_j g_{j-1},   x_j = g_j / b'_j + m_j x_{j+1}.
-// Each warp runs both over its chunk with zero carries (y, then z = B(y)),
-// so by linearity  x_j = z_j + G_{k-1} qa_j + X_{k+1} pm_j  with
+// Each half-warp runs both over its chunk with zero carries (y, then
+// z = B(y)), so by linearity  x_j = z_j + G_{k-1} qa_j + X_{k+1} pm_j  with
 // G_{k-1} = g at the end of the previous chunk, X_{k+1} = x at the start of
 // the next one and the per-row weights qa = B(pa), pm from k_tri_coef.  The
 // chunk end values (y at the end, z at the start) cross warps through
-// shared memory; every warp scans them itself, so one barrier per equation
-// suffices.  HBM sees r and u read once and u written once per equation.
-constexpr int TX = 32;
-constexpr int TCH = 8;   // chunks (warps) per column tile
+// shared memory and every thread scans them itself.  The r and u columns of
+// an equation come into shared memory by cp.async copies that every thread
+// issues for all rows of its chunk at once (no registers held for loads,
+// the whole equation in flight); the staged old u also gives the mixed
+// path its increment.  HBM sees r and u read once and u written once per
+// equation (plus the increment r on the mixed path).
+constexpr int TX = 16;
+
+__device__ __forceinline__ void cp_async_el(void* smem, const void* gmem, int bytes) {
+  const uint32_t a = smem_u32(smem);
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(a), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 template <typename R>
 __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g) {
-  extern __shared__ double tile[];          // [np][TX]
-  __shared__ double ye[2][TCH][TX], zs[2][TCH][TX];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  extern __shared__ __align__(16) unsigned char th_raw[];
+  constexpr bool F64 = sizeof(R) == sizeof(double);
+  constexpr bool INC = !F64;   // FP32 work type: r holds the increment over u (k_zpass_rhs)
   const int np = g.np, Nyp = g.ny;
+  // [np][TX] each: the FP64 y / z tile, staged r (the tile itself when R is
+  // double) and staged u
+  double* tile = reinterpret_cast<double*>(th_raw);
+  R* rs = F64 ? reinterpret_cast<R*>(tile) : reinterpret_cast<R*>(tile + np * TX);
+  R* us = reinterpret_cast<R*>(tile + np * TX) + (F64 ? 0 : np * TX);
+  __shared__ double ye[2][THOMAS_MAXCH][TX], zs[2][THOMAS_MAXCH][TX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int cl = lane & (TX - 1), k = 2 * w + (lane >> 4);   // column, chunk
   const Chunks ch = thomas_chunks(np);
-  const int x = blockIdx.x * TX + lane, z = blockIdx.y;
+  const int x = blockIdx.x * TX + cl, z = blockIdx.y;
   const bool xin = x < g.nx;
   const long long col = (long long)z * g.nx + (xin ? x : 0);
   const long long pp = g.pp;
-  const int j0 = w * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this warp's rows
-  const bool active = w < ch.nch;
-  constexpr bool INC = sizeof(R) == sizeof(float);   // r holds the increment over u (k_zpass_rhs)
+  const int j0 = k * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this thread's rows
+  const bool active = k < ch.nch;
   for (int eq = 0; eq < 4; ++eq) {
     const int par = eq & 1;
     const TriRow* Rw = s.tri + eq * np;
@@ -674,99 +693,75 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
     // rows written back (solver.f90:1056, 1115, 1171, 1227)
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
+    __syncthreads();   // the previous equation is done with the staging buffers
+    if (active) {
+      for (int j = j0; j <= j1; ++j) {
+        cp_async_el(rs + j * TX + cl, r + (long long)j * pp + col, (int)sizeof(R));
+        cp_async_el(us + j * TX + cl, u + (long long)j * pp + col, (int)sizeof(R));
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();   // halo rows of u come from the neighbouring chunks
     if (active) {
       // right-hand side (r + explicit CN term, or the BC value), forward
       // recurrence with carry-in zero
-      double um = (j0 > 0) ? (double)__ldg(u + (long long)(j0 - 1) * pp + col) : 0.0;
-      double uc = (double)__ldg(u + (long long)j0 * pp + col);
+      double um = (j0 > 0) ? (double)us[(j0 - 1) * TX + cl] : 0.0;
+      double uc = (double)us[j0 * TX + cl];
       double y = 0.0;
-      for (int jb = j0; jb <= j1; jb += 8) {
-        double xr[8], xu[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {   // all loads of the batch first
-          const int j = jb + c;
-          xr[c] = (j <= j1) ? (double)__ldg(r + (long long)j * pp + col) : 0.0;
-          xu[c] = (j <= j1 && j + 1 < np) ? (double)__ldg(u + (long long)(j + 1) * pp + col) : 0.0;
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int j = jb + c;
-          if (j > j1) break;
-          const TriRow* row = Rw + j;
-          const double un = xu[c];
-          const double rj = INC ? xr[c] + uc : xr[c];
-          const double v = row->is_bc ? row->bc : rj + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
-          y = (j == j0) ? v : v + row->ap * y;
-          tile[j * TX + lane] = y;
-          um = uc;
-          uc = un;
-        }
+      for (int j = j0; j <= j1; ++j) {
+        const TriRow* row = Rw + j;
+        const double un = (j + 1 < np) ? (double)us[(j + 1) * TX + cl] : 0.0;
+        const double xr = (double)rs[j * TX + cl];
+        const double rj = INC ? xr + uc : xr;
+        const double v = row->is_bc ? row->bc : rj + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+        y = (j == j0) ? v : v + row->ap * y;
+        tile[j * TX + cl] = y;
+        um = uc;
+        uc = un;
       }
-      ye[par][w][lane] = y;
+      ye[par][k][cl] = y;
       // backward recurrence of the chunk's y, carry-in zero
       double zz = 0.0;
       for (int j = j1; j >= j0; --j) {
         const double ib = Rw[j].ibp;
-        const double wv = tile[j * TX + lane] * ib;
+        const double wv = tile[j * TX + cl] * ib;
         zz = (j == j1) ? wv : wv - Rw[j].u * ib * zz;
-        tile[j * TX + lane] = zz;
+        tile[j * TX + cl] = zz;
       }
-      zs[par][w][lane] = zz;
+      zs[par][k][cl] = zz;
     }
     __syncthreads();
     if (active) {
       // chunk carries: G_k = y_end(k) + pa_end(k) G_{k-1};
       // X_k = z_start(k) + G_{k-1} qa_start(k) + pm_start(k) X_{k+1}
-      double G[TCH];
+      double G[THOMAS_MAXCH];
 #pragma unroll
-      for (int k = 0; k < TCH; ++k) {
-        if (k < ch.nch) {
-          const int e = min(np, (k + 1) * ch.len) - 1;
-          G[k] = ye[par][k][lane] + (k > 0 ? Rw[e].pa * G[k - 1] : 0.0);
+      for (int q = 0; q < THOMAS_MAXCH; ++q) {
+        if (q < ch.nch) {
+          const int e = min(np, (q + 1) * ch.len) - 1;
+          G[q] = ye[par][q][cl] + (q > 0 ? Rw[e].pa * G[q - 1] : 0.0);
         } else {
-          G[k] = 0.0;
+          G[q] = 0.0;
         }
       }
       double X = 0.0, Gm = 0.0;
 #pragma unroll
-      for (int k = TCH - 1; k >= 1; --k) {
-        if (k < ch.nch && k > w) {
-          const int b = k * ch.len;
-          X = zs[par][k][lane] + G[k - 1] * Rw[b].qa + (k < ch.nch - 1 ? Rw[b].pm * X : 0.0);
+      for (int q = THOMAS_MAXCH - 1; q >= 1; --q) {
+        if (q < ch.nch && q > k) {
+          const int b = q * ch.len;
+          X = zs[par][q][cl] + G[q - 1] * Rw[b].qa + (q < ch.nch - 1 ? Rw[b].pm * X : 0.0);
         }
-        if (k == w) Gm = G[k - 1];
+        if (q == k) Gm = G[q - 1];
       }
-      // final values and the rows the reference stores
+      // final values and the rows the reference stores; on the mixed path
+      // also the increment (into r) for the forward transform, 0 on rows
+      // the solve does not store
       if (xin) {
-        if (INC) {
-          // new u for courant, and its increment (into r) for the forward
-          // transform; rows the solve does not store keep u, increment 0.
-          // The old u of a batch of rows is loaded before any of them is written.
-          for (int jb = j0; jb <= j1; jb += 8) {
-            R uo[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int j = jb + q;
-              uo[q] = (j <= j1) ? u[(long long)j * pp + col] : (R)0;
-            }
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int j = jb + q;
-              if (j > j1) break;
-              const double xv = tile[j * TX + lane] + Gm * Rw[j].qa + X * Rw[j].pm;
-              if (j >= lo && j <= hi) {
-                u[(long long)j * pp + col] = (R)xv;
-                r[(long long)j * pp + col] = (R)(xv - (double)uo[q]);
-              } else {
-                r[(long long)j * pp + col] = (R)0;
-              }
-            }
-          }
-        } else {
-          for (int j = j0; j <= j1; ++j) {
-            const double xv = tile[j * TX + lane] + Gm * Rw[j].qa + X * Rw[j].pm;
-            if (j >= lo && j <= hi) u[(long long)j * pp + col] = (R)xv;
-          }
+        for (int j = j0; j <= j1; ++j) {
+          const double xv = tile[j * TX + cl] + Gm * Rw[j].qa + X * Rw[j].pm;
+          const bool st = (j >= lo && j <= hi);
+          if (st) u[(long long)j * pp + col] = (R)xv;
+          if (INC) r[(long long)j * pp + col] = st ? (R)(xv - (double)us[j * TX + cl]) : (R)0;
         }
       }
     }
@@ -1102,7 +1097,8 @@ cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int r
   return cudaGetLastError();
 }
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
-  const size_t smem = (size_t)g.np * TX * sizeof(double);
+  // y/z tile (FP64) + staged r and u (the FP64 tile doubles as staged r)
+  const size_t smem = (size_t)g.np * TX * (g.prec ? sizeof(double) + 2 * sizeof(float) : 2 * sizeof(double));
   if (g.prec) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
