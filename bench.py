@@ -442,7 +442,9 @@ def main():
     dom_name = L.STAGES[dom]
     alg = roofline.stage_bytes(p)[dom_name]
     achieved = alg / (per_stage[dom] / 1e3) / 1e9
-    traffic = roofline.profiled_traffic(dom_name, ROOT)
+    traffic = roofline.profiled_traffic(dom_name, ROOT, args.precision)
+    if traffic is not None and args.les:
+        traffic = None   # the committed captures are of the plain substep
 
     # end to end through the C-ABI with host buffers
     e2e = None

@@ -75,10 +75,10 @@ def state_transfer_bytes(p) -> int:
     return 9 * (p.ny + 2) * (2 * (p.nz // 3) + 1) * kxs * 16
 
 
-def profiled_traffic(stage: str, root: str):
-    """dram__bytes_read.sum + dram__bytes_write.sum per launch of a stage,
-    from the ncu summary committed under profiles/ (a line
-    ``traffic_per_launch <stage> <bytes>``), or None."""
+def profiled_traffic(stage: str, root: str, precision: str = "fp64"):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch of a stage at
+    the 512x257x512 size, from the ncu summaries committed under profiles/
+    (a line ``traffic_per_launch <stage> <bytes> <fp64|mixed>``), or None."""
     d = os.path.join(root, "profiles")
     if not os.path.isdir(d):
         return None
@@ -87,7 +87,7 @@ def profiled_traffic(stage: str, root: str):
             continue
         with open(os.path.join(d, fn)) as f:
             for line in f:
-                m = re.match(r"\s*traffic_per_launch\s+(\w+)\s+([0-9.eE+]+)", line)
-                if m and m.group(1) == stage:
+                m = re.match(r"\s*traffic_per_launch\s+(\w+)\s+([0-9.eE+]+)\s+(\w+)", line)
+                if m and m.group(1) == stage and m.group(3) == precision:
                     return float(m.group(2))
     return None
