@@ -125,6 +125,13 @@ class Channel:
         self._ck(self.L.db_divergence(self.h, ctypes.byref(d)))
         return d.value
 
+    def stats(self) -> dict:
+        """Mean and energy-budget profiles (save_stats_chan), FP64: a dict of
+        arrays over the planes 0..Nyp+1 (see include/diablo_b200.h, db_stats)."""
+        out = np.zeros((len(_L.STAT_ROWS), self.p.ny + 2))
+        self._ck(self.L.db_stats(self.h, _L.dptr(out.reshape(-1))))
+        return {k: out[i].copy() for i, k in enumerate(_L.STAT_ROWS)}
+
     def set_sgs_net(self, net):
         """Learned closure for les_model_type 6 (a SgsNet that outlives this channel)."""
         self._sgs = net

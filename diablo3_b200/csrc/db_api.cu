@@ -26,6 +26,7 @@ struct db_ctx {
   bool own_stream = false;
   int device = 0;
   std::vector<void*> allocs;
+  double* stats = nullptr;        // db_stats rows (device), allocated on first use
   double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
   float2* d_twf = nullptr;       // the same in FP32
@@ -1159,6 +1160,28 @@ extern "C" int db_courant(db_ctx* c, double* delta_t_out) {
   int rc = db_get_status(c, &stt);
   if (rc) return rc;
   if (delta_t_out) *delta_t_out = stt.delta_t;
+  return DB_OK;
+}
+
+extern "C" int db_stats(db_ctx* c, double* out) {
+  if (!c || !out) return DB_ERR_ARG;
+  const int np = c->g.np;
+  // the device rows: ume vme wme thme, the four variances, uv wv uw thv,
+  // the gradient sum of epsilon, |grad th|^2 (k_stats.cu)
+  constexpr int NDEV = 14;
+  static_assert(NDEV == DB_NSTAT, "device rows and output rows");
+  if (!c->stats && balloc(c, (void**)&c->stats, (size_t)NDEV * np * sizeof(double)))
+    return fail(c, DB_ERR_CUDA, "db_stats: out of device memory");
+  const int homx = !(c->p.ic_type >= 5 && c->p.ic_type <= 8);   // for/parameters.f90:282-286
+  CK(launch_stats(c->g, c->s, homx, c->stats, c->st));
+  CK(cudaMemcpyAsync(out, c->stats, (size_t)NDEV * np * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const double bg = c->ph.dthdx * c->ph.dthdx + c->ph.dthdz * c->ph.dthdz;
+  for (int j = 0; j < np; ++j) {
+    for (int r = DB_ST_URMS; r <= DB_ST_THRMS; ++r) out[r * np + j] = sqrt(fmax(out[r * np + j], 0.0));
+    out[DB_ST_EPSILON * np + j] *= c->ph.nu;
+    if (j >= 1 && j <= c->g.ny) out[DB_ST_CHI * np + j] += bg;
+  }
   return DB_OK;
 }
 

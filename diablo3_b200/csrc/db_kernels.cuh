@@ -156,6 +156,7 @@ cudaError_t launch_apply_dt(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_end(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_stats(const Geom& g, const State& s, int homx, double* out, cudaStream_t st);
 cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
 
 // k_les.cu

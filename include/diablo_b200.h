@@ -186,6 +186,26 @@ int db_courant(db_ctx* ctx, double* delta_t_out);
  * GYF points j = 2..Nyp-1, the quantity rem_div_chan drives to zero. */
 int db_divergence(db_ctx* ctx, double* max_div_out);
 
+/* Mean and energy-budget profiles of save_stats_chan (for/diagnostics.f90:
+ * 3-480; compute_TKE 1270-1330, compute_TKE_diss 804-1020, production
+ * terms 1385-1425) from the current state, in FP64 on both precision
+ * paths (from the FP64 spectral state by Parseval).  out[DB_NSTAT][Nyp+2],
+ * row r, plane j; rows that do not exist at a plane (GY rows j < 2) are 0.
+ * Averages are over x and z, or over z only for the fronts (IC_Type 5..8),
+ * as the reference's homogeneousX.  Rows:
+ *   ume, vme, wme, thme   horizontal means (vme at GY points)
+ *   urms, vrms, wrms, thrms   rms of the fluctuations (vrms at GY)
+ *   uv, wv                <u1'u2'>, <u3'u2'> at GY (u interpolated)
+ *   uw                    <u1'u3'>
+ *   thv                   <th' (u2'(j) + u2'(j+1))/2>, buoyancy flux
+ *   epsilon               nu x the 9 squared fluctuation gradients at GY
+ *   chi                   |grad th|^2 with the background gradient */
+enum {
+  DB_ST_UME, DB_ST_VME, DB_ST_WME, DB_ST_THME, DB_ST_URMS, DB_ST_VRMS, DB_ST_WRMS, DB_ST_THRMS,
+  DB_ST_UV, DB_ST_WV, DB_ST_UW, DB_ST_THV, DB_ST_EPSILON, DB_ST_CHI, DB_NSTAT
+};
+int db_stats(db_ctx* ctx, double* out);
+
 /*
  * Divergence removal that allocates nothing.  No counterpart in the
  * reference (it follows rem_div_chan's arithmetic, for/solver.f90:1302-1379,
