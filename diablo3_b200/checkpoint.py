@@ -1,0 +1,100 @@
+"""Checkpoint / restart of a channel (the role of save_flow / read_flow,
+for/phdf5.f90:918-1456, without an HDF5 library).
+
+A checkpoint holds the exact device state, so a restarted run continues
+bit-identically: the nine spectral fields of the reference layout
+(cu1, cu2, cu3, cp, cth, cf1, cf2, cf3, cfth; complex128), nu_t and
+kappa_t with LES, the run parameters with dt set to the current step, the
+y-grid and the clock.  (The reference's restart file holds physical U, V,
+W, TH with u2 interpolated to GYF, tools.f90:255-322, and rebuilds the
+pressure with poisson_p_chan; keeping the spectral state and cf avoids
+both approximations.)
+
+File layout: 8-byte magic ``DIABLOB3``, little-endian uint64 length of a
+UTF-8 JSON header, the header, then the arrays back to back in the order
+the header's ``arrays`` list gives (dtype and shape per entry).
+"""
+from __future__ import annotations
+
+import json
+import math
+import struct
+
+import numpy as np
+
+from . import lib as _L
+
+MAGIC = b"DIABLOB3"
+VERSION = 1
+
+
+def _clean(v):
+    if isinstance(v, float) and math.isnan(v):
+        return "nan"
+    return v
+
+
+def save(ch, path: str) -> None:
+    """Write the state, clock and parameters of a Channel to `path`."""
+    st = ch.status()
+    state = ch.download_state()
+    arrays = [(f"spec{fid}", state[fid]) for fid in _L.STATE_FIELDS]
+    if ch.p.use_les:
+        arrays += [("nu_t", ch.download_field(_L.NU_T)), ("kappa_t", ch.download_field(_L.KAPPA_T))]
+    params = {k: _clean(v) for k, v in ch.p.as_dict().items()}
+    params["delta_t"] = st.delta_t
+    hdr = {
+        "version": VERSION, "params": params, "gy": [float(x) for x in ch.gy],
+        "time": st.time, "time_step": int(st.time_step),
+        "arrays": [{"name": n, "dtype": str(a.dtype), "shape": list(a.shape)} for n, a in arrays],
+    }
+    blob = json.dumps(hdr).encode()
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        f.write(struct.pack("<Q", len(blob)))
+        f.write(blob)
+        for _, a in arrays:
+            f.write(np.ascontiguousarray(a).tobytes())
+
+
+def read(path: str):
+    """(header, {name: array}) of a checkpoint file."""
+    with open(path, "rb") as f:
+        if f.read(8) != MAGIC:
+            raise ValueError(f"{path}: not a checkpoint of this library")
+        (n,) = struct.unpack("<Q", f.read(8))
+        hdr = json.loads(f.read(n).decode())
+        if hdr.get("version") != VERSION:
+            raise ValueError(f"{path}: checkpoint version {hdr.get('version')} (expected {VERSION})")
+        arrays = {}
+        for e in hdr["arrays"]:
+            dt = np.dtype(e["dtype"])
+            cnt = int(np.prod(e["shape"]))
+            buf = f.read(cnt * dt.itemsize)
+            if len(buf) != cnt * dt.itemsize:
+                raise ValueError(f"{path}: truncated at {e['name']}")
+            arrays[e["name"]] = np.frombuffer(buf, dtype=dt).reshape(e["shape"]).copy()
+    return hdr, arrays
+
+
+def load(path: str, stream: int | None = None, **overrides):
+    """A new Channel continuing the checkpointed run (parameters from the
+    file, optionally overridden, e.g. ``precision=1`` to continue an FP64
+    run on the mixed path)."""
+    from .channel import Channel
+    from .params import make_params
+    hdr, arrays = read(path)
+    pd = {k: (float("nan") if v == "nan" else v) for k, v in hdr["params"].items()}
+    pd.update(overrides)
+    p = make_params(**pd)
+    ch = Channel(p, np.asarray(hdr["gy"], np.float64), stream=stream)
+    ch.upload_state({fid: arrays[f"spec{fid}"] for fid in _L.STATE_FIELDS})
+    if p.use_les and "nu_t" in arrays:
+        ch.upload_field(_L.NU_T, arrays["nu_t"])
+        ch.upload_field(_L.KAPPA_T, arrays["kappa_t"])
+    t = hdr["time"]
+    ch.set_clock(t, hdr["time_step"], t + p.save_stats_dt, t + p.save_flow_dt)
+    return ch
+
+
+__all__ = ["save", "read", "load", "MAGIC"]
