@@ -655,14 +655,6 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // equation (plus the increment r on the mixed path).
 constexpr int TX = 16;
 
-__device__ __forceinline__ void cp_async_el(void* smem, const void* gmem, int bytes) {
-  const uint32_t a = smem_u32(smem);
-  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(a), "l"(gmem) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(a), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
 
 template <typename R>
 __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g) {
@@ -696,11 +688,12 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
     __syncthreads();   // the previous equation is done with the staging buffers
     if (active) {
       for (int j = j0; j <= j1; ++j) {
-        cp_async_el(rs + j * TX + cl, r + (long long)j * pp + col, (int)sizeof(R));
-        cp_async_el(us + j * TX + cl, u + (long long)j * pp + col, (int)sizeof(R));
+        cp_async<sizeof(R)>(rs + j * TX + cl, r + (long long)j * pp + col);
+        cp_async<sizeof(R)>(us + j * TX + cl, u + (long long)j * pp + col);
       }
     }
-    cp_async_wait_all();
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();   // halo rows of u come from the neighbouring chunks
     if (active) {
       // right-hand side (r + explicit CN term, or the BC value), forward

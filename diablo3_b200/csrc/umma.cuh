@@ -127,6 +127,17 @@ __device__ __forceinline__ void bulk_g2s(void* smem, const void* gmem, uint32_t 
                : "memory");
 }
 
+// per-thread asynchronous copies global -> shared of 4, 8 or 16 bytes
+// (both addresses aligned to the size), grouped and waited for with
+// commit_group / wait_group (hardware-completed; no spin)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(smem)), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory"); }
+
 // 16 consecutive FP32 columns of this thread's tensor-memory lane
 // (warp w reads lanes 32 (w % 4) .. 32 (w % 4) + 31)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
