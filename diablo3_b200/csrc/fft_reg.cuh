@@ -91,6 +91,14 @@ __device__ __forceinline__ void load_twiddles(Twiddles<N, E, C>& tw, int lane, c
 template <int R, int SIGN, typename C>
 __device__ __forceinline__ void twiddle_apply(C* x, C w) {
   if (SIGN > 0) w.y = -w.y;
+  if (R == 8) {   // the powers as a depth-3 tree instead of a chain of 6
+    const C w2 = cmul(w, w);
+    const C w3 = cmul(w2, w), w4 = cmul(w2, w2);
+    const C w5 = cmul(w4, w), w6 = cmul(w3, w3), w7 = cmul(w4, w3);
+    x[1] = cmul(x[1], w); x[2] = cmul(x[2], w2); x[3] = cmul(x[3], w3); x[4] = cmul(x[4], w4);
+    x[5] = cmul(x[5], w5); x[6] = cmul(x[6], w6); x[7] = cmul(x[7], w7);
+    return;
+  }
   C wr = w;
 #pragma unroll
   for (int r = 1; r < R; ++r) {
