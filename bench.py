@@ -452,7 +452,7 @@ def main():
         host = {f: torch.empty(ch.new_spectral().shape, dtype=torch.complex128, pin_memory=True).numpy()
                 for f in L.STATE_FIELDS}
         ke = max(1, min(3, args.steps))
-        dev_bytes = roofline.state_transfer_bytes(p)
+        h2d_bytes, d2h_bytes = roofline.state_transfer_bytes(p)
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -470,7 +470,7 @@ def main():
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e = {"value": npts * 3 * ke * world / (float(te.item()) / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": dev_bytes, "d2h_bytes_per_step": dev_bytes,
+               "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                "steps": ke, "path": "db_upload_state + db_rk_steps(1) + db_download_field x9, reference-layout host arrays"}
 
     cpu = None

@@ -34,6 +34,7 @@ struct db_ctx {
   int time_step = 0;             // host mirror of the driver's time_step
   std::string err;
   double* h_stage = nullptr;     // pinned staging, one physical field
+  double2* d_ref = nullptr;       // one spectral field in the reference layout (device)
   size_t stage_doubles = 0;
   std::vector<double> gy, gyf, dy, dyf, kx, kz;
   double pi_ref = 0.0;
@@ -456,14 +457,34 @@ static int phys_download(db_ctx* c, const void* dev, double* ref) {
   return DB_OK;
 }
 
+// spectral fields cross PCIe in the reference layout as one DMA of the
+// caller's array; the layout change runs on the device (k_layout.cu)
+static size_t ref_spec_bytes(const db_ctx* c) {
+  return (size_t)(c->p.nx / 2 + 1) * (c->p.nz + 2) * c->g.np * sizeof(double2);
+}
+static int ensure_ref(db_ctx* c) {
+  if (!c->d_ref && balloc(c, (void**)&c->d_ref, ref_spec_bytes(c)))
+    return fail(c, DB_ERR_CUDA, "out of device memory for the layout buffer");
+  return DB_OK;
+}
+
 static int upload_spec(db_ctx* c, int id, const double* ref) {
   double2* d = spec_field(c, id);
   if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
   const size_t n = (size_t)c->g.np * c->g.sp;
-  double2* st = (double2*)c->h_stage;
-  if (ref) ref_to_compact(c, ref, st);
-  else memset(st, 0, n * sizeof(double2));
-  CK(cudaMemcpyAsync(d, st, n * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+  if (!ref) {
+    CK(cudaMemsetAsync(d, 0, n * sizeof(double2), c->st));
+  } else {
+    if (int rc = ensure_ref(c)) return rc;
+    // only the retained modes cross PCIe (kx <= Nkx of the first 2 Nkz + 1
+    // rows of every plane); the rest of the reference array is never read
+    const size_t pitch = (size_t)(c->p.nx / 2 + 1) * sizeof(double2);
+    const size_t plane = pitch * (c->p.nz + 2);
+    for (int j = 0; j < c->g.np; ++j)
+      CK(cudaMemcpy2DAsync((char*)c->d_ref + j * plane, pitch, (const char*)ref + j * plane, pitch,
+                           (size_t)(c->g.nkx + 1) * sizeof(double2), c->g.nkzp, cudaMemcpyHostToDevice, c->st));
+    CK(launch_ref_to_spec(c->g, c->p.nx, c->p.nz, c->d_ref, d, c->st));
+  }
   CK(cudaStreamSynchronize(c->st));
   return DB_OK;
 }
@@ -472,11 +493,10 @@ static int download_spec(db_ctx* c, int id, double* ref) {
   double2* d = spec_field(c, id);
   if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
   if (!ref) return DB_OK;
-  const size_t n = (size_t)c->g.np * c->g.sp;
-  double2* st = (double2*)c->h_stage;
-  CK(cudaMemcpyAsync(st, d, n * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+  if (int rc = ensure_ref(c)) return rc;
+  CK(launch_spec_to_ref(c->g, c->p.nx, c->p.nz, d, c->d_ref, c->st));
+  CK(cudaMemcpyAsync(ref, c->d_ref, ref_spec_bytes(c), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  compact_to_ref(c, st, ref);
   return DB_OK;
 }
 

@@ -157,6 +157,9 @@ cudaError_t launch_step_begin(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_step_end(DevScalars* sc, cudaStream_t st);
 cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st);
 cudaError_t launch_stats(const Geom& g, const State& s, int homx, double* out, cudaStream_t st);
+// spectral field: compact device layout <-> reference host layout, on the device
+cudaError_t launch_spec_to_ref(const Geom& g, int nx, int nz, const double2* src, double2* ref, cudaStream_t st);
+cudaError_t launch_ref_to_spec(const Geom& g, int nx, int nz, const double2* ref, double2* dst, cudaStream_t st);
 cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
 
 // k_les.cu

@@ -68,11 +68,16 @@ def substep_bytes(p) -> float:
     return float(sum(stage_bytes(p).values()))
 
 
-def state_transfer_bytes(p) -> int:
-    """Bytes one db_upload_state (or 9 db_download_field) moves over PCIe:
-    nine spectral fields in the device's packed layout."""
-    kxs = ((p.nx // 3 + 1) + 3) // 4 * 4
-    return 9 * (p.ny + 2) * (2 * (p.nz // 3) + 1) * kxs * 16
+def state_transfer_bytes(p) -> tuple:
+    """Bytes one db_upload_state and nine db_download_field move over PCIe,
+    (host to device, device to host).  Upload: the retained modes of each
+    reference-layout array (kx <= Nkx of the first 2 Nkz + 1 rows of every
+    plane); download: the whole reference-layout arrays (their zero padding
+    included)."""
+    nplanes = p.ny + 2
+    h2d = 9 * nplanes * (2 * (p.nz // 3) + 1) * (p.nx // 3 + 1) * 16
+    d2h = 9 * nplanes * (p.nz + 2) * (p.nx // 2 + 1) * 16
+    return h2d, d2h
 
 
 def profiled_traffic(stage: str, root: str, precision: str = "fp64"):
