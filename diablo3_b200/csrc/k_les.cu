@@ -32,6 +32,7 @@
 
 #include "db_bc.cuh"
 #include "db_kernels.cuh"
+#include "umma.cuh"
 
 namespace db {
 
@@ -130,6 +131,8 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 // s1 = -2 nu_GYF / filter at GYF rows with nu_GYF the mean of the two GY
 // neighbours; a point whose features leave the training range
 // (s.sgs_range: lo[16], hi[16]) keeps its AMD value.
+constexpr int AMD_SLOTS = 4;
+
 template <typename R, int MODE>
 __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ State s, Geom g, Phys ph) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
@@ -180,12 +183,37 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   o[5][0] = 0;
   o[6][0] = 0;
 
+  // the 12 values a row needs come through a ring of AMD_SLOTS shared-memory
+  // slots per thread, filled by cp.async AMD_SLOTS - 1 rows ahead: row j's
+  // loads were issued while rows j - 3 .. j - 1 were computed
+  extern __shared__ __align__(16) unsigned char amd_raw[];
+  R* ring = reinterpret_cast<R*>(amd_raw);   // [slot][value][threadIdx.x]
+  const int tb = blockDim.x, tx = threadIdx.x;
+  const R* srcs[12] = {u1, u3, th, u2 + pp, g1x, g2x, g3x, gtx, g1z, g2z, g3z, gtz};
+  auto issue = [&](int jr) {
+    if (jr <= Nyp + 1) {
+      R* sl = ring + (jr % AMD_SLOTS) * 12 * tb + tx;
+      const long long oj = (long long)jr * pp;
+#pragma unroll
+      for (int v = 0; v < 12; ++v) {
+        if (v == 3 && jr + 1 > Nyp + 1) sl[v * tb] = (R)0;   // u2 above the top ghost plane
+        else cp_async<sizeof(R)>(sl + v * tb, srcs[v] + oj);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int jr = 1; jr < AMD_SLOTS; ++jr) issue(jr);
+
   for (int j = 1; j <= Nyp + 1; ++j) {
     const long long oj = (long long)j * pp;
-    const R u1j = __ldg(u1 + oj), u3j = __ldg(u3 + oj), thj = __ldg(th + oj);
-    const R u2n = (j + 1 <= Nyp + 1) ? __ldg(u2 + oj + pp) : (R)0;
-    const R a1x = __ldg(g1x + oj), a2x = __ldg(g2x + oj), a3x = __ldg(g3x + oj), atx = __ldg(gtx + oj);
-    const R a1z = __ldg(g1z + oj), a2z = __ldg(g2z + oj), a3z = __ldg(g3z + oj), atz = __ldg(gtz + oj);
+    issue(j + AMD_SLOTS - 1);
+    cp_async_wait<AMD_SLOTS - 1>();
+    const R* sl = ring + (j % AMD_SLOTS) * 12 * tb + tx;
+    const R u1j = sl[0], u3j = sl[tb], thj = sl[2 * tb];
+    const R u2n = sl[3 * tb];
+    const R a1x = sl[4 * tb], a2x = sl[5 * tb], a3x = sl[6 * tb], atx = sl[7 * tb];
+    const R a1z = sl[8 * tb], a2z = sl[9 * tb], a3z = sl[10 * tb], atz = sl[11 * tb];
     const LesRow lr = LR[j];
     const R idy = (R)lr.idy;
     // GY row j: y-derivatives and the tensors that live there
@@ -403,14 +431,15 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode) {
   const int bx = g.nx < 128 ? g.nx : 128;
   const dim3 grid(g.nx / bx, g.nz);
+  const size_t smem = (size_t)AMD_SLOTS * 12 * bx * (g.prec ? sizeof(float) : sizeof(double));
   if (g.prec) {
-    if (mode == 1) k_les_amd<float, 1><<<grid, bx, 0, st>>>(s, g, ph);
-    else if (mode == 2) k_les_amd<float, 2><<<grid, bx, 0, st>>>(s, g, ph);
-    else k_les_amd<float, 0><<<grid, bx, 0, st>>>(s, g, ph);
+    if (mode == 1) k_les_amd<float, 1><<<grid, bx, smem, st>>>(s, g, ph);
+    else if (mode == 2) k_les_amd<float, 2><<<grid, bx, smem, st>>>(s, g, ph);
+    else k_les_amd<float, 0><<<grid, bx, smem, st>>>(s, g, ph);
   } else {
-    if (mode == 1) k_les_amd<double, 1><<<grid, bx, 0, st>>>(s, g, ph);
-    else if (mode == 2) k_les_amd<double, 2><<<grid, bx, 0, st>>>(s, g, ph);
-    else k_les_amd<double, 0><<<grid, bx, 0, st>>>(s, g, ph);
+    if (mode == 1) k_les_amd<double, 1><<<grid, bx, smem, st>>>(s, g, ph);
+    else if (mode == 2) k_les_amd<double, 2><<<grid, bx, smem, st>>>(s, g, ph);
+    else k_les_amd<double, 0><<<grid, bx, smem, st>>>(s, g, ph);
   }
   return cudaGetLastError();
 }
