@@ -122,16 +122,20 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
   C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
-  const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
+  // column-fastest mapping: a warp reads ns consecutive kx of 32/ns rows
+  // (whole sectors); the sequence's threads are then spread over the CTA
+  // and the exchanges use CTA barriers
+  const int ns = blockDim.x / T;
+  const int seq = threadIdx.x % ns, lane = threadIdx.x / ns;
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
-  C* sq = sm + seq * padded(N);
+  C* sq = sm + seq * (padded(N) + 1);   // staggered so the ns columns use different banks
   const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
   const C* src = (const C*)in.p[f] + (long long)j * g.hp + kx;
   C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
-  fft_reg_lazy<N, -1>(v, lane, active, sq, twt);
+  fft_reg_lazy<N, -1, true>(v, lane, active, sq, twt);
   if (!active) return;
   double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
   const double2* base = dst;
@@ -162,10 +166,11 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant_
   C* sm = reinterpret_cast<C*>(sm_raw);
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
-  const int seq = threadIdx.x / T, lane = threadIdx.x % T;
-  const int kx = blockIdx.x * (blockDim.x / T) + seq, j = blockIdx.y, f = blockIdx.z;
+  const int ns = blockDim.x / T;   // column-fastest mapping, as k_fwd_z
+  const int seq = threadIdx.x % ns, lane = threadIdx.x / ns;
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, f = blockIdx.z;
   const bool active = kx < g.kxs;
-  C* sq = sm + seq * padded(N);
+  C* sq = sm + seq * (padded(N) + 1);
   const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
   const double2* src = (const double2*)in.p[f] + (long long)j * g.sp + kx;
   if (ghost) {   // rows 0, 1, Nyp, Nyp+1 from the overlay
@@ -182,7 +187,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant_
     if (dz && kzp >= 0) a = cmul_i(a, g.kz[kzp]);
     v[q] = from_d2<C>(a);
   }
-  fft_reg_lazy<N, +1>(v, lane, active, sq, twt);
+  fft_reg_lazy<N, +1, true>(v, lane, active, sq, twt);
   if (!active) return;
   C* dst = (C*)out.p[f] + (long long)j * g.hp + kx;
 #pragma unroll
@@ -433,7 +438,7 @@ static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc
                        cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   const int ns = zpass_ns<N>(g);
-  size_t smem = (size_t)ns * padded(N) * sizeof(C);
+  size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
   smem_attr(k_fwd_z<N, R>, smem);
   k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, acc, ghost);
 }
@@ -442,7 +447,7 @@ static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
                        cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   const int ns = zpass_ns<N>(g);
-  size_t smem = (size_t)ns * padded(N) * sizeof(C);
+  size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
   smem_attr(k_inv_z<N, R>, smem);
   k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);
 }
