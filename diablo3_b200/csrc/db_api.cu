@@ -234,6 +234,9 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
   s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
   s.phi_g = sp[9]; s.pfac = sp[10];
+  if (!p->precision)   // the FP64 z-pass runs as three stages through this scratch
+    for (int i = 0; i < 8; ++i)
+      if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   const size_t eP = phys_elem(c), eH = xh_elem(c);
   for (int i = 0; i < 8; ++i)
     if ((rc = balloc(c, (void**)&s.xh[i], H * eH))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }

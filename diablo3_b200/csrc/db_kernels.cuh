@@ -117,6 +117,7 @@ struct State {
   double *u1, *u2, *u3, *th;                 // physical
   double *r1, *r2, *r3, *rth;                // physical RHS
   double2* phi_g;                            // rem_div forward-sweep scratch (spectral)
+  double2* nls[8];                           // z-pass scratch of the FP64 path: Z(N_e), Z(M_e), then cr_e (spectral)
   double2* pfac;                             // rem_div factors (a', 1/b') per (kx,kz,j)
   TriRow* tri;                               // 4 equations x np rows (th, u2, u1, u3)
   DevScalars* sc;

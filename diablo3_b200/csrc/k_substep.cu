@@ -324,6 +324,113 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------------------
+// The spectral RHS at one mode (kx, kzp) of plane j for equation e (0 u1,
+// 1 u3, 2 u2, 3 th): the linear terms into cf (stored), the RK combination
+// cr = cu + zeta h cf_old - h grad p + beta h cf (solver.f90:396-609,
+// 824-838, 966-973, 35-111) returned; with INC the increment cr - base.
+// nl = (Z(N) + i kz Z(M)) / Nz, the nonlinear term of that mode.
+template <bool INC>
+__device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, const Phys& ph, int rk, int e, int j,
+                                             int kx, int kzp, double2 nl, const double2* __restrict__ ghost) {
+  const double hb = s.sc->h_bar[rk];
+  const double temp3 = zeta_bar(rk) * hb, temp4 = hb, temp5 = beta_bar(rk) * hb;
+  const double nu = ph.nu, f = ph.ro_inv / ph.delta;
+  const double tw = ph.delta / ph.ro_inv;  // delta / Ro_inv
+  const double kxv = g.kx[kx], kzv = g.kz[kzp];
+  const long long sp0 = (long long)j * g.sp + kx;
+  const int kxc = kx;
+  const bool beta1 = (ph.beta == 1.0);
+  const long long a = sp0 + (long long)kzp * g.kxs;
+  const double k2 = kxv * kxv + kzv * kzv;
+  const double kk = beta1 ? k2 : pow(k2, ph.beta);
+  double2 cf, cr, cuf;
+  if (e == 0 || e == 1) {
+    const double2 cu1 = s.cu1[a], cu3 = s.cu3[a], cth = s.cth[a], cp = s.cp[a];
+    const double2 c2a = s.cu2[a], c2b = s.cu2[a + g.sp];
+    const double2 v2 = make_double2(0.5 * (c2a.x + c2b.x), 0.5 * (c2a.y + c2b.y));
+    const double2 cu = (e == 0) ? cu1 : cu3;
+    cf = cscale(cu, -nu * kk);
+    if (e == 0) {
+      cf = cadd(cf, cscale(cu3, f));
+      cf = cadd(cf, cscale(cth, ph.grav_x));
+    } else {
+      cf = csub(cf, cscale(cu1, f));
+      cf = cadd(cf, cscale(cth, ph.grav_z));
+    }
+    if (ph.front_tw) {
+      const double y = g.gyf[j] - 0.5 * ph.ly;
+      const double ax = ph.dthdx * y * tw;          // multiplies ikz
+      const double az = -1.0 * ph.dthdz * y * tw;   // multiplies ikx
+      const double2 t1 = cmul_i(cu, 1.0);           // i cu
+      cf = csub(cf, cscale(t1, ax * kzv));
+      cf = csub(cf, cscale(t1, az * kxv));
+      const double c2 = (e == 0) ? (-1.0 * ph.dthdz * tw) : (ph.dthdx * tw);
+      cf = csub(cf, cscale(v2, c2));
+    }
+    cf = csub(cf, nl);
+    const double kd = (e == 0) ? kxv : kzv;
+    cuf = cu;
+    cr = INC ? make_double2(0.0, 0.0) : cu;
+    if (rk > 0) cr = cadd(cr, cscale((e == 0) ? s.cf1[a] : s.cf3[a], temp3));
+    cr = csub(cr, cscale(cmul_i(cp, 1.0), temp4 * kd));
+    if (e == 0 && kx == 0 && kzp == 0) {
+      if (ph.f_type == 1) cr.x -= temp4 * ph.px0;
+      if (ph.f_type == 2) cr.x -= temp4 * (ph.px0 + ph.amp_omega0 * cos(ph.omega0 * s.sc->time));
+    }
+    cr = cadd(cr, cscale(cf, temp5));
+    if (e == 0) s.cf1[a] = cf; else s.cf3[a] = cf;
+  } else if (e == 2) {
+    const double2 cu2 = s.cu2[a];
+    cf = cscale(cu2, -nu * kk);
+    if (!(kx == 0 && kzp == 0)) {
+      const double2 t0 = s.cth[a], tm = s.cth[a - g.sp];
+      const double w = ph.grav_y / (2.0 * g.dy[j]);
+      cf = cadd(cf, make_double2(w * (t0.x * g.dyf[j - 1] + tm.x * g.dyf[j]),
+                                 w * (t0.y * g.dyf[j - 1] + tm.y * g.dyf[j])));
+    }
+    if (ph.front_tw) {
+      const double y = g.gy[j] - 0.5 * ph.ly;
+      const double2 t1 = cmul_i(cu2, 1.0);
+      cf = csub(cf, cscale(t1, ph.dthdx * y * tw * kzv));
+      cf = csub(cf, cscale(t1, -1.0 * ph.dthdz * y * tw * kxv));
+    }
+    cf = csub(cf, nl);
+    cuf = cu2;
+    cr = INC ? make_double2(0.0, 0.0) : cu2;
+    if (rk > 0) cr = cadd(cr, cscale(s.cf2[a], temp3));
+    const double2 dp = csub(s.cp[a], s.cp[a - g.sp]);
+    cr = csub(cr, cscale(dp, temp4 / g.dy[j]));
+    cr = cadd(cr, cscale(cf, temp5));
+    s.cf2[a] = cf;
+  } else {
+    const double2 cth = s.cth[a];
+    cf = cscale(cth, -(nu / ph.pr) * kk);
+    cf = csub(cf, cscale(s.cu1[a], ph.dthdx));
+    cf = csub(cf, cscale(s.cu3[a], ph.dthdz));
+    if (ph.front_tw) {
+      const double y = g.gyf[j] - 0.5 * ph.ly;
+      const double2 t1 = cmul_i(cth, 1.0);
+      cf = csub(cf, cscale(t1, tw * ph.dthdx * y * kzv));
+      cf = csub(cf, cscale(t1, tw * (-1.0) * ph.dthdz * y * kxv));
+    }
+    cf = csub(cf, nl);
+    cuf = cth;
+    cr = INC ? make_double2(0.0, 0.0) : cth;
+    if (rk > 0) cr = cadd(cr, cscale(s.cfth[a], temp3));
+    cr = cadd(cr, cscale(cf, temp5));
+    s.cfth[a] = cf;
+  }
+  if (INC && ghost) {   // ghost rows: base is the overlay, cr - base = (cu - base) + increment
+    const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
+    if (qg >= 0) {
+      const int gf = (e == 0) ? 0 : (e == 1 ? 2 : (e == 2 ? 1 : 3));
+      const double2 base = ghost[(long long)(4 * gf + qg) * g.sp + (long long)kzp * g.kxs + kxc];
+      cr = cadd(cr, csub(cuf, base));
+    }
+  }
+  return cr;
+}
+
 // z-pass of the nonlinear terms + spectral RHS + inverse z-pass of cr.
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
@@ -362,15 +469,8 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
   load_twiddles<N, E>(twd, lane, tw_z<R>(g));
 #define ZFFT(SIGN_, V_) fft_reg<N, SIGN_, true>(V_, lane, active, sx, twd, sx1)
 #endif
-  const double hb = s.sc->h_bar[rk];
-  const double temp3 = zeta_bar(rk) * hb, temp4 = hb, temp5 = beta_bar(rk) * hb;
-  const double nu = ph.nu, f = ph.ro_inv / ph.delta;
-  const double tw = ph.delta / ph.ro_inv;  // delta / Ro_inv
-  const double kxv = g.kx[kxc];
   const double inz = 1.0 / (double)N;
   const long long h0 = (long long)j * g.hp + kxc;
-  const long long sp0 = (long long)j * g.sp + kxc;
-  const bool beta1 = (ph.beta == 1.0);
   {
     const int e = EFAST ? blockIdx.x : blockIdx.z;
     const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
@@ -408,95 +508,7 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       // NL = (Z(N) + i kz Z(M)) / Nz, formed in FP64
       const double2 zmq = to_d2(sm_z[pidx(zz)]), zn = to_d2(vn[q]);
       const double2 nl = make_double2((zn.x - kzv * zmq.y) * inz, (zn.y + kzv * zmq.x) * inz);
-      const long long a = sp0 + (long long)kzp * g.kxs;
-      const double k2 = kxv * kxv + kzv * kzv;
-      const double kk = beta1 ? k2 : pow(k2, ph.beta);
-      double2 cf, cr, cuf;
-      if (e == 0 || e == 1) {
-        const double2 cu1 = s.cu1[a], cu3 = s.cu3[a], cth = s.cth[a], cp = s.cp[a];
-        const double2 c2a = s.cu2[a], c2b = s.cu2[a + g.sp];
-        const double2 v2 = make_double2(0.5 * (c2a.x + c2b.x), 0.5 * (c2a.y + c2b.y));
-        const double2 cu = (e == 0) ? cu1 : cu3;
-        cf = cscale(cu, -nu * kk);
-        if (e == 0) {
-          cf = cadd(cf, cscale(cu3, f));
-          cf = cadd(cf, cscale(cth, ph.grav_x));
-        } else {
-          cf = csub(cf, cscale(cu1, f));
-          cf = cadd(cf, cscale(cth, ph.grav_z));
-        }
-        if (ph.front_tw) {
-          const double y = g.gyf[j] - 0.5 * ph.ly;
-          const double ax = ph.dthdx * y * tw;          // multiplies ikz
-          const double az = -1.0 * ph.dthdz * y * tw;   // multiplies ikx
-          const double2 t1 = cmul_i(cu, 1.0);           // i cu
-          cf = csub(cf, cscale(t1, ax * kzv));
-          cf = csub(cf, cscale(t1, az * kxv));
-          const double c2 = (e == 0) ? (-1.0 * ph.dthdz * tw) : (ph.dthdx * tw);
-          cf = csub(cf, cscale(v2, c2));
-        }
-        cf = csub(cf, nl);
-        const double kd = (e == 0) ? kxv : kzv;
-        cuf = cu;
-        cr = INC ? make_double2(0.0, 0.0) : cu;
-        if (rk > 0) cr = cadd(cr, cscale((e == 0) ? s.cf1[a] : s.cf3[a], temp3));
-        cr = csub(cr, cscale(cmul_i(cp, 1.0), temp4 * kd));
-        if (e == 0 && kx == 0 && kzp == 0) {
-          if (ph.f_type == 1) cr.x -= temp4 * ph.px0;
-          if (ph.f_type == 2) cr.x -= temp4 * (ph.px0 + ph.amp_omega0 * cos(ph.omega0 * s.sc->time));
-        }
-        cr = cadd(cr, cscale(cf, temp5));
-        if (e == 0) s.cf1[a] = cf; else s.cf3[a] = cf;
-      } else if (e == 2) {
-        const double2 cu2 = s.cu2[a];
-        cf = cscale(cu2, -nu * kk);
-        if (!(kx == 0 && kzp == 0)) {
-          const double2 t0 = s.cth[a], tm = s.cth[a - g.sp];
-          const double w = ph.grav_y / (2.0 * g.dy[j]);
-          cf = cadd(cf, make_double2(w * (t0.x * g.dyf[j - 1] + tm.x * g.dyf[j]),
-                                     w * (t0.y * g.dyf[j - 1] + tm.y * g.dyf[j])));
-        }
-        if (ph.front_tw) {
-          const double y = g.gy[j] - 0.5 * ph.ly;
-          const double2 t1 = cmul_i(cu2, 1.0);
-          cf = csub(cf, cscale(t1, ph.dthdx * y * tw * kzv));
-          cf = csub(cf, cscale(t1, -1.0 * ph.dthdz * y * tw * kxv));
-        }
-        cf = csub(cf, nl);
-        cuf = cu2;
-        cr = INC ? make_double2(0.0, 0.0) : cu2;
-        if (rk > 0) cr = cadd(cr, cscale(s.cf2[a], temp3));
-        const double2 dp = csub(s.cp[a], s.cp[a - g.sp]);
-        cr = csub(cr, cscale(dp, temp4 / g.dy[j]));
-        cr = cadd(cr, cscale(cf, temp5));
-        s.cf2[a] = cf;
-      } else {
-        const double2 cth = s.cth[a];
-        cf = cscale(cth, -(nu / ph.pr) * kk);
-        cf = csub(cf, cscale(s.cu1[a], ph.dthdx));
-        cf = csub(cf, cscale(s.cu3[a], ph.dthdz));
-        if (ph.front_tw) {
-          const double y = g.gyf[j] - 0.5 * ph.ly;
-          const double2 t1 = cmul_i(cth, 1.0);
-          cf = csub(cf, cscale(t1, tw * ph.dthdx * y * kzv));
-          cf = csub(cf, cscale(t1, tw * (-1.0) * ph.dthdz * y * kxv));
-        }
-        cf = csub(cf, nl);
-        cuf = cth;
-        cr = INC ? make_double2(0.0, 0.0) : cth;
-        if (rk > 0) cr = cadd(cr, cscale(s.cfth[a], temp3));
-        cr = cadd(cr, cscale(cf, temp5));
-        s.cfth[a] = cf;
-      }
-      if (INC && ghost) {   // ghost rows: base is the overlay, cr - base = (cu - base) + increment
-        const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
-        if (qg >= 0) {
-          const int gf = (e == 0) ? 0 : (e == 1 ? 2 : (e == 2 ? 1 : 3));
-          const double2 base = ghost[(long long)(4 * gf + qg) * g.sp + (long long)kzp * g.kxs + kxc];
-          cr = cadd(cr, csub(cuf, base));
-        }
-      }
-      vn[q] = from_d2<C>(cr);
+      vn[q] = from_d2<C>(rhs_point<INC>(s, g, ph, rk, e, j, kxc, kzp, nl, ghost));
     }
     __syncthreads();
     ZFFT(+1, vn);
@@ -504,6 +516,35 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
 #pragma unroll
       for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = vn[q];
   }
+}
+
+// ---------------------------------------------------------------------------
+// The same z-pass as three lean stages (the FP64 path; the fused kernel keeps
+// 128 registers only by spilling there):
+//  forward z-FFT of the eight x-half product fields (k_fwd_z) into spectral
+//               scratch: Z(N_e)/Nz in nls[e], Z(M_e)/Nz in nls[4 + e]
+//  k_rhs_modes: NL_e = Z(N_e) + i kz Z(M_e) and the spectral RHS mode by mode
+//               (rhs_point), cr_e over nls[e] in place, zero on the planes
+//               the equation does not solve
+//  inverse z-FFT of cr_e into xh[2e] (k_inv_z)
+__global__ void __launch_bounds__(256) k_rhs_modes(const __grid_constant__ State s, Geom g, Phys ph, int rk,
+                                                   const __grid_constant__ FieldSet nl) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, e = blockIdx.z;
+  if (m >= g.nkzp * g.kxs) return;
+  const int kzp = m / g.kxs, kx = m % g.kxs;
+  const long long a = (long long)j * g.sp + m;
+  double2* p = (double2*)nl.p[e] + a;
+  const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
+  const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
+  if (!in_rng(j, jlo, jhi)) {
+    *p = make_double2(0.0, 0.0);
+    return;
+  }
+  const double kzv = g.kz[kzp];
+  const double2 zn = *p, zm = ((const double2*)nl.p[4 + e])[a];
+  const double2 nlv = make_double2(zn.x - kzv * zm.y, zn.y + kzv * zm.x);
+  *p = rhs_point<false>(s, g, ph, rk, e, j, kx, kzp, nlv, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -1057,8 +1098,16 @@ static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, co
   k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost);
 }
 template <int N>
+static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  const FieldSet nl = fset(s.nls[0], s.nls[1], s.nls[2], s.nls[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
+  launch_fwd_z(g, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]), nl, 8, st);
+  k_rhs_modes<<<dim3((g.nkzp * g.kxs + 255) / 256, g.np, 4), 256, 0, st>>>(s, g, ph, rk, nl);
+  launch_inv_z(g, nl, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6]), 4, st);
+}
+template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
   if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, st);
+  else if (s.nls[0]) go_zpass_split<N>(g, ph, s, rk, st);
   else go_zpass_t<N, double>(g, ph, s, rk, nullptr, st);
 }
 
