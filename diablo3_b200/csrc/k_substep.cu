@@ -803,6 +803,72 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
 }
 
 // ---------------------------------------------------------------------------
+// The same CN solves for the FP64 path, one thread per (x, z) column over
+// all rows: the plain Thomas sweeps with the shared LU factors (loads of the
+// row coefficients are uniform over a warp), the forward sweep writing g
+// into u itself; the rows the reference does not store get their old u
+// back.  Batches of TB rows have their loads issued first.  (The FP32 work
+// type keeps the tile solve above, measured faster there.)
+__global__ void __launch_bounds__(128) k_thomas_col(const __grid_constant__ State s, Geom g) {
+  constexpr int TB = 8;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
+  if (x >= g.nx) return;
+  const int np = g.np, Nyp = g.ny;
+  const long long pp = g.pp, col = (long long)z * g.nx + x;
+  for (int eq = 0; eq < 4; ++eq) {
+    const TriRow* Rw = s.tri + eq * np;
+    double* u = (double*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
+    const double* r = (const double*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
+    const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
+    const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
+    // old u of the end rows (the only ones that can lie outside lo..hi)
+    const double k0 = u[0], k1 = u[pp], kb = u[(long long)(np - 2) * pp], kt = u[(long long)(np - 1) * pp];
+    double um = 0.0, uc = k0, y = 0.0;
+    for (int jb = 0; jb < np; jb += TB) {
+      double xr[TB], xu[TB];
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jb + c;
+        xr[c] = (j < np) ? r[(long long)j * pp] : 0.0;
+        xu[c] = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jb + c;
+        if (j >= np) break;
+        const TriRow* row = Rw + j;
+        const double un = xu[c];
+        const double v = row->is_bc ? row->bc : xr[c] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+        y = (j == 0) ? v : v + row->ap * y;
+        u[(long long)j * pp] = y;
+        um = uc;
+        uc = un;
+      }
+    }
+    double xn = 0.0;
+    for (int jt = np - 1; jt >= 0; jt -= TB) {
+      double xg[TB];
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jt - c;
+        xg[c] = (j >= 0) ? u[(long long)j * pp] : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < TB; ++c) {
+        const int j = jt - c;
+        if (j < 0) break;
+        const double ib = Rw[j].ibp;
+        const double xv = (j == np - 1) ? xg[c] * ib : xg[c] * ib - Rw[j].u * ib * xn;
+        xn = xv;
+        const bool st = (j >= lo && j <= hi);
+        const double old = (j == 0) ? k0 : (j == 1 ? k1 : (j == np - 2 ? kb : kt));
+        u[(long long)j * pp] = st ? xv : old;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // rem_div factors: per (kx, kzp) column, rows 1..Nyp of the Poisson system
 // (solver.f90:1326-1333 with apply_BC_rem_div_mpi 2341-2368), forward
 // eliminated once: pfac[j] = (a'_j, 1/b'_j).
@@ -1139,15 +1205,15 @@ cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int r
   return cudaGetLastError();
 }
 cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
-  // y/z tile (FP64) + staged r and u (the FP64 tile doubles as staged r)
-  const size_t smem = (size_t)g.np * TX * (g.prec ? sizeof(double) + 2 * sizeof(float) : 2 * sizeof(double));
-  if (g.prec) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
-  } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_thomas<double><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
+  if (!g.prec) {   // FP64: one thread per column (measured faster than the tile solve there)
+    const int bx = g.nx < 128 ? g.nx : 128;
+    k_thomas_col<<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g);
+    return cudaGetLastError();
   }
+  // FP32 work type: the tile solve; y/z tile (FP64) + staged r and u (FP32)
+  const size_t smem = (size_t)g.np * TX * (sizeof(double) + 2 * sizeof(float));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
