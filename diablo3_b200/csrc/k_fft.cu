@@ -135,14 +135,26 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
   C v[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
+  double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
+  // accumulate (FP32 work type only): the FP64 values the transform adds
+  // to are loaded before the transform, so their latency hides behind it
+  constexpr bool ACC = sizeof(R) == sizeof(float);
+  double2 bv[ACC ? E : 1];
+  if (ACC && accumulate) {
+    const double2* base = dst;
+    if (ghost) {
+      const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
+      if (qg >= 0) base = ghost + (long long)(4 * (f & 3) + qg) * g.sp + kx;
+    }
+#pragma unroll
+    for (int q = 0; q < (ACC ? E : 1); ++q) {
+      const int z = lane + q * T;
+      const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
+      bv[q] = (active && kzp >= 0) ? base[(long long)kzp * g.kxs] : make_double2(0.0, 0.0);
+    }
+  }
   fft_reg_lazy<N, -1, true>(v, lane, active, sq, twt);
   if (!active) return;
-  double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
-  const double2* base = dst;
-  if (accumulate && ghost) {
-    const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
-    if (qg >= 0) base = ghost + (long long)(4 * (f & 3) + qg) * g.sp + kx;
-  }
   const double s = 1.0 / (double)N;
 #pragma unroll
   for (int q = 0; q < E; ++q) {
@@ -150,7 +162,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
     if (kzp >= 0) {
       double2 w = cscale(to_d2(v[q]), s);
-      if (accumulate) w = cadd(base[(long long)kzp * g.kxs], w);
+      if (ACC && accumulate) w = cadd(bv[ACC ? q : 0], w);
       dst[(long long)kzp * g.kxs] = w;
     }
   }

@@ -1005,34 +1005,34 @@ __global__ void __launch_bounds__(256) k_courant_reduce(const __grid_constant__ 
   if (!ctl.force && !(ctl.variable_dt && (sc->time_step % ctl.update_dt) == 0)) return;
   const long long n = (long long)g.pp;
   const int jlo = ph.front ? g.jstart : 1, jhi = ph.front ? g.jend : g.ny;
-  const long long total = (long long)(jhi - jlo + 1) * n;
   const double f = ph.ro_inv / ph.delta;
-  double dmin = __longlong_as_double(0x7ff0000000000000LL);
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const int j = jlo + (int)(idx / n);
-    const long long p = (long long)j * n + idx % n;
-    const double v1 = (double)U1[p], v2 = (double)U2[p], v3 = (double)U3[p];
-    double dx, dyv, dz;
-    if (ph.front) {
-      dx = ctl.cfl * ph.dx / fabs(v1 - ph.dthdz * g.gyf[j] / f);
-      dyv = ctl.cfl * g.dy[j] / fabs(v2);
-      dz = ctl.cfl * ph.dz / fabs(v3 + (1.0 / f) * ph.dthdx * (g.gyf[j] - 0.5 * ph.ly));
-    } else {
-      dx = ctl.cfl * ph.dx / fabs(v1);
-      dyv = ctl.cfl * g.dy[j] / fabs(v2);
-      dz = ctl.cfl * ph.dz / fabs(v3);
+  // min over points of CFL dx / |u1 - U| etc. = CFL / max of |u1 - U| / dx
+  // etc.: a running maximum per thread, one division per CTA
+  const double idx_ = 1.0 / ph.dx, idz_ = 1.0 / ph.dz;
+  double amax = 0.0;
+  bool bad = false;
+  for (int j = jlo + (int)blockIdx.y; j <= jhi; j += gridDim.y) {   // per-row constants once per row
+    const double c1 = ph.front ? ph.dthdz * g.gyf[j] / f : 0.0;
+    const double c3 = ph.front ? (1.0 / f) * ph.dthdx * (g.gyf[j] - 0.5 * ph.ly) : 0.0;
+    const double idy = 1.0 / g.dy[j];
+    const R* u1r = U1 + (long long)j * n;
+    const R* u2r = U2 + (long long)j * n;
+    const R* u3r = U3 + (long long)j * n;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+      const double v1 = (double)u1r[p], v2 = (double)u2r[p], v3 = (double)u3r[p];
+      const double a = fmax(fabs(v1 - c1) * idx_, fmax(fabs(v2) * idy, fabs(v3 + c3) * idz_));
+      bad = bad || !(a <= 1.7976931348623157e308);   // a non-finite velocity
+      amax = fmax(amax, a);
     }
-    dmin = fmin(dmin, fmin(dx, fmin(dyv, dz)));
-    if (!isfinite(v1) || !isfinite(v2) || !isfinite(v3)) atomicOr(&sc->flags, 1);
   }
-  for (int o = 16; o > 0; o >>= 1) dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+  if (bad) atomicOr(&sc->flags, 1);
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   __shared__ double red[8];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dmin;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) dmin = fmin(dmin, red[w]);
-    if (dmin >= 0.0) atomicMin(&sc->dt_min_bits, dbits(dmin));
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax = fmax(amax, red[w]);
+    if (amax > 0.0) atomicMin(&sc->dt_min_bits, dbits(ctl.cfl / amax));
   }
 }
 
@@ -1217,8 +1217,9 @@ cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
-  if (g.prec) k_courant_reduce<float><<<148 * 8, 256, 0, st>>>(s, g, ph, ctl);
-  else k_courant_reduce<double><<<148 * 8, 256, 0, st>>>(s, g, ph, ctl);
+  const dim3 grid(16, 74);   // x: within a row, y: rows
+  if (g.prec) k_courant_reduce<float><<<grid, 256, 0, st>>>(s, g, ph, ctl);
+  else k_courant_reduce<double><<<grid, 256, 0, st>>>(s, g, ph, ctl);
   k_courant_final<<<1, 1, 0, st>>>(s.sc, ph, ctl);
   return cudaGetLastError();
 }
