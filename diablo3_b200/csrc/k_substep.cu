@@ -529,8 +529,10 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
 //  inverse z-FFT of cr_e into xh[2e] (k_inv_z)
 __global__ void __launch_bounds__(256) k_rhs_modes(const __grid_constant__ State s, Geom g, Phys ph, int rk,
                                                    const __grid_constant__ FieldSet nl) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, e = blockIdx.z;
+  // equation fastest in the grid: the four CTAs of one block of modes run
+  // together and share the state reads (cu1, cu2, cu3, cth, cp) through L2
+  const int m = blockIdx.y * blockDim.x + threadIdx.x;
+  const int j = blockIdx.z, e = blockIdx.x;
   if (m >= g.nkzp * g.kxs) return;
   const int kzp = m / g.kxs, kx = m % g.kxs;
   const long long a = (long long)j * g.sp + m;
@@ -1167,7 +1169,7 @@ template <int N>
 static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
   const FieldSet nl = fset(s.nls[0], s.nls[1], s.nls[2], s.nls[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
   launch_fwd_z(g, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]), nl, 8, st);
-  k_rhs_modes<<<dim3((g.nkzp * g.kxs + 255) / 256, g.np, 4), 256, 0, st>>>(s, g, ph, rk, nl);
+  k_rhs_modes<<<dim3(4, (g.nkzp * g.kxs + 255) / 256, g.np), 256, 0, st>>>(s, g, ph, rk, nl);
   launch_inv_z(g, nl, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6]), 4, st);
 }
 template <int N>
