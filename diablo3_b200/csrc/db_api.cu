@@ -31,7 +31,7 @@ struct db_ctx {
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
   float2* d_twf = nullptr;       // the same in FP32
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [LES model active]
-  int time_step = 0;             // host mirror of the driver's time_step
+  int time_step = 0;             // host mirror of time_step (for/diablo.f90:59)
   std::string err;
   double* h_stage = nullptr;     // pinned staging, one physical field
   double2* d_ref = nullptr;       // one spectral field in the reference layout (device)

@@ -1,12 +1,7 @@
-// fft_smem.cuh -- complex helpers (FP64 and FP32), in-register DFTs, and the
-// batched shared-memory Stockham FFT (sm_100a).
-//
-// A CTA transforms S sequences of length N (power of two, 16..4096) held in
-// shared memory; sequence s, element e sits at buf[s * sstride + e].  The
-// work is split as N/8 threads per sequence; every pass each thread holds 8
-// complex values in registers (one radix-8, two radix-4 or four radix-2
-// butterflies), so the whole CTA reads, syncs, computes and writes back in
-// place.  Stockham autosort: the result comes out in natural order.
+// fft_smem.cuh -- complex helpers (FP64 and FP32), the in-register DFTs of
+// radix 2, 4 and 8, and the radix plan of a length-N transform (sm_100a).
+// The transforms themselves are in fft_reg.cuh: register-resident Stockham
+// passes with shared-memory exchanges between them.
 //
 // Pass with radix R after Ns = product of the previous radices, butterfly
 // b in [0, N/R):  x_r = in[b + r N/R] * w^(r (b mod Ns) N/(Ns R)),
@@ -114,80 +109,5 @@ template <>
 struct FftPlan<1> {
   static constexpr int log2n = 0;
 };
-
-// One Stockham pass of radix R for sequence base pointer buf (stride 1),
-// thread lane in [0, N/8).
-template <int N, int R, int SIGN>
-__device__ __forceinline__ void stockham_pass_load(const double2* buf, int lane, int Ns,
-                                                   const double2* __restrict__ tw, double2* v) {
-  constexpr int B = N / R;           // butterflies per sequence
-  constexpr int PER = 8 / R;         // butterflies per thread
-#pragma unroll
-  for (int m = 0; m < PER; ++m) {
-    int b = lane + m * (N / 8);
-    int kk = b % Ns;
-    int tstep = N / (Ns * R);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      double2 x = buf[b + r * B];
-      if (r > 0 && kk > 0) {
-        double2 w = __ldg(&tw[(r * kk * tstep) & (N - 1)]);
-        if (SIGN > 0) w.y = -w.y;
-        x = cmul(x, w);
-      }
-      v[m * R + r] = x;
-    }
-  }
-}
-
-template <int N, int R, int SIGN>
-__device__ __forceinline__ void stockham_pass_store(double2* buf, int lane, int Ns, double2* v) {
-  constexpr int PER = 8 / R;
-#pragma unroll
-  for (int m = 0; m < PER; ++m) {
-    double2* x = v + m * R;
-    if (R == 8) dft8<SIGN>(x);
-    if (R == 4) dft4<SIGN>(x[0], x[1], x[2], x[3]);
-    if (R == 2) dft2<SIGN>(x[0], x[1]);
-    int b = lane + m * (N / 8);
-    int base = (b / Ns) * Ns * R + (b % Ns);
-#pragma unroll
-    for (int r = 0; r < R; ++r) buf[base + r * Ns] = x[r];
-  }
-}
-
-// Full in-place transform of one sequence per thread group; all threads of
-// the CTA must call it (it contains __syncthreads).  active = false lets
-// surplus threads take part in the barriers only.
-template <int N, int SIGN>
-__device__ __forceinline__ void fft_inplace(double2* buf, int lane, bool active,
-                                            const double2* __restrict__ tw) {
-  using P = FftPlan<N>;
-  double2 v[8];
-  int Ns = 1;
-#pragma unroll
-  for (int pass = 0; pass < P::npass; ++pass) {
-    const bool last_small = (pass == P::npass - 1) && (P::rem != 0);
-    if (!last_small) {
-      if (active) stockham_pass_load<N, 8, SIGN>(buf, lane, Ns, tw, v);
-      __syncthreads();
-      if (active) stockham_pass_store<N, 8, SIGN>(buf, lane, Ns, v);
-      __syncthreads();
-      Ns *= 8;
-    } else if (P::rem == 2) {
-      if (active) stockham_pass_load<N, 4, SIGN>(buf, lane, Ns, tw, v);
-      __syncthreads();
-      if (active) stockham_pass_store<N, 4, SIGN>(buf, lane, Ns, v);
-      __syncthreads();
-      Ns *= 4;
-    } else {
-      if (active) stockham_pass_load<N, 2, SIGN>(buf, lane, Ns, tw, v);
-      __syncthreads();
-      if (active) stockham_pass_store<N, 2, SIGN>(buf, lane, Ns, v);
-      __syncthreads();
-      Ns *= 2;
-    }
-  }
-}
 
 }  // namespace db
