@@ -260,3 +260,37 @@ def test_checkpoint_file_round_trip(tmp_path):
         fh.write(b"NOTMAGIC")
     with pytest.raises(ValueError):
         checkpoint.read(path)
+
+
+def test_les_filter_weights():
+    """les_filter: every LES cell averages the fine cells whose centres it
+    holds (weights sum to 1), faces interpolate linearly (exact for a
+    linear profile), and a linear mean profile filters to the dyf-weighted
+    centres of the LES cells."""
+    from diablo3_b200 import les_filter as F
+    gf = create_grid(65, lz=2.0, cs=1.5, grid_type=1)
+    gc = create_grid(17, lz=2.0, cs=1.5, grid_type=1)
+    W, I = F._cell_weights(gf, gc), F._face_interp(gf, gc)
+    assert np.allclose(W.sum(axis=1), 1.0) and np.allclose(I.sum(axis=1), 1.0)
+    mf, mc = metrics(gf), metrics(gc)
+    # every interior fine cell belongs to exactly one interior LES cell
+    assert np.allclose(W[1:-1, 1:-1].astype(bool).sum(axis=0), 1.0)
+    # faces: linear in y is reproduced exactly
+    lin = 3.0 * mf["gy"] - 0.5
+    assert np.allclose((I @ lin)[1:], 3.0 * mc["gy"][1:] - 0.5, atol=1e-12)
+    # cells: the filtered linear profile is the dyf-weighted mean position of the fine cells
+    cen = W @ mf["gyf"]
+    for k in range(2, 17):
+        assert mc["gy"][k] <= cen[k] <= mc["gy"][k + 1]
+    box = F._hbox(np.arange(2 * 8 * 8, dtype=float).reshape(2, 8, 8), 8, 8, 4)
+    assert box.shape == (2, 2, 2) and np.isclose(box[0, 0, 0], np.mean([8 * z + x for z in range(4) for x in range(4)]))
+
+
+def test_profile_error_measures():
+    from diablo3_b200 import les_filter as F
+    ref0 = {"u1": np.zeros(5)}
+    ref = {"u1": np.array([0.0, 1.0, 2.0, 3.0, 0.0])}
+    les = {"u1": np.array([0.0, 1.0, 2.0, 2.0, 0.0])}
+    rows = slice(1, 4)
+    assert np.isclose(F.profile_errors(les, ref, rows)["u1"], 1.0 / np.linalg.norm([1, 2, 3]))
+    assert np.isclose(F.evolution_errors(les, ref0, ref, ref0, rows)["u1"], 1.0 / np.linalg.norm([1, 2, 3]))
