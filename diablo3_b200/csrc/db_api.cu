@@ -12,6 +12,7 @@
 
 #include "../../include/diablo_b200.h"
 #include "db_kernels.cuh"
+#include "les_feat.cuh"
 #include "mlp.cuh"
 
 using namespace db;
@@ -252,7 +253,7 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
     for (int i = 0; i < 19; ++i)
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
-    if ((rc = dalloc(c, &s.tscr, 2 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = dalloc(c, &s.tscr, 8 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = balloc(c, (void**)&s.sgs_feat, Pn * 16 * sizeof(float))) ||
         (rc = balloc(c, (void**)&s.sgs_out, Pn * 2 * sizeof(float)))) {
       db_finalize(c); g_init_err = "db_init: out of device memory"; return rc;
@@ -617,6 +618,24 @@ extern "C" int db_fft_xz_to_physical(db_ctx* c, double* buf) {
 // ---------------------------------------------------------------------------
 // the substep
 
+// the learned closure's feature source: the physical fields and x/z
+// derivatives the LES part of the substep has just formed
+static LesFeatSrc les_feat_src(const db_ctx* c) {
+  const State& s = c->s;
+  LesFeatSrc f{};
+  f.f[0] = s.u1; f.f[1] = s.u2; f.f[2] = s.u3; f.f[3] = s.th;
+  for (int i = 0; i < 4; ++i) {
+    f.f[4 + i] = s.gx[i];
+    f.f[8 + i] = s.gz[i];
+  }
+  f.lrow = s.lrow;
+  f.pp = c->g.pp;
+  f.ny = c->g.ny;
+  f.dxs = c->ph.dx * BETA_SGS;
+  f.dzs = c->ph.dz * BETA_SGS;
+  return f;
+}
+
 // the LES model runs on a substep of driver step time_step (solver.f90:615)
 static bool les_active(const db_ctx* c, int time_step) {
   return c->p.use_les && (!c->p.create_new_flow || time_step > 100);
@@ -642,11 +661,11 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
     for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
     if ((e = launch_inv_x(g, in, out, 12, st, 0xF0u))) return e;
     mark(c, rk, 2);
-    if (c->p.les_model_type == 6) {   // learned closure, AMD outside its range
-      if ((e = launch_les_amd(g, c->ph, s, st, 1))) return e;
-      if (sgs_forward_async(c->sgs, s.sgs_feat, s.sgs_out, (long long)g.np * g.pp, st)) return cudaErrorLaunchFailure;
+    if (c->p.les_model_type == 6) {   // learned closure (features formed in the inference kernel), AMD outside its range
+      if (sgs_forward_les_async(c->sgs, les_feat_src(c), g.prec != 0, s.sgs_out, (long long)g.np * g.pp, st))
+        return cudaErrorLaunchFailure;
       if ((e = launch_les_amd(g, c->ph, s, st, 2))) return e;
-      n += 2;
+      n += 1;
     } else {
       if ((e = launch_les_amd(g, c->ph, s, st))) return e;
     }
@@ -1057,13 +1076,13 @@ extern "C" int db_les_eval(db_ctx* c, int model, double* nu_t, double* kappa_t, 
   FieldSet out = fset(s.u1, s.u2, s.u3, s.th, s.gx[0], s.gx[1], s.gx[2], s.gx[3]);
   for (int i = 0; i < 4; ++i) { in.p[8 + i] = s.xh[4 + i]; out.p[8 + i] = s.gz[i]; }
   CK(launch_inv_x(g, in, out, 12, st, 0xF0u));
-  if (model == 6 || feat) CK(launch_les_amd(g, c->ph, s, st, 1));
+  if (feat) CK(launch_les_amd(g, c->ph, s, st, 1));
   if (model == 6) {
-    if (sgs_forward_async(c->sgs, s.sgs_feat, s.sgs_out, (long long)g.np * g.pp, st))
+    if (sgs_forward_les_async(c->sgs, les_feat_src(c), g.prec != 0, s.sgs_out, (long long)g.np * g.pp, st))
       return fail(c, DB_ERR_CUDA, "closure inference failed");
   }
   CK(launch_les_amd(g, c->ph, s, st, model == 6 ? 2 : 0));
-  c->launches += (model == 6 ? 7 : 5) + (feat && model != 6 ? 1 : 0);
+  c->launches += (model == 6 ? 6 : 5) + (feat ? 1 : 0);
   const size_t np_ = (size_t)g.np * g.pp;
   if (feat) {
     CK(cudaMemcpyAsync(feat, s.sgs_feat, np_ * 16 * sizeof(float), cudaMemcpyDeviceToHost, st));

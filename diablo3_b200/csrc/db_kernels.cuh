@@ -127,7 +127,7 @@ struct State {
   double* les[9];                            // SGS forcing per product slot (k_les.cu)
   double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
-  double* tscr;                              // FP64 Thomas scratch, two fields (LES)
+  double* tscr;                              // FP64 Thomas scratch, two fields per equation (LES)
   const LesRow* lrow;                        // np rows (LES)
   // learned closure (les_model_type 6): features [point][16], outputs
   // [point][2] (nu_t, kappa_t), training range lo[16], hi[16]

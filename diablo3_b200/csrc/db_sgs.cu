@@ -135,6 +135,13 @@ int sgs_forward_async(db_sgs_net* n, const float* d_feat, float* d_out, long lon
   return sgs_fail(db::launch_mlp(a, false, 4 * n->sms, st));
 }
 
+int sgs_forward_les_async(db_sgs_net* n, const db::LesFeatSrc& src, bool fp32, float* d_out, long long npts,
+                          cudaStream_t st) {
+  if (npts > 0x7fffffffLL) return DB_ERR_SIZE;
+  db::MlpArgs a{nullptr, nullptr, d_out, n->params, n->norm, nullptr, nullptr, (int)npts, n->err, src};
+  return sgs_fail(db::launch_mlp_les(a, fp32, st));
+}
+
 extern "C" int db_sgs_forward(db_sgs_net* n, const float* d_feat, float* d_out, long long npts) {
   if (!n || !d_feat || !d_out || npts < 0) return DB_ERR_ARG;
   int rc = sgs_forward_async(n, d_feat, d_out, npts, n->st);

@@ -32,6 +32,7 @@
 
 #include "db_bc.cuh"
 #include "db_kernels.cuh"
+#include "les_feat.cuh"
 #include "umma.cuh"
 
 namespace db {
@@ -76,7 +77,6 @@ __global__ void k_les_bc(const __grid_constant__ State s, Geom g, Phys ph) {
 // AMD model
 
 constexpr double C_AMD = 0.2887;     // les.f90:25
-constexpr double BETA_SGS = 3.0;     // les.f90:43
 
 // max{0, -(I3 - I4)} / (I1 - I2) of the scaled strain SI and rotation O
 // tensors (les.f90:578-619): -tr(SI^3) + tr(SI O^2) over |SI|^2 + |O|^2
@@ -131,6 +131,13 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
 // s1 = -2 nu_GYF / filter at GYF rows with nu_GYF the mean of the two GY
 // neighbours; a point whose features leave the training range
 // (s.sgs_range: lo[16], hi[16]) keeps its AMD value.
+//
+// The walk over j = 1 .. Nyp + 1 is split into gridDim.z chunks run by
+// separate threads.  A chunk [ja, jb] starts from the GYF values of row
+// ja - 2 and computes row ja - 1 without storing it, which rebuilds exactly
+// the values a single walk carries into row ja; it then stores the GY rows
+// ja .. jb and the GYF rows ja - 1 .. jb - 1, so the chunks partition every
+// output and each stored value is the one a single walk would store.
 constexpr int AMD_SLOTS = 4;
 
 template <typename R, int MODE>
@@ -140,6 +147,10 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   const long long pp = g.pp;
   const long long col = (long long)z * g.nx + x;
   const int Nyp = g.ny;
+  const int clen = (Nyp + 1 + gridDim.z - 1) / gridDim.z;
+  const int ja = 1 + blockIdx.z * clen, jb = min(Nyp + 1, ja + clen - 1);
+  if (ja > jb) return;
+  const int j0 = ja >= 2 ? ja - 2 : 0;   // row the walk starts from (GYF values only)
   const int jst = g.jstart_th, jet = g.jend_th;
   const int j1 = g.jstart, j2 = Nyp - 1;
   const R h = 0.5;
@@ -163,25 +174,28 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   float* fo = s.sgs_feat;
   const float* mo = s.sgs_out;
   const float* rng = s.sgs_range;
-  if (MODE == 1) {
+  if (MODE == 1 && ja == 1) {
 #pragma unroll
     for (int f = 0; f < 16; ++f) fo[col * 16 + f] = 0.0f;
   }
   R hnu = 0, hka = 0;     // closure values at the previous GY row
   bool hval = false;
 
-  // row 0: GYF values only (GY row 0 does not exist)
-  R u1m = __ldg(u1), u3m = __ldg(u3), thm = __ldg(th), u2c = __ldg(u2 + pp);
-  R f1x = __ldg(g1x), f3z = __ldg(g3z), f1z = __ldg(g1z), f3x = __ldg(g3x);
-  R ftx = __ldg(gtx), ftz = __ldg(gtz);
-  R f2y = (u2c - __ldg(u2)) * (R)LR[0].idyf;
+  // row j0: GYF values only (GY row 0 does not exist)
+  const long long o0 = (long long)j0 * pp;
+  R u1m = __ldg(u1 + o0), u3m = __ldg(u3 + o0), thm = __ldg(th + o0), u2c = __ldg(u2 + o0 + pp);
+  R f1x = __ldg(g1x + o0), f3z = __ldg(g3z + o0), f1z = __ldg(g1z + o0), f3x = __ldg(g3x + o0);
+  R ftx = __ldg(gtx + o0), ftz = __ldg(gtz + o0);
+  R f2y = (u2c - __ldg(u2 + o0)) * (R)LR[j0].idyf;
   // previous GY row (r = j - 1) values
   R h1y = 0, h3y = 0, hty = 0, h2x = 0, h2z = 0;
   R hSI4 = 0, hSI6 = 0, hO4 = 0, hO6 = 0, hP4 = 0, hP6 = 0, hdl = 0;
-  nut[0] = 0;
-  kat[0] = 0;
-  o[5][0] = 0;
-  o[6][0] = 0;
+  if (MODE != 1 && ja == 1) {
+    nut[0] = 0;
+    kat[0] = 0;
+    o[5][0] = 0;
+    o[6][0] = 0;
+  }
 
   // the 12 values a row needs come through a ring of AMD_SLOTS shared-memory
   // slots per thread, filled by cp.async AMD_SLOTS - 1 rows ahead: row j's
@@ -191,7 +205,7 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   const int tb = blockDim.x, tx = threadIdx.x;
   const R* srcs[12] = {u1, u3, th, u2 + pp, g1x, g2x, g3x, gtx, g1z, g2z, g3z, gtz};
   auto issue = [&](int jr) {
-    if (jr <= Nyp + 1) {
+    if (jr <= jb) {
       R* sl = ring + (jr % AMD_SLOTS) * 12 * tb + tx;
       const long long oj = (long long)jr * pp;
 #pragma unroll
@@ -203,9 +217,10 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     cp_async_commit();
   };
 #pragma unroll
-  for (int jr = 1; jr < AMD_SLOTS; ++jr) issue(jr);
+  for (int jr = 1; jr < AMD_SLOTS; ++jr) issue(j0 + jr);
 
-  for (int j = 1; j <= Nyp + 1; ++j) {
+  for (int j = j0 + 1; j <= jb; ++j) {
+    const bool keep = j >= ja;   // row ja - 1 only rebuilds the carried values
     const long long oj = (long long)j * pp;
     issue(j + AMD_SLOTS - 1);
     cp_async_wait<AMD_SLOTS - 1>();
@@ -232,17 +247,16 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     R nu_m = 0, ka_m = 0;
     bool val = false;
     if (MODE != 0) {
-      const R wa = (R)lr.wa, wb = (R)lr.wb;
+      const LesFeatIn<R> fi{a1x, f1x, a1z, f1z, a2x, a2z, a3x, f3x, a3z, f3z, atx, ftx, atz, ftz,
+                            d1y, d3y, dty, c2y, f2y};
       float fv[16];
-      fv[0] = (float)(a1x * wa + f1x * wb); fv[1] = (float)d1y; fv[2] = (float)(a1z * wa + f1z * wb);
-      fv[3] = (float)a2x; fv[4] = (float)(c2y * wa + f2y * wb); fv[5] = (float)a2z;
-      fv[6] = (float)(a3x * wa + f3x * wb); fv[7] = (float)d3y; fv[8] = (float)(a3z * wa + f3z * wb);
-      fv[9] = (float)(atx * wa + ftx * wb); fv[10] = (float)dty; fv[11] = (float)(atz * wa + ftz * wb);
-      fv[12] = (float)dxs; fv[13] = (float)dly; fv[14] = (float)dzs; fv[15] = (float)dty;
+      les_features<R>(fi, (R)lr.wa, (R)lr.wb, dxs, dly, dzs, fv);
       const long long pt = (oj + col) * 16;
       if (MODE == 1) {
+        if (keep) {
 #pragma unroll
-        for (int f = 0; f < 16; ++f) fo[pt + f] = fv[f];
+          for (int f = 0; f < 16; ++f) fo[pt + f] = fv[f];
+        }
       } else {
         val = true;
 #pragma unroll
@@ -277,10 +291,12 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     const R P4 = (j >= 2) ? temp * (S4 - h * d1y) : S4;
     const R P6 = (j >= 2) ? temp * (S6 - h * d3y) : S6;
     const bool gy2 = (j >= 2 && j <= Nyp);
-    nut[oj] = nu;
-    kat[oj] = ka;
-    o[5][oj] = gy2 ? delt * P4 - nu * d1y : (R)0;
-    o[6][oj] = gy2 ? delt * P6 - nu * d3y : (R)0;
+    if (keep) {
+      nut[oj] = nu;
+      kat[oj] = ka;
+      o[5][oj] = gy2 ? delt * P4 - nu * d1y : (R)0;
+      o[6][oj] = gy2 ? delt * P6 - nu * d3y : (R)0;
+    }
 
     // GYF row r = j - 1: needs GY rows r and r + 1 = j
     {
@@ -309,13 +325,15 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
         L7 = h * dlf * (s1t * ftx);
         L8 = h * dlf * (s1t * ftz);
       }
-      o[0][orr] = L0;
-      o[1][orr] = L1;
-      o[2][orr] = L2;
-      o[3][orr] = L3;
-      o[4][orr] = L4;
-      o[7][orr] = L7;
-      o[8][orr] = L8;
+      if (keep) {
+        o[0][orr] = L0;
+        o[1][orr] = L1;
+        o[2][orr] = L2;
+        o[3][orr] = L3;
+        o[4][orr] = L4;
+        o[7][orr] = L7;
+        o[8][orr] = L8;
+      }
     }
     // shift
     u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
@@ -324,33 +342,34 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
     hnu = nu_m; hka = ka_m; hval = val;
   }
-  if (MODE == 1) return;
+  if (MODE == 1 || jb != Nyp + 1) return;
   const long long oe = (long long)(Nyp + 1) * pp;
   o[0][oe] = 0; o[1][oe] = 0; o[2][oe] = 0; o[3][oe] = 0; o[4][oe] = 0;
   o[7][oe] = 0; o[8][oe] = 0;
 }
 
 // ---------------------------------------------------------------------------
-// CN solves with eddy viscosity: one thread per (x, z) column runs the
-// Thomas sweeps of the four equations (FP64 arithmetic, fields stored as R).
-// The matrix differs per column, so nothing is shared: the eliminated upper
-// coefficients u_j / b'_j and right-hand side g_j / b'_j go to an FP64
-// scratch (2 fields) and come back in the backward sweep.  Rows are handled
-// in batches of TB whose loads are all issued first, so each thread keeps
-// 3 TB loads in flight instead of waiting on every row.
+// CN solves with eddy viscosity: one thread per (x, z) column and equation
+// (blockIdx.z: th, u2, u1, u3) runs a Thomas sweep (FP64 arithmetic, fields
+// stored as R).  The matrix differs per column, so nothing is shared: the
+// eliminated upper coefficients u_j / b'_j and right-hand side g_j / b'_j go
+// to an FP64 scratch (2 fields per equation) and come back in the backward
+// sweep.  Rows are handled in batches of TB whose loads are all issued
+// first, so each thread keeps 3 TB loads in flight instead of waiting on
+// every row.
 constexpr int TB = 8;
 
 template <typename R>
 __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ State s, Geom g, int rk) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, eq = blockIdx.z;
   if (x >= g.nx) return;
   const int np = g.np, Nyp = g.ny;
   const long long pp = g.pp, col = (long long)z * g.nx + x;
   const double temp2 = 0.5 * s.sc->h_bar[rk];
-  double* cmv = s.tscr + col;                        // u_j / b'_j
-  double* gsv = s.tscr + (long long)np * pp + col;   // g_j / b'_j
+  double* cmv = s.tscr + (long long)(2 * eq) * np * pp + col;   // u_j / b'_j
+  double* gsv = cmv + (long long)np * pp;                         // g_j / b'_j
   constexpr bool INC = sizeof(R) == sizeof(float);   // r holds increments over u
-  for (int eq = 0; eq < 4; ++eq) {
+  {
     const TriRow* Rw = s.tri + eq * np;
     R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
     R* r = (R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
@@ -429,8 +448,16 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
   return cudaGetLastError();
 }
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode) {
-  const int bx = g.nx < 128 ? g.nx : 128;
-  const dim3 grid(g.nx / bx, g.nz);
+  // wall-normal chunks until about 16 warps per SM walk columns (each chunk
+  // at least 8 rows), then columns per CTA: 128, narrowed (to 32 at least)
+  // until every SM has two CTAs
+  const long long cols = (long long)g.nx * g.nz, want = 512LL * sm_count();
+  const int maxch = (g.ny + 1) / 8 > 1 ? (g.ny + 1) / 8 : 1;
+  int nch = (int)((want + cols - 1) / cols);
+  nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
+  int bx = g.nx < 128 ? g.nx : 128;
+  while (bx > 32 && bx % 2 == 0 && (long long)((g.nx + bx - 1) / bx) * g.nz * nch < 2LL * sm_count()) bx >>= 1;
+  const dim3 grid((g.nx + bx - 1) / bx, g.nz, nch);
   const size_t smem = (size_t)AMD_SLOTS * 12 * bx * (g.prec ? sizeof(float) : sizeof(double));
   if (g.prec) {
     if (mode == 1) k_les_amd<float, 1><<<grid, bx, smem, st>>>(s, g, ph);
@@ -446,8 +473,8 @@ cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaSt
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
   const int want = (g.tune_les_tb > 0 && g.tune_les_tb <= 128) ? g.tune_les_tb : 128;   // powers of two
   const int bx = g.nx < want ? g.nx : want;
-  if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
-  else k_thomas_les<double><<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g, rk);
+  if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk);
+  else k_thomas_les<double><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk);
   return cudaGetLastError();
 }
 

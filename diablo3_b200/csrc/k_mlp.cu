@@ -5,7 +5,9 @@
 //
 // One CTA of 128 threads works on tiles of 128 points; thread t owns point
 // (row) t of the tile and reads row t of every accumulator from tensor
-// memory.
+// memory.  k_mlp_train runs the forward and backward passes; k_mlp_infer the
+// forward pass only, its features read from an array or formed from the LES
+// substep's physical fields.
 //   forward   X W1^T -> z1 -> h1 = gelu(z1) (tanh form) -> h1 W2^T -> z2 -> ... -> h3,
 //             y = W4 h3 + b4 on CUDA cores (N = 2), out = softplus(y) * scale
 //   backward  (training) dy = dL/dy; dh3 = dy W4, dz3 = dh3 gelu'(z3);
@@ -20,7 +22,10 @@
 #include <cuda_bf16.h>
 #include <math.h>
 
+#include <type_traits>
+
 #include "../../include/diablo_b200.h"
+#include "les_feat.cuh"
 #include "mlp.cuh"
 #include "umma.cuh"
 
@@ -76,10 +81,9 @@ __device__ __forceinline__ void put1(unsigned char* tile, int row, int k, int K,
   *reinterpret_cast<__nv_bfloat16*>(tile + kmajor_offset(row, k, K)) = __float2bfloat16_rn(v);
 }
 
-// shared-memory plan (bytes); training needs the transposed tiles and the
-// gradient operands, inference only X, H1, H2 and the weights
-template <bool TRAIN>
-struct Plan {
+// shared-memory plan of the training kernel (bytes): the forward tiles, the
+// transposed tiles and the gradient operands
+struct PlanTrain {
   static constexpr uint32_t X = 0;                                     // [128][16]
   static constexpr uint32_t H1 = X + TILE * NF * 2;                    // [128][64]
   static constexpr uint32_t H2 = H1 + TILE * NH * 2;                   // [128][64]
@@ -87,26 +91,25 @@ struct Plan {
   static constexpr uint32_t W2 = W1 + NH * NF * 2;                     // [64][64]
   static constexpr uint32_t W3 = W2 + NH * NH * 2;                     // [64][64]
   static constexpr uint32_t XT = W3 + NH * NH * 2;                     // [32][128]: x^T, ones row, zeros
-  static constexpr uint32_t H1T = XT + (TRAIN ? 32 * TILE * 2 : 0);    // [80][128]: h1^T, ones, zeros
-  static constexpr uint32_t H2T = H1T + (TRAIN ? 80 * TILE * 2 : 0);   // [80][128]
-  static constexpr uint32_t DZ = H2T + (TRAIN ? 80 * TILE * 2 : 0);    // [128][64] dz
-  static constexpr uint32_t DZT = DZ + (TRAIN ? TILE * NH * 2 : 0);    // [128][128] dz^T (rows >= 64 zero)
-  static constexpr uint32_t W2T = DZT + (TRAIN ? TILE * TILE * 2 : 0); // [64][64] W2^T
-  static constexpr uint32_t W3T = W2T + (TRAIN ? NH * NH * 2 : 0);     // [64][64] W3^T
-  static constexpr uint32_t RED = W3T + (TRAIN ? NH * NH * 2 : 0);     // dW4, db4 partial sums (floats)
-  static constexpr uint32_t MBAR = RED + (TRAIN ? 136 * 4 : 0);
+  static constexpr uint32_t H1T = XT + 32 * TILE * 2;                  // [80][128]: h1^T, ones, zeros
+  static constexpr uint32_t H2T = H1T + 80 * TILE * 2;                 // [80][128]
+  static constexpr uint32_t DZ = H2T + 80 * TILE * 2;                 // [128][64] dz
+  static constexpr uint32_t DZT = DZ + TILE * NH * 2;                  // [128][128] dz^T (rows >= 64 zero)
+  static constexpr uint32_t W2T = DZT + TILE * TILE * 2; // [64][64] W2^T
+  static constexpr uint32_t W3T = W2T + NH * NH * 2;                   // [64][64] W3^T
+  static constexpr uint32_t RED = W3T + NH * NH * 2;                   // dW4, db4 partial sums (floats)
+  static constexpr uint32_t MBAR = RED + 136 * 4;
   static constexpr uint32_t SLOT = MBAR + 8;
   static constexpr uint32_t BYTES = SLOT + 8;
-  static constexpr uint32_t TMEM_COLS = TRAIN ? 512 : 64;
+  static constexpr uint32_t TMEM_COLS = 512;
   // tensor-memory columns: z accumulator, dh accumulator, [dW3|db3], [dW2|db2], [dW1|db1]
   static constexpr uint32_t C_Z = 0, C_H = 64, C_G3 = 128, C_G2 = 256, C_G1 = 384;
 };
 
 constexpr uint32_t WAIT_ITERS = 1u << 22;   // bounded mbarrier waits
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
-  using PL = Plan<TRAIN>;
+__global__ void __launch_bounds__(TILE, 1) k_mlp_train(MlpArgs a) {
+  using PL = PlanTrain;
   extern __shared__ __align__(1024) unsigned char sm[];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + PL::MBAR);
@@ -125,31 +128,28 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
       put8(sm + PL::W2, r, k0, NH, v);
       for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + r * NH + k0 + i];
       put8(sm + PL::W3, r, k0, NH, v);
-      if (TRAIN) {   // transposes: row r = input index, K = output index
-        for (int i = 0; i < 8; ++i) v[i] = P[P_W2 + (k0 + i) * NH + r];
-        put8(sm + PL::W2T, r, k0, NH, v);
-        for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + (k0 + i) * NH + r];
-        put8(sm + PL::W3T, r, k0, NH, v);
-      }
+      // transposes: row r = input index, K = output index
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W2 + (k0 + i) * NH + r];
+      put8(sm + PL::W2T, r, k0, NH, v);
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + (k0 + i) * NH + r];
+      put8(sm + PL::W3T, r, k0, NH, v);
     }
   }
-  if (TRAIN) {
-    // constant rows of the transposed operands: ones row (bias gradients),
-    // zero padding, and the zero upper half of dz^T
-    for (int m = t; m < TILE; m += TILE) {
-      put1(sm + PL::XT, NF, m, TILE, 1.0f);
-      for (int r = NF + 1; r < 32; ++r) put1(sm + PL::XT, r, m, TILE, 0.0f);
-      put1(sm + PL::H1T, NH, m, TILE, 1.0f);
-      put1(sm + PL::H2T, NH, m, TILE, 1.0f);
-      for (int r = NH + 1; r < 80; ++r) {
-        put1(sm + PL::H1T, r, m, TILE, 0.0f);
-        put1(sm + PL::H2T, r, m, TILE, 0.0f);
-      }
-      for (int r = NH; r < TILE; ++r) put1(sm + PL::DZT, r, m, TILE, 0.0f);
+  // constant rows of the transposed operands: ones row (bias gradients),
+  // zero padding, and the zero upper half of dz^T
+  for (int m = t; m < TILE; m += TILE) {
+    put1(sm + PL::XT, NF, m, TILE, 1.0f);
+    for (int r = NF + 1; r < 32; ++r) put1(sm + PL::XT, r, m, TILE, 0.0f);
+    put1(sm + PL::H1T, NH, m, TILE, 1.0f);
+    put1(sm + PL::H2T, NH, m, TILE, 1.0f);
+    for (int r = NH + 1; r < 80; ++r) {
+      put1(sm + PL::H1T, r, m, TILE, 0.0f);
+      put1(sm + PL::H2T, r, m, TILE, 0.0f);
     }
-    float* red = reinterpret_cast<float*>(sm + PL::RED);
-    for (int i = t; i < 136; i += TILE) red[i] = 0.0f;
+    for (int r = NH; r < TILE; ++r) put1(sm + PL::DZT, r, m, TILE, 0.0f);
   }
+  float* red = reinterpret_cast<float*>(sm + PL::RED);
+  for (int i = t; i < 136; i += TILE) red[i] = 0.0f;
   if (t == 0) mbar_init(mbar, 1);
   if (warp == 0) {
     tmem_alloc(slot, PL::TMEM_COLS);
@@ -198,10 +198,8 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
       for (int i = 0; i < 16; ++i) h[i] = gelu(z[i] + bias[c + i]);
       put8(tileA, t, c, NH, h);
       put8(tileA, t, c + 8, NH, h + 8);
-      if (TRAIN && tileT) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) put1(tileT, c + i, t, TILE, h[i]);
-      }
+      for (int i = 0; i < 16; ++i) put1(tileT, c + i, t, TILE, h[i]);
     }
   };
 
@@ -232,10 +230,8 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
     for (int f = 0; f < NF; ++f) x[f] = live ? (a.feat[(long long)p * NF + f] - mu[f]) * isd[f] : 0.0f;
     put8(sm + PL::X, t, 0, NF, x);
     put8(sm + PL::X, t, 8, NF, x + 8);
-    if (TRAIN) {
 #pragma unroll
-      for (int f = 0; f < NF; ++f) put1(sm + PL::XT, f, t, TILE, x[f]);
-    }
+    for (int f = 0; f < NF; ++f) put1(sm + PL::XT, f, t, TILE, x[f]);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -243,14 +239,14 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
     // ---- layer 1..3
     if (t == 0) gemm(PL::C_Z, aX, NF * 16, aW1, NF * 16, NF, id64, false);
     if (!(ok = sync_mma())) break;
-    hidden_out(b1, sm + PL::H1, TRAIN ? sm + PL::H1T : nullptr);
+    hidden_out(b1, sm + PL::H1, sm + PL::H1T);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (t == 0) gemm(PL::C_Z, aH1, NH * 16, aW2, NH * 16, NH, id64, false);
     if (!(ok = sync_mma())) break;
-    hidden_out(b2, sm + PL::H2, TRAIN ? sm + PL::H2T : nullptr);
+    hidden_out(b2, sm + PL::H2, sm + PL::H2T);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -271,16 +267,6 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
       }
     }
     const float s0 = softplus(y0) * osc0, s1 = softplus(y1) * osc1;
-    if (!TRAIN) {
-      if (live) {
-        a.out[(long long)p * 2] = s0;
-        a.out[(long long)p * 2 + 1] = s1;
-      }
-      tc_fence_before();
-      __syncthreads();   // X, H tiles are rewritten by the next tile
-      tc_fence_after();
-      continue;
-    }
     // ---- loss and dL/dy (mean over the batch of the squared error)
     float dy0 = 0.0f, dy1 = 0.0f;
     if (live) {
@@ -381,7 +367,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
     first = false;
   }
 
-  if (TRAIN && ok && !first) {
+  if (ok && !first) {
     // gradients of this CTA: rows 0..63 of the accumulators are lanes 0..63
     if (warp < 2) {
       const int o = t;   // output unit
@@ -417,10 +403,8 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
     for (int i = t; i < NO * NH; i += TILE) atomicAdd(&a.grads[P_W4 + i], red[i]);
     if (t < NO) atomicAdd(&a.grads[P_B4 + t], red[128 + t]);
   }
-  if (TRAIN) {
-    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-    if (lane == 0 && lsum != 0.0f) atomicAdd(a.loss, lsum);
-  }
+  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  if (lane == 0 && lsum != 0.0f) atomicAdd(a.loss, lsum);
   if (!ok && t == 0) atomicExch(a.err, 1);
   tc_fence_before();
   __syncthreads();
@@ -428,6 +412,205 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp(MlpArgs a) {
 }
 
 // Adam (bias-corrected) on the FP32 master weights; grads are consumed and zeroed
+// ---------------------------------------------------------------------------
+// Inference.  Same arithmetic as the forward half of k_mlp (BF16 operands,
+// FP32 accumulation, the same rounding points), laid out for throughput:
+// the X tile aliases the start of the H tile (layer 1 has finished reading X
+// when its epilogue writes H, and layers 2 and 3 have finished reading H
+// when the next epilogue or the next tile writes it), so a CTA needs 35 KB of
+// shared memory and six CTAs share an SM, whose tiles overlap one another's
+// tensor-core waits.  SRC 0 reads features from a.feat; SRC 1 / 2 form them
+// from the LES substep's FP32 / FP64 physical fields (les_feat.cuh), point
+// p = j * pp + col of GY row j, row 0 getting zero features.
+struct PlanInf {
+  static constexpr uint32_t H = 0;                       // [128][64]; X [128][16] at its start
+  static constexpr uint32_t W1 = H + TILE * NH * 2;      // [64][16]
+  static constexpr uint32_t W2 = W1 + NH * NF * 2;       // [64][64]
+  static constexpr uint32_t W3 = W2 + NH * NH * 2;       // [64][64]
+  static constexpr uint32_t MBAR = W3 + NH * NH * 2;
+  static constexpr uint32_t SLOT = MBAR + 8;
+  static constexpr uint32_t BYTES = SLOT + 8;
+  static constexpr uint32_t TMEM_COLS = 64;
+};
+constexpr int INF_CTAS_PER_SM = 6;
+static_assert(INF_CTAS_PER_SM * PlanInf::TMEM_COLS <= 512, "tensor memory of the resident CTAs");
+
+template <int SRC>
+__global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) {
+  using PL = PlanInf;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int t = threadIdx.x, warp = t >> 5;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + PL::MBAR);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(sm + PL::SLOT);
+  const float* P = a.params;
+  for (int r = t; r < NH; r += TILE) {
+    float v[8];
+    for (int k0 = 0; k0 < NF; k0 += 8) {
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W1 + r * NF + k0 + i];
+      put8(sm + PL::W1, r, k0, NF, v);
+    }
+    for (int k0 = 0; k0 < NH; k0 += 8) {
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W2 + r * NH + k0 + i];
+      put8(sm + PL::W2, r, k0, NH, v);
+      for (int i = 0; i < 8; ++i) v[i] = P[P_W3 + r * NH + k0 + i];
+      put8(sm + PL::W3, r, k0, NH, v);
+    }
+  }
+  __shared__ float sb[3 * NH + NO + NO * NH + 2 * NF];   // b1 b2 b3 b4 W4 mean 1/std (FP32)
+  for (int i = t; i < NH; i += TILE) {
+    sb[i] = P[P_B1 + i];
+    sb[NH + i] = P[P_B2 + i];
+    sb[2 * NH + i] = P[P_B3 + i];
+  }
+  for (int i = t; i < NO * NH; i += TILE) sb[3 * NH + NO + i] = P[P_W4 + i];
+  if (t < NO) sb[3 * NH + t] = P[P_B4 + t];
+  if (t < 2 * NF) sb[3 * NH + NO + NO * NH + t] = a.norm[t];
+  if (t == 0) mbar_init(mbar, 1);
+  if (warp == 0) {
+    tmem_alloc(slot, PL::TMEM_COLS);
+    tmem_relinquish();
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *slot;
+  const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);
+  const float* b1 = sb;
+  const float* b2 = sb + NH;
+  const float* b3 = sb + 2 * NH;
+  const float* b4 = sb + 3 * NH;
+  const float* W4 = sb + 3 * NH + NO;
+  const float* mu = sb + 3 * NH + NO + NO * NH;
+  const float* isd = mu + NF;
+  const float osc0 = a.norm[2 * NF], osc1 = a.norm[2 * NF + 1];
+  const uint32_t id64 = umma_idesc_bf16(128, NH);
+  const uint32_t aH = smem_u32(sm + PL::H);
+  const uint32_t aW1 = smem_u32(sm + PL::W1), aW2 = smem_u32(sm + PL::W2), aW3 = smem_u32(sm + PL::W3);
+  uint32_t phase = 0;
+  bool ok = true;
+  auto gemm = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t b_addr, uint32_t b_sbo, int K) {
+    for (int s = 0; s < K / 16; ++s)
+      umma_bf16(tbase, umma_desc(a_addr + 256 * s, 128, a_sbo), umma_desc(b_addr + 256 * s, 128, b_sbo), id64,
+                s > 0);
+  };
+  // operands written by this CTA's threads are visible to the tensor core,
+  // and every thread's earlier tensor-memory reads are done, before t0 issues
+  auto to_tc = [&]() {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  };
+  auto sync_mma = [&]() -> bool {
+    if (t == 0) umma_commit(mbar);
+    const bool w = mbar_wait(mbar, phase, WAIT_ITERS);
+    phase ^= 1u;
+    tc_fence_after();
+    return __syncthreads_and(w ? 1 : 0) != 0;
+  };
+  auto hidden_out = [&](const float* bias) {
+#pragma unroll
+    for (int c = 0; c < NH; c += 32) {
+      float z0[16], z1[16];
+      tmem_ld16(trow + c, z0);
+      tmem_ld16(trow + c + 16, z1);
+      tmem_wait_ld();
+      float h[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) h[i] = gelu(z0[i] + bias[c + i]);
+      put8(sm + PL::H, t, c, NH, h);
+      put8(sm + PL::H, t, c + 8, NH, h + 8);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) h[i] = gelu(z1[i] + bias[c + 16 + i]);
+      put8(sm + PL::H, t, c + 16, NH, h);
+      put8(sm + PL::H, t, c + 24, NH, h + 8);
+    }
+  };
+
+  const int ntiles = (a.n + TILE - 1) / TILE;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int p = tile * TILE + t;
+    const bool live = p < a.n;
+    float fv[NF];
+    if constexpr (SRC == 0) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) fv[f] = live ? a.feat[(long long)p * NF + f] : 0.0f;
+    } else {
+      const int j = live ? (int)(p / a.les.pp) : 0;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) fv[f] = 0.0f;
+      if (j >= 1) les_features_at<typename std::conditional<SRC == 1, float, double>::type>(
+                      a.les, j, p - (long long)j * a.les.pp, fv);
+    }
+    float x[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) x[f] = live ? (fv[f] - mu[f]) * isd[f] : 0.0f;
+    put8(sm + PL::H, t, 0, NF, x);       // X tile (K = 16) at the start of H
+    put8(sm + PL::H, t, 8, NF, x + 8);
+    to_tc();
+    if (t == 0) gemm(aH, NF * 16, aW1, NF * 16, NF);
+    if (!(ok = sync_mma())) break;
+    hidden_out(b1);
+    to_tc();
+    if (t == 0) gemm(aH, NH * 16, aW2, NH * 16, NH);
+    if (!(ok = sync_mma())) break;
+    hidden_out(b2);
+    to_tc();
+    if (t == 0) gemm(aH, NH * 16, aW3, NH * 16, NH);
+    if (!(ok = sync_mma())) break;
+    float y0 = b4[0], y1 = b4[1];
+#pragma unroll
+    for (int c = 0; c < NH; c += 32) {
+      float z0[16], z1[16];
+      tmem_ld16(trow + c, z0);
+      tmem_ld16(trow + c + 16, z1);
+      tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float h = gelu(z0[i] + b3[c + i]);
+        y0 += W4[c + i] * h;
+        y1 += W4[NH + c + i] * h;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float h = gelu(z1[i] + b3[c + 16 + i]);
+        y0 += W4[c + 16 + i] * h;
+        y1 += W4[NH + c + 16 + i] * h;
+      }
+    }
+    if (live) {
+      a.out[(long long)p * 2] = softplus(y0) * osc0;
+      a.out[(long long)p * 2 + 1] = softplus(y1) * osc1;
+    }
+  }
+  if (!ok && t == 0) atomicExch(a.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tbase, PL::TMEM_COLS);
+}
+
+// INF_CTAS_PER_SM resident CTAs per SM: shared memory (the 1.4 KB static
+// parameter block padded to the dynamic block's 1 KB alignment, the dynamic
+// block, and the 1 KB the SM reserves per CTA) within the SM's 228 KB;
+// registers by the launch bounds
+static_assert(INF_CTAS_PER_SM * (2048 + PlanInf::BYTES + 1024) <= 228 * 1024, "inference CTAs per SM");
+
+// one wave of resident CTAs, each looping over the tiles
+template <int SRC>
+static cudaError_t go_infer(const MlpArgs& a, cudaStream_t st) {
+  const int ntiles = (a.n + TILE - 1) / TILE;
+  if (ntiles == 0) return cudaSuccess;
+  cudaFuncSetAttribute(k_mlp_infer<SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PlanInf::BYTES);
+  const int cap = INF_CTAS_PER_SM * sm_count();
+  k_mlp_infer<SRC><<<ntiles < cap ? ntiles : cap, TILE, PlanInf::BYTES, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_les(const MlpArgs& a, bool fp32, cudaStream_t st) {
+  return fp32 ? go_infer<1>(a, st) : go_infer<2>(a, st);
+}
+
 __global__ void k_adam(float* params, float* grads, float* m1, float* m2, int n, float lr, float b1, float b2,
                        float eps, float c1, float c2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -501,15 +684,12 @@ cudaError_t launch_mlp(const MlpArgs& a, bool train, int max_ctas, cudaStream_t 
   if (ntiles == 0) return cudaSuccess;
   int ctas = ntiles < max_ctas ? ntiles : max_ctas;
   if (train) {
-    const size_t smem = Plan<true>::BYTES;
-    cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_mlp<true><<<ctas, TILE, smem, st>>>(a);
-  } else {
-    const size_t smem = Plan<false>::BYTES;
-    cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_mlp<false><<<ctas, TILE, smem, st>>>(a);
+    const size_t smem = PlanTrain::BYTES;
+    cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mlp_train<<<ctas, TILE, smem, st>>>(a);
+    return cudaGetLastError();
   }
-  return cudaGetLastError();
+  return go_infer<0>(a, st);
 }
 
 cudaError_t launch_adam(float* params, float* grads, float* m1, float* m2, int n, float lr, int step,
@@ -528,6 +708,6 @@ cudaError_t launch_umma_gemm(const uint16_t* A, const uint16_t* B, float* D, int
   return cudaGetLastError();
 }
 
-size_t mlp_smem_bytes(bool train) { return train ? Plan<true>::BYTES : Plan<false>::BYTES; }
+size_t mlp_smem_bytes(bool train) { return train ? PlanTrain::BYTES : PlanInf::BYTES; }
 
 }  // namespace db
