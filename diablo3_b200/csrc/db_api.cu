@@ -247,10 +247,10 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   s.u1 = ph_[0]; s.u2 = ph_[1]; s.u3 = ph_[2]; s.th = ph_[3];
   s.r1 = ph_[4]; s.r2 = ph_[5]; s.r3 = ph_[6]; s.rth = ph_[7];
   if (p->use_les) {
-    double** lf[19] = {&s.gx[0], &s.gx[1], &s.gx[2], &s.gx[3], &s.gz[0], &s.gz[1], &s.gz[2], &s.gz[3],
+    double** lf[21] = {&s.gx[0], &s.gx[1], &s.gx[2], &s.gx[3], &s.gz[0], &s.gz[1], &s.gz[2], &s.gz[3],
                        &s.les[0], &s.les[1], &s.les[2], &s.les[3], &s.les[4], &s.les[5], &s.les[6],
-                       &s.les[7], &s.les[8], &s.nu_t, &s.kappa_t};
-    for (int i = 0; i < 19; ++i)
+                       &s.les[7], &s.les[8], &s.les[9], &s.les[10], &s.nu_t, &s.kappa_t};
+    for (int i = 0; i < 21; ++i)
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.tscr, 8 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }

@@ -92,6 +92,23 @@ struct LesRow {
   double dys_y;            // 2 dy(j)   (GY-row y filter width)
 };
 
+__device__ __forceinline__ bool in_rng(int j, int a, int b) { return j >= a && j <= b; }
+
+// per-plane metric factors of the nonlinear products: 1 / (2 dyf_j),
+// 1 / dy_j, dyf_j / (2 dy_j), dyf_{j-1} / (2 dy_j) (the y-differences and GY
+// interpolations multiply by these instead of dividing per point)
+template <typename R>
+struct ProdY {
+  R i2dyf, idy, wj, wjm;
+  __device__ ProdY(const Geom& g, int j) {
+    const double dyj = g.dy[j], dyfj = g.dyf[j], dyfjm = (j >= 1) ? g.dyf[j - 1] : 0.0;
+    i2dyf = (R)(1.0 / (2.0 * dyfj));
+    idy = (R)(1.0 / dyj);
+    wj = (R)(dyfj / (2.0 * dyj));
+    wjm = (R)(dyfjm / (2.0 * dyj));
+  }
+};
+
 // row chunks of the tiled Thomas solve (k_thomas): nch <= THOMAS_MAXCH
 // chunks of len rows
 constexpr int THOMAS_MAXCH = 16;
@@ -124,7 +141,7 @@ struct State {
   // LES (les_model_type 5), physical [j][z][x]; null without use_les
   double* gx[4];                             // d/dx of u1, u2, u3, th
   double* gz[4];                             // d/dz of u1, u2, u3, th
-  double* les[9];                            // SGS forcing per product slot (k_les.cu)
+  double* les[11];                           // LES: the products' 11 real sequences + SGS forcing (k_les.cu)
   double *nu_t, *kappa_t;                    // eddy viscosity / diffusivity at GY rows
   double2* ghost;                            // [4 fields][rows 0, 1, Nyp, Nyp+1][sp] (k_les_bc)
   double* tscr;                              // FP64 Thomas scratch, two fields per equation (LES)

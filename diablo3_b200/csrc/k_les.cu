@@ -110,20 +110,31 @@ __device__ __forceinline__ double amd_delta(double dxs, double dzs, double h) {
   return -2.0 * C_AMD * C_AMD * 3.0 / (1.0 / (dxs * dxs) + 1.0 / ((h * 2.0) * (h * 2.0)) + 1.0 / (dzs * dzs));
 }
 
-// Outputs, physical [j][z][x], zero outside the rows where the reference
-// applies each term, in the product slots of k_products:
-//  les[0] = dyf-filter * s1 S11            (u1 eq., times i kx)      rows j1..j2
-//  les[1] = Dy(delta_y tau_12)             (u1 eq., no derivative)   rows j1..j2
-//  les[2] = dyf-filter * s1 S13            (u1: i kz, u3: i kx)      rows j1..j2
-//  les[3] = Dy(delta_y tau_23)             (u3 eq., no derivative)   rows j1..j2
-//  les[4] = dyf-filter * s1 S33            (u3 eq., times i kz)      rows j1..j2
-//  les[5] = delta_y tau_12 - nu_t du1/dy   (u2 eq., times i kx)      rows 2..Nyp
-//  les[6] = delta_y tau_23 - nu_t du3/dy   (u2 eq., times i kz)      rows 2..Nyp
-//  les[7] = dyf-filter/2 * s1_th dth/dx    (th eq., times i kx)      rows jst..jet
-//  les[8] = dyf-filter/2 * s1_th dth/dz    (th eq., times i kz)      rows jst..jet
+// SGS forcing terms, zero outside the rows where the reference applies each:
+//  L0 = dyf-filter * s1 S11            (u1 eq., times i kx)      rows j1..j2
+//  L1 = Dy(delta_y tau_12)             (u1 eq., no derivative)   rows j1..j2
+//  L2 = dyf-filter * s1 S13            (u1: i kz, u3: i kx)      rows j1..j2
+//  L3 = Dy(delta_y tau_23)             (u3 eq., no derivative)   rows j1..j2
+//  L4 = dyf-filter * s1 S33            (u3 eq., times i kz)      rows j1..j2
+//  L5 = delta_y tau_12 - nu_t du1/dy   (u2 eq., times i kx)      rows 2..Nyp
+//  L6 = delta_y tau_23 - nu_t du3/dy   (u2 eq., times i kz)      rows 2..Nyp
+//  L7 = dyf-filter/2 * s1_th dth/dx    (th eq., times i kx)      rows jst..jet
+//  L8 = dyf-filter/2 * s1_th dth/dz    (th eq., times i kz)      rows jst..jet
 // with j1 = jstart, j2 = Nyp - 1 (les.f90:46-49, one rank), tau_12 at GY
 // rows = temp (S12 - du1/dy / 2) for j >= 2 and the raw strain at j = 1
-// (les.f90:737-748).  R: arithmetic and storage type (FP32 on the mixed path).
+// (les.f90:737-748).  Each is added to the nonlinear product it shares a
+// derivative with, and the kernel stores the 11 real sequences of every
+// plane the LES products kernel transforms (physical [j][z][x], in the
+// products' (group, sequence, part) order, stored on the rows where that
+// kernel reads them; <.> the GY interpolation, Dy the conservative
+// y-difference):
+//  les[0] = u1 u1 + L0   les[1] = Dy(u1 u2) + L1   les[2] = u3 u1 + L2
+//  les[3] = Dy(u3 u2) + L3   les[4] = u3 u3 + L4                          rows jstart..jend
+//  les[5] = <u1> u2 + L5   les[6] = Dy(u2 u2)   les[9] = <u3> u2 + L6     rows 2..Nyp
+//  les[7] = th u1 + L7   les[8] = Dy(th u2)   les[10] = th u3 + L8        rows jst..jet
+// Plane r needs rows r - 1 .. r + 1, so it is formed with the GYF outputs of
+// row r, one iteration after row r + 1 arrived.  R: arithmetic and storage
+// type (FP32 on the mixed path).
 // MODE 0: AMD.  MODE 1: only the learned closure's 16 features at every GY
 // row (include/diablo_b200.h order) into s.sgs_feat[point][16].  MODE 2:
 // the closure's nu_t, kappa_t (s.sgs_out[point][2], at GY rows) take the
@@ -166,9 +177,9 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
           *gtx = (const R*)s.gx[3] + col;
   const R *g1z = (const R*)s.gz[0] + col, *g2z = (const R*)s.gz[1] + col, *g3z = (const R*)s.gz[2] + col,
           *gtz = (const R*)s.gz[3] + col;
-  R* o[9];
+  R* o[11];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) o[i] = (R*)s.les[i] + col;
+  for (int i = 0; i < 11; ++i) o[i] = (R*)s.les[i] + col;
   R* nut = (R*)s.nu_t + col;
   R* kat = (R*)s.kappa_t + col;
   float* fo = s.sgs_feat;
@@ -186,15 +197,16 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   R u1m = __ldg(u1 + o0), u3m = __ldg(u3 + o0), thm = __ldg(th + o0), u2c = __ldg(u2 + o0 + pp);
   R f1x = __ldg(g1x + o0), f3z = __ldg(g3z + o0), f1z = __ldg(g1z + o0), f3x = __ldg(g3x + o0);
   R ftx = __ldg(gtx + o0), ftz = __ldg(gtz + o0);
-  R f2y = (u2c - __ldg(u2 + o0)) * (R)LR[j0].idyf;
+  R u2m1 = __ldg(u2 + o0);
+  R f2y = (u2c - u2m1) * (R)LR[j0].idyf;
+  // rows j - 2 of u1, u3, th and u2 (the products of plane j - 1)
+  R u1mm = u1m, u3mm = u3m, thmm = thm, u2m2 = u2m1;
   // previous GY row (r = j - 1) values
   R h1y = 0, h3y = 0, hty = 0, h2x = 0, h2z = 0;
-  R hSI4 = 0, hSI6 = 0, hO4 = 0, hO6 = 0, hP4 = 0, hP6 = 0, hdl = 0;
+  R hSI4 = 0, hSI6 = 0, hO4 = 0, hO6 = 0, hP4 = 0, hP6 = 0, hdl = 0, hL5 = 0, hL6 = 0;
   if (MODE != 1 && ja == 1) {
     nut[0] = 0;
     kat[0] = 0;
-    o[5][0] = 0;
-    o[6][0] = 0;
   }
 
   // the 12 values a row needs come through a ring of AMD_SLOTS shared-memory
@@ -291,11 +303,11 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     const R P4 = (j >= 2) ? temp * (S4 - h * d1y) : S4;
     const R P6 = (j >= 2) ? temp * (S6 - h * d3y) : S6;
     const bool gy2 = (j >= 2 && j <= Nyp);
+    const R L5 = gy2 ? delt * P4 - nu * d1y : (R)0;
+    const R L6 = gy2 ? delt * P6 - nu * d3y : (R)0;
     if (keep) {
       nut[oj] = nu;
       kat[oj] = ka;
-      o[5][oj] = gy2 ? delt * P4 - nu * d1y : (R)0;
-      o[6][oj] = gy2 ? delt * P6 - nu * d3y : (R)0;
     }
 
     // GYF row r = j - 1: needs GY rows r and r + 1 = j
@@ -325,27 +337,38 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
         L7 = h * dlf * (s1t * ftx);
         L8 = h * dlf * (s1t * ftz);
       }
-      if (keep) {
-        o[0][orr] = L0;
-        o[1][orr] = L1;
-        o[2][orr] = L2;
-        o[3][orr] = L3;
-        o[4][orr] = L4;
-        o[7][orr] = L7;
-        o[8][orr] = L8;
+      // plane r: rows r - 1, r, r + 1 are u1mm, u1m, u1j (u3, th alike) and
+      // u2m2, u2m1, u2c (products as in k_products' prod_ab)
+      const bool q1 = in_rng(r, g.jstart, g.jend), q2 = in_rng(r, 2, Nyp), qt = in_rng(r, jst, jet);
+      if (keep && q1) {
+        const ProdY<R> y(g, r);
+        o[0][orr] = u1m * u1m + L0;
+        o[1][orr] = (u1j * u2c + u1m * u2c - u1m * u2m1 - u1mm * u2m1) * y.i2dyf + L1;
+        o[2][orr] = u3m * u1m + L2;
+        o[3][orr] = (u3j * u2c + u3m * u2c - u3m * u2m1 - u3mm * u2m1) * y.i2dyf + L3;
+        o[4][orr] = u3m * u3m + L4;
+      }
+      if (keep && (q2 || qt)) {
+        const ProdY<R> y(g, r);
+        const R qrt = 0.25;
+        const R sp = u2m1 + u2c, sm = u2m1 + u2m2;
+        o[5][orr] = q2 ? (y.wj * u1m + y.wjm * u1mm) * u2m1 + hL5 : (R)0;
+        o[6][orr] = q2 ? (qrt * (sp * sp) - qrt * (sm * sm)) * y.idy : (R)0;
+        o[7][orr] = qt ? thm * u1m + L7 : (R)0;
+        o[8][orr] = qt ? (thj * u2c + thm * u2c - thm * u2m1 - thmm * u2m1) * y.i2dyf : (R)0;
+        o[9][orr] = q2 ? (y.wj * u3m + y.wjm * u3mm) * u2m1 + hL6 : (R)0;
+        o[10][orr] = qt ? thm * u3m + L8 : (R)0;
       }
     }
     // shift
+    u1mm = u1m; u3mm = u3m; thmm = thm; u2m2 = u2m1; u2m1 = u2c;
+    hL5 = L5; hL6 = L6;
     u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
     f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
     h1y = d1y; h3y = d3y; hty = dty; h2x = a2x; h2z = a2z;
     hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
     hnu = nu_m; hka = ka_m; hval = val;
   }
-  if (MODE == 1 || jb != Nyp + 1) return;
-  const long long oe = (long long)(Nyp + 1) * pp;
-  o[0][oe] = 0; o[1][oe] = 0; o[2][oe] = 0; o[3][oe] = 0; o[4][oe] = 0;
-  o[7][oe] = 0; o[8][oe] = 0;
 }
 
 // ---------------------------------------------------------------------------

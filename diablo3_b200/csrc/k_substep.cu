@@ -30,8 +30,6 @@
 namespace db {
 
 
-__device__ __forceinline__ bool in_rng(int j, int a, int b) { return j >= a && j <= b; }
-
 // ---------------------------------------------------------------------------
 // nonlinear products + forward x-FFT.  One CTA per (z, j) row and group; each
 // complex sequence carries two real products a + i b:
@@ -60,25 +58,11 @@ struct ProdRows {
   const R *u1m, *u1, *u1p, *u2m, *u2, *u2p, *u3m, *u3, *u3p, *thm, *th, *thp;
 };
 
-// per-plane metric factors: 1 / (2 dyf_j), 1 / dy_j, dyf_j / (2 dy_j),
-// dyf_{j-1} / (2 dy_j) (the y-differences and GY interpolations below
-// multiply by these instead of dividing per point)
-template <typename R>
-struct ProdY {
-  R i2dyf, idy, wj, wjm;
-  __device__ ProdY(const Geom& g, int j) {
-    const double dyj = g.dy[j], dyfj = g.dyf[j], dyfjm = (j >= 1) ? g.dyf[j - 1] : 0.0;
-    i2dyf = (R)(1.0 / (2.0 * dyfj));
-    idy = (R)(1.0 / dyj);
-    wj = (R)(dyfj / (2.0 * dyj));
-    wjm = (R)(dyfjm / (2.0 * dyj));
-  }
-};
-
 // the real pair (a, b) sequence `seq` of group `grp` carries at point x
-template <bool LES, typename R>
-__device__ __forceinline__ void prod_ab(const ProdRows<R>& P, const R* const* LS, long long o0, int grp, int seq, int x,
-                                        bool r2, bool rt, const ProdY<R>& y, R& a, R& b) {
+// (the LES substep forms the same products in k_les.cu's column walk)
+template <typename R>
+__device__ __forceinline__ void prod_ab(const ProdRows<R>& P, int grp, int seq, int x, bool r2, bool rt,
+                                        const ProdY<R>& y, R& a, R& b) {
   const R qrt = 0.25;
   a = 0;
   b = 0;
@@ -89,16 +73,13 @@ __device__ __forceinline__ void prod_ab(const ProdRows<R>& P, const R* const* LS
       const R u2p = P.u2p[x], u2 = P.u2[x];
       a = u1 * u1;
       b = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) * y.i2dyf;
-      if (LES) { a += __ldg(LS[0] + o0 + x); b += __ldg(LS[1] + o0 + x); }
     } else if (seq == 1) {
       const R u3p = P.u3p[x], u3m = P.u3m[x];
       const R u2p = P.u2p[x], u2 = P.u2[x];
       a = u3 * u1;
       b = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) * y.i2dyf;
-      if (LES) { a += __ldg(LS[2] + o0 + x); b += __ldg(LS[3] + o0 + x); }
     } else {
       a = u3 * u3;
-      if (LES) a += __ldg(LS[4] + o0 + x);
     }
   } else {
     const R u2 = P.u2[x];
@@ -108,7 +89,6 @@ __device__ __forceinline__ void prod_ab(const ProdRows<R>& P, const R* const* LS
         const R pp = u2 + P.u2p[x], qq = u2 + P.u2m[x];
         a = (y.wj * u1 + y.wjm * u1m) * u2;
         b = (qrt * (pp * pp) - qrt * (qq * qq)) * y.idy;
-        if (LES) a += __ldg(LS[5] + o0 + x);
       }
     } else if (seq == 1) {
       if (rt) {
@@ -116,15 +96,10 @@ __device__ __forceinline__ void prod_ab(const ProdRows<R>& P, const R* const* LS
         const R u2p = P.u2p[x];
         a = th * P.u1[x];
         b = (thp * u2p + th * u2p - th * u2 - thm * u2) * y.i2dyf;
-        if (LES) a += __ldg(LS[7] + o0 + x);
       }
     } else {
       if (r2) a = (y.wj * P.u3[x] + y.wjm * P.u3m[x]) * u2;
       if (rt) b = P.th[x] * P.u3[x];
-      if (LES) {
-        if (r2) a += __ldg(LS[6] + o0 + x);
-        if (rt) b += __ldg(LS[8] + o0 + x);
-      }
     }
   }
 }
@@ -159,7 +134,7 @@ __device__ __forceinline__ void prod_out(C* const* xh, const C* sq, const Geom& 
 }
 
 // One CTA per (z, j, group), rows read from global memory (Nx > 512).
-template <int N, bool LES, typename R>
+template <int N, typename R>
 __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(const __grid_constant__ State s, Geom g) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -180,7 +155,6 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(con
   }
   C* sq = sm + seq * padded(N);
   const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
-  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
   const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
   const long long om = o0 - g.pp, op = o0 + g.pp;
   const R* U1 = (const R*)s.u1;
@@ -194,7 +168,7 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(con
 #pragma unroll
   for (int q = 0; q < E; ++q) {
     R a, b;
-    prod_ab<LES>(P, LS, o0, grp, seq, lane + q * T, r2, rt, y, a, b);
+    prod_ab(P, grp, seq, lane + q * T, r2, rt, y, a, b);
     v[q] = mkc<C>(a, b);
   }
   fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
@@ -217,7 +191,7 @@ constexpr uint32_t PROD_WAIT = 1u << 24;
 template <int N>
 constexpr int prod_zr() { return FftShape<N>::T >= 64 ? 1 : 64 / FftShape<N>::T; }
 
-template <int N, bool LES, typename R>
+template <int N, typename R>
 __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ State s, Geom g, int zr, int nzb,
                                                         int jlen, int nitems) {
   using C = typename CplxOf<R>::type;
@@ -233,7 +207,6 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
   const int zi = sidx / 3, seq = sidx % 3;
   C* sq = xbuf + sidx * padded(N);
   const C* twt = tw_x<R>(g);
-  const R* const* LS = reinterpret_cast<const R* const*>(s.les);
   C* const* xh = reinterpret_cast<C* const*>(s.xh);
   const int np = g.np;
   if (threadIdx.x < PROD_SLOTS) mbar_init(&mbar[threadIdx.x], 1);
@@ -308,7 +281,7 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
 #pragma unroll
         for (int q = 0; q < E; ++q) {
           R a, b;
-          prod_ab<LES>(P, LS, o0, grp, seq, lane + q * T, r2, rt, y, a, b);
+          prod_ab(P, grp, seq, lane + q * T, r2, rt, y, a, b);
           v[q] = mkc<C>(a, b);
         }
         fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
@@ -321,6 +294,52 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
       }
     }
   }
+}
+
+// LES substep form: the 11 real sequences of each plane come ready from the
+// closure's column walk (product + SGS forcing, k_les.cu, les[0..10] in
+// (group, sequence, part) order), so a CTA of zr z rows of one plane and one
+// group loads its pairs, transforms and separates; no neighbouring planes.
+template <int N, typename R>
+__global__ void __launch_bounds__(3 * FftShape<N>::T * prod_zr<N>()) k_products_les(const __grid_constant__ State s,
+                                                                                    Geom g, int zr) {
+  using C = typename CplxOf<R>::type;
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int sidx = threadIdx.x / T, lane = threadIdx.x % T;
+  const int zi = sidx / 3, seq = sidx % 3;
+  const int z0 = blockIdx.x * zr, z = z0 + zi, j = blockIdx.y, grp = blockIdx.z;
+  const bool r1 = in_rng(j, g.jstart, g.jend);
+  const bool r2 = in_rng(j, 2, g.ny);
+  const bool rt = in_rng(j, g.jstart_th, g.jend_th);
+  C* const* xh = reinterpret_cast<C* const*>(s.xh);
+  if ((grp == 0 && !r1) || (grp == 1 && !(r2 || rt))) {   // uniform over the CTA
+    const long long hrow0 = (long long)j * g.hp + (long long)z0 * g.kxs;
+    const int w = zr * g.kxs;
+    for (int idx = threadIdx.x; idx < 4 * w; idx += blockDim.x)
+      xh[4 * grp + idx / w][hrow0 + idx % w] = mkc<C>(0, 0);
+    return;
+  }
+  C* sq = reinterpret_cast<C*>(sm_raw) + sidx * padded(N);
+  const C* twt = tw_x<R>(g);
+  const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
+  const int ia = grp == 0 ? 2 * seq : 5 + 2 * seq;   // fields of parts a, b (group 0 sequence 2: b = 0)
+  const bool hasb = !(grp == 0 && seq == 2);
+  const R* A = (const R*)s.les[ia] + o0;
+  const R* B = (const R*)s.les[hasb ? ia + 1 : ia] + o0;
+  C v[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const int x = lane + q * T;
+    v[q] = mkc<C>(A[x], hasb ? B[x] : (R)0);
+  }
+  fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
+  SEQ_SYNC(N);
+#pragma unroll
+  for (int q = 0; q < E; ++q) sq[pidx(lane + q * T)] = v[q];
+  SEQ_SYNC(N);
+  prod_out<N>(xh, sq, g, (long long)j * g.hp + (long long)z * g.kxs, grp, seq, lane, r2, rt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1122,7 +1141,7 @@ __global__ void k_bc_vel_post(const __grid_constant__ State s, Geom g, Phys ph) 
 // ---------------------------------------------------------------------------
 // launchers
 
-template <int N, bool LES, typename R>
+template <int N, typename R>
 static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   if constexpr (N <= 512) {
@@ -1130,7 +1149,7 @@ static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
     const size_t smem = (size_t)PROD_SLOTS * 4 * zr * N * sizeof(R) + (size_t)3 * zr * padded(N) * sizeof(C) +
                         PROD_SLOTS * sizeof(uint64_t);
     if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_products_st<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_products_st<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int nzb = g.nz / zr;
     const int gmax = (g.tune_pgrid > 0 ? g.tune_pgrid : 2) * sm_count();
     // plane ranges: about four items per CTA, at least four planes each
@@ -1140,19 +1159,28 @@ static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
     nch = (g.np + jlen - 1) / jlen;
     const int nitems = nzb * nch;
     const int grid = nitems < gmax ? nitems : gmax;
-    k_products_st<N, LES, R><<<grid, 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr, nzb, jlen, nitems);
+    k_products_st<N, R><<<grid, 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr, nzb, jlen, nitems);
   } else {
     const size_t smem = (size_t)3 * padded(N) * sizeof(C);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, LES, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<N, LES, R><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<N, R><<<dim3(g.nz, g.np, 2), 3 * FftShape<N>::T, smem, st>>>(s, g);
   }
+}
+template <int N, typename R>
+static void go_products_les_t(const Geom& g, const State& s, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int zr = prod_zr<N>() < g.nz ? prod_zr<N>() : g.nz;
+  const size_t smem = (size_t)3 * zr * padded(N) * sizeof(C);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_products_les<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_products_les<N, R><<<dim3(g.nz / zr, g.np, 2), 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr);
 }
 template <int N>
 static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les) {
-  if (g.prec) {
-    if (les) go_products_t<N, true, float>(g, s, st); else go_products_t<N, false, float>(g, s, st);
+  if (les) {
+    if (g.prec) go_products_les_t<N, float>(g, s, st); else go_products_les_t<N, double>(g, s, st);
   } else {
-    if (les) go_products_t<N, true, double>(g, s, st); else go_products_t<N, false, double>(g, s, st);
+    if (g.prec) go_products_t<N, float>(g, s, st); else go_products_t<N, double>(g, s, st);
   }
 }
 template <int N, typename R>
