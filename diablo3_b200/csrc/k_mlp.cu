@@ -433,6 +433,52 @@ struct PlanInf {
   static constexpr uint32_t TMEM_COLS = 64;
 };
 constexpr int INF_CTAS_PER_SM = 6;
+
+// biases, output weights interleaved per hidden unit, feature normalisation
+struct __align__(16) InfConst {
+  float b[3][NH];
+  float2 w4[NH];   // (W4[0][i], W4[1][i])
+  float b4[4];     // b4[0..1], padding
+  float mu[NF], isd[NF];
+};
+
+// packed FP32 pair arithmetic (the f32x2 instructions of sm_100): one
+// instruction rounds each lane exactly like its scalar form
+__device__ __forceinline__ uint64_t f2(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2split(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// gelu of two pre-activations z + c (the tanh form of gelu(), two lanes at
+// a time: x = z + c, u = K x (1 + C x^2), h = x/2 + x/2 tanh(u))
+__device__ __forceinline__ void gelu_pair(float z0, float z1, float c0, float c1, float& h0, float& h1) {
+  const uint64_t x = add2(f2(z0, z1), f2(c0, c1));
+  const uint64_t w = fma2(mul2(x, x), f2(GELU_C, GELU_C), f2(1.0f, 1.0f));
+  const uint64_t u = mul2(mul2(x, f2(GELU_K, GELU_K)), w);
+  float u0, u1;
+  f2split(u, u0, u1);
+  const uint64_t hx = mul2(x, f2(0.5f, 0.5f));
+  const uint64_t hh = fma2(hx, f2(tanh_hw(u0), tanh_hw(u1)), hx);
+  f2split(hh, h0, h1);
+}
 static_assert(INF_CTAS_PER_SM * PlanInf::TMEM_COLS <= 512, "tensor memory of the resident CTAs");
 
 template <int SRC>
@@ -456,15 +502,18 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
       put8(sm + PL::W3, r, k0, NH, v);
     }
   }
-  __shared__ float sb[3 * NH + NO + NO * NH + 2 * NF];   // b1 b2 b3 b4 W4 mean 1/std (FP32)
+  __shared__ InfConst cs;
   for (int i = t; i < NH; i += TILE) {
-    sb[i] = P[P_B1 + i];
-    sb[NH + i] = P[P_B2 + i];
-    sb[2 * NH + i] = P[P_B3 + i];
+    cs.b[0][i] = P[P_B1 + i];
+    cs.b[1][i] = P[P_B2 + i];
+    cs.b[2][i] = P[P_B3 + i];
+    cs.w4[i] = make_float2(P[P_W4 + i], P[P_W4 + NH + i]);
   }
-  for (int i = t; i < NO * NH; i += TILE) sb[3 * NH + NO + i] = P[P_W4 + i];
-  if (t < NO) sb[3 * NH + t] = P[P_B4 + t];
-  if (t < 2 * NF) sb[3 * NH + NO + NO * NH + t] = a.norm[t];
+  if (t < NO) cs.b4[t] = P[P_B4 + t];
+  if (t < NF) {
+    cs.mu[t] = a.norm[t];
+    cs.isd[t] = a.norm[NF + t];
+  }
   if (t == 0) mbar_init(mbar, 1);
   if (warp == 0) {
     tmem_alloc(slot, PL::TMEM_COLS);
@@ -476,13 +525,6 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
   tc_fence_after();
   const uint32_t tbase = *slot;
   const uint32_t trow = tbase + ((uint32_t)(warp * 32) << 16);
-  const float* b1 = sb;
-  const float* b2 = sb + NH;
-  const float* b3 = sb + 2 * NH;
-  const float* b4 = sb + 3 * NH;
-  const float* W4 = sb + 3 * NH + NO;
-  const float* mu = sb + 3 * NH + NO + NO * NH;
-  const float* isd = mu + NF;
   const float osc0 = a.norm[2 * NF], osc1 = a.norm[2 * NF + 1];
   const uint32_t id64 = umma_idesc_bf16(128, NH);
   const uint32_t aH = smem_u32(sm + PL::H);
@@ -509,6 +551,15 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
     tc_fence_after();
     return __syncthreads_and(w ? 1 : 0) != 0;
   };
+  // gelu(z + bias) of 16 columns from c, bias read four at a time
+  auto gelu16 = [&](const float (&z)[16], const float* bias, float (&h)[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; i += 4) {
+      const float4 b = *reinterpret_cast<const float4*>(bias + i);
+      gelu_pair(z[i], z[i + 1], b.x, b.y, h[i], h[i + 1]);
+      gelu_pair(z[i + 2], z[i + 3], b.z, b.w, h[i + 2], h[i + 3]);
+    }
+  };
   auto hidden_out = [&](const float* bias) {
 #pragma unroll
     for (int c = 0; c < NH; c += 32) {
@@ -517,12 +568,10 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
       tmem_ld16(trow + c + 16, z1);
       tmem_wait_ld();
       float h[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) h[i] = gelu(z0[i] + bias[c + i]);
+      gelu16(z0, bias + c, h);
       put8(sm + PL::H, t, c, NH, h);
       put8(sm + PL::H, t, c + 8, NH, h + 8);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) h[i] = gelu(z1[i] + bias[c + 16 + i]);
+      gelu16(z1, bias + c + 16, h);
       put8(sm + PL::H, t, c + 16, NH, h);
       put8(sm + PL::H, t, c + 24, NH, h + 8);
     }
@@ -545,40 +594,46 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
     }
     float x[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) x[f] = live ? (fv[f] - mu[f]) * isd[f] : 0.0f;
+    for (int f = 0; f < NF; ++f) x[f] = live ? (fv[f] - cs.mu[f]) * cs.isd[f] : 0.0f;
     put8(sm + PL::H, t, 0, NF, x);       // X tile (K = 16) at the start of H
     put8(sm + PL::H, t, 8, NF, x + 8);
     to_tc();
     if (t == 0) gemm(aH, NF * 16, aW1, NF * 16, NF);
     if (!(ok = sync_mma())) break;
-    hidden_out(b1);
+    hidden_out(cs.b[0]);
     to_tc();
     if (t == 0) gemm(aH, NH * 16, aW2, NH * 16, NH);
     if (!(ok = sync_mma())) break;
-    hidden_out(b2);
+    hidden_out(cs.b[1]);
     to_tc();
     if (t == 0) gemm(aH, NH * 16, aW3, NH * 16, NH);
     if (!(ok = sync_mma())) break;
-    float y0 = b4[0], y1 = b4[1];
+    // output layer: (y0, y1) += (W4[0][i], W4[1][i]) h_i in order of i
+    uint64_t y = f2(cs.b4[0], cs.b4[1]);
 #pragma unroll
     for (int c = 0; c < NH; c += 32) {
       float z0[16], z1[16];
       tmem_ld16(trow + c, z0);
       tmem_ld16(trow + c + 16, z1);
       tmem_wait_ld();
+      float h[16];
+      gelu16(z0, cs.b[2] + c, h);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float h = gelu(z0[i] + b3[c + i]);
-        y0 += W4[c + i] * h;
-        y1 += W4[NH + c + i] * h;
+      for (int i = 0; i < 16; i += 2) {
+        const float4 w = *reinterpret_cast<const float4*>(&cs.w4[c + i]);
+        y = fma2(f2(w.x, w.y), f2(h[i], h[i]), y);
+        y = fma2(f2(w.z, w.w), f2(h[i + 1], h[i + 1]), y);
       }
+      gelu16(z1, cs.b[2] + c + 16, h);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float h = gelu(z1[i] + b3[c + 16 + i]);
-        y0 += W4[c + 16 + i] * h;
-        y1 += W4[NH + c + 16 + i] * h;
+      for (int i = 0; i < 16; i += 2) {
+        const float4 w = *reinterpret_cast<const float4*>(&cs.w4[c + 16 + i]);
+        y = fma2(f2(w.x, w.y), f2(h[i], h[i]), y);
+        y = fma2(f2(w.z, w.w), f2(h[i + 1], h[i + 1]), y);
       }
     }
+    float y0, y1;
+    f2split(y, y0, y1);
     if (live) {
       a.out[(long long)p * 2] = softplus(y0) * osc0;
       a.out[(long long)p * 2 + 1] = softplus(y1) * osc1;
@@ -590,10 +645,11 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
   if (warp == 0) tmem_free(tbase, PL::TMEM_COLS);
 }
 
-// INF_CTAS_PER_SM resident CTAs per SM: shared memory (the 1.4 KB static
-// parameter block padded to the dynamic block's 1 KB alignment, the dynamic
+// INF_CTAS_PER_SM resident CTAs per SM: shared memory (the static
+// parameter block, InfConst, padded to the dynamic block's 1 KB alignment, the dynamic
 // block, and the 1 KB the SM reserves per CTA) within the SM's 228 KB;
 // registers by the launch bounds
+static_assert(sizeof(InfConst) <= 2048, "parameter block");
 static_assert(INF_CTAS_PER_SM * (2048 + PlanInf::BYTES + 1024) <= 228 * 1024, "inference CTAs per SM");
 
 // one wave of resident CTAs, each looping over the tiles
