@@ -687,17 +687,19 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
   if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
   mark(c, rk, 5);
-  // implicit CN solves (solver.f90:1012-1233)
+  // implicit CN solves (solver.f90:1012-1233); the mixed path's solves
+  // store the new physical u only where the CFL below reads it
+  const bool cfl_step = rk == 2 && c->p.variable_dt;
   if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
   if (c->p.use_les) {   // eddy terms whether or not the model ran this step
-    if ((e = launch_thomas_les(g, s, rk, st))) return e;
+    if ((e = launch_thomas_les(g, s, rk, st, cfl_step))) return e;
   } else {
-    if ((e = launch_thomas(g, s, st))) return e;
+    if ((e = launch_thomas(g, s, st, cfl_step))) return e;
   }
   mark(c, rk, 6);
   n += 7;
   // CFL on the last substep (solver.f90:1241-1244)
-  if (rk == 2 && c->p.variable_dt) {
+  if (cfl_step) {
     CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
     if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
     n += 2;
@@ -993,7 +995,7 @@ extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
     int bt = 0;
     for (int tb = 32; tb <= 128; tb *= 2) {   // kernel bound: 128 threads
       g.tune_les_tb = tb;
-      const float ms = time_ms(c, [&] { launch_thomas_les(g, s, 0, c->st); });
+      const float ms = time_ms(c, [&] { launch_thomas_les(g, s, 0, c->st, true); });
       if (cudaGetLastError() != cudaSuccess) continue;
       snprintf(buf, sizeof buf, "LES Thomas threads/CTA %d: %.3f ms\n", tb, ms);
       rep += buf;

@@ -160,7 +160,9 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
                              const double2* ghost = nullptr);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
-cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st);
+// keep_u: also store the new physical u on the mixed path (the CFL of the
+// third substep reads it); the FP64 path always stores it
+cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st, bool keep_u);
 
 struct CflCtl {
   double cfl, time_limit;
@@ -184,6 +186,6 @@ cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cu
 cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
 // mode 0: AMD; 1: closure features only; 2: closure nu_t, kappa_t with AMD fallback
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode = 0);
-cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st);
+cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st, bool keep_u);
 
 }  // namespace db

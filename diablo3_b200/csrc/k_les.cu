@@ -379,11 +379,12 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
 // to an FP64 scratch (2 fields per equation) and come back in the backward
 // sweep.  Rows are handled in batches of TB whose loads are all issued
 // first, so each thread keeps 3 TB loads in flight instead of waiting on
-// every row.
+// every row.  On the mixed path r receives the increment and u itself is
+// written only when keep_u (the third substep's CFL reads it).
 constexpr int TB = 8;
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ State s, Geom g, int rk) {
+__global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ State s, Geom g, int rk, int keep_u) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, eq = blockIdx.z;
   if (x >= g.nx) return;
   const int np = g.np, Nyp = g.ny;
@@ -457,7 +458,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
         if (j < 0) break;
         const double xv = xg[c] - xc[c] * xnext;
         const bool stored = (j >= lo && j <= hi);
-        if (stored) u[(long long)j * pp] = (R)xv;
+        if (stored && (!INC || keep_u)) u[(long long)j * pp] = (R)xv;
         if (INC) r[(long long)j * pp] = stored ? (R)(xv - xo[c]) : (R)0;   // increment for the transform
         xnext = xv;
       }
@@ -493,11 +494,11 @@ cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaSt
   }
   return cudaGetLastError();
 }
-cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st) {
+cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st, bool keep_u) {
   const int want = (g.tune_les_tb > 0 && g.tune_les_tb <= 128) ? g.tune_les_tb : 128;   // powers of two
   const int bx = g.nx < want ? g.nx : want;
-  if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk);
-  else k_thomas_les<double><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk);
+  if (g.prec) k_thomas_les<float><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk, keep_u ? 1 : 0);
+  else k_thomas_les<double><<<dim3(g.nx / bx, g.nz, 4), bx, 0, st>>>(s, g, rk, 1);
   return cudaGetLastError();
 }
 

@@ -714,12 +714,13 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // issues for all rows of its chunk at once (no registers held for loads,
 // the whole equation in flight); the staged old u also gives the mixed
 // path its increment.  HBM sees r and u read once and u written once per
-// equation (plus the increment r on the mixed path).
+// equation (plus the increment r on the mixed path, where u itself is
+// written only when keep_u: the third substep's CFL reads it, nothing else).
 constexpr int TX = 16;
 
 
 template <typename R>
-__global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g) {
+__global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g, int keep_u) {
   extern __shared__ __align__(16) unsigned char th_raw[];
   constexpr bool F64 = sizeof(R) == sizeof(double);
   constexpr bool INC = !F64;   // FP32 work type: r holds the increment over u (k_zpass_rhs)
@@ -815,7 +816,7 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
         for (int j = j0; j <= j1; ++j) {
           const double xv = tile[j * TX + cl] + Gm * Rw[j].qa + X * Rw[j].pm;
           const bool st = (j >= lo && j <= hi);
-          if (st) u[(long long)j * pp + col] = (R)xv;
+          if (st && (!INC || keep_u)) u[(long long)j * pp + col] = (R)xv;
           if (INC) r[(long long)j * pp + col] = st ? (R)(xv - (double)us[j * TX + cl]) : (R)0;
         }
       }
@@ -1234,7 +1235,7 @@ cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int r
   k_tri_coef<<<4, 256, smem, st>>>(g, ph, s.tri, s.sc, rk);
   return cudaGetLastError();
 }
-cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
+cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st, bool keep_u) {
   if (!g.prec) {   // FP64: one thread per column (measured faster than the tile solve there)
     const int bx = g.nx < 128 ? g.nx : 128;
     k_thomas_col<<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g);
@@ -1243,7 +1244,7 @@ cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st) {
   // FP32 work type: the tile solve; y/z tile (FP64) + staged r and u (FP32)
   const size_t smem = (size_t)g.np * TX * (sizeof(double) + 2 * sizeof(float));
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g);
+  k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g, keep_u ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
