@@ -458,9 +458,11 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         saved = ch.download_state()
+        for f in L.STATE_FIELDS:   # the first step's inputs, in the pinned buffers too
+            host[f][...] = saved[f]
         e0.record(stream)
         for _ in range(ke):
-            ch.upload_state(saved if _ == 0 else host)
+            ch.upload_state(host)
             ch.step(1)
             for f in L.STATE_FIELDS:
                 ch._ck(ch.L.db_download_field(ch.h, f, L.dptr(host[f].view(np.float64).reshape(-1))))

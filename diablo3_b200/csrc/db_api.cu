@@ -481,12 +481,15 @@ static int upload_spec(db_ctx* c, int id, const double* ref) {
   } else {
     if (int rc = ensure_ref(c)) return rc;
     // only the retained modes cross PCIe (kx <= Nkx of the first 2 Nkz + 1
-    // rows of every plane); the rest of the reference array is never read
+    // rows of every plane), as one 3D copy; the rest of the reference array
+    // is never read
     const size_t pitch = (size_t)(c->p.nx / 2 + 1) * sizeof(double2);
-    const size_t plane = pitch * (c->p.nz + 2);
-    for (int j = 0; j < c->g.np; ++j)
-      CK(cudaMemcpy2DAsync((char*)c->d_ref + j * plane, pitch, (const char*)ref + j * plane, pitch,
-                           (size_t)(c->g.nkx + 1) * sizeof(double2), c->g.nkzp, cudaMemcpyHostToDevice, c->st));
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<double*>(ref), pitch, (size_t)(c->p.nx / 2 + 1), (size_t)(c->p.nz + 2));
+    cp.dstPtr = make_cudaPitchedPtr(c->d_ref, pitch, (size_t)(c->p.nx / 2 + 1), (size_t)(c->p.nz + 2));
+    cp.extent = make_cudaExtent((size_t)(c->g.nkx + 1) * sizeof(double2), (size_t)c->g.nkzp, (size_t)c->g.np);
+    cp.kind = cudaMemcpyHostToDevice;
+    CK(cudaMemcpy3DAsync(&cp, c->st));
     CK(launch_ref_to_spec(c->g, c->p.nx, c->p.nz, c->d_ref, d, c->st));
   }
   CK(cudaStreamSynchronize(c->st));
