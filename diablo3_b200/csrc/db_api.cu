@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/diablo_b200.h"
@@ -472,6 +473,43 @@ static int ensure_ref(db_ctx* c) {
   return DB_OK;
 }
 
+// The retained block of a reference-layout array (kx <= Nkx of the first
+// 2 Nkz + 1 rows of every plane) between d_ref and a host array, as one 3D
+// copy on the context's stream.
+static cudaError_t copy_retained(const db_ctx* c, double* host, cudaMemcpyKind kind) {
+  const size_t nxh = (size_t)(c->p.nx / 2 + 1), rows = (size_t)(c->p.nz + 2), pitch = nxh * sizeof(double2);
+  cudaMemcpy3DParms cp = {};
+  cudaPitchedPtr h = make_cudaPitchedPtr(host, pitch, nxh, rows);
+  cudaPitchedPtr d = make_cudaPitchedPtr(c->d_ref, pitch, nxh, rows);
+  cp.srcPtr = kind == cudaMemcpyHostToDevice ? h : d;
+  cp.dstPtr = kind == cudaMemcpyHostToDevice ? d : h;
+  cp.extent = make_cudaExtent((size_t)(c->g.nkx + 1) * sizeof(double2), (size_t)c->g.nkzp, (size_t)c->g.np);
+  cp.kind = kind;
+  return cudaMemcpy3DAsync(&cp, c->st);
+}
+
+// Zero everything of a reference-layout host array outside the retained
+// block (the reference keeps those entries zero), planes split over host
+// threads.
+static void zero_ref_padding(const db_ctx* c, double* host) {
+  const size_t nxh = (size_t)(c->p.nx / 2 + 1), rows = (size_t)(c->p.nz + 2);
+  const size_t keep = (size_t)(c->g.nkx + 1), krows = (size_t)c->g.nkzp, plane = nxh * rows;
+  const int np = c->g.np;
+  auto work = [=](int j0, int j1) {
+    for (int j = j0; j < j1; ++j) {
+      double2* pl = reinterpret_cast<double2*>(host) + (size_t)j * plane;
+      for (size_t r = 0; r < krows; ++r) memset(pl + r * nxh + keep, 0, (nxh - keep) * sizeof(double2));
+      memset(pl + krows * nxh, 0, (rows - krows) * nxh * sizeof(double2));
+    }
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, np}));
+  std::vector<std::thread> th;
+  for (int k = 1; k < nt; ++k) th.emplace_back(work, (int)((long long)np * k / nt), (int)((long long)np * (k + 1) / nt));
+  work(0, (int)((long long)np / nt));
+  for (auto& t : th) t.join();
+}
+
 static int upload_spec(db_ctx* c, int id, const double* ref) {
   double2* d = spec_field(c, id);
   if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
@@ -480,16 +518,9 @@ static int upload_spec(db_ctx* c, int id, const double* ref) {
     CK(cudaMemsetAsync(d, 0, n * sizeof(double2), c->st));
   } else {
     if (int rc = ensure_ref(c)) return rc;
-    // only the retained modes cross PCIe (kx <= Nkx of the first 2 Nkz + 1
-    // rows of every plane), as one 3D copy; the rest of the reference array
+    // only the retained modes cross PCIe; the rest of the reference array
     // is never read
-    const size_t pitch = (size_t)(c->p.nx / 2 + 1) * sizeof(double2);
-    cudaMemcpy3DParms cp = {};
-    cp.srcPtr = make_cudaPitchedPtr(const_cast<double*>(ref), pitch, (size_t)(c->p.nx / 2 + 1), (size_t)(c->p.nz + 2));
-    cp.dstPtr = make_cudaPitchedPtr(c->d_ref, pitch, (size_t)(c->p.nx / 2 + 1), (size_t)(c->p.nz + 2));
-    cp.extent = make_cudaExtent((size_t)(c->g.nkx + 1) * sizeof(double2), (size_t)c->g.nkzp, (size_t)c->g.np);
-    cp.kind = cudaMemcpyHostToDevice;
-    CK(cudaMemcpy3DAsync(&cp, c->st));
+    CK(copy_retained(c, const_cast<double*>(ref), cudaMemcpyHostToDevice));
     CK(launch_ref_to_spec(c->g, c->p.nx, c->p.nz, c->d_ref, d, c->st));
   }
   CK(cudaStreamSynchronize(c->st));
@@ -501,8 +532,11 @@ static int download_spec(db_ctx* c, int id, double* ref) {
   if (!d) return fail(c, DB_ERR_ARG, "bad spectral field id");
   if (!ref) return DB_OK;
   if (int rc = ensure_ref(c)) return rc;
+  // only the retained modes cross PCIe; the host threads write the zero
+  // padding while the copy runs (disjoint parts of the array)
   CK(launch_spec_to_ref(c->g, c->p.nx, c->p.nz, d, c->d_ref, c->st));
-  CK(cudaMemcpyAsync(ref, c->d_ref, ref_spec_bytes(c), cudaMemcpyDeviceToHost, c->st));
+  CK(copy_retained(c, ref, cudaMemcpyDeviceToHost));
+  zero_ref_padding(c, ref);
   CK(cudaStreamSynchronize(c->st));
   return DB_OK;
 }

@@ -70,14 +70,12 @@ def substep_bytes(p) -> float:
 
 def state_transfer_bytes(p) -> tuple:
     """Bytes one db_upload_state and nine db_download_field move over PCIe,
-    (host to device, device to host).  Upload: the retained modes of each
+    (host to device, device to host): both ways the retained modes of each
     reference-layout array (kx <= Nkx of the first 2 Nkz + 1 rows of every
-    plane); download: the whole reference-layout arrays (their zero padding
-    included)."""
+    plane); the download writes the zero padding on the host."""
     nplanes = p.ny + 2
     h2d = 9 * nplanes * (2 * (p.nz // 3) + 1) * (p.nx // 3 + 1) * 16
-    d2h = 9 * nplanes * (p.nz + 2) * (p.nx // 2 + 1) * 16
-    return h2d, d2h
+    return h2d, h2d
 
 
 def profiled_traffic(stage: str, root: str, precision: str = "fp64"):
