@@ -181,18 +181,29 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(con
 
 // Persistent y-marching form (Nx <= 512).  A work item is a block of zr
 // consecutive z rows and a range of planes j; the CTA walks the planes in
-// order, keeping the rows j-1, j, j+1 of u1, u2, u3, th in a ring of four
-// shared-memory slots.  While plane j is transformed, a TMA bulk copy brings
-// plane j+2 into the slot plane j-2 occupied, so the loads overlap the
-// FFTs.  Thread layout: sequence (zi, seq) = (sidx / 3, sidx % 3).
-constexpr int PROD_SLOTS = 4;
+// order, keeping the rows j-1, j, j+1 of u1, u2, u3, th in a ring of
+// shared-memory slots filled by TMA bulk copies that overlap the FFTs.
+//  FP64: four slots; at the start of plane j, plane j+2 goes into the slot
+//        plane j-2 occupied.  Two CTAs per SM (the registers of the FP64
+//        transform).
+//  FP32: three slots; once both groups have read plane j-1 (a CTA barrier
+//        after the second group's products), plane j+2 goes into its slot,
+//        overlapping the second group's FFT and the next plane's first
+//        group.  With an exchange stride of padded(N) - 1 a CTA holds
+//        < 76 KB of shared memory, and three CTAs share an SM.
+// Thread layout: sequence (zi, seq) = (sidx / 3, sidx % 3).
+template <typename R>
+constexpr int prod_slots() { return sizeof(R) == sizeof(double) ? 4 : 3; }
 constexpr uint32_t PROD_WAIT = 1u << 24;
 
 template <int N>
 constexpr int prod_zr() { return FftShape<N>::T >= 64 ? 1 : 64 / FftShape<N>::T; }
+// exchange-buffer stride of one sequence: the largest index pidx(N - 1) + 1
+template <int N>
+constexpr int prod_sq() { return padded(N) - 1; }
 
 template <int N, typename R>
-__global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ State s, Geom g, int zr, int nzb,
+__global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_st(const __grid_constant__ State s, Geom g, int zr, int nzb,
                                                         int jlen, int nitems) {
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
@@ -200,12 +211,13 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const uint32_t fbytes = (uint32_t)zr * N * sizeof(R);   // one field, zr rows of one plane
   const uint32_t slot_bytes = 4u * fbytes;
+  constexpr int SQ = prod_sq<N>();
+  constexpr int PROD_SLOTS = prod_slots<R>();
   C* xbuf = reinterpret_cast<C*>(sm_raw + PROD_SLOTS * slot_bytes);
-  uint64_t* mbar =
-      reinterpret_cast<uint64_t*>(sm_raw + PROD_SLOTS * slot_bytes + (size_t)3 * zr * padded(N) * sizeof(C));
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm_raw + PROD_SLOTS * slot_bytes + (size_t)3 * zr * SQ * sizeof(C));
   const int sidx = threadIdx.x / T, lane = threadIdx.x % T;
   const int zi = sidx / 3, seq = sidx % 3;
-  C* sq = xbuf + sidx * padded(N);
+  C* sq = xbuf + sidx * SQ;
   const C* twt = tw_x<R>(g);
   C* const* xh = reinterpret_cast<C* const*>(s.xh);
   const int np = g.np;
@@ -214,7 +226,7 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
   uint32_t par = 0;    // parity of the next completion of each slot
   uint32_t pend = 0;   // slots with a copy issued and not yet waited for
   auto issue = [&](int jr, int z0) {   // plane jr of the four fields into its slot
-    const int sl = jr & (PROD_SLOTS - 1);
+    const int sl = jr % PROD_SLOTS;
     if (threadIdx.x == 0) {
       fence_async_smem();
       unsigned char* dst = sm_raw + sl * slot_bytes;
@@ -228,14 +240,14 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
     pend |= 1u << sl;
   };
   auto wait_row = [&](int jr) -> bool {
-    const int sl = jr & (PROD_SLOTS - 1);
+    const int sl = jr % PROD_SLOTS;
     const bool ok = mbar_wait(&mbar[sl], (par >> sl) & 1u, PROD_WAIT);
     par ^= 1u << sl;
     pend &= ~(1u << sl);
     return ok;
   };
   auto row = [&](int jr, int f) -> const R* {
-    return reinterpret_cast<const R*>(sm_raw + (jr & (PROD_SLOTS - 1)) * slot_bytes + f * fbytes) + zi * N;
+    return reinterpret_cast<const R*>(sm_raw + (jr % PROD_SLOTS) * slot_bytes + f * fbytes) + zi * N;
   };
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int zb = it % nzb, jc = it / nzb;
@@ -259,7 +271,7 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
         }
         return;
       }
-      if (j + 2 <= jtop) issue(j + 2, z0);   // into the slot of plane j - 2
+      if (PROD_SLOTS == 4 && j + 2 <= jtop) issue(j + 2, z0);   // into the slot of plane j - 2
       const bool r1 = in_rng(j, g.jstart, g.jend);
       const bool r2 = in_rng(j, 2, g.ny);
       const bool rt = in_rng(j, g.jstart_th, g.jend_th);
@@ -267,22 +279,29 @@ __global__ void __launch_bounds__(192, 2) k_products_st(const __grid_constant__ 
       const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
       const long long hrow = (long long)j * g.hp + (long long)z * g.kxs;
       for (int grp = 0; grp < 2; ++grp) {
-        if ((grp == 0 && !r1) || (grp == 1 && !(r2 || rt))) {   // uniform over the CTA
+        const bool zero = (grp == 0 && !r1) || (grp == 1 && !(r2 || rt));   // uniform over the CTA
+        C v[E];
+        if (!zero) {
+          const int jm = j >= 1 ? j - 1 : j, jp = j + 1 <= np - 1 ? j + 1 : j;
+          const ProdRows<R> P{row(jm, 0), row(j, 0), row(jp, 0), row(jm, 1), row(j, 1), row(jp, 1),
+                              row(jm, 2), row(j, 2), row(jp, 2), row(jm, 3), row(j, 3), row(jp, 3)};
+#pragma unroll
+          for (int q = 0; q < E; ++q) {
+            R a, b;
+            prod_ab(P, grp, seq, lane + q * T, r2, rt, y, a, b);
+            v[q] = mkc<C>(a, b);
+          }
+        }
+        if (PROD_SLOTS == 3 && grp == 1) {   // plane j - 1 is read for the last time: its slot takes plane j + 2
+          __syncthreads();
+          if (j + 2 <= jtop) issue(j + 2, z0);
+        }
+        if (zero) {
           const long long hrow0 = (long long)j * g.hp + (long long)z0 * g.kxs;
           const int w = zr * g.kxs;
           for (int idx = threadIdx.x; idx < 4 * w; idx += blockDim.x)
             xh[4 * grp + idx / w][hrow0 + idx % w] = mkc<C>(0, 0);
           continue;
-        }
-        const int jm = j >= 1 ? j - 1 : j, jp = j + 1 <= np - 1 ? j + 1 : j;
-        const ProdRows<R> P{row(jm, 0), row(j, 0), row(jp, 0), row(jm, 1), row(j, 1), row(jp, 1),
-                            row(jm, 2), row(j, 2), row(jp, 2), row(jm, 3), row(j, 3), row(jp, 3)};
-        C v[E];
-#pragma unroll
-        for (int q = 0; q < E; ++q) {
-          R a, b;
-          prod_ab(P, grp, seq, lane + q * T, r2, rt, y, a, b);
-          v[q] = mkc<C>(a, b);
         }
         fft_reg_lazy<N, -1>(v, lane, true, sq, twt);
         SEQ_SYNC(N);
@@ -1147,7 +1166,8 @@ static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   if constexpr (N <= 512) {
     const int zr = prod_zr<N>() < g.nz ? prod_zr<N>() : g.nz;
-    const size_t smem = (size_t)PROD_SLOTS * 4 * zr * N * sizeof(R) + (size_t)3 * zr * padded(N) * sizeof(C) +
+    constexpr int PROD_SLOTS = prod_slots<R>();
+    const size_t smem = (size_t)PROD_SLOTS * 4 * zr * N * sizeof(R) + (size_t)3 * zr * prod_sq<N>() * sizeof(C) +
                         PROD_SLOTS * sizeof(uint64_t);
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_products_st<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
