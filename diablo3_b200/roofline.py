@@ -24,8 +24,8 @@ At 512x257x512 this is ~67 P, i.e. ~540 B per grid point and substep.
 With the LES model (les_model_type 5) the stages change to
   inv_z      4 S  -> 8 Xh           state and its z-derivatives
   inv_x      8 Xh -> 12 P           state, x- and z-derivatives
-  products   12 P -> 11 P (AMD: nu_t, kappa_t, 9 SGS forcing fields),
-             then 4 P + 9 P -> 8 Xh
+  products   12 P -> 13 P (AMD walk: nu_t, kappa_t and the 11 product +
+             SGS-forcing sequences), then 11 P -> 8 Xh
   thomas     per equation r, u, nu in, u out: 16 P
 """
 from __future__ import annotations
@@ -53,7 +53,7 @@ def stage_bytes(p) -> dict:
     return {
         "inv_z": 4 * S + (8 if les else 4) * X,
         "inv_x": (8 * X + 12 * P) if les else (4 * X + 4 * P),
-        "products": (23 * P + 13 * P + 8 * X) if les else (4 * P + 8 * X),
+        "products": (12 * P + 13 * P + 11 * P + 8 * X) if les else (4 * P + 8 * X),
         "zpass_rhs": 8 * X + 9 * S + 4 * S + 4 * X,
         "inv_x_r": 4 * X + 4 * P,
         "thomas": 16 * P if les else 12 * P,
