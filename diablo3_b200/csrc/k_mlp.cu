@@ -178,11 +178,14 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(MlpArgs a) {
       umma_bf16(tbase + dcol, umma_desc(a_addr + 256 * s, 128, a_sbo), umma_desc(b_addr + 256 * s, 128, b_sbo),
                 idesc, acc || s > 0);
   };
-  // commit, wait, and agree on the outcome
+  // commit, wait, and agree on the outcome (a wait that gave up leaves the
+  // layer pending for the drain at the end)
+  bool pend = false;
   auto sync_mma = [&]() -> bool {
     if (t == 0) umma_commit(mbar);
     const bool w = mbar_wait(mbar, phase, WAIT_ITERS);
-    phase ^= 1u;
+    if (w) phase ^= 1u;
+    else pend = true;
     tc_fence_after();
     return __syncthreads_and(w ? 1 : 0) != 0;
   };
@@ -405,7 +408,10 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(MlpArgs a) {
   }
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   if (lane == 0 && lsum != 0.0f) atomicAdd(a.loss, lsum);
-  if (!ok && t == 0) atomicExch(a.err, 1);
+  if (!ok && t == 0) {
+    atomicExch(a.err, 1);
+    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);   // the layer still in flight (bounded) before freeing
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_free(tbase, PL::TMEM_COLS);
@@ -544,10 +550,12 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
     __syncthreads();
     tc_fence_after();
   };
+  bool pend = false;   // a layer whose wait gave up (thread 0's view)
   auto sync_mma = [&]() -> bool {
     if (t == 0) umma_commit(mbar);
     const bool w = mbar_wait(mbar, phase, WAIT_ITERS);
-    phase ^= 1u;
+    if (w) phase ^= 1u;
+    else pend = true;
     tc_fence_after();
     return __syncthreads_and(w ? 1 : 0) != 0;
   };
@@ -639,7 +647,10 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
       a.out[(long long)p * 2 + 1] = softplus(y1) * osc1;
     }
   }
-  if (!ok && t == 0) atomicExch(a.err, 1);
+  if (!ok && t == 0) {
+    atomicExch(a.err, 1);
+    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);   // the layer still in flight (bounded) before freeing
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_free(tbase, PL::TMEM_COLS);
@@ -727,6 +738,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const uint16_t* A, const u
     }
   } else if (t == 0) {
     atomicExch(err, 1);
+    if (!w) mbar_wait(mbar, 0, WAIT_ITERS);   // the MMA still in flight (bounded) before freeing
   }
   tc_fence_before();
   __syncthreads();

@@ -4,7 +4,7 @@ Checks: the closure features the substep hands to the network equal a numpy
 evaluation from the same state (FP32 storage: 1e-6 relative); with every
 point outside the training range the substep is the AMD substep (1e-13);
 with no range limit nu_t / kappa_t inside the channel are the network's
-outputs on those features (1e-6); and a run with the closure stays finite
+outputs on those features (1e-6, FP64 and FP32 fields); and a run with the closure stays finite
 and divergence free.
 """
 import numpy as np
@@ -78,8 +78,12 @@ def test_closure_outside_range_is_amd(oracle_mod, Channel):
         assert rel_l2(b[f], a[f]) <= 1e-13, f
 
 
-def test_closure_nu_is_network_output(oracle_mod, Channel):
-    p = les_params(6)
+@pytest.mark.parametrize("prec", [0, 1])
+def test_closure_nu_is_network_output(oracle_mod, Channel, prec):
+    # the substep's inference forms the features from the FP64 (prec 0) or
+    # FP32 (prec 1) physical fields itself; the reference is the network on
+    # the features the AMD kernel's feature mode writes from the same fields
+    p = les_params(6, precision=prec)
     gy = grid_for(p)
     _, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=33)
     net = _net(2)
