@@ -102,6 +102,18 @@ class Channel:
         self._ck(self.L.db_fft_xz_to_physical(self.h, _L.dptr(d.reshape(-1))))
         return d.reshape(-1).reshape(ref_shape(self.p))
 
+    def fft_xz_to_fourier_dev(self, t) -> None:
+        """In place on a device reference-layout real array (a contiguous
+        float64 CUDA tensor), ordered on the context's stream."""
+        assert t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()
+        self._ck(self.L.db_fft_xz_to_fourier_dev(self.h, ctypes.c_void_p(t.data_ptr())))
+
+    def fft_xz_to_physical_dev(self, t) -> None:
+        """In place on a device reference-layout complex array (a contiguous
+        complex128 or float64 CUDA tensor), ordered on the context's stream."""
+        assert t.is_cuda and t.element_size() in (8, 16) and t.is_contiguous()
+        self._ck(self.L.db_fft_xz_to_physical_dev(self.h, ctypes.c_void_p(t.data_ptr())))
+
     def rk_chan_1(self, rk_step: int):
         self._ck(self.L.db_rk_substep(self.h, rk_step))
 

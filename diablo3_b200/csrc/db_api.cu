@@ -652,6 +652,31 @@ extern "C" int db_fft_xz_to_physical(db_ctx* c, double* buf) {
   return phys_download(c, c->s.r1, buf);
 }
 
+// device-resident forms: the same transforms on a device array in the
+// reference layout, every layout change on the device, stream-ordered on
+// the context's stream (no host synchronisation)
+extern "C" int db_fft_xz_to_fourier_dev(db_ctx* c, double* d) {
+  if (!c || !d) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  CK(launch_phys_from_ref(g, c->p.nx, c->p.nz, d, c->s.r1, c->st));
+  CK(launch_fwd_x(g, fset(c->s.r1), fset(c->s.xh[0]), 1, c->st));
+  CK(launch_fwd_z(g, fset(c->s.xh[0]), fset(c->s.phi_g), 1, c->st));
+  CK(launch_spec_to_ref(g, c->p.nx, c->p.nz, c->s.phi_g, reinterpret_cast<double2*>(d), c->st));
+  c->launches += 4;
+  return DB_OK;
+}
+
+extern "C" int db_fft_xz_to_physical_dev(db_ctx* c, double* d) {
+  if (!c || !d) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  CK(launch_ref_to_spec(g, c->p.nx, c->p.nz, reinterpret_cast<const double2*>(d), c->s.phi_g, c->st));
+  CK(launch_inv_z(g, fset(c->s.phi_g), fset(c->s.xh[0]), 1, c->st));
+  CK(launch_inv_x(g, fset(c->s.xh[0]), fset(c->s.r1), 1, c->st));
+  CK(launch_phys_to_ref(g, c->p.nx, c->p.nz, c->s.r1, d, c->st));
+  c->launches += 4;
+  return DB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // the substep
 

@@ -180,6 +180,10 @@ cudaError_t launch_stats(const Geom& g, const State& s, int homx, double* out, c
 // spectral field: compact device layout <-> reference host layout, on the device
 cudaError_t launch_spec_to_ref(const Geom& g, int nx, int nz, const double2* src, double2* ref, cudaStream_t st);
 cudaError_t launch_ref_to_spec(const Geom& g, int nx, int nz, const double2* ref, double2* dst, cudaStream_t st);
+// one physical field between the reference layout (device doubles) and the
+// compact layout at the context's precision
+cudaError_t launch_phys_from_ref(const Geom& g, int nx, int nz, const double* ref, void* dst, cudaStream_t st);
+cudaError_t launch_phys_to_ref(const Geom& g, int nx, int nz, const void* src, double* ref, cudaStream_t st);
 cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st);
 
 // k_les.cu

@@ -25,7 +25,7 @@ EXPORTS = (
     "db_abi_version", "db_last_error", "db_init", "db_finalize",
     "db_upload_state", "db_download_state", "db_upload_field", "db_download_field",
     "db_set_clock", "db_get_status", "db_clear_status",
-    "db_fft_xz_to_fourier", "db_fft_xz_to_physical",
+    "db_fft_xz_to_fourier", "db_fft_xz_to_physical", "db_fft_xz_to_fourier_dev", "db_fft_xz_to_physical_dev",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
     "db_courant", "db_divergence", "db_stats",
     "db_autotune", "db_set_timing", "db_stage_times", "db_kernel_launches",
@@ -79,6 +79,8 @@ def load(path: str | None = None):
     L.db_clear_status.argtypes = [vp]
     L.db_fft_xz_to_fourier.argtypes = [vp, dp]
     L.db_fft_xz_to_physical.argtypes = [vp, dp]
+    L.db_fft_xz_to_fourier_dev.argtypes = [vp, vp]
+    L.db_fft_xz_to_physical_dev.argtypes = [vp, vp]
     L.db_rk_substep.argtypes = [vp, ctypes.c_int]
     L.db_rk_steps.argtypes = [vp, ctypes.c_int]
     L.db_rem_div.argtypes = [vp]

@@ -160,6 +160,14 @@ int db_clear_status(db_ctx* ctx);
 int db_fft_xz_to_fourier(db_ctx* ctx, double* inout);
 int db_fft_xz_to_physical(db_ctx* ctx, double* inout);
 
+/* The same two transforms on a DEVICE array in the reference layout (for
+ * callers whose fields already live in device memory), in place, with every
+ * layout change on the device.  Stream-ordered on the context's stream: the
+ * call returns once the work is enqueued.  The physical layout's padding
+ * (x >= Nx, z >= Nz) is neither read nor written, as in the host forms. */
+int db_fft_xz_to_fourier_dev(db_ctx* ctx, double* d_inout);
+int db_fft_xz_to_physical_dev(db_ctx* ctx, double* d_inout);
+
 /* RKW3 + Crank-Nicolson substep rk_step in {1,2,3} on the device state.
  * Replaces rk_chan_1 (for/solver.f90:366-1273). */
 int db_rk_substep(db_ctx* ctx, int rk_step);
