@@ -2,6 +2,9 @@
 // between the reference layout and the device layout, and the substep
 // orchestration (one CUDA graph per RK step).
 #include <cuda_runtime.h>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -488,6 +491,18 @@ static cudaError_t copy_retained(const db_ctx* c, double* host, cudaMemcpyKind k
   return cudaMemcpy3DAsync(&cp, c->st);
 }
 
+// n complex zeros from p (16-byte aligned): non-temporal stores, so the
+// lines are not read before being overwritten (x86-64), else memset
+static void zero_c16(double2* p, size_t n) {
+#if defined(__x86_64__)
+  const __m128i z = _mm_setzero_si128();
+  __m128i* q = reinterpret_cast<__m128i*>(p);
+  for (size_t i = 0; i < n; ++i) _mm_stream_si128(q + i, z);
+#else
+  memset(p, 0, n * sizeof(double2));
+#endif
+}
+
 // Zero everything of a reference-layout host array outside the retained
 // block (the reference keeps those entries zero), planes split over host
 // threads.
@@ -498,9 +513,12 @@ static void zero_ref_padding(const db_ctx* c, double* host) {
   auto work = [=](int j0, int j1) {
     for (int j = j0; j < j1; ++j) {
       double2* pl = reinterpret_cast<double2*>(host) + (size_t)j * plane;
-      for (size_t r = 0; r < krows; ++r) memset(pl + r * nxh + keep, 0, (nxh - keep) * sizeof(double2));
-      memset(pl + krows * nxh, 0, (rows - krows) * nxh * sizeof(double2));
+      for (size_t r = 0; r < krows; ++r) zero_c16(pl + r * nxh + keep, nxh - keep);
+      zero_c16(pl + krows * nxh, (rows - krows) * nxh);
     }
+#if defined(__x86_64__)
+    _mm_sfence();   // the streamed zeros are visible before the thread is joined
+#endif
   };
   const unsigned hw = std::thread::hardware_concurrency();
   const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, np}));
