@@ -178,6 +178,17 @@ class Channel:
         self._ck(self.L.db_autotune(self.h, buf, len(buf)))
         return buf.value.decode()
 
+    def tuning(self) -> list:
+        """The launch shapes in use (db_get_tuning order)."""
+        v = (ctypes.c_int * _L.NTUNE)()
+        self._ck(self.L.db_get_tuning(self.h, v, _L.NTUNE))
+        return list(v)
+
+    def set_tuning(self, shapes) -> None:
+        """Set launch shapes (db_get_tuning order; 0 = built-in default)."""
+        v = (ctypes.c_int * _L.NTUNE)(*[int(x) for x in shapes])
+        self._ck(self.L.db_set_tuning(self.h, v, _L.NTUNE))
+
     def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
         self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
 

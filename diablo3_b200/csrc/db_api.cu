@@ -1010,6 +1010,38 @@ static float time_ms(db_ctx* c, F&& launch, int reps = 3) {
   return ms / reps;
 }
 
+// the step graphs hold the launch shapes they were captured with
+static void drop_graphs(db_ctx* c) {
+  for (int i = 0; i < 2; ++i)
+    if (c->graph[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph[i] = nullptr;
+    }
+}
+
+extern "C" int db_get_tuning(db_ctx* c, int* shapes, int n) {
+  if (!c || !shapes || n < DB_NTUNE) return DB_ERR_ARG;
+  const Geom& g = c->g;
+  const int v[DB_NTUNE] = {g.tune_xcps, g.tune_xgrid, g.tune_zns, g.tune_pgrid, g.tune_les_tb, g.tune_amd_ch};
+  for (int i = 0; i < DB_NTUNE; ++i) shapes[i] = v[i];
+  return DB_OK;
+}
+
+extern "C" int db_set_tuning(db_ctx* c, const int* shapes, int n) {
+  if (!c || !shapes || n < DB_NTUNE) return DB_ERR_ARG;
+  for (int i = 0; i < DB_NTUNE; ++i)
+    if (shapes[i] < 0 || shapes[i] > 1024) return fail(c, DB_ERR_ARG, "launch shape out of range");
+  Geom& g = c->g;
+  g.tune_xcps = shapes[0];
+  g.tune_xgrid = shapes[1];
+  g.tune_zns = shapes[2];
+  g.tune_pgrid = shapes[3];
+  g.tune_les_tb = shapes[4];
+  g.tune_amd_ch = shapes[5];
+  drop_graphs(c);
+  return DB_OK;
+}
+
 extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
   if (!c) return DB_ERR_ARG;
   if (c->timing) return fail(c, DB_ERR_STATE, "turn stage timing off before db_autotune");
@@ -1083,15 +1115,35 @@ extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
     }
     g.tune_les_tb = bt;
   }
-  CK(cudaStreamSynchronize(c->st));
-  snprintf(buf, sizeof buf, "chosen: x-pass cps %d ctas/SM %d, z-pass seqs/CTA %d, products ctas/SM %d, LES Thomas %d\n",
-           g.tune_xcps, g.tune_xgrid, g.tune_zns, g.tune_pgrid, g.tune_les_tb);
-  rep += buf;
-  for (int i = 0; i < 2; ++i)   // captured steps hold the old launch shapes
-    if (c->graph[i]) {
-      cudaGraphExecDestroy(c->graph[i]);
-      c->graph[i] = nullptr;
+  // LES closure walk: wall-normal chunks (nu_t, kappa_t kept: a substep
+  // without the model reuses them)
+  if (c->p.use_les) {
+    const size_t pb = (size_t)g.np * g.pp * (g.prec ? sizeof(float) : sizeof(double));
+    char* keep = reinterpret_cast<char*>(s.tscr);
+    CK(cudaMemcpyAsync(keep, s.nu_t, pb, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(keep + pb, s.kappa_t, pb, cudaMemcpyDeviceToDevice, c->st));
+    float best = 1e30f;
+    int bch = 0;
+    const int maxch = (g.ny + 1) / 8 > 1 ? (g.ny + 1) / 8 : 1;
+    for (int ch = 1; ch <= maxch; ch *= 2) {
+      g.tune_amd_ch = ch;
+      const float ms = time_ms(c, [&] { launch_les_amd(g, c->ph, s, c->st); });
+      if (cudaGetLastError() != cudaSuccess) continue;
+      snprintf(buf, sizeof buf, "LES closure chunks %d: %.3f ms\n", ch, ms);
+      rep += buf;
+      if (ms < best) { best = ms; bch = ch; }
     }
+    g.tune_amd_ch = bch;
+    CK(cudaMemcpyAsync(s.nu_t, keep, pb, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(s.kappa_t, keep + pb, pb, cudaMemcpyDeviceToDevice, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  snprintf(buf, sizeof buf,
+           "chosen: x-pass cps %d ctas/SM %d, z-pass seqs/CTA %d, products ctas/SM %d, LES Thomas %d, LES closure "
+           "chunks %d\n",
+           g.tune_xcps, g.tune_xgrid, g.tune_zns, g.tune_pgrid, g.tune_les_tb, g.tune_amd_ch);
+  rep += buf;
+  drop_graphs(c);   // captured steps hold the old launch shapes
   if (report && report_len > 0) {
     strncpy(report, rep.c_str(), (size_t)report_len - 1);
     report[report_len - 1] = 0;

@@ -45,6 +45,7 @@ struct Geom {
   int tune_zns;            // z-pass: sequences (kx columns) per CTA
   int tune_les_tb;         // LES Thomas: threads per CTA
   int tune_pgrid;          // products: persistent CTAs per SM
+  int tune_amd_ch;         // LES closure walk: wall-normal chunks
 };
 
 // Physics constants of the substep (host-computed once at init).

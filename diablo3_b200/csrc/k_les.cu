@@ -472,12 +472,12 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
   return cudaGetLastError();
 }
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode) {
-  // wall-normal chunks until about 16 warps per SM walk columns (each chunk
-  // at least 8 rows), then columns per CTA: 128, narrowed (to 32 at least)
+  // wall-normal chunks (tuned, else until about 16 warps per SM walk
+  // columns; each chunk at least 8 rows), then columns per CTA: 128, narrowed (to 32 at least)
   // until every SM has two CTAs
   const long long cols = (long long)g.nx * g.nz, want = 512LL * sm_count();
   const int maxch = (g.ny + 1) / 8 > 1 ? (g.ny + 1) / 8 : 1;
-  int nch = (int)((want + cols - 1) / cols);
+  int nch = g.tune_amd_ch > 0 ? g.tune_amd_ch : (int)((want + cols - 1) / cols);
   nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
   int bx = g.nx < 128 ? g.nx : 128;
   while (bx > 32 && bx % 2 == 0 && (long long)((g.nx + bx - 1) / bx) * g.nz * nch < 2LL * sm_count()) bx >>= 1;

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libdiablo_b200.so")
 # enum db_field
 CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH, NU_T, KAPPA_T = range(11)
 # rows of db_stats (include/diablo_b200.h order)
+NTUNE = 6   # DB_NTUNE
 STAT_ROWS = ("ume", "vme", "wme", "thme", "urms", "vrms", "wrms", "thrms", "uv", "wv", "uw", "thv", "epsilon", "chi")
 STATE_FIELDS = (CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH)
 
@@ -28,7 +29,7 @@ EXPORTS = (
     "db_fft_xz_to_fourier", "db_fft_xz_to_physical", "db_fft_xz_to_fourier_dev", "db_fft_xz_to_physical_dev",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
     "db_courant", "db_divergence", "db_stats",
-    "db_autotune", "db_set_timing", "db_stage_times", "db_kernel_launches",
+    "db_autotune", "db_get_tuning", "db_set_tuning", "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
@@ -89,6 +90,8 @@ def load(path: str | None = None):
     L.db_divergence.argtypes = [vp, dp]
     L.db_stats.argtypes = [vp, dp]
     L.db_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.db_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    L.db_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     L.db_set_timing.argtypes = [vp, ctypes.c_int]
     L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
     L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]

@@ -344,12 +344,24 @@ enum db_stage {
 
 /* Autotuner (no counterpart in the reference): times candidate launch shapes
  * of the x-pass (row pairs per TMA-staged item, persistent CTAs per SM), the
- * z-pass (kx columns per CTA) and, with LES, the per-column Thomas (threads
- * per CTA) on this context's scratch buffers, keeps the fastest, and writes
+ * z-pass (kx columns per CTA), the products (CTAs per SM) and, with LES,
+ * the per-column Thomas (threads per CTA) and the closure walk (wall-normal
+ * chunks) on this context's scratch buffers, keeps the fastest, and writes
  * the timings and choices as text into report (may be NULL).  Call between
  * steps; it overwrites only scratch fields (the next substep recomputes
  * them). */
 int db_autotune(db_ctx* ctx, char* report, int report_len);
+
+/* The launch shapes in use, or set ones found earlier (0 = built-in
+ * default), as DB_NTUNE ints in this order: x-pass row pairs per TMA item,
+ * x-pass CTAs per SM, z-pass kx columns per CTA, products CTAs per SM, LES
+ * Thomas threads per CTA, LES closure wall-normal chunks.  Shapes change
+ * how work is split, never the arithmetic: results are bit-identical for
+ * every setting.  Use values db_get_tuning reported after db_autotune; a
+ * shape a kernel cannot launch with makes the next step return an error. */
+#define DB_NTUNE 6
+int db_get_tuning(db_ctx* ctx, int* shapes, int n);
+int db_set_tuning(db_ctx* ctx, const int* shapes, int n);
 
 /* Record CUDA events between the stages of every substep (the step graph is
  * re-captured with event nodes).  Off by default. */
