@@ -134,8 +134,10 @@ __device__ __forceinline__ void prod_out(C* const* xh, const C* sq, const Geom& 
 }
 
 // One CTA per (z, j, group), rows read from global memory (Nx > 512).
+// Sequences of 128 threads and more: no minimum of resident CTAs, so the
+// FFT's registers do not spill.
 template <int N, typename R>
-__global__ void __launch_bounds__(3 * FftShape<N>::T, DB_LB_PROD) k_products(const __grid_constant__ State s, Geom g) {
+__global__ void __launch_bounds__(3 * FftShape<N>::T, FftShape<N>::T >= 128 ? 1 : DB_LB_PROD) k_products(const __grid_constant__ State s, Geom g) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);

@@ -34,7 +34,7 @@ def _cmp(o, ch, p, tol, fields=STATE, cp_tol=None, cp_base=None):
     return errs
 
 
-@pytest.mark.parametrize("n", [(16, 17, 16), (64, 33, 32), (32, 65, 128)])
+@pytest.mark.parametrize("n", [(16, 17, 16), (64, 33, 32), (32, 65, 128), (1024, 9, 16)])
 def test_fft_xz_matches_oracle(oracle_mod, Channel, n):
     nx, ny, nz = n
     p = config0_params(nx=nx, ny=ny, nz=nz)
@@ -75,9 +75,11 @@ def test_rem_div_matches_oracle_and_zeroes_divergence(oracle_mod, Channel):
     assert ch.divergence() < 1e-12
 
 
-@pytest.mark.parametrize("rk", [1, 2, 3])
-def test_single_substep_matches_oracle(oracle_mod, Channel, rk):
-    p = config0_params(nx=32, ny=33, nz=32)
+@pytest.mark.parametrize("rk,n", [(1, (32, 33, 32)), (2, (32, 33, 32)), (3, (32, 33, 32)),
+                                  (2, (1024, 9, 16))])   # Nx > 512: the row-per-CTA products kernel
+def test_single_substep_matches_oracle(oracle_mod, Channel, rk, n):
+    nx, ny, nz = n
+    p = config0_params(nx=nx, ny=ny, nz=nz)
     gy = grid_for(p)
     o, ch = seed_pair(oracle_mod.Oracle, Channel, p, gy, seed=5)
     # give cf a non-trivial history so rk > 1 exercises zeta*h*cf
