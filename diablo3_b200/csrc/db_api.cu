@@ -53,22 +53,45 @@ struct db_ctx {
 
 static std::string g_init_err;
 
+static void set_err(db_ctx* c, const char* a, const char* b) noexcept {
+  if (!c) return;
+  try {
+    c->err = b ? std::string(a) + ": " + b : std::string(a);
+  } catch (...) {
+  }
+}
+
 static void mark(db_ctx* c, int rk, int stage) {
   if (c->timing) cudaEventRecordWithFlags(c->ev[rk][stage], c->st, cudaEventRecordExternal);
 }
+
+// error text of a context; recording it never throws (nothing may throw
+// past the C-ABI)
+static void set_err(db_ctx* c, const char* a, const char* b = nullptr) noexcept;
 
 #define CK(call)                                                                         \
   do {                                                                                   \
     cudaError_t e_ = (call);                                                             \
     if (e_ != cudaSuccess) {                                                             \
-      c->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+      set_err(c, #call, cudaGetErrorString(e_));                                         \
       return DB_ERR_CUDA;                                                                \
     }                                                                                    \
   } while (0)
 
 static int fail(db_ctx* c, int code, const char* msg) {
-  if (c) c->err = msg;
+  set_err(c, msg);
   return code;
+}
+
+// an entry point whose body allocates host memory: an allocation failure
+// becomes an error code
+template <typename F>
+static int guarded(F&& body) noexcept {
+  try {
+    return body();
+  } catch (...) {
+    return DB_ERR_CUDA;
+  }
 }
 
 static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
@@ -145,7 +168,7 @@ static int dalloc(db_ctx* c, T** ptr, size_t count) {
   return DB_OK;
 }
 
-extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db_ctx** out) {
+static int init_impl(const db_params* p, const double* gy_in, void* stream, db_ctx** out) {
   if (!p || !gy_in || !out) { g_init_err = "db_init: NULL argument"; return DB_ERR_ARG; }
   *out = nullptr;
   std::string why;
@@ -358,6 +381,19 @@ extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db
   return DB_OK;
 }
 
+extern "C" int db_init(const db_params* p, const double* gy_in, void* stream, db_ctx** out) {
+  try {
+    return init_impl(p, gy_in, stream, out);
+  } catch (...) {   // a host allocation failed
+    try {
+      g_init_err = "db_init: host allocation failed";
+    } catch (...) {
+    }
+    if (out) *out = nullptr;
+    return DB_ERR_CUDA;
+  }
+}
+
 extern "C" int db_finalize(db_ctx* c) {
   if (!c) return DB_ERR_ARG;
   for (int i = 0; i < 2; ++i)
@@ -522,10 +558,20 @@ static void zero_ref_padding(const db_ctx* c, double* host) {
   };
   const unsigned hw = std::thread::hardware_concurrency();
   const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, np}));
-  std::vector<std::thread> th;
-  for (int k = 1; k < nt; ++k) th.emplace_back(work, (int)((long long)np * k / nt), (int)((long long)np * (k + 1) / nt));
+  std::thread th[16];
+  bool started[16] = {};
+  for (int k = 1; k < nt; ++k) {
+    const int a = (int)((long long)np * k / nt), b = (int)((long long)np * (k + 1) / nt);
+    try {   // a thread that cannot be created: its planes run here (nothing may throw past the C-ABI)
+      th[k] = std::thread(work, a, b);
+      started[k] = true;
+    } catch (...) {
+      work(a, b);
+    }
+  }
   work(0, (int)((long long)np / nt));
-  for (auto& t : th) t.join();
+  for (int k = 1; k < nt; ++k)
+    if (started[k]) th[k].join();
 }
 
 static int upload_spec(db_ctx* c, int id, const double* ref) {
@@ -879,7 +925,7 @@ struct db_ensemble {
   std::string err;
 };
 
-extern "C" int db_ensemble_create(db_ctx** members, int n, void* stream, db_ensemble** out) {
+static int ensemble_create_impl(db_ctx** members, int n, void* stream, db_ensemble** out) {
   if (!members || n < 1 || !out) return DB_ERR_ARG;
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
@@ -918,6 +964,10 @@ extern "C" int db_ensemble_create(db_ctx** members, int n, void* stream, db_ense
     }
   *out = e;
   return DB_OK;
+}
+
+extern "C" int db_ensemble_create(db_ctx** members, int n, void* stream, db_ensemble** out) {
+  return guarded([&] { return ensemble_create_impl(members, n, stream, out); });
 }
 
 extern "C" int db_ensemble_destroy(db_ensemble* e) {
@@ -1042,7 +1092,7 @@ extern "C" int db_set_tuning(db_ctx* c, const int* shapes, int n) {
   return DB_OK;
 }
 
-extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
+static int autotune_impl(db_ctx* c, char* report, int report_len) {
   if (!c) return DB_ERR_ARG;
   if (c->timing) return fail(c, DB_ERR_STATE, "turn stage timing off before db_autotune");
   Geom& g = c->g;
@@ -1149,6 +1199,10 @@ extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
     report[report_len - 1] = 0;
   }
   return DB_OK;
+}
+
+extern "C" int db_autotune(db_ctx* c, char* report, int report_len) {
+  return guarded([&] { return autotune_impl(c, report, report_len); });
 }
 
 extern "C" int db_set_timing(db_ctx* c, int enable) {

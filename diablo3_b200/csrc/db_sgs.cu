@@ -1,6 +1,8 @@
 // db_sgs.cu -- C-ABI of the learned SGS closure (include/diablo_b200.h):
 // device buffers of one network and the calls into k_mlp.cu.
 #include <cuda_runtime.h>
+
+#include <new>
 #include <string.h>
 
 #include <string>
@@ -34,7 +36,8 @@ static int sgs_fail(cudaError_t e) { return e == cudaSuccess ? DB_OK : DB_ERR_CU
 extern "C" int db_sgs_create(void* stream, db_sgs_net** out) {
   if (!out) return DB_ERR_ARG;
   *out = nullptr;
-  db_sgs_net* n = new db_sgs_net();
+  db_sgs_net* n = new (std::nothrow) db_sgs_net();
+  if (!n) return DB_ERR_CUDA;   // host allocation failed (nothing may throw past the C-ABI)
   n->st = (cudaStream_t)stream;
   int dev = 0;
   cudaGetDevice(&dev);
