@@ -173,8 +173,8 @@ def cpu_baseline(name: str, min_seconds: float = 10.0) -> dict:
 
 
 def run_reference(args) -> None:
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    from diablo3_b200 import replicas
+    if not replicas.from_env().leader:   # under torchrun rank 0 alone runs and prints it
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     per = []
@@ -361,20 +361,17 @@ def main():
 
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     from diablo3_b200 import lib as L
     from diablo3_b200 import roofline
     from diablo3_b200.channel import Channel
     from diablo3_b200.grid import create_grid
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from diablo3_b200 import replicas
+    rk = replicas.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    replicas.init(rk, "nccl")
 
     p = workload_params(args.config)
     if args.precision == "mixed":
@@ -388,8 +385,7 @@ def main():
     npts = p.nx * p.ny * p.nz
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(rk)
 
     tuned = None
     if not args.no_autotune:   # launch shapes timed before the warm-up (not in the timed region)
@@ -426,11 +422,8 @@ def main():
     clk = clocks.stop()
     n1 = ctypes.c_longlong()
     ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n1)))
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = npts * 3 * args.steps * world / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(rk, ms)
+    value = replicas.job_rate(npts, 3 * args.steps, rk, ms_max)
     st = ch.status()
     if st.flags & 1:
         raise SystemExit("non-finite values in the flow: run rejected")
@@ -468,10 +461,8 @@ def main():
                 ch._ck(ch.L.db_download_field(ch.h, f, L.dptr(host[f].view(np.float64).reshape(-1))))
         e1.record(stream)
         torch.cuda.synchronize()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": npts * 3 * ke * world / (float(te.item()) / 1e3), "unit": UNIT,
+        te = replicas.max_over_ranks(rk, e0.elapsed_time(e1))
+        e2e = {"value": replicas.job_rate(npts, 3 * ke, rk, te), "unit": UNIT,
                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                "steps": ke, "path": "db_upload_state + db_rk_steps(1) + db_download_field x9, reference-layout host arrays"}
 
@@ -505,9 +496,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     ch.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(rk)
 
 
 if __name__ == "__main__":
