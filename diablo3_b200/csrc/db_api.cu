@@ -808,7 +808,11 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   if ((e = launch_products(g, s, st, les))) return e;
   mark(c, rk, 3);
   const double2* ov = les ? s.ghost : nullptr;   // ghost rows the transforms saw
-  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov))) return e;
+  // the CN rows first: the mixed path without LES forms the increment
+  // system's right-hand side from them in the z-pass
+  if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
+  const bool qform = c->p.precision != 0 && !c->p.use_les;
+  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov, qform))) return e;
   mark(c, rk, 4);
   // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
   if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
@@ -816,7 +820,6 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   // implicit CN solves (solver.f90:1012-1233); the mixed path's solves
   // store the new physical u only where the CFL below reads it
   const bool cfl_step = rk == 2 && c->p.variable_dt;
-  if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
   if (c->p.use_les) {   // eddy terms whether or not the model ran this step
     if ((e = launch_thomas_les(g, s, rk, st, cfl_step))) return e;
   } else {

@@ -156,9 +156,11 @@ struct State {
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
 int sm_count();   // SMs of the current device (cached)
 cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les = false);
-// ghost: the LES overlay, when the inverse transforms of this substep used it
+// ghost: the LES overlay, when the inverse transforms of this substep used it;
+// qform (mixed path without LES): write the increment system's right-hand
+// side on every plane, the CN rows (launch_tri_coef) already formed
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
-                             const double2* ghost = nullptr);
+                             const double2* ghost = nullptr, bool qform = false);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 // keep_u: also store the new physical u on the mixed path (the CFL of the
 // third substep reads it); the FP64 path always stores it

@@ -471,16 +471,51 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
   return cr;
 }
 
+// Right-hand side of the implicit system written for the increment
+// D = u_new - u (mixed path without LES): with the CN rows
+// l u_{j-1} + d u_j + uu u_{j+1} = b_j of `row` (k_tri_coef), D solves the
+// same rows with b_j - (A u)_j, which for a solved row is
+//   (cr - cu) + 2 (cn_hi (u_{j+1} - u_j) - cn_lo (u_j - u_{j-1}))
+// (the reference's explicit CN half, solver.f90:850-870, 981-989, plus the
+// implicit half of the old state) and for a BC row the BC value (the (0,0)
+// mode only: it is constant over x and z) minus the BC row applied to the
+// old state.  Both are formed here in FP64 from the spectral state, so the
+// FP32 transform carries a substep's change only and the solve never
+// differentiates an FP32 field across rows: FP32 rounding of a large mean
+// (the stratification in th) amplified by 1/dy^2 no longer enters.
+__device__ __forceinline__ double2 inc_rhs(const State& s, const Geom& g, const TriRow& row, int e, int j, int kx,
+                                           int kzp, double2 cr_inc) {
+  const double2* cu = (e == 0) ? s.cu1 : (e == 1 ? s.cu3 : (e == 2 ? s.cu2 : s.cth));
+  const long long a = (long long)j * g.sp + (long long)kzp * g.kxs + kx;
+  const double2 Z = make_double2(0.0, 0.0);
+  const double2 c0 = cu[a];
+  const double2 cm = (j > 0) ? cu[a - g.sp] : Z;
+  const double2 cp = (j + 1 < g.np) ? cu[a + g.sp] : Z;
+  if (row.is_bc) {
+    const double b = (kx == 0 && kzp == 0) ? row.bc : 0.0;
+    return make_double2(b - (row.l * cm.x + row.d * c0.x + row.u * cp.x),
+                        -(row.l * cm.y + row.d * c0.y + row.u * cp.y));
+  }
+  const double hx = row.cn_hi * (cp.x - c0.x) - row.cn_lo * (c0.x - cm.x);
+  const double hy = row.cn_hi * (cp.y - c0.y) - row.cn_lo * (c0.y - cm.y);
+  return make_double2(cr_inc.x + 2.0 * hx, cr_inc.y + 2.0 * hy);
+}
+
+// the CN system (k_tri_coef order th, u2, u1, u3) of z-pass equation e
+// (0 u1, 1 u3, 2 u2, 3 th)
+__device__ __forceinline__ int tri_eq(int e) { return e == 0 ? 2 : (e == 1 ? 3 : (e == 2 ? 1 : 0)); }
+
 // z-pass of the nonlinear terms + spectral RHS + inverse z-pass of cr.
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
 template <int N, typename R, bool EFAST>
 __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1))
-    k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost) {
+    k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost, int qform) {
   // FP32 work type: write the increment cr - base (base = the state as the
   // inverse transforms saw it), so FP32 rounding scales with the substep's
-  // change, not with the field
+  // change, not with the field; with qform (no LES) the whole right-hand
+  // side of the increment system (inc_rhs) on every plane, BC planes too
   constexpr bool INC = sizeof(R) == sizeof(float);
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -517,10 +552,29 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
     C* xin_n = (C*)s.xh[2 * e];
     const C* xin_m = (const C*)s.xh[2 * e + 1];
+    const bool qf = INC && qform;
+    const TriRow* trow = s.tri + tri_eq(e) * g.np + j;
     if (!in_rng(j, jlo, jhi)) {
+      if (!qf) {
+        if (active)
+#pragma unroll
+          for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
+        return;
+      }
+      // a BC plane of the increment system: its right-hand side, to physical z
+      const TriRow row = *trow;
+      C vb[E];
+#pragma unroll
+      for (int q = 0; q < E; ++q) {
+        const int zz = lane + q * T;
+        const int kzp = (zz <= g.nkz) ? zz : (zz >= N - g.nkz ? zz - N + g.nkzp : -1);
+        vb[q] = (kzp < 0 || !active) ? mkc<C>(0, 0)
+                                     : from_d2<C>(inc_rhs(s, g, row, e, j, kxc, kzp, make_double2(0.0, 0.0)));
+      }
+      ZFFT(+1, vb);
       if (active)
 #pragma unroll
-        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
+        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = vb[q];
       return;
     }
     C vn[E];
@@ -548,7 +602,9 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       // NL = (Z(N) + i kz Z(M)) / Nz, formed in FP64
       const double2 zmq = to_d2(sm_z[pidx(zz)]), zn = to_d2(vn[q]);
       const double2 nl = make_double2((zn.x - kzv * zmq.y) * inz, (zn.y + kzv * zmq.x) * inz);
-      vn[q] = from_d2<C>(rhs_point<INC>(s, g, ph, rk, e, j, kxc, kzp, nl, ghost));
+      double2 cr = rhs_point<INC>(s, g, ph, rk, e, j, kxc, kzp, nl, ghost);
+      if (qf) cr = inc_rhs(s, g, *trow, e, j, kxc, kzp, cr);
+      vn[q] = from_d2<C>(cr);
     }
     __syncthreads();
     ZFFT(+1, vn);
@@ -733,10 +789,12 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // shared memory and every thread scans them itself.  The r and u columns of
 // an equation come into shared memory by cp.async copies that every thread
 // issues for all rows of its chunk at once (no registers held for loads,
-// the whole equation in flight); the staged old u also gives the mixed
-// path its increment.  HBM sees r and u read once and u written once per
-// equation (plus the increment r on the mixed path, where u itself is
-// written only when keep_u: the third substep's CFL reads it, nothing else).
+// the whole equation in flight).  HBM sees r and u read once and u written
+// once per equation.  On the mixed path r holds the right-hand side of the
+// increment system on every row (inc_rhs, BC rows included), the solve
+// yields the increment itself and writes it back into r; u is read and
+// written only when keep_u (u + increment: the third substep's CFL reads
+// it, nothing else).
 constexpr int TX = 16;
 
 
@@ -744,7 +802,7 @@ template <typename R>
 __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g, int keep_u) {
   extern __shared__ __align__(16) unsigned char th_raw[];
   constexpr bool F64 = sizeof(R) == sizeof(double);
-  constexpr bool INC = !F64;   // FP32 work type: r holds the increment over u (k_zpass_rhs)
+  constexpr bool INC = !F64;   // FP32 work type: r is the increment system's right-hand side
   const int np = g.np, Nyp = g.ny;
   // [np][TX] each: the FP64 y / z tile, staged r (the tile itself when R is
   // double) and staged u
@@ -773,28 +831,32 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
     if (active) {
       for (int j = j0; j <= j1; ++j) {
         cp_async<sizeof(R)>(rs + j * TX + cl, r + (long long)j * pp + col);
-        cp_async<sizeof(R)>(us + j * TX + cl, u + (long long)j * pp + col);
+        if (!INC || keep_u) cp_async<sizeof(R)>(us + j * TX + cl, u + (long long)j * pp + col);
       }
     }
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();   // halo rows of u come from the neighbouring chunks
     if (active) {
-      // right-hand side (r + explicit CN term, or the BC value), forward
-      // recurrence with carry-in zero
-      double um = (j0 > 0) ? (double)us[(j0 - 1) * TX + cl] : 0.0;
-      double uc = (double)us[j0 * TX + cl];
+      // right-hand side (r + explicit CN term, or the BC value; the mixed
+      // path's r is complete), forward recurrence with carry-in zero
+      double um = (!INC && j0 > 0) ? (double)us[(j0 - 1) * TX + cl] : 0.0;
+      double uc = INC ? 0.0 : (double)us[j0 * TX + cl];
       double y = 0.0;
       for (int j = j0; j <= j1; ++j) {
         const TriRow* row = Rw + j;
-        const double un = (j + 1 < np) ? (double)us[(j + 1) * TX + cl] : 0.0;
         const double xr = (double)rs[j * TX + cl];
-        const double rj = INC ? xr + uc : xr;
-        const double v = row->is_bc ? row->bc : rj + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+        double v;
+        if (INC) {
+          v = xr;
+        } else {
+          const double un = (j + 1 < np) ? (double)us[(j + 1) * TX + cl] : 0.0;
+          v = row->is_bc ? row->bc : xr + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+          um = uc;
+          uc = un;
+        }
         y = (j == j0) ? v : v + row->ap * y;
         tile[j * TX + cl] = y;
-        um = uc;
-        uc = un;
       }
       ye[par][k][cl] = y;
       // backward recurrence of the chunk's y, carry-in zero
@@ -831,14 +893,18 @@ __global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State
         if (q == k) Gm = G[q - 1];
       }
       // final values and the rows the reference stores; on the mixed path
-      // also the increment (into r) for the forward transform, 0 on rows
-      // the solve does not store
+      // the value is the increment: into r for the forward transform (0 on
+      // rows the solve does not store), and u + increment into u if keep_u
       if (xin) {
         for (int j = j0; j <= j1; ++j) {
           const double xv = tile[j * TX + cl] + Gm * Rw[j].qa + X * Rw[j].pm;
           const bool st = (j >= lo && j <= hi);
-          if (st && (!INC || keep_u)) u[(long long)j * pp + col] = (R)xv;
-          if (INC) r[(long long)j * pp + col] = st ? (R)(xv - (double)us[j * TX + cl]) : (R)0;
+          if (INC) {
+            r[(long long)j * pp + col] = st ? (R)xv : (R)0;
+            if (st && keep_u) u[(long long)j * pp + col] = (R)((double)us[j * TX + cl] + xv);
+          } else if (st) {
+            u[(long long)j * pp + col] = (R)xv;
+          }
         }
       }
     }
@@ -1207,14 +1273,15 @@ static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les
   }
 }
 template <int N, typename R>
-static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
+static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, int qform,
+                       cudaStream_t st) {
   constexpr int T = FftShape<N>::T;
   constexpr bool EFAST = sizeof(R) == sizeof(double);
   size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_zpass_rhs<N, R, EFAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
-  k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost);
+  k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost, qform);
 }
 template <int N>
 static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
@@ -1224,10 +1291,11 @@ static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk
   launch_inv_z(g, nl, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6]), 4, st);
 }
 template <int N>
-static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
-  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, st);
+static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, bool qform,
+                     cudaStream_t st) {
+  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, qform ? 1 : 0, st);
   else if (s.nls[0]) go_zpass_split<N>(g, ph, s, rk, st);
-  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, st);
+  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, 0, st);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -1247,8 +1315,8 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
   return cudaGetLastError();
 }
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
-                             const double2* ghost) {
-  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, st);
+                             const double2* ghost, bool qform) {
+  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, qform, st);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
