@@ -49,7 +49,14 @@ struct db_ctx {
   cudaEvent_t ev[3][DB_NSTAGES + 1] = {};
   long long launches = 0;          // kernels issued so far
   long long graph_kernels[2] = {0, 0};   // kernel nodes in one captured step
+  // nu_t / kappa_t may be non-zero: the LES model has run or they were
+  // uploaded.  Until then (they start at zero, for/flow.f90:49-50) a substep
+  // without the model has no eddy terms and takes the spectral CN solve.
+  bool eddy_live = false;
+  bool graph_eddy[2] = {false, false};   // eddy_live when each step graph was captured
 };
+
+static void drop_graphs(db_ctx* c);
 
 static std::string g_init_err;
 
@@ -262,9 +269,11 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
   s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
   s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
   s.phi_g = sp[9]; s.pfac = sp[10];
-  if (!p->precision)   // the FP64 z-pass runs as three stages through this scratch
+  if (!p->precision && p->use_les)   // the FP64 LES z-pass runs as three stages through this scratch
     for (int i = 0; i < 8; ++i)
       if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  for (int i = 0; i < 4; ++i)   // cr of the spectral CN solve
+    if ((rc = dalloc(c, &s.crs[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   const size_t eP = phys_elem(c), eH = xh_elem(c);
   for (int i = 0; i < 8; ++i)
     if ((rc = balloc(c, (void**)&s.xh[i], H * eH))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
@@ -280,6 +289,10 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
     for (int i = 0; i < 21; ++i)
       if ((rc = balloc(c, (void**)lf[i], Pn * eP))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = dalloc(c, &s.ghost, 16 * (size_t)g.sp))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if ((rc = dalloc(c, &s.umean, 4 * (size_t)np))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    // the mixed path's FP64 x-pass of the solve's increments writes its
+    // x-half field over one physical FP64 field of the solve scratch
+    if (p->precision && 2 * g.kxs > Nx) { db_finalize(c); g_init_err = "db_init: Nx too small for the mixed LES path"; return DB_ERR_ARG; }
     if ((rc = dalloc(c, &s.tscr, 8 * Pn))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
     if ((rc = balloc(c, (void**)&s.sgs_feat, Pn * 16 * sizeof(float))) ||
         (rc = balloc(c, (void**)&s.sgs_out, Pn * 2 * sizeof(float)))) {
@@ -639,6 +652,10 @@ extern "C" int db_upload_field(db_ctx* c, int field, const double* host) {
   if (field == DB_NU_T || field == DB_KAPPA_T) {
     double* d = les_field(c, field);
     if (!d) return fail(c, DB_ERR_STATE, "nu_t / kappa_t exist only with use_les");
+    // a substep without the model now has eddy terms: drop the step graph
+    // captured with the spectral CN solve
+    if (!c->eddy_live) drop_graphs(c);
+    c->eddy_live = true;
     return phys_upload(c, host, d);
   }
   return fail(c, DB_ERR_ARG, "bad field id");
@@ -759,6 +776,7 @@ static LesFeatSrc les_feat_src(const db_ctx* c) {
   f.ny = c->g.ny;
   f.dxs = c->ph.dx * BETA_SGS;
   f.dzs = c->ph.dz * BETA_SGS;
+  f.mean = s.pmean;
   return f;
 }
 
@@ -767,12 +785,27 @@ static bool les_active(const db_ctx* c, int time_step) {
   return c->p.use_les && (!c->p.create_new_flow || time_step > 100);
 }
 
+// the plane-mean split of the physical fields holds for the kernels of one
+// substep only
+struct MeanSplit {
+  State& s;
+  MeanSplit(State& s_, bool on) : s(s_) { s.pmean = on ? s.umean : nullptr; }
+  ~MeanSplit() { s.pmean = nullptr; }
+};
+
 static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   const Geom& g = c->g;
   State& s = c->s;
   cudaStream_t st = c->st;
   cudaError_t e;
   long long n = 0;
+  // mixed path with LES: the physical fields hold fluctuations about their
+  // plane means (FP64), which the closure walk, the features and the
+  // eddy-viscosity solves add back
+  const MeanSplit split(s, les && g.prec != 0);
+  if (les) c->eddy_live = true;
+  // without eddy terms the CN matrices are the same in every column
+  const bool spectral = !c->p.use_les || (!les && !c->eddy_live);
   mark(c, rk, 0);
   if (les) {
     // les_chan / les_chan_th: ghost rows, then the state and its x and z
@@ -780,7 +813,7 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
     if ((e = launch_les_bc(g, c->ph, s, st))) return e;
     if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3, s.cth, s.cu1, s.cu2, s.cu3, s.cth),
                           fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]), 8, st,
-                          0xF0u, s.ghost))) return e;
+                          0xF0u, s.ghost, s.pmean ? s.umean : nullptr))) return e;
     mark(c, rk, 1);
     FieldSet in = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[0], s.xh[1], s.xh[2], s.xh[3]);
     FieldSet out = fset(s.u1, s.u2, s.u3, s.th, s.gx[0], s.gx[1], s.gx[2], s.gx[3]);
@@ -803,46 +836,78 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
     if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.u1, s.u2, s.u3, s.th), 4, st))) return e;
     mark(c, rk, 2);
   }
-  // nonlinear products (+ SGS forcing) + x-FFT, then z-FFT + spectral RHS +
-  // inverse z of cr
+  // nonlinear products (+ SGS forcing) + x-FFT
   if ((e = launch_products(g, s, st, les))) return e;
   mark(c, rk, 3);
-  const double2* ov = les ? s.ghost : nullptr;   // ghost rows the transforms saw
-  // the CN rows first: the mixed path without LES forms the increment
-  // system's right-hand side from them in the z-pass
-  if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
-  const bool qform = c->p.precision != 0 && !c->p.use_les;
-  if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov, qform))) return e;
-  mark(c, rk, 4);
-  // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
-  if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
-  mark(c, rk, 5);
-  // implicit CN solves (solver.f90:1012-1233); the mixed path's solves
-  // store the new physical u only where the CFL below reads it
   const bool cfl_step = rk == 2 && c->p.variable_dt;
-  if (c->p.use_les) {   // eddy terms whether or not the model ran this step
-    if ((e = launch_thomas_les(g, s, rk, st, cfl_step))) return e;
+  if (spectral) {
+    // without eddy viscosity the CN matrices are the same in every column:
+    // z-FFT + spectral RHS into cr (FP64), the CN solves on the retained
+    // modes in spectral space (k_thomas_spec), no transforms of cr or u
+    if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
+    if ((e = launch_zpass_spec(g, c->ph, s, rk, st))) return e;
+    mark(c, rk, 4);
+    mark(c, rk, 5);
+    if ((e = launch_thomas_spec(g, s, st))) return e;
+    mark(c, rk, 6);
+    n += 3;
+    // CFL on the last substep from the new velocity before the projection
+    // (solver.f90:1241-1244): u1..u3 to physical space for it
+    if (cfl_step) {
+      if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3), fset(s.xh[0], s.xh[1], s.xh[2]), 3, st))) return e;
+      if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2]), fset(s.u1, s.u2, s.u3), 3, st))) return e;
+      CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
+      if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
+      n += 4;
+    }
+    mark(c, rk, 7);
+    mark(c, rk, 8);
   } else {
-    if ((e = launch_thomas(g, s, st, cfl_step))) return e;
+    // z-FFT + spectral RHS + inverse z of cr
+    const double2* ov = les ? s.ghost : nullptr;   // ghost rows the transforms saw
+    if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
+    if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov))) return e;
+    mark(c, rk, 4);
+    // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
+    if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[4], s.xh[2], s.xh[6]), fset(s.r1, s.r2, s.r3, s.rth), 4, st))) return e;
+    mark(c, rk, 5);
+    // implicit CN solves with the eddy terms (solver.f90:1012-1233); the
+    // mixed path's solves store the new physical u only where the CFL below
+    // reads it
+    if ((e = launch_thomas_les(g, s, rk, st, cfl_step))) return e;
+    mark(c, rk, 6);
+    n += 7;
+    // CFL on the last substep (solver.f90:1241-1244)
+    if (cfl_step) {
+      CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
+      if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
+      n += 2;
+    }
+    mark(c, rk, 7);
+    // back to Fourier space (solver.f90:1247-1252) and projection
+    if (c->p.precision != 0) {
+      // mixed path: the solve left u's increment in FP64; transform it in
+      // FP64 and add it to the state the substep started from (an FP32
+      // increment's rounding is not divergence free, and the projection
+      // would carry it into cp amplified by 1 / h_bar)
+      double* dinc[4];
+      double2* dxh[4];
+      thomas_les_inc(g, s, dinc, dxh);
+      Geom g64 = g;
+      g64.prec = 0;
+      if ((e = launch_fwd_x(g64, fset(dinc[0], dinc[1], dinc[2], dinc[3]), fset(dxh[0], dxh[1], dxh[2], dxh[3]), 4,
+                            st))) return e;
+      mark(c, rk, 8);
+      if ((e = launch_fwd_z(g64, fset(dxh[0], dxh[1], dxh[2], dxh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st, 1,
+                            ov))) return e;
+    } else {
+      if ((e = launch_fwd_x(g, fset(s.u1, s.u2, s.u3, s.th), fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st)))
+        return e;
+      mark(c, rk, 8);
+      if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st, 0,
+                            ov))) return e;
+    }
   }
-  mark(c, rk, 6);
-  n += 7;
-  // CFL on the last substep (solver.f90:1241-1244)
-  if (cfl_step) {
-    CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
-    if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
-    n += 2;
-  }
-  mark(c, rk, 7);
-  // back to Fourier space (solver.f90:1247-1252) and projection
-  // mixed path: the solve left u's increment in r; transform it and add it
-  // to the state the substep started from
-  const bool inc = c->p.precision != 0;
-  const FieldSet src = inc ? fset(s.r1, s.r2, s.r3, s.rth) : fset(s.u1, s.u2, s.u3, s.th);
-  if ((e = launch_fwd_x(g, src, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), 4, st))) return e;
-  mark(c, rk, 8);
-  if ((e = launch_fwd_z(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]), fset(s.cu1, s.cu2, s.cu3, s.cth), 4, st,
-                        inc ? 1 : 0, ov))) return e;
   mark(c, rk, 9);
   if ((e = launch_rem_div(g, s, rk, 1, st))) return e;
   if (rk == 2 && c->p.variable_dt) {
@@ -886,6 +951,10 @@ extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
   for (int i = 0; i < nsteps; ++i) {
     // time_step is incremented at the start of the step (diablo.f90:58-61)
     const int m = les_active(c, c->time_step + 1) ? 1 : 0;
+    if (c->graph[m] && c->graph_eddy[m] != c->eddy_live) {   // captured for the other CN path
+      cudaGraphExecDestroy(c->graph[m]);
+      c->graph[m] = nullptr;
+    }
     if (!c->graph[m]) {
       cudaGraph_t gr;
       const long long before = c->launches;
@@ -900,6 +969,7 @@ extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
       }
       e = cudaGraphInstantiate(&c->graph[m], gr, 0);
       cudaGraphDestroy(gr);
+      c->graph_eddy[m] = c->eddy_live;
       if (e != cudaSuccess) {
         c->graph[m] = nullptr;
         c->err = std::string("graph instantiate failed: ") + cudaGetErrorString(e);
@@ -925,6 +995,7 @@ struct db_ensemble {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [LES model active]
   std::vector<cudaEvent_t> ev;                     // fork event + one join event per member
   long long kernels[2] = {0, 0};
+  bool graph_eddy[2] = {false, false};             // eddy terms when each graph was captured
   std::string err;
 };
 
@@ -995,6 +1066,12 @@ extern "C" int db_ensemble_steps(db_ensemble* e, int nsteps) {
   const int n = (int)e->members.size();
   for (int it = 0; it < nsteps; ++it) {
     const int m = les_active(c0, c0->time_step + 1) ? 1 : 0;
+    bool eddy = false;   // some member's substeps carry eddy terms
+    for (db_ctx* c : e->members) eddy = eddy || c->eddy_live;
+    if (e->graph[m] && e->graph_eddy[m] != eddy) {   // captured for the other CN path
+      cudaGraphExecDestroy(e->graph[m]);
+      e->graph[m] = nullptr;
+    }
     if (!e->graph[m]) {
       cudaGraph_t gr;
       if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
@@ -1026,6 +1103,9 @@ extern "C" int db_ensemble_steps(db_ensemble* e, int nsteps) {
         return DB_ERR_CUDA;
       }
       e->kernels[m] = k0;
+      eddy = false;
+      for (db_ctx* c : e->members) eddy = eddy || c->eddy_live;
+      e->graph_eddy[m] = eddy;
     }
     if (cudaGraphLaunch(e->graph[m], e->st) != cudaSuccess) {
       e->err = "ensemble graph launch failed";

@@ -54,9 +54,11 @@ cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, int accumulate = 0,
                          const double2* ghost = nullptr);
 // ghost (optional): rows 0, 1, Nyp, Nyp+1 of field f are read from
-// ghost + (4 (f % 4) + q) sp instead (q = 0..3 for those rows)
+// ghost + (4 (f % 4) + q) sp instead (q = 0..3 for those rows);
+// mean (optional): fields 0..3 leave their plane mean ((0,0) mode) out of the
+// transform and store it in mean[f np + j] (FP64)
 cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0,
-                         const double2* ghost = nullptr);
+                         const double2* ghost = nullptr, double* mean = nullptr);
 
 // Tridiagonal row description of one implicit equation (one per row j of
 // 0..Nyp+1): coefficients l, d, u; is_bc marks rows whose right-hand side
@@ -66,15 +68,10 @@ struct TriRow {
   double ap;      // forward-eliminated multiplier a'_j (Thomas)
   double ibp;     // 1 / b'_j
   double cn_lo, cn_hi;  // explicit CN: term = cn_hi*(u_{j+1}-u_j) - cn_lo*(u_j-u_{j-1})
-  double pa;      // prod of a'_i from the start of j's chunk to j (forward carry weight)
-  double pm;      // prod of m_i = -u_i / b'_i from j to the end of its chunk (backward)
   // eddy-viscosity metric factors of the row (LES): the lower / upper
   // coupling is nu_lo * ef_lo, nu_hi * ef_hi (per-column nu), with
   // ef = 1/(dy dyf) at the neighbouring GY / GYF spacing
   double ef_lo, ef_hi;
-  // weight of the chunk's carry-in g in the zero-carry backward sweep:
-  // qa_j = pa_j / b'_j + m_j qa_{j+1}, zero past the chunk's end
-  double qa;
   int is_bc, interior;
 };
 
@@ -109,21 +106,6 @@ struct ProdY {
   }
 };
 
-// row chunks of the tiled Thomas solve (k_thomas): nch <= THOMAS_MAXCH
-// chunks of len rows
-constexpr int THOMAS_MAXCH = 16;
-struct Chunks {
-  int nch, len;
-};
-__host__ __device__ inline Chunks thomas_chunks(int np) {
-  Chunks c;
-  c.nch = np / 2 < THOMAS_MAXCH ? np / 2 : THOMAS_MAXCH;
-  if (c.nch < 1) c.nch = 1;
-  c.len = (np + c.nch - 1) / c.nch;
-  c.nch = (np + c.len - 1) / c.len;
-  return c;
-}
-
 // Pointers of the full device state for the substep kernels.  Physical and
 // x-half fields are typed double / double2 here; with Geom::prec = 1 they
 // hold float / float2 and the kernels cast them to their work type.
@@ -135,6 +117,7 @@ struct State {
   double *r1, *r2, *r3, *rth;                // physical RHS
   double2* phi_g;                            // rem_div forward-sweep scratch (spectral)
   double2* nls[8];                           // z-pass scratch of the FP64 path: Z(N_e), Z(M_e), then cr_e (spectral)
+  double2* crs[4];                           // cr of u1, u3, u2, th (spectral FP64) for the spectral CN solve (no LES)
   double2* pfac;                             // rem_div factors (a', 1/b') per (kx,kz,j)
   TriRow* tri;                               // 4 equations x np rows (th, u2, u1, u3)
   DevScalars* sc;
@@ -151,20 +134,40 @@ struct State {
   float* sgs_feat;
   float* sgs_out;
   const float* sgs_range;
+  // plane means of u1, u2, u3, th ([f][j], FP64) when the physical fields of
+  // this substep hold fluctuations about them (mixed path with LES), else null
+  double* umean;                             // the table (allocated with LES)
+  const double* pmean;                       // umean while the split is in effect
 };
+
+// a physical field value with its plane mean added back (pmean non-null):
+// the single rounding every consumer of the split fields shares
+template <typename R>
+__device__ __forceinline__ R with_mean(R v, const double* pmean, int f, int np, int j) {
+  return pmean ? v + (R)pmean[(long long)f * np + j] : v;
+}
+
+// (a - b) * id for the values a, b of field f at rows ja, jb: with split
+// fields the difference of the fluctuations plus that of the FP64 means, so
+// a large mean (the stratification in th) adds no rounding noise to a
+// y-derivative; one explicit fma, so every call site rounds alike
+template <typename R>
+__device__ __forceinline__ R ydiff(R a, R b, const double* pmean, int f, int np, int ja, int jb, double id) {
+  const R dm = pmean ? (R)((pmean[(long long)f * np + ja] - pmean[(long long)f * np + jb]) * id) : (R)0;
+  return fma(a - b, (R)id, dm);
+}
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
 int sm_count();   // SMs of the current device (cached)
 cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool les = false);
-// ghost: the LES overlay, when the inverse transforms of this substep used it;
-// qform (mixed path without LES): write the increment system's right-hand
-// side on every plane, the CN rows (launch_tri_coef) already formed
+// ghost: the LES overlay, when the inverse transforms of this substep used it
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
-                             const double2* ghost = nullptr, bool qform = false);
+                             const double2* ghost = nullptr);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
-// keep_u: also store the new physical u on the mixed path (the CFL of the
-// third substep reads it); the FP64 path always stores it
-cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st, bool keep_u);
+// the substep without LES: forward z-pass of the products + spectral RHS
+// into s.crs (FP64), then the CN solves in spectral space on the state
+cudaError_t launch_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
+cudaError_t launch_thomas_spec(const Geom& g, const State& s, cudaStream_t st);
 
 struct CflCtl {
   double cfl, time_limit;
@@ -193,5 +196,8 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
 // mode 0: AMD; 1: closure features only; 2: closure nu_t, kappa_t with AMD fallback
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode = 0);
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st, bool keep_u);
+// mixed path: the LES solve's FP64 increments (u1, u2, u3, th) and the
+// FP64 x-half scratch beside them (k_les.cu)
+void thomas_les_inc(const Geom& g, const State& s, double* inc[4], double2* xh64[4]);
 
 }  // namespace db

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(const __grid_constant_
 // Xh -> packed spectral (FP64), scaled by 1/Nz; sequence = one kx column of a plane.
 // accumulate: out = base + transform, base = out itself, or for rows 0, 1,
 // Nyp, Nyp+1 the ghost overlay (field f % 4) when one is given
-template <int N, typename R>
+template <int N, typename R, bool ACC>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int accumulate,
                                                           const double2* __restrict__ ghost) {
   using C = typename CplxOf<R>::type;
@@ -136,11 +136,10 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
   double2* dst = (double2*)out.p[f] + (long long)j * g.sp + kx;
-  // accumulate (FP32 work type only): the FP64 values the transform adds
-  // to are loaded before the transform, so their latency hides behind it
-  constexpr bool ACC = sizeof(R) == sizeof(float);
+  // ACC: the FP64 values the transform adds to are loaded before the
+  // transform, so their latency hides behind it
   double2 bv[ACC ? E : 1];
-  if (ACC && accumulate) {
+  if (ACC) {
     const double2* base = dst;
     if (ghost) {
       const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
@@ -162,17 +161,22 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
     if (kzp >= 0) {
       double2 w = cscale(to_d2(v[q]), s);
-      if (ACC && accumulate) w = cadd(bv[ACC ? q : 0], w);
+      if (ACC) w = cadd(bv[ACC ? q : 0], w);
       dst[(long long)kzp * g.kxs] = w;
     }
   }
 }
 
 // packed spectral (FP64) -> Xh (zero-filled de-aliased rows, unnormalised);
-// fields f with bit f of dmask set are differentiated in z (times i kz)
+// fields f with bit f of dmask set are differentiated in z (times i kz).
+// mean (optional): the (0,0) mode of fields 0..3, i.e. the plane mean of
+// the physical field, goes to mean[f np + j] in FP64 and is left out of the
+// transform, so the physical field holds the fluctuation about the mean
+// and its FP32 rounding scales with the fluctuation (the consumers add the
+// mean back)
 template <int N, typename R>
 __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, unsigned dmask,
-                                                          const double2* __restrict__ ghost) {
+                                                          const double2* __restrict__ ghost, double* __restrict__ mean) {
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -197,6 +201,10 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant_
     const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
     double2 a = (active && kzp >= 0) ? __ldg(src + (long long)kzp * g.kxs) : make_double2(0.0, 0.0);
     if (dz && kzp >= 0) a = cmul_i(a, g.kz[kzp]);
+    if (mean && f < 4 && kx == 0 && z == 0) {
+      mean[(long long)f * g.np + j] = a.x;
+      a = make_double2(0.0, 0.0);
+    }
     v[q] = from_d2<C>(a);
   }
   fft_reg_lazy<N, +1, true>(v, lane, active, sq, twt);
@@ -451,17 +459,24 @@ static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc
   using C = typename CplxOf<R>::type;
   const int ns = zpass_ns<N>(g);
   size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
-  smem_attr(k_fwd_z<N, R>, smem);
-  k_fwd_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, acc, ghost);
+  const dim3 grid((g.kxs + ns - 1) / ns, g.np, nf);
+  if (acc) {
+    smem_attr(k_fwd_z<N, R, true>, smem);
+    k_fwd_z<N, R, true><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 1, ghost);
+  } else {
+    smem_attr(k_fwd_z<N, R, false>, smem);
+    k_fwd_z<N, R, false><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 0, ghost);
+  }
 }
 template <int N, typename R>
 static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
-                       cudaStream_t st) {
+                       double* mean, cudaStream_t st) {
   using C = typename CplxOf<R>::type;
   const int ns = zpass_ns<N>(g);
   size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
   smem_attr(k_inv_z<N, R>, smem);
-  k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost);
+  k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost,
+                                                                                          mean);
 }
 template <int N>
 static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
@@ -481,9 +496,9 @@ static void go_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, 
 }
 template <int N>
 static void go_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, unsigned dmask, const double2* ghost,
-                     cudaStream_t st) {
-  if (g.prec) go_inv_z_t<N, float>(g, in, out, nf, dmask, ghost, st);
-  else go_inv_z_t<N, double>(g, in, out, nf, dmask, ghost, st);
+                     double* mean, cudaStream_t st) {
+  if (g.prec) go_inv_z_t<N, float>(g, in, out, nf, dmask, ghost, mean, st);
+  else go_inv_z_t<N, double>(g, in, out, nf, dmask, ghost, mean, st);
 }
 
 cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
@@ -503,9 +518,9 @@ cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
   return cudaGetLastError();
 }
 cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask,
-                         const double2* ghost) {
+                         const double2* ghost, double* mean) {
   if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
-  DB_DISPATCH_N(g.nz, go_inv_z, g, in, out, nf, dmask, ghost, st);
+  DB_DISPATCH_N(g.nz, go_inv_z, g, in, out, nf, dmask, ghost, mean, st);
   return cudaGetLastError();
 }
 

@@ -192,13 +192,21 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
   R hnu = 0, hka = 0;     // closure values at the previous GY row
   bool hval = false;
 
-  // row j0: GYF values only (GY row 0 does not exist)
+  // row j0: GYF values only (GY row 0 does not exist); with_mean: the
+  // plane means when the fields hold fluctuations (mixed path)
+  // (the products take the full values, the y-differences (ydiff) the
+  // fluctuations, suffix _f, and the differences of the means)
   const long long o0 = (long long)j0 * pp;
-  R u1m = __ldg(u1 + o0), u3m = __ldg(u3 + o0), thm = __ldg(th + o0), u2c = __ldg(u2 + o0 + pp);
+  const double* pm = (sizeof(R) == sizeof(float)) ? s.pmean : nullptr;   // the split is a mixed-path form
+  const int np = g.np;
+  R u1m_f = __ldg(u1 + o0), u3m_f = __ldg(u3 + o0), thm_f = __ldg(th + o0), u2c_f = __ldg(u2 + o0 + pp);
+  R u1m = with_mean(u1m_f, pm, 0, np, j0), u3m = with_mean(u3m_f, pm, 2, np, j0);
+  R thm = with_mean(thm_f, pm, 3, np, j0), u2c = with_mean(u2c_f, pm, 1, np, j0 + 1);
   R f1x = __ldg(g1x + o0), f3z = __ldg(g3z + o0), f1z = __ldg(g1z + o0), f3x = __ldg(g3x + o0);
   R ftx = __ldg(gtx + o0), ftz = __ldg(gtz + o0);
-  R u2m1 = __ldg(u2 + o0);
-  R f2y = (u2c - u2m1) * (R)LR[j0].idyf;
+  const R u2m1_f = __ldg(u2 + o0);
+  R u2m1 = with_mean(u2m1_f, pm, 1, np, j0);
+  R f2y = ydiff<R>(u2c_f, u2m1_f, pm, 1, np, j0 + 1, j0, LR[j0].idyf);
   // rows j - 2 of u1, u3, th and u2 (the products of plane j - 1)
   R u1mm = u1m, u3mm = u3m, thmm = thm, u2m2 = u2m1;
   // previous GY row (r = j - 1) values
@@ -237,14 +245,18 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     issue(j + AMD_SLOTS - 1);
     cp_async_wait<AMD_SLOTS - 1>();
     const R* sl = ring + (j % AMD_SLOTS) * 12 * tb + tx;
-    const R u1j = sl[0], u3j = sl[tb], thj = sl[2 * tb];
-    const R u2n = sl[3 * tb];
+    const R u1j_f = sl[0], u3j_f = sl[tb], thj_f = sl[2 * tb], u2n_f = sl[3 * tb];
+    const R u1j = with_mean(u1j_f, pm, 0, np, j), u3j = with_mean(u3j_f, pm, 2, np, j);
+    const R thj = with_mean(thj_f, pm, 3, np, j);
+    const bool top = j + 1 > Nyp + 1;   // u2 above the top ghost plane (zero, no mean)
+    const R u2n = top ? u2n_f : with_mean(u2n_f, pm, 1, np, j + 1);
     const R a1x = sl[4 * tb], a2x = sl[5 * tb], a3x = sl[6 * tb], atx = sl[7 * tb];
     const R a1z = sl[8 * tb], a2z = sl[9 * tb], a3z = sl[10 * tb], atz = sl[11 * tb];
     const LesRow lr = LR[j];
-    const R idy = (R)lr.idy;
     // GY row j: y-derivatives and the tensors that live there
-    const R d1y = (u1j - u1m) * idy, d3y = (u3j - u3m) * idy, dty = (thj - thm) * idy;
+    const R d1y = ydiff<R>(u1j_f, u1m_f, pm, 0, np, j, j - 1, lr.idy);
+    const R d3y = ydiff<R>(u3j_f, u3m_f, pm, 2, np, j, j - 1, lr.idy);
+    const R dty = ydiff<R>(thj_f, thm_f, pm, 3, np, j, j - 1, lr.idy);
     const R dly = (R)lr.dys_y;
     const R ryx = (R)lr.ryx, rxy = (R)lr.rxy, rzy = (R)lr.rzy, ryz = (R)lr.ryz;
     const R SI4 = h * (d1y * ryx + a2x * rxy);
@@ -253,7 +265,7 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     const R O6 = h * (a2z * rzy - d3y * ryz);
     const R S4 = h * (d1y + a2x), S6 = h * (a2z + d3y);
     // GYF row j (d u2/dy there needs u2 at j + 1; row Nyp + 1 is unused)
-    const R c2y = (j <= Nyp) ? (u2n - u2c) * (R)lr.idyf : (R)0;
+    const R c2y = (j <= Nyp) ? ydiff<R>(u2n_f, u2c_f, pm, 1, np, j + 1, j, lr.idyf) : (R)0;
     const R delt = (R)lr.dgy;
     R temp = 0, temp_th = 0;
     R nu_m = 0, ka_m = 0;
@@ -279,6 +291,7 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     }
     if (MODE == 1) {
       u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
+      u1m_f = u1j_f; u3m_f = u3j_f; thm_f = thj_f; u2c_f = u2n_f;
       f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
       continue;
     }
@@ -364,6 +377,7 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
     u1mm = u1m; u3mm = u3m; thmm = thm; u2m2 = u2m1; u2m1 = u2c;
     hL5 = L5; hL6 = L6;
     u1m = u1j; u3m = u3j; thm = thj; u2c = u2n;
+    u1m_f = u1j_f; u3m_f = u3j_f; thm_f = thj_f; u2c_f = u2n_f;
     f1x = a1x; f3z = a3z; f1z = a1z; f3x = a3x; ftx = atx; ftz = atz; f2y = c2y;
     h1y = d1y; h3y = d3y; hty = dty; h2x = a2x; h2z = a2z;
     hSI4 = SI4; hSI6 = SI6; hO4 = O4; hO6 = O6; hP4 = P4; hP6 = P6; hdl = delt;
@@ -379,8 +393,10 @@ __global__ void __launch_bounds__(128, 3) k_les_amd(const __grid_constant__ Stat
 // to an FP64 scratch (2 fields per equation) and come back in the backward
 // sweep.  Rows are handled in batches of TB whose loads are all issued
 // first, so each thread keeps 3 TB loads in flight instead of waiting on
-// every row.  On the mixed path r receives the increment and u itself is
-// written only when keep_u (the third substep's CFL reads it).
+// every row.  On the mixed path the increment u_new - u goes out in FP64
+// over the g / b' scratch of its equation (launch_thomas_les_inc gives the
+// layout), and u itself is written only when keep_u (the third substep's
+// CFL reads it).
 constexpr int TB = 8;
 
 template <typename R>
@@ -400,7 +416,13 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
     const R* nv = (const R*)((eq == 0) ? s.kappa_t : s.nu_t) + col;
     const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
     const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    double um = 0.0, uc = (double)u[0], nm = 0.0, nc = (double)nv[0];
+    // plane means of the old u when the fields hold fluctuations (mixed
+    // path), added in FP64: the explicit and implicit terms then see the
+    // FP32 rounding of the fluctuation only
+    const double* pm = s.pmean ? s.pmean + (long long)((eq == 0) ? 3 : (eq == 1 ? 1 : (eq == 2 ? 0 : 2))) * np
+                               : nullptr;
+    auto old_u = [&](int j) { return (double)u[(long long)j * pp] + (pm ? pm[j] : 0.0); };
+    double um = 0.0, uc = old_u(0), nm = 0.0, nc = (double)nv[0];
     double ibprev = 1.0, gprev = 0.0, uprev = 0.0;
     for (int jb = 0; jb < np; jb += TB) {
       double xr[TB], xu[TB], xn[TB];
@@ -408,7 +430,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
       for (int c = 0; c < TB; ++c) {
         const int j = jb + c;
         xr[c] = (j < np) ? (double)r[(long long)j * pp] : 0.0;
-        xu[c] = (j + 1 < np) ? (double)u[(long long)(j + 1) * pp] : 0.0;
+        xu[c] = (j + 1 < np) ? old_u(j + 1) : 0.0;
         xn[c] = (j + 1 < np) ? (double)nv[(long long)(j + 1) * pp] : 0.0;
       }
 #pragma unroll
@@ -450,7 +472,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
         const int j = jt - c;
         xc[c] = (j >= 0) ? cmv[(long long)j * pp] : 0.0;
         xg[c] = (j >= 0) ? gsv[(long long)j * pp] : 0.0;
-        xo[c] = (INC && j >= 0) ? (double)u[(long long)j * pp] : 0.0;
+        xo[c] = (INC && j >= 0) ? old_u(j) : 0.0;
       }
 #pragma unroll
       for (int c = 0; c < TB; ++c) {
@@ -459,7 +481,8 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
         const double xv = xg[c] - xc[c] * xnext;
         const bool stored = (j >= lo && j <= hi);
         if (stored && (!INC || keep_u)) u[(long long)j * pp] = (R)xv;
-        if (INC) r[(long long)j * pp] = stored ? (R)(xv - xo[c]) : (R)0;   // increment for the transform
+        // increment for the FP64 forward transforms, over g_j / b'_j (read above)
+        if (INC) gsv[(long long)j * pp] = stored ? xv - xo[c] : 0.0;
         xnext = xv;
       }
     }
@@ -493,6 +516,17 @@ cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaSt
     else k_les_amd<double, 0><<<grid, bx, smem, st>>>(s, g, ph);
   }
   return cudaGetLastError();
+}
+// where the mixed path's LES solve leaves its FP64 increments (physical,
+// fields u1, u2, u3, th) and the FP64 x-half scratch their forward x-pass
+// can use (the other half of each equation's solve scratch)
+void thomas_les_inc(const Geom& g, const State& s, double* inc[4], double2* xh64[4]) {
+  const int eq_of[4] = {2, 1, 3, 0};   // u1, u2, u3, th -> th, u2, u1, u3 order
+  const long long f = (long long)g.np * g.pp;
+  for (int i = 0; i < 4; ++i) {
+    inc[i] = s.tscr + (2 * eq_of[i] + 1) * f;
+    xh64[i] = reinterpret_cast<double2*>(s.tscr + 2 * eq_of[i] * f);
+  }
 }
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st, bool keep_u) {
   const int want = (g.tune_les_tb > 0 && g.tune_les_tb <= 128) ? g.tune_les_tb : 128;   // powers of two

@@ -1,24 +1,28 @@
 // k_substep.cu -- the RKW3 + Crank-Nicolson substep (rk_chan_1,
-// for/solver.f90:366-1273) as fused B200 kernels, FP64.
+// for/solver.f90:366-1273) as fused B200 kernels; arithmetic in FP64, or
+// FP32 transforms and products on the mixed path.
 //
-//  k_products   : 11 nonlinear products of u1,u2,u3,th in physical space
-//                 (solver.f90:655-815, 914-956) fused with their forward
-//                 x-FFTs; x-derivatives (i kx) applied in the x-half space so
-//                 only 8 x-half fields leave the kernel.
-//  k_zpass_rhs  : forward z-FFT of those 8 fields, the spectral linear terms
-//                 (viscous, Coriolis, buoyancy, background-front advection,
-//                 thermal-wind advection: solver.f90:396-609, 35-111), the RK
-//                 combination cr = cu + zeta h cf_old - h grad p + beta h cf
-//                 (solver.f90:396-456, 824-838, 966-973), and the inverse
-//                 z-FFT of cr.
-//  k_tri_coef   : the four implicit systems' rows incl. BC rows
-//                 (solver.f90:1012-1233, 1901-2324), LU-factored once per
-//                 substep (all (x,z) columns share them without LES).
-//  k_thomas     : per (x,z) column, explicit CN term + Thomas sweeps for
-//                 th, u2, u1, u3 (solver.f90:850-870, 981-989, 1691-1852).
-//  k_rem_div    : per (kx,kz) column, divergence, complex Thomas, projection
-//                 and pressure update (solver.f90:1302-1379, 1261-1267).
-//  k_courant    : CFL reduction and dt scheduling (flow.f90:746-857).
+//  k_products    : 11 nonlinear products of u1,u2,u3,th in physical space
+//                  (solver.f90:655-815, 914-956) fused with their forward
+//                  x-FFTs; x-derivatives (i kx) applied in the x-half space so
+//                  only 8 x-half fields leave the kernel.
+//  k_zpass_rhs   : forward z-FFT of those 8 fields, the spectral linear terms
+//                  (viscous, Coriolis, buoyancy, background-front advection,
+//                  thermal-wind advection: solver.f90:396-609, 35-111) and the
+//                  RK combination cr = cu + zeta h cf_old - h grad p + beta h cf
+//                  (solver.f90:396-456, 824-838, 966-973); cr goes out as an
+//                  FP64 spectral field (no LES) or through the inverse z-FFT
+//                  to the physical solve (LES).
+//  k_tri_coef    : the four implicit systems' rows incl. BC rows
+//                  (solver.f90:1012-1233, 1901-2324), LU-factored once per
+//                  substep (all (x,z) columns share them without LES).
+//  k_thomas_spec : without LES, the CN solves of th, u2, u1, u3 per retained
+//                  Fourier mode (explicit CN term + Thomas sweeps,
+//                  solver.f90:850-870, 981-989, 1691-1852), FP64.
+//  k_rem_div     : per (kx,kz) column, divergence, complex Thomas, projection
+//                  and pressure update (solver.f90:1302-1379, 1261-1267).
+//  k_courant     : CFL reduction and dt scheduling (flow.f90:746-857).
+// The CN solves with eddy viscosity (one matrix per column) are in k_les.cu.
 #include <math.h>
 
 #include "../../include/diablo_b200.h"
@@ -471,52 +475,20 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
   return cr;
 }
 
-// Right-hand side of the implicit system written for the increment
-// D = u_new - u (mixed path without LES): with the CN rows
-// l u_{j-1} + d u_j + uu u_{j+1} = b_j of `row` (k_tri_coef), D solves the
-// same rows with b_j - (A u)_j, which for a solved row is
-//   (cr - cu) + 2 (cn_hi (u_{j+1} - u_j) - cn_lo (u_j - u_{j-1}))
-// (the reference's explicit CN half, solver.f90:850-870, 981-989, plus the
-// implicit half of the old state) and for a BC row the BC value (the (0,0)
-// mode only: it is constant over x and z) minus the BC row applied to the
-// old state.  Both are formed here in FP64 from the spectral state, so the
-// FP32 transform carries a substep's change only and the solve never
-// differentiates an FP32 field across rows: FP32 rounding of a large mean
-// (the stratification in th) amplified by 1/dy^2 no longer enters.
-__device__ __forceinline__ double2 inc_rhs(const State& s, const Geom& g, const TriRow& row, int e, int j, int kx,
-                                           int kzp, double2 cr_inc) {
-  const double2* cu = (e == 0) ? s.cu1 : (e == 1 ? s.cu3 : (e == 2 ? s.cu2 : s.cth));
-  const long long a = (long long)j * g.sp + (long long)kzp * g.kxs + kx;
-  const double2 Z = make_double2(0.0, 0.0);
-  const double2 c0 = cu[a];
-  const double2 cm = (j > 0) ? cu[a - g.sp] : Z;
-  const double2 cp = (j + 1 < g.np) ? cu[a + g.sp] : Z;
-  if (row.is_bc) {
-    const double b = (kx == 0 && kzp == 0) ? row.bc : 0.0;
-    return make_double2(b - (row.l * cm.x + row.d * c0.x + row.u * cp.x),
-                        -(row.l * cm.y + row.d * c0.y + row.u * cp.y));
-  }
-  const double hx = row.cn_hi * (cp.x - c0.x) - row.cn_lo * (c0.x - cm.x);
-  const double hy = row.cn_hi * (cp.y - c0.y) - row.cn_lo * (c0.y - cm.y);
-  return make_double2(cr_inc.x + 2.0 * hx, cr_inc.y + 2.0 * hy);
-}
-
-// the CN system (k_tri_coef order th, u2, u1, u3) of z-pass equation e
-// (0 u1, 1 u3, 2 u2, 3 th)
-__device__ __forceinline__ int tri_eq(int e) { return e == 0 ? 2 : (e == 1 ? 3 : (e == 2 ? 1 : 0)); }
-
 // z-pass of the nonlinear terms + spectral RHS + inverse z-pass of cr.
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
-template <int N, typename R, bool EFAST>
+// SPEC (the substep without LES, either work type): no inverse z-pass; cr
+// goes out in FP64 as a packed spectral field (s.crs[e]) for the CN solve
+// in spectral space (k_thomas_spec).
+template <int N, typename R, bool EFAST, bool SPEC = false>
 __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1))
-    k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost, int qform) {
+    k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost) {
   // FP32 work type: write the increment cr - base (base = the state as the
   // inverse transforms saw it), so FP32 rounding scales with the substep's
-  // change, not with the field; with qform (no LES) the whole right-hand
-  // side of the increment system (inc_rhs) on every plane, BC planes too
-  constexpr bool INC = sizeof(R) == sizeof(float);
+  // change, not with the field
+  constexpr bool INC = sizeof(R) == sizeof(float) && !SPEC;
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -552,29 +524,11 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
     const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
     C* xin_n = (C*)s.xh[2 * e];
     const C* xin_m = (const C*)s.xh[2 * e + 1];
-    const bool qf = INC && qform;
-    const TriRow* trow = s.tri + tri_eq(e) * g.np + j;
     if (!in_rng(j, jlo, jhi)) {
-      if (!qf) {
-        if (active)
-#pragma unroll
-          for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
-        return;
-      }
-      // a BC plane of the increment system: its right-hand side, to physical z
-      const TriRow row = *trow;
-      C vb[E];
-#pragma unroll
-      for (int q = 0; q < E; ++q) {
-        const int zz = lane + q * T;
-        const int kzp = (zz <= g.nkz) ? zz : (zz >= N - g.nkz ? zz - N + g.nkzp : -1);
-        vb[q] = (kzp < 0 || !active) ? mkc<C>(0, 0)
-                                     : from_d2<C>(inc_rhs(s, g, row, e, j, kxc, kzp, make_double2(0.0, 0.0)));
-      }
-      ZFFT(+1, vb);
+      if (SPEC) return;   // the spectral solve takes BC values on these planes
       if (active)
 #pragma unroll
-        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = vb[q];
+        for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
       return;
     }
     C vn[E];
@@ -603,9 +557,13 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       const double2 zmq = to_d2(sm_z[pidx(zz)]), zn = to_d2(vn[q]);
       const double2 nl = make_double2((zn.x - kzv * zmq.y) * inz, (zn.y + kzv * zmq.x) * inz);
       double2 cr = rhs_point<INC>(s, g, ph, rk, e, j, kxc, kzp, nl, ghost);
-      if (qf) cr = inc_rhs(s, g, *trow, e, j, kxc, kzp, cr);
+      if (SPEC) {
+        s.crs[e][(long long)j * g.sp + (long long)kzp * g.kxs + kxc] = (kxc <= g.nkx) ? cr : make_double2(0.0, 0.0);
+        continue;
+      }
       vn[q] = from_d2<C>(cr);
     }
+    if (SPEC) return;
     __syncthreads();
     ZFFT(+1, vn);
     if (active)
@@ -663,8 +621,8 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
   for (int j = threadIdx.x; j < np; j += blockDim.x) {
     TriRow r;
     r.l = 0.0; r.d = 1.0; r.u = 0.0; r.bc = 0.0; r.ap = 0.0; r.ibp = 1.0;
-    r.cn_lo = 0.0; r.cn_hi = 0.0; r.pa = 1.0; r.pm = 1.0; r.ef_lo = 0.0; r.ef_hi = 0.0;
-    r.is_bc = 1; r.interior = 0; r.qa = 0.0;
+    r.cn_lo = 0.0; r.cn_hi = 0.0; r.ef_lo = 0.0; r.ef_hi = 0.0;
+    r.is_bc = 1; r.interior = 0;
     if (j >= lo && j <= hi) {
       if (eq == 0) {  // solver.f90:1023-1026
         r.l = -(tth) / (dy[j] * dyf[j]);
@@ -755,224 +713,86 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
       bprev = b;
       uprev = Rs[j].u;
     }
-    // chunk carry weights of the two recurrences g_j = v_j + a'_j g_{j-1}
-    // and x_j = g_j / b'_j + m_j x_{j+1}, m_j = -u_j / b'_j
-    const Chunks ch = thomas_chunks(np);
-    for (int k = 0; k < ch.nch; ++k) {
-      const int j0 = k * ch.len, j1 = min(np, j0 + ch.len) - 1;
-      double pa = 1.0;
-      for (int j = j0; j <= j1; ++j) { pa *= Rs[j].ap; Rs[j].pa = pa; }
-      double pm = 1.0;
-      for (int j = j1; j >= j0; --j) { pm *= -Rs[j].u * Rs[j].ibp; Rs[j].pm = pm; }
-      double qa = 0.0;
-      for (int j = j1; j >= j0; --j) {
-        qa = Rs[j].pa * Rs[j].ibp + (j < j1 ? -Rs[j].u * Rs[j].ibp * qa : 0.0);
-        Rs[j].qa = qa;
-      }
-    }
   }
   __syncthreads();
   TriRow* R = tri + eq * np;
   for (int j = threadIdx.x; j < np; j += blockDim.x) R[j] = Rs[j];
 }
 
-// Implicit CN solves of th, u2, u1, u3 (solver.f90:1012-1233) for all (x,z)
-// columns.  One CTA = TX consecutive x columns at one z; half-warp k owns
-// row chunk k.  The shared LU factors (a'_j, 1/b'_j from k_tri_coef) turn
-// the Thomas sweeps into two first-order linear recurrences
-//   g_j = v_j + a'_j g_{j-1},   x_j = g_j / b'_j + m_j x_{j+1}.
-// Each half-warp runs both over its chunk with zero carries (y, then
-// z = B(y)), so by linearity  x_j = z_j + G_{k-1} qa_j + X_{k+1} pm_j  with
-// G_{k-1} = g at the end of the previous chunk, X_{k+1} = x at the start of
-// the next one and the per-row weights qa = B(pa), pm from k_tri_coef.  The
-// chunk end values (y at the end, z at the start) cross warps through
-// shared memory and every thread scans them itself.  The r and u columns of
-// an equation come into shared memory by cp.async copies that every thread
-// issues for all rows of its chunk at once (no registers held for loads,
-// the whole equation in flight).  HBM sees r and u read once and u written
-// once per equation.  On the mixed path r holds the right-hand side of the
-// increment system on every row (inc_rhs, BC rows included), the solve
-// yields the increment itself and writes it back into r; u is read and
-// written only when keep_u (u + increment: the third substep's CFL reads
-// it, nothing else).
-constexpr int TX = 16;
-
-
-template <typename R>
-__global__ void __launch_bounds__(256, 3) k_thomas(const __grid_constant__ State s, Geom g, int keep_u) {
-  extern __shared__ __align__(16) unsigned char th_raw[];
-  constexpr bool F64 = sizeof(R) == sizeof(double);
-  constexpr bool INC = !F64;   // FP32 work type: r is the increment system's right-hand side
+// ---------------------------------------------------------------------------
+// The CN solves of the substep without LES in spectral space.  Without eddy
+// viscosity the four implicit systems (solver.f90:1012-1233) have the same
+// matrix in every (x, z) column, and their right-hand side (r plus the
+// explicit CN term, solver.f90:850-870, 981-989) is linear in the state,
+// so solving every physical column and transforming the result to Fourier
+// space (solver.f90:1247-1252) equals solving every retained Fourier mode's
+// column: the BC rows carry their constant value in the (0,0) mode and zero
+// in every other mode.  The inverse x/z transforms of cr, the physical
+// solve and the forward transforms of the new state drop out, and the
+// solve runs in FP64 on both work types.  A spectral plane is viewed as
+// 2 sp doubles (real and imaginary parts are separate real columns of the
+// real matrix); one thread per column and equation (blockIdx.y, k_tri_coef
+// order th, u2, u1, u3) runs the plain Thomas sweeps with the shared LU
+// factors (row-coefficient loads uniform over a warp, batches of TB rows
+// with their loads issued first, g written into the state in place), cr from s.crs, the state updated in place.
+__global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ State s, Geom g) {
+  constexpr int TB = 8;
+  const long long ncol = 2 * g.sp;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int eq = blockIdx.y;
+  if (c >= ncol) return;
   const int np = g.np, Nyp = g.ny;
-  // [np][TX] each: the FP64 y / z tile, staged r (the tile itself when R is
-  // double) and staged u
-  double* tile = reinterpret_cast<double*>(th_raw);
-  R* rs = F64 ? reinterpret_cast<R*>(tile) : reinterpret_cast<R*>(tile + np * TX);
-  R* us = reinterpret_cast<R*>(tile + np * TX) + (F64 ? 0 : np * TX);
-  __shared__ double ye[2][THOMAS_MAXCH][TX], zs[2][THOMAS_MAXCH][TX];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int cl = lane & (TX - 1), k = 2 * w + (lane >> 4);   // column, chunk
-  const Chunks ch = thomas_chunks(np);
-  const int x = blockIdx.x * TX + cl, z = blockIdx.y;
-  const bool xin = x < g.nx;
-  const long long col = (long long)z * g.nx + (xin ? x : 0);
-  const long long pp = g.pp;
-  const int j0 = k * ch.len, j1 = min(np, j0 + ch.len) - 1;   // this thread's rows
-  const bool active = k < ch.nch;
-  for (int eq = 0; eq < 4; ++eq) {
-    const int par = eq & 1;
-    const TriRow* Rw = s.tri + eq * np;
-    R* u = (R*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3)));
-    R* r = (R*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3)));
-    // rows written back (solver.f90:1056, 1115, 1171, 1227)
-    const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
-    const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    __syncthreads();   // the previous equation is done with the staging buffers
-    if (active) {
-      for (int j = j0; j <= j1; ++j) {
-        cp_async<sizeof(R)>(rs + j * TX + cl, r + (long long)j * pp + col);
-        if (!INC || keep_u) cp_async<sizeof(R)>(us + j * TX + cl, u + (long long)j * pp + col);
-      }
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();   // halo rows of u come from the neighbouring chunks
-    if (active) {
-      // right-hand side (r + explicit CN term, or the BC value; the mixed
-      // path's r is complete), forward recurrence with carry-in zero
-      double um = (!INC && j0 > 0) ? (double)us[(j0 - 1) * TX + cl] : 0.0;
-      double uc = INC ? 0.0 : (double)us[j0 * TX + cl];
-      double y = 0.0;
-      for (int j = j0; j <= j1; ++j) {
-        const TriRow* row = Rw + j;
-        const double xr = (double)rs[j * TX + cl];
-        double v;
-        if (INC) {
-          v = xr;
-        } else {
-          const double un = (j + 1 < np) ? (double)us[(j + 1) * TX + cl] : 0.0;
-          v = row->is_bc ? row->bc : xr + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
-          um = uc;
-          uc = un;
-        }
-        y = (j == j0) ? v : v + row->ap * y;
-        tile[j * TX + cl] = y;
-      }
-      ye[par][k][cl] = y;
-      // backward recurrence of the chunk's y, carry-in zero
-      double zz = 0.0;
-      for (int j = j1; j >= j0; --j) {
-        const double ib = Rw[j].ibp;
-        const double wv = tile[j * TX + cl] * ib;
-        zz = (j == j1) ? wv : wv - Rw[j].u * ib * zz;
-        tile[j * TX + cl] = zz;
-      }
-      zs[par][k][cl] = zz;
-    }
-    __syncthreads();
-    if (active) {
-      // chunk carries: G_k = y_end(k) + pa_end(k) G_{k-1};
-      // X_k = z_start(k) + G_{k-1} qa_start(k) + pm_start(k) X_{k+1}
-      double G[THOMAS_MAXCH];
+  const long long pp = ncol;
+  const TriRow* Rw = s.tri + eq * np;
+  // z-pass equation order of s.crs: 0 u1, 1 u3, 2 u2, 3 th
+  const int ze = (eq == 0) ? 3 : (eq == 1 ? 2 : (eq == 2 ? 0 : 1));
+  double* u = (double*)((eq == 0) ? s.cth : (eq == 1 ? s.cu2 : (eq == 2 ? s.cu1 : s.cu3))) + c;
+  const double* r = (const double*)s.crs[ze] + c;
+  const bool m0 = (c == 0);   // real part of the (0,0) mode
+  const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
+  const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
+  const double k0 = u[0], k1 = u[pp], kb = u[(long long)(np - 2) * pp], kt = u[(long long)(np - 1) * pp];
+  double um = 0.0, uc = k0, y = 0.0;
+  for (int jb = 0; jb < np; jb += TB) {
+    double xr[TB], xu[TB];
 #pragma unroll
-      for (int q = 0; q < THOMAS_MAXCH; ++q) {
-        if (q < ch.nch) {
-          const int e = min(np, (q + 1) * ch.len) - 1;
-          G[q] = ye[par][q][cl] + (q > 0 ? Rw[e].pa * G[q - 1] : 0.0);
-        } else {
-          G[q] = 0.0;
-        }
-      }
-      double X = 0.0, Gm = 0.0;
+    for (int q = 0; q < TB; ++q) {
+      const int j = jb + q;
+      xr[q] = (j < np) ? r[(long long)j * pp] : 0.0;
+      xu[q] = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
+    }
 #pragma unroll
-      for (int q = THOMAS_MAXCH - 1; q >= 1; --q) {
-        if (q < ch.nch && q > k) {
-          const int b = q * ch.len;
-          X = zs[par][q][cl] + G[q - 1] * Rw[b].qa + (q < ch.nch - 1 ? Rw[b].pm * X : 0.0);
-        }
-        if (q == k) Gm = G[q - 1];
-      }
-      // final values and the rows the reference stores; on the mixed path
-      // the value is the increment: into r for the forward transform (0 on
-      // rows the solve does not store), and u + increment into u if keep_u
-      if (xin) {
-        for (int j = j0; j <= j1; ++j) {
-          const double xv = tile[j * TX + cl] + Gm * Rw[j].qa + X * Rw[j].pm;
-          const bool st = (j >= lo && j <= hi);
-          if (INC) {
-            r[(long long)j * pp + col] = st ? (R)xv : (R)0;
-            if (st && keep_u) u[(long long)j * pp + col] = (R)((double)us[j * TX + cl] + xv);
-          } else if (st) {
-            u[(long long)j * pp + col] = (R)xv;
-          }
-        }
-      }
+    for (int q = 0; q < TB; ++q) {
+      const int j = jb + q;
+      if (j >= np) break;
+      const TriRow* row = Rw + j;
+      const double un = xu[q];
+      const double v = row->is_bc ? (m0 ? row->bc : 0.0)
+                                  : xr[q] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
+      y = (j == 0) ? v : v + row->ap * y;
+      u[(long long)j * pp] = y;
+      um = uc;
+      uc = un;
     }
   }
-}
-
-// ---------------------------------------------------------------------------
-// The same CN solves for the FP64 path, one thread per (x, z) column over
-// all rows: the plain Thomas sweeps with the shared LU factors (loads of the
-// row coefficients are uniform over a warp), the forward sweep writing g
-// into u itself; the rows the reference does not store get their old u
-// back.  Batches of TB rows have their loads issued first.  (The FP32 work
-// type keeps the tile solve above, measured faster there.)
-__global__ void __launch_bounds__(128) k_thomas_col(const __grid_constant__ State s, Geom g) {
-  constexpr int TB = 8;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
-  if (x >= g.nx) return;
-  const int np = g.np, Nyp = g.ny;
-  const long long pp = g.pp, col = (long long)z * g.nx + x;
-  for (int eq = 0; eq < 4; ++eq) {
-    const TriRow* Rw = s.tri + eq * np;
-    double* u = (double*)((eq == 0) ? s.th : (eq == 1 ? s.u2 : (eq == 2 ? s.u1 : s.u3))) + col;
-    const double* r = (const double*)((eq == 0) ? s.rth : (eq == 1 ? s.r2 : (eq == 2 ? s.r1 : s.r3))) + col;
-    const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
-    const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-    // old u of the end rows (the only ones that can lie outside lo..hi)
-    const double k0 = u[0], k1 = u[pp], kb = u[(long long)(np - 2) * pp], kt = u[(long long)(np - 1) * pp];
-    double um = 0.0, uc = k0, y = 0.0;
-    for (int jb = 0; jb < np; jb += TB) {
-      double xr[TB], xu[TB];
+  double xn = 0.0;
+  for (int jt = np - 1; jt >= 0; jt -= TB) {
+    double xg[TB];
 #pragma unroll
-      for (int c = 0; c < TB; ++c) {
-        const int j = jb + c;
-        xr[c] = (j < np) ? r[(long long)j * pp] : 0.0;
-        xu[c] = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
-      }
-#pragma unroll
-      for (int c = 0; c < TB; ++c) {
-        const int j = jb + c;
-        if (j >= np) break;
-        const TriRow* row = Rw + j;
-        const double un = xu[c];
-        const double v = row->is_bc ? row->bc : xr[c] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
-        y = (j == 0) ? v : v + row->ap * y;
-        u[(long long)j * pp] = y;
-        um = uc;
-        uc = un;
-      }
+    for (int q = 0; q < TB; ++q) {
+      const int j = jt - q;
+      xg[q] = (j >= 0) ? u[(long long)j * pp] : 0.0;
     }
-    double xn = 0.0;
-    for (int jt = np - 1; jt >= 0; jt -= TB) {
-      double xg[TB];
 #pragma unroll
-      for (int c = 0; c < TB; ++c) {
-        const int j = jt - c;
-        xg[c] = (j >= 0) ? u[(long long)j * pp] : 0.0;
-      }
-#pragma unroll
-      for (int c = 0; c < TB; ++c) {
-        const int j = jt - c;
-        if (j < 0) break;
-        const double ib = Rw[j].ibp;
-        const double xv = (j == np - 1) ? xg[c] * ib : xg[c] * ib - Rw[j].u * ib * xn;
-        xn = xv;
-        const bool st = (j >= lo && j <= hi);
-        const double old = (j == 0) ? k0 : (j == 1 ? k1 : (j == np - 2 ? kb : kt));
-        u[(long long)j * pp] = st ? xv : old;
-      }
+    for (int q = 0; q < TB; ++q) {
+      const int j = jt - q;
+      if (j < 0) break;
+      const double ib = Rw[j].ibp;
+      const double xv = (j == np - 1) ? xg[q] * ib : xg[q] * ib - Rw[j].u * ib * xn;
+      xn = xv;
+      const bool st = (j >= lo && j <= hi);
+      const double old = (j == 0) ? k0 : (j == 1 ? k1 : (j == np - 2 ? kb : kt));
+      u[(long long)j * pp] = st ? xv : old;
     }
   }
 }
@@ -1273,15 +1093,29 @@ static void go_products(const Geom& g, const State& s, cudaStream_t st, bool les
   }
 }
 template <int N, typename R>
-static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, int qform,
-                       cudaStream_t st) {
+static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
   constexpr int T = FftShape<N>::T;
   constexpr bool EFAST = sizeof(R) == sizeof(double);
   size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_zpass_rhs<N, R, EFAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
-  k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost, qform);
+  k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost);
+}
+template <int N, typename R>
+static void go_zpass_spec_t(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  constexpr int T = FftShape<N>::T;
+  constexpr bool EFAST = sizeof(R) == sizeof(double);
+  size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_zpass_rhs<N, R, EFAST, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
+  k_zpass_rhs<N, R, EFAST, true><<<grid, KT * T, smem, st>>>(s, g, ph, rk, nullptr);
+}
+template <int N>
+static void go_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  if (g.prec) go_zpass_spec_t<N, float>(g, ph, s, rk, st);
+  else go_zpass_spec_t<N, double>(g, ph, s, rk, st);
 }
 template <int N>
 static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
@@ -1291,11 +1125,10 @@ static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk
   launch_inv_z(g, nl, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6]), 4, st);
 }
 template <int N>
-static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, bool qform,
-                     cudaStream_t st) {
-  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, qform ? 1 : 0, st);
+static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
+  if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, st);
   else if (s.nls[0]) go_zpass_split<N>(g, ph, s, rk, st);
-  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, 0, st);
+  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, st);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -1315,26 +1148,24 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
   return cudaGetLastError();
 }
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
-                             const double2* ghost, bool qform) {
-  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, qform, st);
+                             const double2* ghost) {
+  DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  if (!s.crs[0]) return cudaErrorInvalidValue;
+  DB_DISPATCH_N2(g.nz, go_zpass_spec, g, ph, s, rk, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_thomas_spec(const Geom& g, const State& s, cudaStream_t st) {
+  const long long ncol = 2 * g.sp;
+  k_thomas_spec<<<dim3((unsigned)((ncol + 127) / 128), 4), 128, 0, st>>>(s, g);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
   const size_t smem = (size_t)g.np * sizeof(TriRow);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_tri_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_tri_coef<<<4, 256, smem, st>>>(g, ph, s.tri, s.sc, rk);
-  return cudaGetLastError();
-}
-cudaError_t launch_thomas(const Geom& g, const State& s, cudaStream_t st, bool keep_u) {
-  if (!g.prec) {   // FP64: one thread per column (measured faster than the tile solve there)
-    const int bx = g.nx < 128 ? g.nx : 128;
-    k_thomas_col<<<dim3(g.nx / bx, g.nz), bx, 0, st>>>(s, g);
-    return cudaGetLastError();
-  }
-  // FP32 work type: the tile solve; y/z tile (FP64) + staged r and u (FP32)
-  const size_t smem = (size_t)g.np * TX * (sizeof(double) + 2 * sizeof(float));
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_thomas<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_thomas<float><<<dim3((g.nx + TX - 1) / TX, g.nz), 256, smem, st>>>(s, g, keep_u ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {

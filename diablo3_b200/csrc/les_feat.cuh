@@ -66,13 +66,16 @@ __device__ __forceinline__ void les_features_at(const LesFeatSrc& s, int j, long
   v.atx = G[7][o]; v.ftx = G[7][om];
   v.atz = G[11][o]; v.ftz = G[11][om];
   const LesRow& lr = s.lrow[j];
-  const R idy = (R)lr.idy;
-  v.d1y = (G[0][o] - G[0][om]) * idy;
-  v.d3y = (G[2][o] - G[2][om]) * idy;
-  v.dty = (G[3][o] - G[3][om]) * idy;
+  // ydiff: y-differences of fluctuations plus those of the plane means when
+  // the fields hold fluctuations, formed as the column walk forms them
+  const double* pm = s.mean;
+  const int np = s.ny + 2;
+  v.d1y = ydiff<R>(G[0][o], G[0][om], pm, 0, np, j, j - 1, lr.idy);
+  v.d3y = ydiff<R>(G[2][o], G[2][om], pm, 2, np, j, j - 1, lr.idy);
+  v.dty = ydiff<R>(G[3][o], G[3][om], pm, 3, np, j, j - 1, lr.idy);
   const R u2j = G[1][o];
-  v.c2y = (j <= s.ny) ? (G[1][o + s.pp] - u2j) * (R)lr.idyf : (R)0;
-  v.f2y = (u2j - G[1][om]) * (R)s.lrow[j - 1].idyf;
+  v.c2y = (j <= s.ny) ? ydiff<R>(G[1][o + s.pp], u2j, pm, 1, np, j + 1, j, lr.idyf) : (R)0;
+  v.f2y = ydiff<R>(u2j, G[1][om], pm, 1, np, j, j - 1, s.lrow[j - 1].idyf);
   les_features<R>(v, (R)lr.wa, (R)lr.wb, (R)s.dxs, (R)lr.dys_y, (R)s.dzs, fv);
 }
 

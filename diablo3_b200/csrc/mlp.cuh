@@ -16,6 +16,7 @@ struct LesFeatSrc {
   long long pp;           // points per plane (Nx Nz)
   int ny;                 // Nyp
   double dxs, dzs;        // x, z filter widths
+  const double* mean;     // plane means of u1 u2 u3 th ([f][Nyp+2]) when f[0..3] hold fluctuations, else null
 };
 
 struct MlpArgs {

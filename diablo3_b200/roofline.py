@@ -6,20 +6,29 @@ Units per wall-normal plane set (Nyp+2 planes, ghosts included):
                                  (8 B per complex on the mixed path)
   S  = (Nkx+1) * (2Nkz+1) * 16 B one dealiased packed spectral field (always FP64)
 Each stage counts the bytes it must read and write once when everything
-inside it is fused (neighbour planes in y are L2 hits):
+inside it is fused (neighbour planes in y are L2 hits).
 
+Without eddy viscosity (no LES) the CN matrices are the same in every
+column, so the implicit solves run on the retained Fourier modes and the
+transforms of cr and of the new state drop out:
   inv_z      4 S  -> 4 Xh           cu1, cu2, cu3, cth to x-half
   inv_x      4 Xh -> 4 P            to physical u1, u2, u3, th
   products   4 P  -> 8 Xh           11 products + x-FFT, x-derivatives folded
-  zpass_rhs  8 Xh + 9 S -> 4 S + 4 Xh   z-FFT, spectral RHS (cu, cp, cth,
-                                        cf_old in; cf out), inverse z of cr
-  inv_x_r    4 Xh -> 4 P            r1, r2, r3, rth
+  zpass_rhs  8 Xh + 9 S -> 8 S      z-FFT, spectral RHS (cu, cp, cth, cf_old
+                                    in; cf and cr out)
+  thomas     8 S  -> 4 S            cr and cu in (CN explicit), cu out
+  courant    (3 S + 6 Xh + 6 P) / 3 u1..u3 to physical space and the CFL
+                                    reduction, on the third substep only
+  rem_div    4 S  -> 4 S            cu1, cu2, cu3, cp in and out
+At 512x257x512 this is ~46 P, i.e. ~370 B per grid point and substep.
+
+The reference's own sequence (cr to physical space, physical CN solves,
+new state back to Fourier space; the LES substep still runs it) adds
+  inv_x_r    4 Xh -> 4 P            r1, r2, r3, rth (after an inverse z of cr)
   thomas     8 P  -> 4 P            r and u in (CN explicit), u out
-  courant    3 P  -> 0              only on the third substep (averaged /3)
   fwd_x      4 P  -> 4 Xh
   fwd_z      4 Xh -> 4 S
-  rem_div    4 S  -> 4 S            cu1, cu2, cu3, cp in and out
-At 512x257x512 this is ~67 P, i.e. ~540 B per grid point and substep.
+for ~67 P (~540 B per point and substep): reference_substep_bytes.
 
 With the LES model (les_model_type 5) the stages change to
   inv_z      4 S  -> 8 Xh           state and its z-derivatives
@@ -45,10 +54,10 @@ def units(p) -> dict:
     }
 
 
-def stage_bytes(p) -> dict:
+def _physical_path_bytes(p) -> dict:
+    """The reference's stage sequence: CN solves in physical space."""
     u = units(p)
     P, X, S = u["P"], u["Xh"], u["S"]
-    cour = (3 * P / 3.0) if p.variable_dt else 0.0
     les = bool(getattr(p, "use_les", 0))
     return {
         "inv_z": 4 * S + (8 if les else 4) * X,
@@ -57,15 +66,42 @@ def stage_bytes(p) -> dict:
         "zpass_rhs": 8 * X + 9 * S + 4 * S + 4 * X,
         "inv_x_r": 4 * X + 4 * P,
         "thomas": 16 * P if les else 12 * P,
-        "courant": cour,
+        "courant": (3 * P / 3.0) if p.variable_dt else 0.0,
         "fwd_x": 4 * P + 4 * X,
         "fwd_z": 4 * X + 4 * S,
         "rem_div": 8 * S,
     }
 
 
+def stage_bytes(p) -> dict:
+    """Algorithmic bytes of each stage as the library runs it (spectral CN
+    solves without LES, physical ones with it)."""
+    if getattr(p, "use_les", 0):
+        return _physical_path_bytes(p)
+    u = units(p)
+    P, X, S = u["P"], u["Xh"], u["S"]
+    return {
+        "inv_z": 4 * S + 4 * X,
+        "inv_x": 4 * X + 4 * P,
+        "products": 4 * P + 8 * X,
+        "zpass_rhs": 8 * X + 17 * S,
+        "inv_x_r": 0.0,
+        "thomas": 12 * S,
+        "courant": ((3 * S + 6 * X + 6 * P) / 3.0) if p.variable_dt else 0.0,
+        "fwd_x": 0.0,
+        "fwd_z": 0.0,
+        "rem_div": 8 * S,
+    }
+
+
 def substep_bytes(p) -> float:
     return float(sum(stage_bytes(p).values()))
+
+
+def reference_substep_bytes(p) -> float:
+    """Bytes of the reference's stage sequence (transforms of cr and of the
+    new state, physical CN solves), every stage fused as far as it goes."""
+    return float(sum(_physical_path_bytes(p).values()))
 
 
 def state_transfer_bytes(p) -> tuple:

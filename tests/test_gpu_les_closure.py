@@ -74,8 +74,11 @@ def test_closure_outside_range_is_amd(oracle_mod, Channel):
     ch5.step(5)
     ch6.step(5)
     a, b = channel_state(ch5, p5), channel_state(ch6, p6)
+    # the same AMD arithmetic in two instantiations of the closure walk, whose
+    # multiply-adds the compiler may contract differently: last-bit
+    # differences, which cp (the running sum of phi / h) grows the most
     for f in STATE:
-        assert rel_l2(b[f], a[f]) <= 1e-13, f
+        assert rel_l2(b[f], a[f]) <= 1e-12, f
 
 
 @pytest.mark.parametrize("prec", [0, 1])

@@ -1,18 +1,16 @@
 """Mixed-precision path (precision 1: FP32 transforms, products and SGS;
 FP64 state, CN solves, projection) against the FP64 oracle.
 
-The mixed path transforms increments (cr - cu into the solve, u_new - u
-out of it, added to the FP64 state), so FP32 rounding scales with the
-change of a substep, not with the field.  Bars: transforms 1e-6 relative
-(FP32 round-off over log2 N passes); one substep 1e-6; after 20 steps,
-relative L2 1e-6 for cu1, cu2, cu3, cth.  The RK history cf is a rate,
-recomputed in FP32 every substep from products of full fields (th u1 with
-th carrying the background stratification), and can be a small difference
-of large terms; it is judged by what it does to the next update,
-dt |cf_gpu - cf_oracle| / |field|, bar 1e-6.  cp, the running sum of
-phi / h_bar, amplifies velocity rounding by about 1 / h_bar and is held to
-1e-4.  The projection is FP64, so the divergence after it stays <= 1e-12
-of the velocity scale.
+Without LES the CN solves run in FP64 on the spectral state, so FP32
+rounding enters through the nonlinear terms only.  With LES the physical
+fields hold fluctuations about their FP64 plane means and the solves
+transform increments, so FP32 rounding scales with the fluctuation and the
+change of a substep, not with the stratification the buoyancy carries.
+Bars: transforms 1e-6 relative (FP32 round-off over log2 N passes); one
+substep 1e-6; after 20 steps, relative L2 1e-5 on each of the nine fields
+(cu1, cu2, cu3, cp, cth and the RK history cf1, cf2, cf3, cfth), the
+accuracy the mixed path is specified to.  The projection is FP64, so the
+divergence after it stays <= 1e-12 of the velocity scale.
 """
 import numpy as np
 import pytest
@@ -28,24 +26,17 @@ def Channel():
     return Channel
 
 
-BARS = {"cu1": 1e-6, "cu2": 1e-6, "cu3": 1e-6, "cth": 1e-6, "cp": 1e-4,
-        "cf1": 1e-6, "cf2": 1e-6, "cf3": 1e-6, "cfth": 1e-6}
-# RK history field -> the state field it advances
-CF_OF = {5: 0, 6: 1, 7: 2, 8: 4}
+BAR_20 = 1e-5   # relative L2 per field after 20 steps
 
 
 def _check_20(e):
-    bad = {k: v for k, v in e.items() if not (v <= BARS[k])}
-    assert not bad, f"above bar: {bad} (all: {e})"
+    bad = {k: v for k, v in e.items() if not (v <= BAR_20)}
+    assert not bad, f"above {BAR_20}: {bad} (all: {e})"
 
 
-def _errs(o, ch, p, fields=STATE, cp_base=None, cf_rate=False):
+def _errs(o, ch, p, fields=STATE, cp_base=None):
     so, sg = oracle_state(o, p), channel_state(ch, p)
     e = {NAMES[f]: rel_l2(sg[f], so[f]) for f in fields}
-    if cf_rate:
-        dt = p.delta_t
-        for f, u in CF_OF.items():
-            e[NAMES[f]] = float(dt * np.linalg.norm(sg[f] - so[f]) / np.linalg.norm(so[u]))
     if cp_base is not None:
         e["cp"] = rel_l2(sg[3] - cp_base, so[3] - cp_base)
     return e
@@ -86,7 +77,7 @@ def test_mixed_config0_20_steps(oracle_mod, Channel):
     for _ in range(20):
         o.step()
     ch.step(20)
-    e = _errs(o, ch, p, cf_rate=True)
+    e = _errs(o, ch, p)
     _check_20(e)
     u = float(np.abs(significant(p, ch.download_field(0))).max())
     assert ch.divergence() <= 1e-12 * max(1.0, u)
@@ -100,7 +91,7 @@ def test_mixed_les_20_steps(oracle_mod, Channel):
     for _ in range(20):
         o.step()
     ch.step(20)
-    e = _errs(o, ch, p, cf_rate=True)
+    e = _errs(o, ch, p)
     _check_20(e)
     a = ch.download_field(9)[:, : p.nz, : p.nx]
     b = o.real(9)[:, : p.nz, : p.nx]

@@ -190,14 +190,21 @@ def test_reference_setup_parses_when_present():
 
 
 def test_roofline_model_totals():
+    # without LES the CN solves run on the spectral state: ~46 P per substep;
+    # the reference's sequence (physical solves, transforms of cr and of the
+    # new state) ~67 P, ~550 B per point and substep
     p = make_params(nx=512, ny=257, nz=512, variable_dt=1)
     b = roofline.stage_bytes(p)
     u = roofline.units(p)
     total_p = roofline.substep_bytes(p) / u["P"]
-    assert 60 < total_p < 75
-    per_point = roofline.substep_bytes(p) / (512 * 257 * 512)
-    assert 500 < per_point < 600
-    assert b["thomas"] == 12 * u["P"]
+    assert 40 < total_p < 50
+    assert b["thomas"] == 12 * u["S"]
+    assert b["inv_x_r"] == b["fwd_x"] == b["fwd_z"] == 0
+    ref_p = roofline.reference_substep_bytes(p) / u["P"]
+    assert 60 < ref_p < 75
+    assert 500 < roofline.reference_substep_bytes(p) / (512 * 257 * 512) < 600
+    les = make_params(nx=512, ny=257, nz=512, variable_dt=1, use_les=1)
+    assert roofline.stage_bytes(les)["thomas"] == 16 * u["P"]
 
 
 def test_header_compiles_as_c_and_links(tmp_path):
