@@ -269,9 +269,10 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
   s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
   s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
   s.phi_g = sp[9]; s.pfac = sp[10];
-  if (!p->precision && p->use_les)   // the FP64 LES z-pass runs as three stages through this scratch
-    for (int i = 0; i < 8; ++i)
-      if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  // z-pass scratch: all 8 for the FP64 LES z-pass (three stages), the last 4
+  // for the split spectral z-pass (Z(M_e))
+  for (int i = (!p->precision && p->use_les) ? 0 : 4; i < 8; ++i)
+    if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   for (int i = 0; i < 4; ++i)   // cr of the spectral CN solve
     if ((rc = dalloc(c, &s.crs[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
   const size_t eP = phys_elem(c), eH = xh_elem(c);

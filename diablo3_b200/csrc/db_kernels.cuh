@@ -31,6 +31,15 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #ifndef DB_LB_PROD
 #define DB_LB_PROD 4
 #endif
+// the z-pass of the substep without LES per work type: 1 = forward z-FFT of
+// the 8 product fields into spectral scratch, then the RHS mode by mode
+// (k_rhs_modes); 0 = one fused kernel (the FP64 one spills at 128 registers)
+#ifndef DB_ZSPEC_SPLIT_F64
+#define DB_ZSPEC_SPLIT_F64 1
+#endif
+#ifndef DB_ZSPEC_SPLIT_F32
+#define DB_ZSPEC_SPLIT_F32 1
+#endif
 constexpr int MAXF = 12;
 
 struct FieldSet {

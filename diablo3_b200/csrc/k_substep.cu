@@ -1112,10 +1112,22 @@ static void go_zpass_spec_t(const Geom& g, const Phys& ph, const State& s, int r
   const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
   k_zpass_rhs<N, R, EFAST, true><<<grid, KT * T, smem, st>>>(s, g, ph, rk, nullptr);
 }
+// split form: Z(N_e) / Nz into s.crs[e], Z(M_e) / Nz into s.nls[4 + e], then
+// cr over s.crs[e] in place (k_rhs_modes)
+static void go_zpass_spec_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  const FieldSet nl = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
+  launch_fwd_z(g, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]), nl, 8, st);
+  k_rhs_modes<<<dim3(4, (g.nkzp * g.kxs + 255) / 256, g.np), 256, 0, st>>>(s, g, ph, rk, nl);
+}
 template <int N>
 static void go_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  if (g.prec) go_zpass_spec_t<N, float>(g, ph, s, rk, st);
-  else go_zpass_spec_t<N, double>(g, ph, s, rk, st);
+  if (g.prec) {
+    if (DB_ZSPEC_SPLIT_F32) go_zpass_spec_split(g, ph, s, rk, st);
+    else go_zpass_spec_t<N, float>(g, ph, s, rk, st);
+  } else {
+    if (DB_ZSPEC_SPLIT_F64) go_zpass_spec_split(g, ph, s, rk, st);
+    else go_zpass_spec_t<N, double>(g, ph, s, rk, st);
+  }
 }
 template <int N>
 static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
@@ -1153,7 +1165,7 @@ cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int 
   return cudaGetLastError();
 }
 cudaError_t launch_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  if (!s.crs[0]) return cudaErrorInvalidValue;
+  if (!s.crs[0] || !s.nls[4]) return cudaErrorInvalidValue;
   DB_DISPATCH_N2(g.nz, go_zpass_spec, g, ph, s, rk, st);
   return cudaGetLastError();
 }
