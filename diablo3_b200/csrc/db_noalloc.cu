@@ -14,13 +14,18 @@
 // a kernel (on the host the name is only a stand-in).  Its device address is
 // fetched once per device with cudaGetSymbolAddress, on the first call made
 // while that device is current; that first call should therefore come
-// before any stream capture.  Every call shares the array, so calls that
-// overlap on the GPU (two streams, two threads) race; serialise them.
+// before any stream capture.  The grid GY is kept in the array too: a call
+// copies the caller's (host, pageable) gy to the device only when its
+// values or ny differ from the ones the previous call on that device left
+// there.  Every call shares the array, so calls that overlap on the GPU
+// (two streams, two threads) race; serialise them.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "../../include/diablo_b200.h"
 
@@ -36,6 +41,8 @@ static __device__ __align__(256) double2 g_rd_scratch[kScratchElems];
 
 std::mutex g_mu;
 double2* g_scratch_ptr[kMaxDevices] = {};
+// the GY values the scratch of each device holds (host copy; empty = none)
+std::vector<double> g_gy_held[kMaxDevices];
 
 
 struct RefGeomLite {
@@ -63,7 +70,9 @@ __device__ __forceinline__ double dyfv(const double2* s, int j, int nyp) {
 }
 
 // rem_div_chan (for/solver.f90:1302-1379) for one chunk of (kx, kz) columns,
-// arrays in the reference layout cu(0:Nxp, 0:Nz+1, 0:Nyp+1).
+// arrays in the reference layout cu(0:Nxp, 0:Nz+1, 0:Nyp+1).  The scratch
+// of the chunk's columns is interleaved by column (row j of column t at
+// j * chunk + t), so the loads and stores of a warp are contiguous.
 __global__ void k_rem_div_static(double2* cu1, double2* cu2, double2* cu3, double2* scratch,
                                  RefGeomLite G, int col0) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,9 +81,10 @@ __global__ void k_rem_div_static(double2* cu1, double2* cu2, double2* cu3, doubl
   if (t >= G.chunk || col >= ncols) return;
   const int kx = col % (G.nkx + 1), kzp = col / (G.nkx + 1);
   const int nyp = G.nyp, np = nyp + 2;
-  const double2* gys = scratch;                             // GY values
-  double2* gbuf = scratch + np + (long long)t * np;          // g_j
-  double* ibuf = (double*)(scratch + np + (long long)G.chunk * np) + (long long)t * np;  // 1/b'_j
+  const long long cs = G.chunk;
+  const double2* gys = scratch;                                   // GY values
+  double2* gbuf = scratch + np + t;                               // g_j at gbuf[j cs]
+  double* ibuf = (double*)(scratch + np + cs * np) + t;           // 1/b'_j at ibuf[j cs]
   const double kxv = kx * G.two_pi_lx;
   const double kzv = (kzp <= G.nkz ? kzp : kzp - G.nkzp) * G.two_pi_lz;
   const double kx2 = kxv * kxv, kz2 = kzv * kzv;
@@ -85,8 +95,8 @@ __global__ void k_rem_div_static(double2* cu1, double2* cu2, double2* cu3, doubl
   double bprev = 1.0;                    // b'_1 = 1
   double uprev = zero_mode ? 0.0 : -1.0; // u_1
   double2 gp = make_double2(0.0, 0.0);
-  gbuf[1] = gp;
-  ibuf[1] = 1.0;
+  gbuf[cs] = gp;
+  ibuf[cs] = 1.0;
   for (int j = 2; j <= nyp; ++j) {
     double l, d, u;
     double2 rhs = make_double2(0.0, 0.0);
@@ -105,8 +115,8 @@ __global__ void k_rem_div_static(double2* cu1, double2* cu2, double2* cu3, doubl
     const double a = -l / bprev;
     const double b = d + a * uprev;
     gp = make_double2(rhs.x + a * gp.x, rhs.y + a * gp.y);
-    gbuf[j] = gp;
-    ibuf[j] = 1.0 / b;
+    gbuf[j * cs] = gp;
+    ibuf[j * cs] = 1.0 / b;
     bprev = b;
     uprev = u;
   }
@@ -117,8 +127,8 @@ __global__ void k_rem_div_static(double2* cu1, double2* cu2, double2* cu3, doubl
     if (j == nyp) cj = 0.0;
     else if (j == 1) cj = zero_mode ? 0.0 : -1.0;
     else cj = 1.0 / (dyv(gys, j + 1, nyp) * dyfv(gys, j, nyp));
-    const double2 gj = gbuf[j];
-    const double ib = ibuf[j];
+    const double2 gj = gbuf[j * cs];
+    const double ib = ibuf[j * cs];
     const double2 phi = make_double2((gj.x - cj * phin.x) * ib, (gj.y - cj * phin.y) * ib);
     const long long a = j * plane + c0;
     double2 v1 = cu1[a], v3 = cu3[a];
@@ -159,6 +169,7 @@ extern "C" int db_rem_div_static(const db_params* p, const double* gy, double* c
     return DB_ERR_CUDA;
   }
   double2* scratch = nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_ptr[dev]) {
@@ -170,14 +181,24 @@ extern "C" int db_rem_div_static(const db_params* p, const double* gy, double* c
       g_scratch_ptr[dev] = (double2*)ptr;
     }
     scratch = g_scratch_ptr[dev];
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  // GY(1:Nyp+1) into the first entries (.x); nothing else must start at zero:
-  // every scratch entry a launch reads is written earlier in the same launch
-  e = cudaMemcpy2DAsync(scratch, sizeof(double2), gy, sizeof(double), sizeof(double), (size_t)p->ny + 1,
-                        cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    return DB_ERR_CUDA;
+    // GY(1:Nyp+1) into the first entries (.x), unless the previous call on
+    // this device left the same values there; nothing else must start at
+    // zero: every scratch entry a launch reads is written earlier in it
+    std::vector<double>& held = g_gy_held[dev];
+    const size_t ngy = (size_t)p->ny + 1;
+    if (held.size() != ngy || !std::equal(held.begin(), held.end(), gy)) {
+      e = cudaMemcpy2DAsync(scratch, sizeof(double2), gy, sizeof(double), sizeof(double), ngy,
+                            cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) {
+        held.clear();
+        return DB_ERR_CUDA;
+      }
+      try {
+        held.assign(gy, gy + ngy);
+      } catch (...) {
+        held.clear();   // copy again next time
+      }
+    }
   }
   RefGeomLite G;
   G.nyp = p->ny;

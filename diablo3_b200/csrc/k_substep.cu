@@ -828,64 +828,79 @@ __global__ void k_pfac(Geom g, double2* pfac) {
   }
 }
 
-// divergence removal + pressure update, one thread per (kx, kzp) column
-__global__ void __launch_bounds__(128) k_rem_div(const __grid_constant__ State s, Geom g, int rk, int update_cp) {
+// divergence removal + pressure update (solver.f90:1302-1379, 1261-1267).
+// The Poisson matrix of a (kx, kzp) column is real, so the real and the
+// imaginary part of phi are two independent real systems: one thread per
+// column and part (part = threadIdx.x & 1, the pair in adjacent lanes, so a
+// warp reads 16 consecutive modes).  Part 0 (phi real) sees the divergence
+// -kx Im u1 + Dy Re u2 - kz Im u3 and corrects Im u1, Im u3, Re u2, Re cp;
+// part 1 the other halves, so the two threads never touch the same value.
+__global__ void __launch_bounds__(128, 6) k_rem_div(const __grid_constant__ State s, Geom g, int rk, int update_cp) {
   // the rows of both sweeps are handled in batches of RB whose loads are all
-  // issued first (each thread keeps several rows in flight)
+  // issued first (each thread keeps several rows in flight); 80 registers,
+  // six CTAs per SM
   constexpr int RB = 4;
-  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
+  const int kx = t >> 1, part = t & 1;
   if (kx > g.nkx) return;
   const int Nyp = g.ny;
   const long long c0 = (long long)kzp * g.kxs + kx, sp = g.sp;
-  const double kxv = g.kx[kx], kzv = g.kz[kzp];
+  const long long q0 = 2 * c0 + part, qs = 2 * sp;   // this part, as doubles
+  const double* u1 = reinterpret_cast<const double*>(s.cu1);
+  const double* u3 = reinterpret_cast<const double*>(s.cu3);
+  double* w1p = reinterpret_cast<double*>(s.cu1);
+  double* w3p = reinterpret_cast<double*>(s.cu3);
+  double* u2 = reinterpret_cast<double*>(s.cu2);
+  double* cpp = reinterpret_cast<double*>(s.cp);
+  double* ph = reinterpret_cast<double*>(s.phi_g);
+  // d/dx, d/dz of the other part: Re(i k a) = -k Im a, Im(i k a) = k Re a
+  const long long qo = 2 * c0 + (part ^ 1);
+  const double sgn = part ? 1.0 : -1.0;
+  const double kxv = sgn * g.kx[kx], kzv = sgn * g.kz[kzp];
   const bool zero_mode = (kx == 0 && kzp == 0);
   // forward sweep: g_1 = 0 (BC row), g_j = rhs_j + a'_j g_{j-1}; rhs_Nyp = 0
-  double2 gp = make_double2(0.0, 0.0);
-  s.phi_g[1 * sp + c0] = gp;
-  double2 u2c = s.cu2[2 * sp + c0];
+  double gp = 0.0;
+  ph[1 * qs + q0] = gp;
+  double u2c = u2[2 * qs + q0];
   for (int jb = 2; jb <= Nyp; jb += RB) {
-    double2 pf[RB], u2n[RB], a1[RB], a3[RB];
+    double pa[RB], u2n[RB], a1[RB], a3[RB];
 #pragma unroll
     for (int c = 0; c < RB; ++c) {
       const int j = jb + c;
-      const long long a = (long long)j * sp + c0;
       const bool in = j <= Nyp, mid = j < Nyp;
-      pf[c] = in ? s.pfac[a] : make_double2(0.0, 0.0);
-      u2n[c] = in ? s.cu2[a + sp] : make_double2(0.0, 0.0);
-      a1[c] = mid ? s.cu1[a] : make_double2(0.0, 0.0);
-      a3[c] = mid ? s.cu3[a] : make_double2(0.0, 0.0);
+      pa[c] = in ? s.pfac[(long long)j * sp + c0].x : 0.0;
+      u2n[c] = in ? u2[(long long)(j + 1) * qs + q0] : 0.0;
+      a1[c] = mid ? u1[(long long)j * qs + qo] : 0.0;
+      a3[c] = mid ? u3[(long long)j * qs + qo] : 0.0;
     }
 #pragma unroll
     for (int c = 0; c < RB; ++c) {
       const int j = jb + c;
       if (j > Nyp) break;
-      double2 rhs = make_double2(0.0, 0.0);
-      if (j < Nyp) {
-        const double idf = 1.0 / g.dyf[j];
-        rhs = make_double2(-kxv * a1[c].y + (u2n[c].x - u2c.x) * idf - kzv * a3[c].y,
-                           kxv * a1[c].x + (u2n[c].y - u2c.y) * idf + kzv * a3[c].x);
-      }
-      gp = make_double2(rhs.x + pf[c].x * gp.x, rhs.y + pf[c].x * gp.y);
-      s.phi_g[(long long)j * sp + c0] = gp;
+      const double rhs = (j < Nyp) ? kxv * a1[c] + (u2n[c] - u2c) / g.dyf[j] + kzv * a3[c] : 0.0;
+      gp = rhs + pa[c] * gp;
+      ph[(long long)j * qs + q0] = gp;
       u2c = u2n[c];
     }
   }
-  // backward sweep with the projection (solver.f90:1361-1376) and cp update
+  // backward sweep with the projection (solver.f90:1361-1376) and cp update:
+  // u1 -= i kx phi, u3 -= i kz phi touch the other part of u1, u3 (sign as
+  // above with phi in place of a)
   const double itemp4 = 1.0 / s.sc->h_bar[rk];
-  double2 phin = make_double2(0.0, 0.0);
+  double phin = 0.0;
   for (int jt = Nyp; jt >= 1; jt -= RB) {
-    double2 pf[RB], gj[RB], v1[RB], v3[RB], v2[RB], pc[RB];
+    double ib[RB], gj[RB], v1[RB], v3[RB], v2[RB], pc[RB];
 #pragma unroll
     for (int c = 0; c < RB; ++c) {
       const int j = jt - c;
-      const long long a = (long long)j * sp + c0;
       const bool in = j >= 1;
-      pf[c] = in ? s.pfac[a] : make_double2(0.0, 0.0);
-      gj[c] = in ? s.phi_g[a] : make_double2(0.0, 0.0);
-      v1[c] = in ? s.cu1[a] : make_double2(0.0, 0.0);
-      v3[c] = in ? s.cu3[a] : make_double2(0.0, 0.0);
-      v2[c] = (in && j + 1 <= Nyp) ? s.cu2[a + sp] : make_double2(0.0, 0.0);
-      pc[c] = (in && update_cp && j >= g.jstart && j <= g.jend) ? s.cp[a] : make_double2(0.0, 0.0);
+      const long long a = (long long)j * qs;
+      ib[c] = in ? s.pfac[(long long)j * sp + c0].y : 0.0;
+      gj[c] = in ? ph[a + q0] : 0.0;
+      v1[c] = in ? u1[a + qo] : 0.0;
+      v3[c] = in ? u3[a + qo] : 0.0;
+      v2[c] = (in && j + 1 <= Nyp) ? u2[a + qs + q0] : 0.0;
+      pc[c] = (in && update_cp && j >= g.jstart && j <= g.jend) ? cpp[a + q0] : 0.0;
     }
 #pragma unroll
     for (int c = 0; c < RB; ++c) {
@@ -895,27 +910,12 @@ __global__ void __launch_bounds__(128) k_rem_div(const __grid_constant__ State s
       if (j == Nyp) cj = 0.0;
       else if (j == 1) cj = zero_mode ? 0.0 : -1.0;
       else cj = 1.0 / (g.dy[j + 1] * g.dyf[j]);
-      const double2 phi = (j == Nyp) ? make_double2(gj[c].x * pf[c].y, gj[c].y * pf[c].y)
-                                     : make_double2((gj[c].x - cj * phin.x) * pf[c].y, (gj[c].y - cj * phin.y) * pf[c].y);
-      const long long a = (long long)j * sp + c0;
-      double2 w1 = v1[c], w3 = v3[c];
-      w1.x += kxv * phi.y; w1.y -= kxv * phi.x;   // cu1 -= i kx phi
-      w3.x += kzv * phi.y; w3.y -= kzv * phi.x;   // cu3 -= i kz phi
-      s.cu1[a] = w1;
-      s.cu3[a] = w3;
-      if (j + 1 <= Nyp) {  // cu2(j+1) -= (phi(j+1) - phi(j)) / dy(j+1)
-        const double w = 1.0 / g.dy[j + 1];
-        double2 w2 = v2[c];
-        w2.x -= (phin.x - phi.x) * w;
-        w2.y -= (phin.y - phi.y) * w;
-        s.cu2[a + sp] = w2;
-      }
-      if (update_cp && j >= g.jstart && j <= g.jend) {
-        double2 p = pc[c];
-        p.x += phi.x * itemp4;
-        p.y += phi.y * itemp4;
-        s.cp[a] = p;
-      }
+      const double phi = (j == Nyp) ? gj[c] * ib[c] : (gj[c] - cj * phin) * ib[c];
+      const long long a = (long long)j * qs;
+      w1p[a + qo] = v1[c] + kxv * phi;   // (u1 - i kx phi) in the other part
+      w3p[a + qo] = v3[c] + kzv * phi;
+      if (j + 1 <= Nyp) u2[a + qs + q0] = v2[c] - (phin - phi) / g.dy[j + 1];   // u2(j+1) -= Dy phi
+      if (update_cp && j >= g.jstart && j <= g.jend) cpp[a + q0] = pc[c] + phi * itemp4;
       phin = phi;
     }
   }
@@ -1188,7 +1188,7 @@ cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl
   return cudaGetLastError();
 }
 cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp, cudaStream_t st) {
-  k_rem_div<<<dim3((g.nkx + 1 + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, rk, update_cp);
+  k_rem_div<<<dim3((2 * (g.nkx + 1) + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, rk, update_cp);
   return cudaGetLastError();
 }
 cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st) {

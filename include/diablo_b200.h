@@ -226,9 +226,12 @@ int db_stats(db_ctx* ctx, double* out);
  * `stream` and is complete when the stream is.  Working memory is an 8 MiB
  * static device array held by every GPU that loads the library; it limits
  * ny to 10697 (DB_ERR_SIZE above that).  The first call on each device looks
- * up that array's address and should come before any stream capture.  All
- * calls share the array: calls overlapping on the GPU race, so serialise
- * them.  Returns DB_ERR_ARG / DB_ERR_SIZE / DB_ERR_CUDA on failure.
+ * up that array's address and should come before any stream capture.  The
+ * grid is kept in the array: a call copies gy to the device (a host-to-device
+ * copy from the caller's array, queued on `stream`) only when ny or the
+ * values differ from those of the previous call on that device.  All calls
+ * share the array: calls overlapping on the GPU race, so serialise them.
+ * Returns DB_ERR_ARG / DB_ERR_SIZE / DB_ERR_CUDA on failure.
  */
 int db_rem_div_static(const db_params* p, const double* gy, double* cu1,
                       double* cu2, double* cu3, void* cuda_stream);

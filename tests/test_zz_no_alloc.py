@@ -6,7 +6,9 @@ own device arrays; the entry point's working memory is a fixed static device
 array.  This file is named to be collected last.  It checks, on two calls in
 a row with different inputs (so the second call runs on scratch the first
 one left behind), that the result matches the context-based db_rem_div to
-the same 1e-12 relative tolerance as the other rem_div parity test.
+the same 1e-12 relative tolerance as the other rem_div parity test, and on
+the first call of the small grid the CPU oracle's rem_div_chan as well.  The
+second grid is tall enough that one call runs the chunk loop six times.
 """
 import ctypes
 
@@ -26,13 +28,16 @@ def _field(ch, p, rng, scale):
     return a
 
 
-def test_rem_div_static_matches_rem_div_twice():
+@pytest.mark.parametrize("ny", [65, 2049])
+def test_rem_div_static_matches_rem_div_twice(oracle_mod, ny):
+    # ny = 2049: the static scratch holds 169 columns per launch, so the 946
+    # (kx, kz) columns take six launches of the chunk loop
     import torch
 
     from diablo3_b200 import lib as L
     from diablo3_b200.channel import Channel
 
-    p = config0_params(nx=64, ny=65, nz=64)
+    p = config0_params(nx=64, ny=ny, nz=64)
     gy = grid_for(p)
     rng = np.random.default_rng(2024)
     with Channel(p, gy) as ch:
@@ -51,10 +56,20 @@ def test_rem_div_static_matches_rem_div_twice():
                                             ctypes.c_void_p(dev[2].data_ptr()), None)
             assert rc == 0
             torch.cuda.synchronize()
+            got = [dev[f].cpu().numpy().view(np.complex128).reshape(u[f].shape) for f in range(3)]
             for f in range(3):
-                got = dev[f].cpu().numpy().view(np.complex128).reshape(u[f].shape)
-                err = rel_l2(significant(p, got), significant(p, ref[f]))
+                err = rel_l2(significant(p, got[f]), significant(p, ref[f]))
                 assert err < 1e-12, (call, f, err)
+            if ny == 65 and call == 0:
+                # and directly against the oracle's rem_div_chan
+                o = oracle_mod.Oracle(p, gy)
+                for f in range(3):
+                    o.cplx(f)[...] = u[f]
+                o.rem_div()
+                for f in range(3):
+                    err = rel_l2(significant(p, got[f]), significant(p, o.cplx(f)))
+                    assert err < 1e-12, ("oracle", f, err)
+                o.close()
 
 
 def test_rem_div_static_rejects_oversized_grid():
