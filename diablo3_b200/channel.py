@@ -192,6 +192,15 @@ class Channel:
     def set_clock(self, time=0.0, time_step=0, save_stats_time=1e300, save_flow_time=1e300):
         self._ck(self.L.db_set_clock(self.h, time, time_step, save_stats_time, save_flow_time))
 
+    def clear_status(self) -> None:
+        """Clear the accumulated DB_FLAG_* bits."""
+        self._ck(self.L.db_clear_status(self.h))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Failure-handling hook for tests: polls of the first wait on each
+        TMA copy before it gives up (0 = built-in bound); db_set_wait_limit."""
+        self._ck(self.L.db_set_wait_limit(self.h, int(polls)))
+
     def status(self) -> _L.DbStatus:
         s = _L.DbStatus()
         self._ck(self.L.db_get_status(self.h, ctypes.byref(s)))

@@ -1441,6 +1441,13 @@ static int need_net(db_ctx* c) {
   return DB_OK;
 }
 
+extern "C" int db_set_wait_limit(db_ctx* c, uint32_t polls) {
+  if (!c) return DB_ERR_ARG;
+  c->g.wait_first = polls;
+  drop_graphs(c);   // captured steps hold the old Geom
+  return DB_OK;
+}
+
 extern "C" int db_kernel_launches(db_ctx* c, long long* count) {
   if (!c || !count) return DB_ERR_ARG;
   *count = c->launches;

@@ -46,6 +46,11 @@ struct Geom {
   int tune_les_tb;         // LES Thomas: threads per CTA
   int tune_pgrid;          // products: persistent CTAs per SM
   int tune_amd_ch;         // LES closure walk: wall-normal chunks
+  // non-blocking checks the first wait on a TMA copy in the products and
+  // x-pass kernels makes before it gives up (0 = the built-in bound of
+  // blocking polls); draining a copy still in flight before a CTA leaves
+  // always uses the built-in bound
+  unsigned wait_first;
 };
 
 // Physics constants of the substep (host-computed once at init).

@@ -260,10 +260,12 @@ __global__ void __launch_bounds__(256, 2) k_fwd_x_st(const __grid_constant__ Fie
       mbar_expect_tx(&mbar[s ^ 1], item_bytes);
       bulk_g2s(reinterpret_cast<unsigned char*>(stage0) + (s ^ 1) * item_bytes, src(nxt), item_bytes, &mbar[s ^ 1]);
     }
-    const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
-    if (!got) {   // record it, let the prefetch in flight land (bounded), leave
+    const bool got =
+        __syncthreads_and(mbar_wait_first(&mbar[s], (uint32_t)((k >> 1) & 1), g.wait_first, STAGE_WAIT) ? 1 : 0) != 0;
+    if (!got) {   // record it, let the copies in flight land (bounded), leave
       if (threadIdx.x == 0) {
         atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
+        mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT);
         if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
       }
       return;
@@ -335,10 +337,12 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
       mbar_expect_tx(&mbar[s ^ 1], item_bytes);
       bulk_g2s(reinterpret_cast<unsigned char*>(stage0) + (s ^ 1) * item_bytes, src(nxt), item_bytes, &mbar[s ^ 1]);
     }
-    const bool got = __syncthreads_and(mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT) ? 1 : 0) != 0;
-    if (!got) {   // record it, let the prefetch in flight land (bounded), leave
+    const bool got =
+        __syncthreads_and(mbar_wait_first(&mbar[s], (uint32_t)((k >> 1) & 1), g.wait_first, STAGE_WAIT) ? 1 : 0) != 0;
+    if (!got) {   // record it, let the copies in flight land (bounded), leave
       if (threadIdx.x == 0) {
         atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
+        mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT);
         if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
       }
       return;

@@ -30,6 +30,7 @@
 //                 coefficients and batched row loads.
 #include <math.h>
 
+#include "../../include/diablo_b200.h"
 #include "db_bc.cuh"
 #include "db_kernels.cuh"
 #include "les_feat.cuh"
@@ -465,6 +466,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
       }
     }
     double xnext = 0.0;
+    bool bad = false;   // a non-finite new state (reported as DB_FLAG_NONFINITE)
     for (int jt = np - 1; jt >= 0; jt -= TB) {
       double xc[TB], xg[TB], xo[TB];
 #pragma unroll
@@ -479,6 +481,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
         const int j = jt - c;
         if (j < 0) break;
         const double xv = xg[c] - xc[c] * xnext;
+        bad = bad || !(fabs(xv) <= 1.7976931348623157e308);
         const bool stored = (j >= lo && j <= hi);
         if (stored && (!INC || keep_u)) u[(long long)j * pp] = (R)xv;
         // increment for the FP64 forward transforms, over g_j / b'_j (read above)
@@ -486,6 +489,7 @@ __global__ void __launch_bounds__(128) k_thomas_les(const __grid_constant__ Stat
         xnext = xv;
       }
     }
+    if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
   }
 }
 

@@ -245,11 +245,15 @@ __global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_
     }
     pend |= 1u << sl;
   };
+  // a wait that gives up leaves its slot pending (same parity), so the
+  // drain below waits for that copy before the CTA leaves
   auto wait_row = [&](int jr) -> bool {
     const int sl = jr % PROD_SLOTS;
-    const bool ok = mbar_wait(&mbar[sl], (par >> sl) & 1u, PROD_WAIT);
-    par ^= 1u << sl;
-    pend &= ~(1u << sl);
+    const bool ok = mbar_wait_first(&mbar[sl], (par >> sl) & 1u, g.wait_first, PROD_WAIT);
+    if (ok) {
+      par ^= 1u << sl;
+      pend &= ~(1u << sl);
+    }
     return ok;
   };
   auto row = [&](int jr, int f) -> const R* {
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_
       } else if (j + 1 <= jtop) {
         ok = wait_row(j + 1);
       }
-      if (__syncthreads_and(ok ? 1 : 0) == 0) {   // a copy never landed: record, drain (bounded), leave
+      if (__syncthreads_and(ok ? 1 : 0) == 0) {   // a copy did not land in time: record, drain (bounded), leave
         if (threadIdx.x == 0) {
           atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
           for (int sl = 0; sl < PROD_SLOTS; ++sl)
@@ -776,6 +780,7 @@ __global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ Sta
     }
   }
   double xn = 0.0;
+  bool bad = false;   // a non-finite new state (reported as DB_FLAG_NONFINITE)
   for (int jt = np - 1; jt >= 0; jt -= TB) {
     double xg[TB];
 #pragma unroll
@@ -790,11 +795,13 @@ __global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ Sta
       const double ib = Rw[j].ibp;
       const double xv = (j == np - 1) ? xg[q] * ib : xg[q] * ib - Rw[j].u * ib * xn;
       xn = xv;
+      bad = bad || !(fabs(xv) <= 1.7976931348623157e308);
       const bool st = (j >= lo && j <= hi);
       const double old = (j == 0) ? k0 : (j == 1 ? k1 : (j == np - 2 ? kb : kt));
       u[(long long)j * pp] = st ? xv : old;
     }
   }
+  if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
 }
 
 // ---------------------------------------------------------------------------

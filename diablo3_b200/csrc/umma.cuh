@@ -93,6 +93,33 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
 }
 
 // bounded wait for phase `parity` of the mbarrier; false when it gave up
+// up to `polls` non-blocking checks (mbarrier.test_wait) of the phase with
+// this parity; unlike try_wait no check suspends the thread
+__device__ __forceinline__ bool mbar_poll(uint64_t* mbar, uint32_t parity, uint32_t polls) {
+  const uint32_t a = smem_u32(mbar);
+  for (uint32_t it = 0; it < polls; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t"
+        "}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// the first wait on a copy: the built-in bound, or `limit` non-blocking
+// polls when a limit is set (db_set_wait_limit)
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t max_iter);
+__device__ __forceinline__ bool mbar_wait_first(uint64_t* mbar, uint32_t parity, uint32_t limit, uint32_t max_iter) {
+  return limit ? mbar_poll(mbar, parity, limit) : mbar_wait(mbar, parity, max_iter);
+}
+
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t max_iter) {
   const uint32_t a = smem_u32(mbar);
   for (uint32_t it = 0; it < max_iter; ++it) {

@@ -35,6 +35,7 @@ EXPORTS = (
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
     "db_sgs_targets",
     "db_ensemble_create", "db_ensemble_steps", "db_ensemble_destroy", "db_ensemble_error",
+    "db_set_wait_limit",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
           "fwd_x", "fwd_z", "rem_div")
@@ -95,6 +96,7 @@ def load(path: str | None = None):
     L.db_set_timing.argtypes = [vp, ctypes.c_int]
     L.db_stage_times.argtypes = [vp, dp, ctypes.c_int]
     L.db_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.db_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
     L.db_rem_div_static.argtypes = [ctypes.POINTER(DbParams), dp, vp, vp, vp, vp]
     fp, ll = ctypes.POINTER(ctypes.c_float), ctypes.c_longlong
     L.db_sgs_create.argtypes = [vp, ctypes.POINTER(vp)]

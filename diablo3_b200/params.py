@@ -151,7 +151,22 @@ def read_inputs(run_dir: str, version_check: bool = True) -> DbParams:
     """Parse ``input.dat``, ``input_chan.dat`` and ``grid_def.all`` of a run
     directory exactly as init_parameters/input_chan do (comment lines are
     skipped by position; version 3.4 is required, for/parameters.f90:96,211).
+    A missing file, a file that ends early or a value that does not read as
+    its type raises InputError (the reference stops there too).
     """
+    try:
+        return _read_inputs(run_dir, version_check)
+    except InputError:
+        raise
+    except FileNotFoundError as e:
+        raise InputError(f"{run_dir}: missing {os.path.basename(e.filename or '?')}") from None
+    except StopIteration:
+        raise InputError(f"{run_dir}: an input file ends before all its entries") from None
+    except (ValueError, IndexError) as e:
+        raise InputError(f"{run_dir}: unreadable entry ({e})") from None
+
+
+def _read_inputs(run_dir: str, version_check: bool) -> DbParams:
     nx, ny, nz, nth = read_grid_def(os.path.join(run_dir, "grid_def.all"))
     L = _data_lines(os.path.join(run_dir, "input.dat"))
     # for/parameters.f90:91-121: 4 comment lines, then data/comment pairs

@@ -377,6 +377,17 @@ int db_stage_times(db_ctx* ctx, double* ms, int nstages);
 /* Number of this library's kernels issued on the context so far. */
 int db_kernel_launches(db_ctx* ctx, long long* count);
 
+/* Failure-handling hook for tests (no counterpart in the reference): the
+ * number of non-blocking checks the first wait on each TMA copy in the
+ * products and x-pass kernels makes before it gives up (0 restores the
+ * built-in bound of about 1.7e7 blocking polls).  With a small value those
+ * waits give up before their
+ * copies land: the kernel records DB_FLAG_WAIT_TIMEOUT, waits (within the
+ * built-in bound) for every copy it issued, and returns, so the context
+ * stays usable and the next db_get_status reports the flag; the data of
+ * that step are invalid.  Captured step graphs are dropped. */
+int db_set_wait_limit(db_ctx* ctx, uint32_t polls);
+
 #ifdef __cplusplus
 }
 #endif
