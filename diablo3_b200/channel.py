@@ -144,6 +144,23 @@ class Channel:
         self._ck(self.L.db_stats(self.h, _L.dptr(out.reshape(-1))))
         return {k: out[i].copy() for i, k in enumerate(_L.STAT_ROWS)}
 
+    def budget(self) -> dict:
+        """Energy-budget rows that need the mean flow as a function of x
+        (compute_TKE, compute_TKE_Production, compute_MKE_diss,
+        compute_Vorticity), FP64: a dict of arrays over the planes 0..Nyp+1
+        (see include/diablo_b200.h, db_budget)."""
+        out = np.zeros((len(_L.BUDGET_ROWS), self.p.ny + 2))
+        self._ck(self.L.db_budget(self.h, _L.dptr(out.reshape(-1))))
+        return {k: out[i].copy() for i, k in enumerate(_L.BUDGET_ROWS)}
+
+    def bpe(self, nbin: int | None = None):
+        """(BPE, PDF[nbin], bin edges[nbin + 1]) of compute_BPE; nbin
+        defaults to Nx as in the reference."""
+        n = int(nbin or self.p.nx)
+        pdf, edges, e = np.zeros(n), np.zeros(n + 1), ctypes.c_double()
+        self._ck(self.L.db_bpe(self.h, n, _L.dptr(pdf), _L.dptr(edges), ctypes.byref(e)))
+        return e.value, pdf, edges
+
     def set_sgs_net(self, net):
         """Learned closure for les_model_type 6 (a SgsNet that outlives this channel)."""
         self._sgs = net

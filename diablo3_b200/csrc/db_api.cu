@@ -32,6 +32,14 @@ struct db_ctx {
   int device = 0;
   std::vector<void*> allocs;
   double* stats = nullptr;        // db_stats rows (device), allocated on first use
+  // db_budget / db_bpe scratch (device, first use): FP64 physical u1, u2,
+  // u3, th, one FP64 x-half field, the z-means, the rows, the PDF
+  double* bud_phys[4] = {nullptr, nullptr, nullptr, nullptr};
+  double2* bud_xh = nullptr;
+  double* bud_mxy = nullptr;
+  double* bud_out = nullptr;
+  double* bud_pdf = nullptr;
+  int bud_nbin = 0;
   double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
   float2* d_twf = nullptr;       // the same in FP32
@@ -201,11 +209,14 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
   g.sp = (long long)g.nkzp * g.kxs;
   g.hp = (long long)Nz * g.kxs;
   g.pp = (long long)Nz * Nx;
-  // init_chan_mpi, for/domain.f90:321-361 (one rank: lower sets jstart, upper jend)
+  // init_chan_mpi, for/domain.f90:321-340 with one rank in y: rankY == 0
+  // takes the first branch, so jstart follows the lower BC and jend =
+  // jend_th = Nyp whatever the upper BC (the upper branch, 341-361, runs
+  // only on the top rank of several)
   g.jstart = (p->u_bc_ymin == 1) ? 1 : 2;
-  g.jend = (p->u_bc_ymax == 1) ? Nyp : Nyp - 1;
+  g.jend = Nyp;
   g.jstart_th = (p->th_bc_ymin == 1) ? 1 : 2;
-  g.jend_th = (p->th_bc_ymax == 1) ? Nyp : Nyp - 1;
+  g.jend_th = Nyp;
   g.prec = p->precision;
 
   // grid metrics, for/domain.f90:276-300, 538-565
@@ -233,6 +244,7 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
   ph.ro_inv = 1.0 / p->ro; ph.delta = p->delta;
   ph.grav_x = p->grav_x; ph.grav_y = p->grav_y; ph.grav_z = p->grav_z;
   ph.ly = p->ly;
+  ph.lx = p->lx;
   ph.front = p->flavor_front ? 1 : 0;
   ph.front_tw = (p->flavor_front && ph.ro_inv != 0.0) ? 1 : 0;
   ph.f_type = p->f_type; ph.px0 = p->px0; ph.omega0 = p->omega0;
@@ -1503,6 +1515,88 @@ extern "C" int db_stats(db_ctx* c, double* out) {
     out[DB_ST_EPSILON * np + j] *= c->ph.nu;
     if (j >= 1 && j <= c->g.ny) out[DB_ST_CHI * np + j] += bg;
   }
+  return DB_OK;
+}
+
+// the state's u1, u2, u3, th in FP64 physical space (the budget scratch),
+// whatever the work type of the context
+static int budget_fields(db_ctx* c) {
+  const Geom& g = c->g;
+  const size_t Pn = (size_t)g.np * g.pp, H = (size_t)g.np * g.hp;
+  for (int f = 0; f < 4; ++f)
+    if (!c->bud_phys[f] && balloc(c, (void**)&c->bud_phys[f], Pn * sizeof(double)))
+      return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
+  if (!c->bud_xh && balloc(c, (void**)&c->bud_xh, H * sizeof(double2)))
+    return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
+  Geom g64 = g;   // FP64 transforms with the built-in launch shapes
+  g64.prec = 0;
+  g64.tune_xcps = g64.tune_xgrid = g64.tune_zns = 0;
+  double2* src[4] = {c->s.cu1, c->s.cu2, c->s.cu3, c->s.cth};
+  for (int f = 0; f < 4; ++f) {
+    CK(launch_inv_z(g64, fset(src[f]), fset(c->bud_xh), 1, c->st));
+    CK(launch_inv_x(g64, fset(c->bud_xh), fset(c->bud_phys[f]), 1, c->st));
+  }
+  return DB_OK;
+}
+
+static int homogeneous_x(const db_ctx* c) { return !(c->p.ic_type >= 5 && c->p.ic_type <= 8); }   // parameters.f90:282-286
+
+extern "C" int db_budget(db_ctx* c, double* out) {
+  if (!c || !out) return DB_ERR_ARG;
+  const int np = c->g.np;
+  if (!c->bud_mxy && balloc(c, (void**)&c->bud_mxy, (size_t)3 * np * c->g.nx * sizeof(double)))
+    return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
+  if (!c->bud_out && balloc(c, (void**)&c->bud_out, (size_t)DB_NBUD * np * sizeof(double)))
+    return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
+  int rc = budget_fields(c);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(c->bud_out, 0, (size_t)DB_NBUD * np * sizeof(double), c->st));
+  CK(launch_budget(c->g, c->ph, c->s, fset(c->bud_phys[0], c->bud_phys[1], c->bud_phys[2], c->bud_phys[3]),
+                   homogeneous_x(c), c->bud_mxy, c->bud_out, c->st));
+  CK(cudaMemcpyAsync(out, c->bud_out, (size_t)DB_NBUD * np * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->launches += 3 + 8;
+  return DB_OK;
+}
+
+extern "C" int db_bpe(db_ctx* c, int nbin, double* pdf, double* th_bin, double* bpe) {
+  if (!c || nbin < 1 || nbin > (1 << 16)) return DB_ERR_ARG;
+  if (c->bud_nbin < nbin) {
+    if (balloc(c, (void**)&c->bud_pdf, (size_t)nbin * sizeof(double)))
+      return fail(c, DB_ERR_CUDA, "db_bpe: out of device memory");
+    c->bud_nbin = nbin;
+  }
+  int rc = budget_fields(c);
+  if (rc) return rc;
+  const int homx = homogeneous_x(c);
+  CK(cudaMemsetAsync(c->bud_pdf, 0, (size_t)nbin * sizeof(double), c->st));
+  CK(launch_bpe_pdf(c->g, c->ph, c->bud_phys[3], homx, nbin, c->bud_pdf, c->st));
+  std::vector<double> P((size_t)nbin), B((size_t)nbin + 1), Y((size_t)nbin + 1);
+  CK(cudaMemcpyAsync(P.data(), c->bud_pdf, (size_t)nbin * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->launches += 1 + 8;
+  // bins, normalised PDF, sorted heights Y_r and the BPE (diagnostics.f90:1762-1835)
+  const Phys& ph = c->ph;
+  if (homx) {
+    const double thmin = -ph.dthdx * 0.5 * ph.lx * 1.1, thmax = ph.dthdx * 0.5 * ph.lx * 1.1;
+    const double dth = (thmax - thmin) / nbin + 1.e-14;
+    for (int i = 0; i <= nbin; ++i) B[i] = thmin + i * dth;
+  } else {
+    for (int i = 0; i <= nbin; ++i) B[i] = -(ph.ro_inv + 1.e-14) * cos(i * c->pi_ref / nbin);
+  }
+  double sum = 0.0;
+  for (double v : P) sum += v;
+  if (sum > 0.0)
+    for (double& v : P) v /= sum;
+  Y[0] = 0.0;
+  for (int i = 1; i <= nbin; ++i) Y[i] = Y[i - 1] + P[i - 1];
+  for (double& v : Y) v *= c->p.ly;
+  double e = 0.0;
+  for (int i = 0; i < nbin; ++i)
+    e -= (0.5 * (B[i + 1] + B[i]) * 0.5 * (Y[i + 1] + Y[i])) * (Y[i + 1] - Y[i]) / c->p.ly;
+  if (pdf) std::copy(P.begin(), P.end(), pdf);
+  if (th_bin) std::copy(B.begin(), B.end(), th_bin);
+  if (bpe) *bpe = e;
   return DB_OK;
 }
 

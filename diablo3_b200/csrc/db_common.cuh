@@ -57,7 +57,7 @@ struct Geom {
 struct Phys {
   double nu, beta, nu_v_scale, pr;
   double ro_inv, delta, grav_x, grav_y, grav_z;
-  double dthdx, dthdz, ly;
+  double dthdx, dthdz, ly, lx;
   int front;               // FLAVOUR == 'Front' (for/flow.f90:781)
   int front_tw;            // flavor 'Front' and Ro_inv != 0 (for/solver.f90:48)
   int f_type;

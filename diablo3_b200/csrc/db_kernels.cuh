@@ -205,6 +205,14 @@ cudaError_t launch_les_bc(const Geom& g, const Phys& ph, const State& s, cudaStr
 // mode 0: AMD; 1: closure features only; 2: closure nu_t, kappa_t with AMD fallback
 cudaError_t launch_les_amd(const Geom& g, const Phys& ph, const State& s, cudaStream_t st, int mode = 0);
 cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_t st, bool keep_u);
+// k_budget.cu: energy-budget rows (homx: x-z means, else z-means per x)
+// from the FP64 physical u1, u2, u3 (phys.p[0..2]) and the spectral state;
+// mxy scratch [3][np][Nx], out [DB_NBUD][np]
+cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSet phys, int homx, double* mxy,
+                          double* out, cudaStream_t st);
+// PDF of th + dTHdX (x - Lx/2) over planes jstart_th..jend_th (weights dyf)
+cudaError_t launch_bpe_pdf(const Geom& g, const Phys& ph, const double* th, int homx, int nbin, double* pdf,
+                           cudaStream_t st);
 // mixed path: the LES solve's FP64 increments (u1, u2, u3, th) and the
 // FP64 x-half scratch beside them (k_les.cu)
 void thomas_les_inc(const Geom& g, const State& s, double* inc[4], double2* xh64[4]);

@@ -410,7 +410,11 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(MlpArgs a) {
   if (lane == 0 && lsum != 0.0f) atomicAdd(a.loss, lsum);
   if (!ok && t == 0) {
     atomicExch(a.err, 1);
-    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);   // the layer still in flight (bounded) before freeing
+    // the layer still in flight (bounded) before freeing; should this wait
+    // give up too, the tensor memory is freed all the same: a CTA that kept
+    // it would leave later CTAs on its SM waiting in tcgen05.alloc, and the
+    // flag already marks this launch's outputs invalid
+    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);
   }
   tc_fence_before();
   __syncthreads();
@@ -649,7 +653,11 @@ __global__ void __launch_bounds__(TILE, INF_CTAS_PER_SM) k_mlp_infer(MlpArgs a) 
   }
   if (!ok && t == 0) {
     atomicExch(a.err, 1);
-    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);   // the layer still in flight (bounded) before freeing
+    // the layer still in flight (bounded) before freeing; should this wait
+    // give up too, the tensor memory is freed all the same: a CTA that kept
+    // it would leave later CTAs on its SM waiting in tcgen05.alloc, and the
+    // flag already marks this launch's outputs invalid
+    if (pend) mbar_wait(mbar, phase, WAIT_ITERS);
   }
   tc_fence_before();
   __syncthreads();
@@ -738,7 +746,9 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const uint16_t* A, const u
     }
   } else if (t == 0) {
     atomicExch(err, 1);
-    if (!w) mbar_wait(mbar, 0, WAIT_ITERS);   // the MMA still in flight (bounded) before freeing
+    // the MMA still in flight (bounded) before freeing; freed even if this
+    // wait gives up too (see k_mlp_train)
+    if (!w) mbar_wait(mbar, 0, WAIT_ITERS);
   }
   tc_fence_before();
   __syncthreads();

@@ -19,6 +19,9 @@ CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH, NU_T, KAPPA_T = range(11)
 # rows of db_stats (include/diablo_b200.h order)
 NTUNE = 6   # DB_NTUNE
 STAT_ROWS = ("ume", "vme", "wme", "thme", "urms", "vrms", "wrms", "thrms", "uv", "wv", "uw", "thv", "epsilon", "chi")
+# rows of db_budget
+BUDGET_ROWS = ("tke", "uu_dudx", "wu_dwdx", "vu_dvdx", "vv_dvdy", "uv_dudy", "wv_dwdy", "epsilon_m",
+               "omega_x", "omega_y", "omega_z")
 STATE_FIELDS = (CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH)
 
 # exported symbols, in header order
@@ -28,7 +31,7 @@ EXPORTS = (
     "db_set_clock", "db_get_status", "db_clear_status",
     "db_fft_xz_to_fourier", "db_fft_xz_to_physical", "db_fft_xz_to_fourier_dev", "db_fft_xz_to_physical_dev",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
-    "db_courant", "db_divergence", "db_stats",
+    "db_courant", "db_divergence", "db_stats", "db_budget", "db_bpe",
     "db_autotune", "db_get_tuning", "db_set_tuning", "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
@@ -90,6 +93,8 @@ def load(path: str | None = None):
     L.db_courant.argtypes = [vp, dp]
     L.db_divergence.argtypes = [vp, dp]
     L.db_stats.argtypes = [vp, dp]
+    L.db_budget.argtypes = [vp, dp]
+    L.db_bpe.argtypes = [vp, ctypes.c_int, dp, dp, dp]
     L.db_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.db_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     L.db_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]

@@ -214,6 +214,37 @@ enum {
 };
 int db_stats(db_ctx* ctx, double* out);
 
+/* The energy-budget terms that need the mean flow as a function of x
+ * (for/diagnostics.f90: compute_TKE 1254-1360, compute_TKE_Production
+ * 1366-1520, compute_MKE_diss 1097-1250, compute_Vorticity 1525-1730), in
+ * FP64 on both precision paths.  The means are those of compute_averages
+ * (676-800): x-z means with homogeneousX, z-means per x for the fronts
+ * (IC_Type 5..8).  out[DB_NBUD][Nyp+2], row r, plane j; zero where a row
+ * does not exist.  Rows:
+ *   tke                  0.5 (u'u' + v'v' + w'w') about the means (GYF rows, v at GY)
+ *   uu_dudx, wu_dwdx     <u'u'>_z dU/dx, <u'w'>_z dW/dx, x-averaged (GYF)
+ *   vu_dvdx, vv_dvdy, uv_dudy, wv_dwdy   the GY-row production terms, with
+ *                        the thermal-wind shear in dW/dy
+ *   epsilon_m            nu <|grad U_mean|^2> (0 with homogeneousX, where
+ *                        the reference skips compute_MKE_diss)
+ *   omega_x, omega_y, omega_z   rms vorticity (omega_x about minus the
+ *                        thermal-wind shear)
+ * The first call allocates FP64 scratch: four physical fields and one
+ * x-half field. */
+enum {
+  DB_BU_TKE, DB_BU_UU_DUDX, DB_BU_WU_DWDX, DB_BU_VU_DVDX, DB_BU_VV_DVDY, DB_BU_UV_DUDY, DB_BU_WV_DWDY,
+  DB_BU_EPSILON_M, DB_BU_OMEGA_X, DB_BU_OMEGA_Y, DB_BU_OMEGA_Z, DB_NBUD
+};
+int db_budget(db_ctx* ctx, double* out);
+
+/* Background potential energy (compute_BPE, for/diagnostics.f90:1733-1856,
+ * after Tseng & Ferziger 2001) from the FP64 buoyancy plus its background
+ * gradient dTHdX (x - Lx/2): the dyf-weighted PDF over nbin bins (the
+ * reference uses nbin = Nx; constant bins over +-1.1 dTHdX Lx/2 with
+ * homogeneousX, cos-spaced over +-Ro_inv for the fronts), normalised to sum
+ * 1, the bin edges th_bin[nbin + 1] and the BPE.  Any output may be NULL. */
+int db_bpe(db_ctx* ctx, int nbin, double* pdf, double* th_bin, double* bpe);
+
 /*
  * Divergence removal that allocates nothing.  No counterpart in the
  * reference (it follows rem_div_chan's arithmetic, for/solver.f90:1302-1379,

@@ -402,12 +402,14 @@ orc_ctx* orc_create(const db_params* p, const double* gy_in) {
   }
   c->w_bc_ymax_c1_transient = c->w_bc_ymax_c1;
 
-  /* init_chan_mpi, for/domain.f90:321-340 and 341-361 with one rank: the
-   * lower branch sets jstart, the upper (same rank) sets jend. */
+  /* init_chan_mpi, for/domain.f90:321-340 with one rank in y: rankY == 0
+   * takes the first branch of the if / else if chain, so jstart follows the
+   * lower BC and jend = jend_th = Nyp whatever the upper BC (the upper
+   * branch, 341-361, runs only on the top rank of several). */
   c->jstart = (p->u_bc_ymin == 1) ? 1 : 2;
-  c->jend = (p->u_bc_ymax == 1) ? Nyp : Nyp - 1;
+  c->jend = Nyp;
   c->jstart_th = (p->th_bc_ymin == 1) ? 1 : 2;
-  c->jend_th = (p->th_bc_ymax == 1) ? Nyp : Nyp - 1;
+  c->jend_th = Nyp;
 
   /* RKW3, for/parameters.f90:176-184 */
   c->delta_t = p->delta_t;
