@@ -124,6 +124,10 @@ class Channel:
     def rem_div_chan(self):
         self._ck(self.L.db_rem_div(self.h))
 
+    def poisson_p_chan(self):
+        """cp from the velocity and buoyancy (restart without pressure)."""
+        self._ck(self.L.db_poisson_p(self.h))
+
     def apply_bc_vel_post(self):
         self._ck(self.L.db_apply_bc_vel_post(self.h))
 

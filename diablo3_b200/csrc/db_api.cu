@@ -1518,19 +1518,34 @@ extern "C" int db_stats(db_ctx* c, double* out) {
   return DB_OK;
 }
 
-// the state's u1, u2, u3, th in FP64 physical space (the budget scratch),
-// whatever the work type of the context
-static int budget_fields(db_ctx* c) {
+// FP64 scratch of the diagnostics (first use): four physical fields and one
+// x-half field
+static int budget_alloc(db_ctx* c) {
   const Geom& g = c->g;
   const size_t Pn = (size_t)g.np * g.pp, H = (size_t)g.np * g.hp;
   for (int f = 0; f < 4; ++f)
     if (!c->bud_phys[f] && balloc(c, (void**)&c->bud_phys[f], Pn * sizeof(double)))
-      return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
+      return fail(c, DB_ERR_CUDA, "diagnostics scratch: out of device memory");
   if (!c->bud_xh && balloc(c, (void**)&c->bud_xh, H * sizeof(double2)))
-    return fail(c, DB_ERR_CUDA, "db_budget: out of device memory");
-  Geom g64 = g;   // FP64 transforms with the built-in launch shapes
+    return fail(c, DB_ERR_CUDA, "diagnostics scratch: out of device memory");
+  return DB_OK;
+}
+
+// FP64 transforms with the built-in launch shapes, whatever the context's
+// work type and tuning
+static Geom fp64_geom(const Geom& g) {
+  Geom g64 = g;
   g64.prec = 0;
   g64.tune_xcps = g64.tune_xgrid = g64.tune_zns = 0;
+  return g64;
+}
+
+// the state's u1, u2, u3, th in FP64 physical space (the budget scratch),
+// whatever the work type of the context
+static int budget_fields(db_ctx* c) {
+  int rc = budget_alloc(c);
+  if (rc) return rc;
+  const Geom g64 = fp64_geom(c->g);
   double2* src[4] = {c->s.cu1, c->s.cu2, c->s.cu3, c->s.cth};
   for (int f = 0; f < 4; ++f) {
     CK(launch_inv_z(g64, fset(src[f]), fset(c->bud_xh), 1, c->st));
@@ -1597,6 +1612,36 @@ extern "C" int db_bpe(db_ctx* c, int nbin, double* pdf, double* th_bin, double* 
   if (pdf) std::copy(P.begin(), P.end(), pdf);
   if (th_bin) std::copy(B.begin(), B.end(), th_bin);
   if (bpe) *bpe = e;
+  return DB_OK;
+}
+
+// poisson_p_chan (for/solver.f90:1382-1590), k_pressure.cu
+extern "C" int db_poisson_p(db_ctx* c) {
+  if (!c) return DB_ERR_ARG;
+  int rc = budget_alloc(c);
+  if (rc) return rc;
+  const Geom g64 = fp64_geom(c->g);
+  const State& s = c->s;
+  cudaStream_t st = c->st;
+  double2 *w1 = s.crs[0], *w2 = s.crs[1], *R = s.crs[2];   // free between substeps
+  double *P1 = c->bud_phys[0], *P2 = c->bud_phys[1], *Q = c->bud_phys[2];
+  CK(cudaMemsetAsync(Q, 0, (size_t)c->g.np * c->g.pp * sizeof(double), st));
+  for (int term = 0; term < 6; ++term) {
+    const bool pair = term >= 3;
+    CK(launch_pp_terms(c->g, s, term, w1, pair ? w2 : nullptr, st));
+    CK(launch_inv_z(g64, fset(w1), fset(c->bud_xh), 1, st));
+    CK(launch_inv_x(g64, fset(c->bud_xh), fset(P1), 1, st));
+    if (pair) {
+      CK(launch_inv_z(g64, fset(w2), fset(c->bud_xh), 1, st));
+      CK(launch_inv_x(g64, fset(c->bud_xh), fset(P2), 1, st));
+    }
+    CK(launch_pp_accum(c->g, P1, P2, pair ? 0 : 1, Q, st));
+  }
+  CK(launch_fwd_x(g64, fset(Q), fset(c->bud_xh), 1, st));
+  CK(launch_fwd_z(g64, fset(c->bud_xh), fset(R), 1, st));
+  CK(launch_pp_solve(c->g, s, R, s.phi_g, reinterpret_cast<double*>(s.crs[3]), st));
+  CK(cudaStreamSynchronize(st));
+  c->launches += 6 * 3 + 3 * 2 + 3;
   return DB_OK;
 }
 

@@ -213,6 +213,13 @@ cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSe
 // PDF of th + dTHdX (x - Lx/2) over planes jstart_th..jend_th (weights dyf)
 cudaError_t launch_bpe_pdf(const Geom& g, const Phys& ph, const double* th, int homx, int nbin, double* pdf,
                            cudaStream_t st);
+// k_pressure.cu: poisson_p_chan's term factors, physical products and the
+// Poisson solve of cp
+cudaError_t launch_pp_terms(const Geom& g, const State& s, int term, double2* w1, double2* w2, cudaStream_t st);
+cudaError_t launch_pp_accum(const Geom& g, const double* p1, const double* p2, int square, double* q,
+                            cudaStream_t st);
+cudaError_t launch_pp_solve(const Geom& g, const State& s, const double2* rhs, double2* gsc, double* bsc,
+                            cudaStream_t st);
 // mixed path: the LES solve's FP64 increments (u1, u2, u3, th) and the
 // FP64 x-half scratch beside them (k_les.cu)
 void thomas_les_inc(const Geom& g, const State& s, double* inc[4], double2* xh64[4]);

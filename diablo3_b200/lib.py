@@ -31,7 +31,7 @@ EXPORTS = (
     "db_set_clock", "db_get_status", "db_clear_status",
     "db_fft_xz_to_fourier", "db_fft_xz_to_physical", "db_fft_xz_to_fourier_dev", "db_fft_xz_to_physical_dev",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
-    "db_courant", "db_divergence", "db_stats", "db_budget", "db_bpe",
+    "db_courant", "db_divergence", "db_stats", "db_budget", "db_bpe", "db_poisson_p",
     "db_autotune", "db_get_tuning", "db_set_tuning", "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
@@ -94,6 +94,7 @@ def load(path: str | None = None):
     L.db_divergence.argtypes = [vp, dp]
     L.db_stats.argtypes = [vp, dp]
     L.db_budget.argtypes = [vp, dp]
+    L.db_poisson_p.argtypes = [vp]
     L.db_bpe.argtypes = [vp, ctypes.c_int, dp, dp, dp]
     L.db_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.db_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]

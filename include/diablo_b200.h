@@ -190,6 +190,12 @@ int db_apply_bc_vel_post(db_ctx* ctx);
  * coefficients.  Replaces courant (for/flow.f90:746-857). */
 int db_courant(db_ctx* ctx, double* delta_t_out);
 
+/* Pressure cp from the velocity and the buoyancy (planes 1..Nyp), for a
+ * restart whose file holds no pressure.  Replaces poisson_p_chan
+ * (for/solver.f90:1382-1590).  FP64 on both precision paths; the first call
+ * allocates the diagnostics scratch (see db_budget). */
+int db_poisson_p(db_ctx* ctx);
+
 /* max over (kx,kz,j) of |ikx u1 + d(u2)/dy + ikz u3| in spectral space at
  * GYF points j = 2..Nyp-1, the quantity rem_div_chan drives to zero. */
 int db_divergence(db_ctx* ctx, double* max_div_out);

@@ -618,6 +618,103 @@ void orc_rem_div_chan(orc_ctx* c) {
 }
 
 /* ---------------------------------------------------------------------- */
+/* poisson_p_chan (for/solver.f90:1382-1590): cp from the velocity and      */
+/* buoyancy, for restarts without pressure.  The right-hand side is the sum */
+/* of (dui/dxj)(duj/dxi) over the three diagonal and the three off-diagonal */
+/* pairs, each formed in physical space from spectral derivatives and sent  */
+/* back, plus the y-derivative of the buoyancy (the (0,0) mode skipped);    */
+/* then one complex Thomas per (kx, kz) with apply_BC_poisson_mpi's rows    */
+/* (2375-2411).  The reference uses cf1..cf3 as its work arrays; here they  */
+/* are separate buffers.                                                    */
+
+static void pp_product(orc_ctx* c, double* w1, double* w2, double fac, int square, cplx* cs) {
+  int Nyp = c->Nyp;
+  orc_fft_xz_to_physical(c, w1);
+  if (!square) orc_fft_xz_to_physical(c, w2);
+  for (int j = 2; j <= Nyp; ++j)
+    for (int k = 0; k < c->Nzp; ++k)
+      for (int i = 0; i < c->Nx; ++i) {
+        const double a = RV(c, w1, i, k, j);
+        RV(c, w1, i, k, j) = square ? a * a : fac * a * RV(c, w2, i, k, j);
+      }
+  orc_fft_xz_to_fourier(c, w1);
+  for (int j = 2; j <= Nyp; ++j)
+    for (int k = 0; k <= c->twoNkz; ++k)
+      for (int i = 0; i < c->Nxp; ++i) cs[(long)j * (c->plane_r / 2) + (long)k * c->NXP1 + i] += CV(c, w1, i, k, j);
+}
+
+void orc_poisson_p_chan(orc_ctx* c) {
+  int Nyp = c->Nyp;
+  double* cu1 = c->arr[DB_CU1]; double* cu2 = c->arr[DB_CU2]; double* cu3 = c->arr[DB_CU3];
+  double* cth = c->arr[DB_CTH]; double* cp = c->arr[DB_CP];
+  double* w1 = (double*)calloc((size_t)c->len, sizeof(double));
+  double* w2 = (double*)calloc((size_t)c->len, sizeof(double));
+  cplx* cs = (cplx*)calloc((size_t)c->len / 2, sizeof(cplx));
+  /* the diagonal terms (dui/dxi)^2 */
+  for (int t = 0; t < 3; ++t) {
+    memset(w1, 0, sizeof(double) * (size_t)c->len);
+    for (int j = 2; j <= Nyp; ++j)
+      for (int k = 0; k <= c->twoNkz; ++k)
+        for (int i = 0; i < c->Nxp; ++i)
+          CV(c, w1, i, k, j) = t == 0 ? c->cikx[i] * CV(c, cu1, i, k, j)
+                             : t == 1 ? (CV(c, cu2, i, k, j + 1) - CV(c, cu2, i, k, j)) / c->dyf[j]
+                                      : c->cikz[k] * CV(c, cu3, i, k, j);
+    pp_product(c, w1, NULL, 1.0, 1, cs);
+  }
+  /* the off-diagonal terms 2 (du1/dy)(du2/dx), 2 (du3/dy)(du2/dz), 2 (du1/dz)(du3/dx) */
+  for (int t = 0; t < 3; ++t) {
+    memset(w1, 0, sizeof(double) * (size_t)c->len);
+    memset(w2, 0, sizeof(double) * (size_t)c->len);
+    for (int j = 2; j <= Nyp; ++j)
+      for (int k = 0; k <= c->twoNkz; ++k)
+        for (int i = 0; i < c->Nxp; ++i) {
+          const cplx v = 0.5 * (CV(c, cu2, i, k, j) + CV(c, cu2, i, k, j + 1));
+          if (t == 0) {
+            CV(c, w1, i, k, j) = (CV(c, cu1, i, k, j + 1) - CV(c, cu1, i, k, j - 1)) / (2. * c->dyf[j]);
+            CV(c, w2, i, k, j) = c->cikx[i] * v;
+          } else if (t == 1) {
+            CV(c, w1, i, k, j) = (CV(c, cu3, i, k, j + 1) - CV(c, cu3, i, k, j - 1)) / (2. * c->dyf[j]);
+            CV(c, w2, i, k, j) = c->cikz[k] * v;
+          } else {
+            CV(c, w1, i, k, j) = c->cikz[k] * CV(c, cu1, i, k, j);
+            CV(c, w2, i, k, j) = c->cikx[i] * CV(c, cu3, i, k, j);
+          }
+        }
+    pp_product(c, w1, w2, 2.0, 0, cs);
+  }
+  /* buoyancy, the (0,0) mode skipped (its hydrostatic part was cancelled) */
+  for (int j = 2; j <= Nyp; ++j)
+    for (int k = 0; k <= c->twoNkz; ++k)
+      for (int i = 0; i < c->Nxp; ++i)
+        if (i != 0 || k != 0)
+          cs[(long)j * (c->plane_r / 2) + (long)k * c->NXP1 + i] +=
+              (CV(c, cth, i, k, j + 1) - CV(c, cth, i, k, j - 1)) / (c->gyf[j + 1] - c->gyf[j - 1]);
+  /* the Poisson solve per (kx, kz) */
+  double* a = (double*)malloc(sizeof(double) * (size_t)(Nyp + 2));
+  double* b = (double*)malloc(sizeof(double) * (size_t)(Nyp + 2));
+  double* u = (double*)malloc(sizeof(double) * (size_t)(Nyp + 2));
+  cplx* g = (cplx*)malloc(sizeof(cplx) * (size_t)(Nyp + 2));
+  for (int k = 0; k <= c->twoNkz; ++k)
+    for (int i = 0; i < c->Nxp; ++i) {
+      for (int j = 0; j <= Nyp + 1; ++j) { a[j] = 0.; b[j] = 1.; u[j] = 0.; g[j] = 0.; }
+      for (int j = 2; j <= Nyp; ++j) {
+        a[j] = 1. / (c->dy[j] * c->dyf[j]);
+        b[j] = -c->kx2[i] - c->kz2[k] - 1. / (c->dy[j + 1] * c->dyf[j]) - 1. / (c->dy[j] * c->dyf[j]);
+        u[j] = 1. / (c->dy[j + 1] * c->dyf[j]);
+        g[j] = -1. * cs[(long)j * (c->plane_r / 2) + (long)k * c->NXP1 + i];
+      }
+      /* apply_BC_poisson_mpi: row 1 Dirichlet for (0,0), Neumann otherwise; row Nyp Neumann */
+      if (i == 0 && k == 0) { b[1] = 1.; u[1] = 0.; g[1] = 0.; }
+      else { b[1] = 1.; u[1] = -1.; g[1] = 0.; }
+      b[Nyp] = -1.; a[Nyp] = 1.; g[Nyp] = 0.;
+      thomas_complex_col(a, b, u, g, Nyp);
+      for (int j = 1; j <= Nyp; ++j) CV(c, cp, i, k, j) = g[j];
+    }
+  free(a); free(b); free(u); free(g);
+  free(w1); free(w2); free(cs);
+}
+
+/* ---------------------------------------------------------------------- */
 /* apply_BC_vel_mpi_post (for/flow.f90:1161-1360)                            */
 
 void orc_apply_bc_vel_post(orc_ctx* c) {

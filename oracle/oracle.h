@@ -54,6 +54,8 @@ int orc_rk_chan_1(orc_ctx* c, int rk_step);
 int orc_step(orc_ctx* c);
 /* rem_div_chan (for/solver.f90:1302-1379). */
 void orc_rem_div_chan(orc_ctx* c);
+/* poisson_p_chan (for/solver.f90:1382-1590): cp from u and th. */
+void orc_poisson_p_chan(orc_ctx* c);
 /* apply_BC_vel_mpi_post (for/flow.f90:1161-1360). */
 void orc_apply_bc_vel_post(orc_ctx* c);
 /* courant (for/flow.f90:746-857) on the physical velocity currently held

@@ -50,6 +50,7 @@ def lib():
         L.orc_step.argtypes = [vp]
         L.orc_step.restype = ip
         L.orc_rem_div_chan.argtypes = [vp]
+        L.orc_poisson_p_chan.argtypes = [vp]
         L.orc_apply_bc_vel_post.argtypes = [vp]
         L.orc_courant_physical.argtypes = [vp]
         L.orc_courant_physical.restype = ctypes.c_double
@@ -146,6 +147,9 @@ class Oracle:
 
     def rem_div(self):
         lib().orc_rem_div_chan(self._h)
+
+    def poisson_p(self):
+        lib().orc_poisson_p_chan(self._h)
 
     def apply_bc_vel_post(self):
         lib().orc_apply_bc_vel_post(self._h)
