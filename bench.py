@@ -7,6 +7,11 @@ front, Re 5000, Ri 1, CFL 0.5 with variable dt), state resident in HBM.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+With the defaults the line also carries, measured in the same run, the
+metric's second arm: ``mixed_dns`` (the same DNS on the mixed-precision
+path) and ``config3`` (the 128x65x128 LES, FP64 AMD against the mixed
+learned closure, per unit simulated time).
+
 N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
 substep has no data-parallel exchange on one instance, so nothing is sharded
 and no collective sits on the data path; rank timings are reduced with MAX.
@@ -297,31 +302,96 @@ def _timed_run(ch, stream, steps, warmup):
     return ms / steps, (st.time - t0) / (ms / 1e3)
 
 
-def run_les_compare(args) -> None:
+def _dns_timed(ch, p, stream, steps, rk, local, precision, les):
+    """Time `steps` steps of a warmed-up channel: CUDA events around the
+    region (max over ranks), stage events inside the step graph, clocks
+    sampled meanwhile; the dominant stage's roofline against the measured
+    HBM copy bandwidth."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from diablo3_b200 import lib as L
+    from diablo3_b200 import replicas, roofline
+    ch._ck(ch.L.db_set_timing(ch.h, 1))
+    ch.step(1)  # capture the timed graph (not timed)
+    torch.cuda.synchronize()
+    n0 = ctypes.c_longlong()
+    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n0)))
+    stage_ms = np.zeros(len(L.STAGES))
+    buf = (ctypes.c_double * len(L.STAGES))()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    replicas.barrier(rk)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        ch.step(1)
+        ch._ck(ch.L.db_stage_times(ch.h, buf, len(L.STAGES)))
+        stage_ms += np.array(buf[:])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    replicas.barrier(rk)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    ch._ck(ch.L.db_set_timing(ch.h, 0))
+    n1 = ctypes.c_longlong()
+    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n1)))
+    ms_max = replicas.max_over_ranks(rk, ms)
+    npts = p.nx * p.ny * p.nz
+    value = replicas.job_rate(npts, 3 * steps, rk, ms_max)
+    if ch.status().flags & 1:
+        raise SystemExit("non-finite values in the flow: run rejected")
+    peak, peak_kind = measured_peak_hbm()
+    per_stage = stage_ms / (3 * steps)  # ms per launch (per substep)
+    dom = int(np.argmax(per_stage))
+    dom_name = L.STAGES[dom]
+    alg = roofline.stage_bytes(p)[dom_name]
+    achieved = alg / (per_stage[dom] / 1e3) / 1e9
+    traffic = None if les else roofline.profiled_traffic(dom_name, ROOT, precision)
+    t_sub = ms_max / steps / 3 / 1e3
+    return {
+        "ms_max": ms_max, "value": value, "clocks": clk, "gpu_launches": int(n1.value - n0.value),
+        "stages_ms_per_substep": {L.STAGES[i]: round(float(per_stage[i]), 4) for i in range(len(L.STAGES))},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "step_alg_bytes": roofline.substep_bytes(p),
+                     "step_frac": roofline.substep_bytes(p) / t_sub / 1e9 / peak,
+                     "ref_seq_bytes": roofline.reference_substep_bytes(p),
+                     "ref_seq_frac": roofline.reference_substep_bytes(p) / t_sub / 1e9 / peak},
+    }
+
+
+def les_compare(config: str, steps: int, warmup: int, autotune: bool = True) -> dict:
     """Config 2 (256x129x256): FP64 AMD LES against the mixed-precision AMD
     LES.  Config 3 (128x65x128): FP64 AMD LES against the mixed-precision
     LES with the learned closure (les_model_type 6).  Both arms run the same
     IC with CFL-limited dt; the comparison is simulated time per wall second.
     The network of config 3 is fitted (tensor-core Adam) to AMD's eddy
     coefficients on the FP64 run's own closure features: its weights do not
-    change its cost, and its accuracy against filtered DNS is what the
-    closure tests establish."""
+    change its cost (AMD is evaluated at every point as the fallback), and
+    its accuracy against filtered DNS is what the closure tests establish."""
     import numpy as np
     import torch
     from diablo3_b200 import sgs_train
     from diablo3_b200.channel import Channel
     from diablo3_b200.grid import create_grid
-    p64 = workload_params(args.config)
+    p64 = workload_params(config)
     gy = create_grid(p64.ny, lz=p64.ly, cs=1.5, grid_type=1)
     stream = torch.cuda.Stream()
     npts = p64.nx * p64.ny * p64.nz
     a = Channel(p64, gy, stream=stream.cuda_stream)
     a.init_flow(seed=0)
-    if not args.no_autotune:
+    if autotune:
         a.autotune()
-    ms_a, rate_a = _timed_run(a, stream, args.steps, args.warmup)
+    ms_a, rate_a = _timed_run(a, stream, steps, warmup)
     net = None
-    if args.config == "config3":
+    if config == "config3":
         nu, ka, feat = a.les_eval(5, features=True)
         rows = slice(3, p64.ny)
         f = torch.from_numpy(np.ascontiguousarray(feat[rows].reshape(-1, 16))).cuda()
@@ -329,7 +399,7 @@ def run_les_compare(args) -> None:
                                        ka[rows, : p64.nz, : p64.nx].reshape(-1)], 1).astype(np.float32)).cuda()
         net, _ = sgs_train.train(f, t, steps=300, batch=65536, lr=1e-3, seed=0)
     a.close()
-    pm = workload_params(args.config)
+    pm = workload_params(config)
     pm.precision = 1
     if net is not None:
         pm.les_model_type = 6
@@ -337,29 +407,40 @@ def run_les_compare(args) -> None:
     if net is not None:
         b.set_sgs_net(net)
     b.init_flow(seed=0)
-    if not args.no_autotune:
+    if autotune:
         b.autotune()
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
     time.sleep(0.5)
-    ms_b, rate_b = _timed_run(b, stream, args.steps, args.warmup)
+    ms_b, rate_b = _timed_run(b, stream, steps, warmup)
     clk = clocks.stop()
     b.close()
     arm_b = "mixed precision, learned closure (les_model_type 6)" if net is not None else "mixed precision, AMD"
+    return {
+        "workload": WORKLOAD_DESC[config] + "; " + arm_b + " vs FP64 AMD", "grid_xyz": [p64.nx, p64.ny, p64.nz],
+        "points": npts, "l2": l2_note(resident_bytes(pm)), "steps": steps, "warmup": warmup,
+        "fp64_amd": {"ms_per_step": ms_a, "sim_time_per_wall_s": rate_a,
+                     "grid_pt_substeps_per_s": npts * 3 / (ms_a / 1e3)},
+        "candidate": {"arm": arm_b, "ms_per_step": ms_b, "sim_time_per_wall_s": rate_b,
+                      "grid_pt_substeps_per_s": npts * 3 / (ms_b / 1e3)},
+        "speedup_per_unit_sim_time": rate_b / rate_a,
+        "network": "fitted to AMD on the FP64 run's closure features (cost does not depend on the weights)"
+        if net is not None else None,
+        "clocks": clk,
+    }
+
+
+def run_les_compare(args) -> None:
+    c = les_compare(args.config, args.steps, args.warmup, not args.no_autotune)
+    ms_b = c["candidate"]["ms_per_step"]
     line = {
-        "metric": METRIC, "value": npts * 3 / (ms_b / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "metric": METRIC, "value": c["points"] * 3 / (ms_b / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded finite-front IC, no dataset)",
-        "config": {"workload": WORKLOAD_DESC[args.config] + "; " + arm_b + " vs FP64 AMD",
-                   "grid_xyz": [p64.nx, p64.ny, p64.nz], "points": npts, "parallelism": "single GPU",
-                   "l2": l2_note(resident_bytes(pm))},
-        "les_compare": {
-            "fp64_amd": {"ms_per_step": ms_a, "sim_time_per_wall_s": rate_a,
-                         "grid_pt_substeps_per_s": npts * 3 / (ms_a / 1e3)},
-            "candidate": {"arm": arm_b, "ms_per_step": ms_b, "sim_time_per_wall_s": rate_b,
-                          "grid_pt_substeps_per_s": npts * 3 / (ms_b / 1e3)},
-            "speedup_per_unit_sim_time": rate_b / rate_a},
-        "clocks": clk,
+        "config": {"workload": c["workload"], "grid_xyz": c["grid_xyz"], "points": c["points"],
+                   "parallelism": "single GPU", "l2": c["l2"]},
+        "les_compare": {k: c[k] for k in ("fp64_amd", "candidate", "speedup_per_unit_sim_time", "network")},
+        "clocks": c["clocks"],
     }
     print(json.dumps(line), flush=True)
 
@@ -377,6 +458,8 @@ def main():
                     help="mixed: FP32 transforms/products/SGS, FP64 state and solves")
     ap.add_argument("--les", action="store_true", help="AMD LES closure (les_model_type 5) on")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision DNS and the 128x65x128 LES comparison keys")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -425,49 +508,8 @@ def main():
         ch.step(1)
     torch.cuda.synchronize()
 
-    # timed region: K steps, stage events recorded inside the step graph
-    ch._ck(ch.L.db_set_timing(ch.h, 1))
-    ch.step(1)  # capture the timed graph (not timed)
-    torch.cuda.synchronize()
-    n0 = ctypes.c_longlong()
-    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n0)))
-    stage_ms = np.zeros(L.DB_NSTAGES if hasattr(L, "DB_NSTAGES") else len(L.STAGES))
-    buf = (ctypes.c_double * len(L.STAGES))()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.5)
-    barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        ch.step(1)
-        ch._ck(ch.L.db_stage_times(ch.h, buf, len(L.STAGES)))
-        stage_ms += np.array(buf[:])
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    clk = clocks.stop()
-    n1 = ctypes.c_longlong()
-    ch._ck(ch.L.db_kernel_launches(ch.h, ctypes.byref(n1)))
-    ms_max = replicas.max_over_ranks(rk, ms)
-    value = replicas.job_rate(npts, 3 * args.steps, rk, ms_max)
-    st = ch.status()
-    if st.flags & 1:
-        raise SystemExit("non-finite values in the flow: run rejected")
-
-    # roofline of the dominant kernel
-    peak, peak_kind = measured_peak_hbm()
-    per_stage = stage_ms / (3 * args.steps)  # ms per launch (per substep)
-    dom = int(np.argmax(per_stage))
-    dom_name = L.STAGES[dom]
-    alg = roofline.stage_bytes(p)[dom_name]
-    achieved = alg / (per_stage[dom] / 1e3) / 1e9
-    traffic = roofline.profiled_traffic(dom_name, ROOT, args.precision)
-    if traffic is not None and args.les:
-        traffic = None   # the committed captures are of the plain substep
+    dns = _dns_timed(ch, p, stream, args.steps, rk, local, args.precision, args.les)
+    ms_max, value, clk = dns["ms_max"], dns["value"], dns["clocks"]
 
     # end to end through the C-ABI with host buffers
     e2e = None
@@ -500,6 +542,34 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.config)
 
+    # the metric's second arm in the same run (one GPU, the default workload):
+    # the mixed-precision DNS, and the 128x65x128 LES comparison (FP64 AMD
+    # against the mixed learned closure, per unit simulated time)
+    extras = {}
+    if world == 1 and not args.no_extras and args.config == "config1" and args.precision == "fp64" and not args.les:
+        ch.close()
+        ch = None
+        ke = max(3, min(args.steps, 10))
+        pm = workload_params("config1")
+        pm.precision = 1
+        chm = Channel(pm, gy, stream=stream.cuda_stream)
+        chm.init_flow(seed=rank)
+        tm = None
+        if not args.no_autotune:
+            tm = chm.autotune().strip().splitlines()[-1].replace("chosen: ", "")
+        for _ in range(args.warmup):
+            chm.step(1)
+        torch.cuda.synchronize()
+        dm = _dns_timed(chm, pm, stream, ke, rk, local, "mixed", False)
+        chm.close()
+        extras["mixed_dns"] = {
+            "workload": WORKLOAD_DESC["config1"] + workload_suffix(argparse.Namespace(les=False, precision="mixed")),
+            "value": dm["value"], "unit": UNIT, "steps": ke, "ms_per_step": dm["ms_max"] / ke,
+            "dtype": "f32+f64", "launch_shapes": tm or "built-in defaults", "gpu_launches": dm["gpu_launches"],
+            "stages_ms_per_substep": dm["stages_ms_per_substep"], "roofline": dm["roofline"],
+            "clocks": dm["clocks"]}
+        extras["config3"] = les_compare("config3", ke, args.warmup, not args.no_autotune)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -510,25 +580,20 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": l2_note(resident_bytes(p)),
                    "launch_shapes": tuned or "built-in defaults"},
-        "gpu_launches": int(n1.value - n0.value),
-        "stages_ms_per_substep": {L.STAGES[i]: round(float(per_stage[i]), 4) for i in range(len(L.STAGES))},
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "alg_bytes_per_launch": alg,
-                     "step_alg_bytes": roofline.substep_bytes(p),
-                     "step_frac": roofline.substep_bytes(p) / (ms_max / args.steps / 3 / 1e3) / 1e9 / peak,
-                     "ref_seq_bytes": roofline.reference_substep_bytes(p),
-                     "ref_seq_frac": roofline.reference_substep_bytes(p) / (ms_max / args.steps / 3 / 1e3) / 1e9
-                     / peak},
+        "gpu_launches": dns["gpu_launches"],
+        "stages_ms_per_substep": dns["stages_ms_per_substep"],
+        "roofline": dns["roofline"],
         "clocks": clk,
     }
     if e2e:
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    line.update(extras)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ch.close()
+    if ch is not None:
+        ch.close()
     replicas.finish(rk)
 
 
