@@ -1,4 +1,4 @@
-// fft_smem.cuh -- complex helpers (FP64 and FP32), the in-register DFTs of
+// cplx_dft.cuh -- complex helpers (FP64 and FP32), the in-register DFTs of
 // radix 2, 4 and 8, and the radix plan of a length-N transform (sm_100a).
 // The transforms themselves are in fft_reg.cuh: register-resident Stockham
 // passes with shared-memory exchanges between them.

@@ -5,7 +5,7 @@
 #pragma once
 
 #include "db_kernels.cuh"
-#include "fft_smem.cuh"
+#include "cplx_dft.cuh"
 
 namespace db {
 

@@ -4,7 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "db_common.cuh"
-#include "fft_smem.cuh"
+#include "cplx_dft.cuh"
 
 namespace db {
 

@@ -23,7 +23,7 @@
 // bank conflicts), optionally a second one to alternate exchanges.
 #pragma once
 
-#include "fft_smem.cuh"
+#include "cplx_dft.cuh"
 
 // barrier over the threads of the calling sequence (see fft_sync_t)
 #define SEQ_SYNC(N) ::db::fft_sync_t<::db::FftShape<N>::warp>(::db::FftShape<N>::T)

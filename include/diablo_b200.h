@@ -4,8 +4,9 @@
  * This is the drop-in boundary for DIABLO 3.0's channel solver
  * (wienkers/diablo3, Fortran 90).  Each entry point replaces one Fortran
  * subroutine; the reference interface it stands in for is cited beside it.
- * A Fortran caller binds these through ISO_C_BINDING (interface block in
- * INTEGRATION.md); Python binds them through ctypes (diablo3_b200/lib.py).
+ * A Fortran caller binds these through an ISO_C_BINDING interface block
+ * (one bind(C) function per entry, arguments by value or as arrays);
+ * Python binds them through ctypes (diablo3_b200/lib.py).
  *
  * Conventions
  *  - Coordinates follow the Fortran code: x streamwise (periodic), y

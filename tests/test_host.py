@@ -181,9 +181,12 @@ def test_read_inputs_rejects_old_versions(tmp_path):
 
 
 def test_reference_setup_parses_when_present():
-    d = "/root/reference/setups/finite_front_LES"
-    if not os.path.isdir(d):
-        pytest.skip("reference tree not mounted")
+    """The reference's own finite_front_LES setup files, when the
+    DIABLO3_REFERENCE environment variable names a reference checkout."""
+    root = os.environ.get("DIABLO3_REFERENCE", "")
+    d = os.path.join(root, "setups", "finite_front_LES")
+    if not root or not os.path.isdir(d):
+        pytest.skip("set DIABLO3_REFERENCE to a reference checkout")
     p = read_inputs(d)
     assert (p.nx, p.ny, p.nz) == (2048, 65, 128)
     assert p.use_les == 1 and p.les_model_type == 5 and p.ic_type == 7
