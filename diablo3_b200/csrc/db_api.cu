@@ -281,12 +281,17 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
   s.cu1 = sp[0]; s.cu2 = sp[1]; s.cu3 = sp[2]; s.cp = sp[3]; s.cth = sp[4];
   s.cf1 = sp[5]; s.cf2 = sp[6]; s.cf3 = sp[7]; s.cfth = sp[8];
   s.phi_g = sp[9]; s.pfac = sp[10];
-  // z-pass scratch: all 8 for the FP64 LES z-pass (three stages), the last 4
-  // for the split spectral z-pass (Z(M_e))
-  for (int i = (!p->precision && p->use_les) ? 0 : 4; i < 8; ++i)
-    if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
-  for (int i = 0; i < 4; ++i)   // cr of the spectral CN solve
+  for (int i = 0; i < 4; ++i)   // NL (or Z(N)) and the forward sweep of the spectral CN solve
     if ((rc = dalloc(c, &s.crs[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+  // FP64: Z(M) of the spectral solve's z-pass (nls[4..7]); the FP64 LES
+  // z-pass (three stages) uses all 8, the first 4 shared with the spectral
+  // solve, which never runs in the same substep
+  if (!p->precision) {
+    for (int i = 4; i < 8; ++i)
+      if ((rc = dalloc(c, &s.nls[i], S))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
+    if (p->use_les)
+      for (int i = 0; i < 4; ++i) s.nls[i] = s.crs[i];
+  }
   const size_t eP = phys_elem(c), eH = xh_elem(c);
   for (int i = 0; i < 8; ++i)
     if ((rc = balloc(c, (void**)&s.xh[i], H * eH))) { db_finalize(c); g_init_err = "db_init: out of device memory"; return rc; }
@@ -855,23 +860,23 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   const bool cfl_step = rk == 2 && c->p.variable_dt;
   if (spectral) {
     // without eddy viscosity the CN matrices are the same in every column:
-    // z-FFT + spectral RHS into cr (FP64), the CN solves on the retained
-    // modes in spectral space (k_thomas_spec), no transforms of cr or u
+    // z-FFT of the products, then the spectral RHS and the CN solves on the
+    // retained modes (FP64), no transforms of cr or u
     if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
-    if ((e = launch_zpass_spec(g, c->ph, s, rk, st))) return e;
+    if ((e = launch_zpass_spec(g, s, st))) return e;
     mark(c, rk, 4);
     mark(c, rk, 5);
-    if ((e = launch_thomas_spec(g, s, st))) return e;
+    if ((e = launch_rhs_cn(g, c->ph, s, rk, st))) return e;
     mark(c, rk, 6);
-    n += 3;
+    n += 4;
     // CFL on the last substep from the new velocity before the projection
     // (solver.f90:1241-1244): u1..u3 to physical space for it
     if (cfl_step) {
-      if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3), fset(s.xh[0], s.xh[1], s.xh[2]), 3, st))) return e;
-      if ((e = launch_inv_x(g, fset(s.xh[0], s.xh[1], s.xh[2]), fset(s.u1, s.u2, s.u3), 3, st))) return e;
       CflCtl ctl{c->p.cfl, c->p.time_limit, c->p.variable_dt, c->p.update_dt, 0};
-      if ((e = launch_courant(g, c->ph, s, ctl, st))) return e;
-      n += 4;
+      if ((e = launch_inv_z(g, fset(s.cu1, s.cu2, s.cu3), fset(s.xh[0], s.xh[1], s.xh[2]), 3, st))) return e;
+      if ((e = launch_inv_x_cfl(g, c->ph, s, ctl, fset(s.xh[0], s.xh[1], s.xh[2]), st))) return e;
+      if ((e = launch_courant_final(c->ph, s, ctl, st))) return e;
+      n += 3;
     }
     mark(c, rk, 7);
     mark(c, rk, 8);

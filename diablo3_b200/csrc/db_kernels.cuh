@@ -22,6 +22,11 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #ifndef DB_LB_FFT
 #define DB_LB_FFT 3
 #endif
+// k_rhs_cn: minimum resident 32-thread CTAs per SM (13 keeps every mode's
+// thread of a 512x512 plane resident at once: 128 registers)
+#ifndef DB_RHSCN_LB
+#define DB_RHSCN_LB 13
+#endif
 #ifndef DB_LB_ZPASS
 #define DB_LB_ZPASS 2
 #endif
@@ -30,15 +35,6 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #endif
 #ifndef DB_LB_PROD
 #define DB_LB_PROD 4
-#endif
-// the z-pass of the substep without LES per work type: 1 = forward z-FFT of
-// the 8 product fields into spectral scratch, then the RHS mode by mode
-// (k_rhs_modes); 0 = one fused kernel (the FP64 one spills at 128 registers)
-#ifndef DB_ZSPEC_SPLIT_F64
-#define DB_ZSPEC_SPLIT_F64 1
-#endif
-#ifndef DB_ZSPEC_SPLIT_F32
-#define DB_ZSPEC_SPLIT_F32 1
 #endif
 constexpr int MAXF = 12;
 
@@ -60,6 +56,9 @@ cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
 cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask = 0);
 // accumulate: out += transform, with rows 0, 1, Nyp, Nyp+1 based on ghost
 // (when given) instead of out
+// NL_e = (Z(N_e) + i kz Z(M_e)) / Nz of the four equations from the 8 x-half
+// product fields (in.p[2e], in.p[2e+1]) into out.p[e], FP64 packed spectral
+cudaError_t launch_fwd_z_nl(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st);
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, int accumulate = 0,
                          const double2* ghost = nullptr);
 // ghost (optional): rows 0, 1, Nyp, Nyp+1 of field f are read from
@@ -173,10 +172,11 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
                              const double2* ghost = nullptr);
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
-// the substep without LES: forward z-pass of the products + spectral RHS
-// into s.crs (FP64), then the CN solves in spectral space on the state
-cudaError_t launch_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
-cudaError_t launch_thomas_spec(const Geom& g, const State& s, cudaStream_t st);
+// the substep without LES: the nonlinear terms NL_e of the 4 equations into
+// spectral scratch (s.crs), then the spectral RHS joined with the CN solves
+// in spectral space (k_rhs_cn, k_cn_back), the state in place
+cudaError_t launch_zpass_spec(const Geom& g, const State& s, cudaStream_t st);
+cudaError_t launch_rhs_cn(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st);
 
 struct CflCtl {
   double cfl, time_limit;
@@ -184,6 +184,10 @@ struct CflCtl {
   int force;               // 1: evaluate regardless of variable_dt/time_step
 };
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st);
+// courant from the x-half u1, u2, u3 (in): their inverse x-pass reduces the
+// CFL terms instead of storing the physical fields, then k_courant_final
+cudaError_t launch_inv_x_cfl(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, FieldSet in, cudaStream_t st);
+cudaError_t launch_courant_final(const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st);
 cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp, cudaStream_t st);
 cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st);
 cudaError_t launch_apply_dt(DevScalars* sc, cudaStream_t st);

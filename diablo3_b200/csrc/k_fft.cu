@@ -167,6 +167,62 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
   }
 }
 
+// The nonlinear terms of the substep without LES on the mixed path: for
+// equation e (blockIdx.z; 0 u1, 1 u3, 2 u2, 3 th) and ns kx columns of
+// plane j, NL_e = (Z(N_e) + i kz Z(M_e)) / Nz from the x-half product fields
+// in.p[2e] (N_e) and in.p[2e+1] (M_e), FP64 into out.p[e] (packed
+// spectral): one output field instead of two.  The first half of the CTA
+// transforms M, the second half N (one transform per thread, so neither
+// holds two sequences' registers); the M half parks Z(M) in shared memory
+// in natural order for the N half.  Planes outside the equation's solved
+// range (which the RHS does not read) are skipped.  (For FP64 fields the
+// two-field form of k_fwd_z measured faster: its 4-column CTAs read 64-byte
+// row segments, where the halves of a 256-thread CTA hold 2 columns.)
+template <int N>
+constexpr int znl_threads() { return FftShape<N>::T >= 256 ? 2 * FftShape<N>::T : 256; }
+template <int N, typename R>
+__global__ void __launch_bounds__(znl_threads<N>(), FftShape<N>::T >= 256 ? 1 : DB_LB_FFT)
+    k_fwd_z_nl(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int ns) {
+  using C = typename CplxOf<R>::type;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  C* sm = reinterpret_cast<C*>(sm_raw);
+  using S = FftShape<N>;
+  constexpr int E = S::E, T = S::T;
+  const int half = threadIdx.x / (ns * T);   // 0: M, 1: N (whole warps)
+  const int t = threadIdx.x % (ns * T);
+  const int seq = t % ns, lane = t / ns;     // column-fastest, as k_fwd_z
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, e = blockIdx.z;
+  const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
+  const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
+  if (j < jlo || j > jhi) return;   // uniform over the CTA
+  const bool active = kx < g.kxs;
+  C* sq = sm + (half * ns + seq) * (padded(N) + 1);    // exchange buffer of this sequence
+  C* sz = sm + (2 * ns + seq) * (padded(N) + 1);       // Z(M) of column seq
+  const C* src = (const C*)in.p[2 * e + 1 - half] + (long long)j * g.hp + kx;
+  C v[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) v[q] = active ? __ldg(src + (long long)(lane + q * T) * g.kxs) : mkc<C>(0, 0);
+  fft_reg_lazy<N, -1, true>(v, lane, active, sq, tw_z<R>(g));
+  if (half == 0) {
+#pragma unroll
+    for (int q = 0; q < E; ++q) sz[pidx(lane + q * T)] = v[q];
+  }
+  __syncthreads();
+  if (half == 0 || !active) return;
+  const double inz = 1.0 / (double)N;
+  double2* dst = (double2*)out.p[e] + (long long)j * g.sp + kx;
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const int z = lane + q * T;
+    const int kzp = (z <= g.nkz) ? z : (z >= N - g.nkz ? z - N + g.nkzp : -1);
+    if (kzp >= 0) {
+      const double kzv = g.kz[kzp];
+      const double2 zm = to_d2(sz[pidx(z)]), zn = to_d2(v[q]);
+      dst[(long long)kzp * g.kxs] = make_double2((zn.x - kzv * zm.y) * inz, (zn.y + kzv * zm.x) * inz);
+    }
+  }
+}
+
 // packed spectral (FP64) -> Xh (zero-filled de-aliased rows, unnormalised);
 // fields f with bit f of dmask set are differentiated in z (times i kz).
 // mean (optional): the (0,0) mode of fields 0..3, i.e. the plane mean of
@@ -299,9 +355,23 @@ __global__ void __launch_bounds__(256, 2) k_fwd_x_st(const __grid_constant__ Fie
   }
 }
 
-template <int N, typename R>
+// CFL: instead of storing u1, u2, u3 (fields 0..2), reduce the courant
+// terms of their physical values (k_courant_reduce's per-point maximum is
+// the maximum over the three fields' own terms, so each field reduces its
+// own): |u1 - U| / dx, |u2| / dy(j), |u3 + W| / dz over the planes the
+// reference's courant visits (for/flow.f90:777-806), then CFL / max per CTA
+// into the device minimum, as k_courant_reduce does.  Planes outside that
+// range are not transformed.
+struct CflArgs {
+  Phys ph;
+  CflCtl ctl;
+  DevScalars* sc;
+};
+
+template <int N, typename R, bool CFL>
 __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g,
-                                                      unsigned dmask, int nblk, int nitems) {
+                                                      unsigned dmask, int nblk, int nitems,
+                                                      const __grid_constant__ CflArgs cf) {
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -319,6 +389,12 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
     const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
     return (const C*)in.p[f] + (long long)j * g.hp + (long long)(2 * ns * b) * g.kxs;
   };
+  // CFL: courant's gate (for/flow.f90:746-750) and plane range
+  if (CFL && !cf.ctl.force && !(cf.ctl.variable_dt && (cf.sc->time_step % cf.ctl.update_dt) == 0)) return;
+  const int jlo = CFL ? (cf.ph.front ? g.jstart : 1) : 0;
+  const int jhi = CFL ? (cf.ph.front ? g.jend : g.ny) : 0;
+  double amax = 0.0;
+  bool bad = false;
   if (threadIdx.x == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
@@ -348,6 +424,10 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
       return;
     }
     const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    if (CFL && (j < jlo || j > jhi)) {   // uniform over the CTA: not a courant plane
+      __syncthreads();
+      continue;
+    }
     const C* ia = reinterpret_cast<const C*>(reinterpret_cast<const unsigned char*>(stage0) + s * item_bytes) +
                   (2 * seq) * g.kxs;
     const C* ib = ia + g.kxs;
@@ -370,14 +450,49 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
       v[q] = z;
     }
     fft_reg_lazy<N, +1>(v, lane, true, sq, twt);
-    R* ra = (R*)out.p[f] + (long long)j * g.pp + (long long)(2 * (ns * b + seq)) * g.nx;
-    R* rb = ra + g.nx;
+    if (CFL) {
+      // |u1 - c1| / dx, |u2| / dy, |u3 + c3| / dz with k_courant_reduce's operations
+      const double fr = cf.ph.ro_inv / cf.ph.delta;
+      double c = 0.0, w;
+      if (f == 0) {
+        c = cf.ph.front ? cf.ph.dthdz * g.gyf[j] / fr : 0.0;   // -c1, subtracted below as v - c1
+        w = 1.0 / cf.ph.dx;
+      } else if (f == 1) {
+        w = 1.0 / g.dy[j];
+      } else {
+        c = cf.ph.front ? (1.0 / fr) * cf.ph.dthdx * (g.gyf[j] - 0.5 * cf.ph.ly) : 0.0;   // c3
+        w = 1.0 / cf.ph.dz;
+      }
 #pragma unroll
-    for (int q = 0; q < E; ++q) {
-      ra[lane + q * T] = v[q].x;
-      rb[lane + q * T] = v[q].y;
+      for (int q = 0; q < E; ++q) {
+        const double va = (double)v[q].x, vb = (double)v[q].y;
+        const double ta = (f == 0 ? fabs(va - c) : (f == 1 ? fabs(va) : fabs(va + c))) * w;
+        const double tb = (f == 0 ? fabs(vb - c) : (f == 1 ? fabs(vb) : fabs(vb + c))) * w;
+        bad = bad || !(ta <= 1.7976931348623157e308) || !(tb <= 1.7976931348623157e308);
+        amax = fmax(amax, fmax(ta, tb));
+      }
+    } else {
+      R* ra = (R*)out.p[f] + (long long)j * g.pp + (long long)(2 * (ns * b + seq)) * g.nx;
+      R* rb = ra + g.nx;
+#pragma unroll
+      for (int q = 0; q < E; ++q) {
+        ra[lane + q * T] = v[q].x;
+        rb[lane + q * T] = v[q].y;
+      }
     }
     __syncthreads();
+  }
+  if (CFL) {
+    if (bad) atomicOr(&cf.sc->flags, DB_FLAG_NONFINITE);
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax = fmax(amax, red[w]);
+      if (amax > 0.0)
+        atomicMin(&cf.sc->dt_min_bits, (unsigned long long)__double_as_longlong(cf.ctl.cfl / amax));
+    }
   }
 }
 
@@ -452,10 +567,26 @@ static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   const int cps = xpass_cps<N>(g);
   const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * nf;
   const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
-  smem_attr(k_inv_x_st<N, R>, smem);
+  smem_attr(k_inv_x_st<N, R, false>, smem);
   const int gmax = xpass_ctas_per_sm(g) * sm_count();
   const int grid = nitems < gmax ? nitems : gmax;
-  k_inv_x_st<N, R><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems);
+  k_inv_x_st<N, R, false><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems, CflArgs{});
+}
+template <int N, typename R>
+static void go_inv_x_cfl_t(const Geom& g, FieldSet in, const CflArgs& cf, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int cps = xpass_cps<N>(g);
+  const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * 3;
+  const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
+  smem_attr(k_inv_x_st<N, R, true>, smem);
+  const int gmax = xpass_ctas_per_sm(g) * sm_count();
+  const int grid = nitems < gmax ? nitems : gmax;
+  k_inv_x_st<N, R, true><<<grid, cps * FftShape<N>::T, smem, st>>>(in, FieldSet{}, g, 0u, nblk, nitems, cf);
+}
+template <int N>
+static void go_inv_x_cfl(const Geom& g, FieldSet in, const CflArgs& cf, cudaStream_t st) {
+  if (g.prec) go_inv_x_cfl_t<N, float>(g, in, cf, st);
+  else go_inv_x_cfl_t<N, double>(g, in, cf, st);
 }
 template <int N, typename R>
 static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc, const double2* ghost,
@@ -481,6 +612,20 @@ static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   smem_attr(k_inv_z<N, R>, smem);
   k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost,
                                                                                           mean);
+}
+template <int N, typename R>
+static void go_fwd_z_nl_t(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  constexpr int T = FftShape<N>::T;
+  const int ns = znl_threads<N>() / (2 * T);
+  const size_t smem = (size_t)3 * ns * (padded(N) + 1) * sizeof(C);
+  smem_attr(k_fwd_z_nl<N, R>, smem);
+  k_fwd_z_nl<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, 4), 2 * ns * T, smem, st>>>(in, out, g, ns);
+}
+template <int N>
+static void go_fwd_z_nl(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st) {
+  if (g.prec) go_fwd_z_nl_t<N, float>(g, in, out, st);
+  else go_fwd_z_nl_t<N, double>(g, in, out, st);
 }
 template <int N>
 static void go_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st) {
@@ -513,6 +658,15 @@ cudaError_t launch_fwd_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
 cudaError_t launch_inv_x(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, unsigned dmask) {
   if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
   DB_DISPATCH_N(g.nx, go_inv_x, g, in, out, nf, dmask, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_inv_x_cfl(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, FieldSet in, cudaStream_t st) {
+  const CflArgs cf{ph, ctl, s.sc};
+  DB_DISPATCH_N(g.nx, go_inv_x_cfl, g, in, cf, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_fwd_z_nl(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st) {
+  DB_DISPATCH_N(g.nz, go_fwd_z_nl, g, in, out, st);
   return cudaGetLastError();
 }
 cudaError_t launch_fwd_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaStream_t st, int accumulate,

@@ -6,18 +6,18 @@
 //                  (solver.f90:655-815, 914-956) fused with their forward
 //                  x-FFTs; x-derivatives (i kx) applied in the x-half space so
 //                  only 8 x-half fields leave the kernel.
-//  k_zpass_rhs   : forward z-FFT of those 8 fields, the spectral linear terms
-//                  (viscous, Coriolis, buoyancy, background-front advection,
-//                  thermal-wind advection: solver.f90:396-609, 35-111) and the
-//                  RK combination cr = cu + zeta h cf_old - h grad p + beta h cf
-//                  (solver.f90:396-456, 824-838, 966-973); cr goes out as an
-//                  FP64 spectral field (no LES) or through the inverse z-FFT
-//                  to the physical solve (LES).
+//  k_zpass_rhs   : (with LES) forward z-FFT of those 8 fields, the spectral
+//                  linear terms (viscous, Coriolis, buoyancy, background-front
+//                  advection, thermal-wind advection: solver.f90:396-609,
+//                  35-111) and the RK combination cr = cu + zeta h cf_old -
+//                  h grad p + beta h cf (solver.f90:396-456, 824-838,
+//                  966-973), cr through the inverse z-FFT to the physical solve.
 //  k_tri_coef    : the four implicit systems' rows incl. BC rows
 //                  (solver.f90:1012-1233, 1901-2324), LU-factored once per
 //                  substep (all (x,z) columns share them without LES).
-//  k_thomas_spec : without LES, the CN solves of th, u2, u1, u3 per retained
-//                  Fourier mode (explicit CN term + Thomas sweeps,
+//  k_rhs_cn,     : without LES, after the forward z-FFT of the 8 fields: the
+//  k_cn_back       spectral RHS and the CN solves of th, u2, u1, u3 per
+//                  retained Fourier mode (explicit CN term + Thomas sweeps,
 //                  solver.f90:850-870, 981-989, 1691-1852), FP64.
 //  k_rem_div     : per (kx,kz) column, divergence, complex Thomas, projection
 //                  and pressure update (solver.f90:1302-1379, 1261-1267).
@@ -286,7 +286,6 @@ __global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_
       const bool r2 = in_rng(j, 2, g.ny);
       const bool rt = in_rng(j, g.jstart_th, g.jend_th);
       const ProdY<R> y(g, j);
-      const long long o0 = (long long)j * g.pp + (long long)z * g.nx;
       const long long hrow = (long long)j * g.hp + (long long)z * g.kxs;
       for (int grp = 0; grp < 2; ++grp) {
         const bool zero = (grp == 0 && !r1) || (grp == 1 && !(r2 || rt));   // uniform over the CTA
@@ -373,37 +372,76 @@ __global__ void __launch_bounds__(3 * FftShape<N>::T * prod_zr<N>()) k_products_
 
 // ---------------------------------------------------------------------------
 // The spectral RHS at one mode (kx, kzp) of plane j for equation e (0 u1,
-// 1 u3, 2 u2, 3 th): the linear terms into cf (stored), the RK combination
+// 1 u3, 2 u2, 3 th): the linear terms cf (to be stored), the RK combination
 // cr = cu + zeta h cf_old - h grad p + beta h cf (solver.f90:396-609,
-// 824-838, 966-973, 35-111) returned; with INC the increment cr - base.
-// nl = (Z(N) + i kz Z(M)) / Nz, the nonlinear term of that mode.
-template <bool INC>
-__device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, const Phys& ph, int rk, int e, int j,
-                                             int kx, int kzp, double2 nl, const double2* __restrict__ ghost) {
+// 824-838, 966-973, 35-111).  rhs_load reads the state values equation e
+// needs at address a (the others stay zero), rhs_eval combines them, so a
+// caller can issue the loads of several planes before their arithmetic.
+struct RhsIn {
+  double2 own;          // the equation's own field
+  double2 cu1, cu3, cth, cp;
+  double2 nb2, nbp;     // e 0/1: cu2 of planes j and j+1; e 2: cth and cp of plane j-1
+  double2 cfo;          // cf of the previous substep (rk > 0)
+};
+__device__ __forceinline__ RhsIn rhs_load(const State& s, const Geom& g, int rk, int e, long long a) {
+  const double2 z = make_double2(0.0, 0.0);
+  RhsIn v{z, z, z, z, z, z, z, z};
+  if (e == 0 || e == 1) {
+    v.cu1 = s.cu1[a]; v.cu3 = s.cu3[a]; v.cth = s.cth[a]; v.cp = s.cp[a];
+    v.own = (e == 0) ? v.cu1 : v.cu3;
+    v.nb2 = s.cu2[a]; v.nbp = s.cu2[a + g.sp];
+    if (rk > 0) v.cfo = (e == 0) ? s.cf1[a] : s.cf3[a];
+  } else if (e == 2) {
+    v.own = s.cu2[a]; v.cth = s.cth[a]; v.cp = s.cp[a];
+    v.nb2 = s.cth[a - g.sp]; v.nbp = s.cp[a - g.sp];
+    if (rk > 0) v.cfo = s.cf2[a];
+  } else {
+    v.own = s.cth[a]; v.cu1 = s.cu1[a]; v.cu3 = s.cu3[a];
+    if (rk > 0) v.cfo = s.cfth[a];
+  }
+  return v;
+}
+__device__ __forceinline__ double2* rhs_cf(const State& s, int e) {
+  return (e == 0) ? s.cf1 : (e == 1 ? s.cf3 : (e == 2 ? s.cf2 : s.cfth));
+}
+// The constants of one mode and substep (the same on every plane):
+// temp3..5 = zeta h, h, beta h; the wavenumbers; |k|^(2 beta).
+struct RhsK {
+  double temp3, temp4, temp5, kxv, kzv, kk;
+};
+__device__ __forceinline__ RhsK rhs_consts(const State& s, const Geom& g, const Phys& ph, int rk, int kx, int kzp) {
+  RhsK c;
   const double hb = s.sc->h_bar[rk];
-  const double temp3 = zeta_bar(rk) * hb, temp4 = hb, temp5 = beta_bar(rk) * hb;
+  c.temp3 = zeta_bar(rk) * hb;
+  c.temp4 = hb;
+  c.temp5 = beta_bar(rk) * hb;
+  c.kxv = g.kx[kx];
+  c.kzv = g.kz[kzp];
+  const double k2 = c.kxv * c.kxv + c.kzv * c.kzv;
+  c.kk = (ph.beta == 1.0) ? k2 : pow(k2, ph.beta);
+  return c;
+}
+// nl = (Z(N) + i kz Z(M)) / Nz, the nonlinear term of the mode; with INC the
+// increment cr - own is returned.
+template <bool INC>
+__device__ __forceinline__ double2 rhs_eval(const State& s, const Geom& g, const Phys& ph, int rk, int e, int j,
+                                            int kx, int kzp, double2 nl, const RhsIn& v, const RhsK& c,
+                                            double2& cf) {
+  const double temp3 = c.temp3, temp4 = c.temp4, temp5 = c.temp5;
   const double nu = ph.nu, f = ph.ro_inv / ph.delta;
   const double tw = ph.delta / ph.ro_inv;  // delta / Ro_inv
-  const double kxv = g.kx[kx], kzv = g.kz[kzp];
-  const long long sp0 = (long long)j * g.sp + kx;
-  const int kxc = kx;
-  const bool beta1 = (ph.beta == 1.0);
-  const long long a = sp0 + (long long)kzp * g.kxs;
-  const double k2 = kxv * kxv + kzv * kzv;
-  const double kk = beta1 ? k2 : pow(k2, ph.beta);
-  double2 cf, cr, cuf;
+  const double kxv = c.kxv, kzv = c.kzv, kk = c.kk;
+  double2 cr;
   if (e == 0 || e == 1) {
-    const double2 cu1 = s.cu1[a], cu3 = s.cu3[a], cth = s.cth[a], cp = s.cp[a];
-    const double2 c2a = s.cu2[a], c2b = s.cu2[a + g.sp];
-    const double2 v2 = make_double2(0.5 * (c2a.x + c2b.x), 0.5 * (c2a.y + c2b.y));
-    const double2 cu = (e == 0) ? cu1 : cu3;
+    const double2 v2 = make_double2(0.5 * (v.nb2.x + v.nbp.x), 0.5 * (v.nb2.y + v.nbp.y));
+    const double2 cu = v.own;
     cf = cscale(cu, -nu * kk);
     if (e == 0) {
-      cf = cadd(cf, cscale(cu3, f));
-      cf = cadd(cf, cscale(cth, ph.grav_x));
+      cf = cadd(cf, cscale(v.cu3, f));
+      cf = cadd(cf, cscale(v.cth, ph.grav_x));
     } else {
-      cf = csub(cf, cscale(cu1, f));
-      cf = cadd(cf, cscale(cth, ph.grav_z));
+      cf = csub(cf, cscale(v.cu1, f));
+      cf = cadd(cf, cscale(v.cth, ph.grav_z));
     }
     if (ph.front_tw) {
       const double y = g.gyf[j] - 0.5 * ph.ly;
@@ -417,21 +455,19 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
     }
     cf = csub(cf, nl);
     const double kd = (e == 0) ? kxv : kzv;
-    cuf = cu;
     cr = INC ? make_double2(0.0, 0.0) : cu;
-    if (rk > 0) cr = cadd(cr, cscale((e == 0) ? s.cf1[a] : s.cf3[a], temp3));
-    cr = csub(cr, cscale(cmul_i(cp, 1.0), temp4 * kd));
+    if (rk > 0) cr = cadd(cr, cscale(v.cfo, temp3));
+    cr = csub(cr, cscale(cmul_i(v.cp, 1.0), temp4 * kd));
     if (e == 0 && kx == 0 && kzp == 0) {
       if (ph.f_type == 1) cr.x -= temp4 * ph.px0;
       if (ph.f_type == 2) cr.x -= temp4 * (ph.px0 + ph.amp_omega0 * cos(ph.omega0 * s.sc->time));
     }
     cr = cadd(cr, cscale(cf, temp5));
-    if (e == 0) s.cf1[a] = cf; else s.cf3[a] = cf;
   } else if (e == 2) {
-    const double2 cu2 = s.cu2[a];
+    const double2 cu2 = v.own;
     cf = cscale(cu2, -nu * kk);
     if (!(kx == 0 && kzp == 0)) {
-      const double2 t0 = s.cth[a], tm = s.cth[a - g.sp];
+      const double2 t0 = v.cth, tm = v.nb2;
       const double w = ph.grav_y / (2.0 * g.dy[j]);
       cf = cadd(cf, make_double2(w * (t0.x * g.dyf[j - 1] + tm.x * g.dyf[j]),
                                  w * (t0.y * g.dyf[j - 1] + tm.y * g.dyf[j])));
@@ -443,18 +479,16 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
       cf = csub(cf, cscale(t1, -1.0 * ph.dthdz * y * tw * kxv));
     }
     cf = csub(cf, nl);
-    cuf = cu2;
     cr = INC ? make_double2(0.0, 0.0) : cu2;
-    if (rk > 0) cr = cadd(cr, cscale(s.cf2[a], temp3));
-    const double2 dp = csub(s.cp[a], s.cp[a - g.sp]);
+    if (rk > 0) cr = cadd(cr, cscale(v.cfo, temp3));
+    const double2 dp = csub(v.cp, v.nbp);
     cr = csub(cr, cscale(dp, temp4 / g.dy[j]));
     cr = cadd(cr, cscale(cf, temp5));
-    s.cf2[a] = cf;
   } else {
-    const double2 cth = s.cth[a];
+    const double2 cth = v.own;
     cf = cscale(cth, -(nu / ph.pr) * kk);
-    cf = csub(cf, cscale(s.cu1[a], ph.dthdx));
-    cf = csub(cf, cscale(s.cu3[a], ph.dthdz));
+    cf = csub(cf, cscale(v.cu1, ph.dthdx));
+    cf = csub(cf, cscale(v.cu3, ph.dthdz));
     if (ph.front_tw) {
       const double y = g.gyf[j] - 0.5 * ph.ly;
       const double2 t1 = cmul_i(cth, 1.0);
@@ -462,18 +496,29 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
       cf = csub(cf, cscale(t1, tw * (-1.0) * ph.dthdz * y * kxv));
     }
     cf = csub(cf, nl);
-    cuf = cth;
     cr = INC ? make_double2(0.0, 0.0) : cth;
-    if (rk > 0) cr = cadd(cr, cscale(s.cfth[a], temp3));
+    if (rk > 0) cr = cadd(cr, cscale(v.cfo, temp3));
     cr = cadd(cr, cscale(cf, temp5));
-    s.cfth[a] = cf;
   }
-  if (INC && ghost) {   // ghost rows: base is the overlay, cr - base = (cu - base) + increment
+  return cr;
+}
+// Load, evaluate and store cf at one mode; with INC and a ghost overlay
+// the rows whose base the inverse transforms took from the overlay return
+// cr - base = (cu - base) + increment.
+template <bool INC>
+__device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, const Phys& ph, int rk, int e, int j,
+                                             int kx, int kzp, double2 nl, const double2* __restrict__ ghost) {
+  const long long a = (long long)j * g.sp + (long long)kzp * g.kxs + kx;
+  const RhsIn v = rhs_load(s, g, rk, e, a);
+  double2 cf;
+  double2 cr = rhs_eval<INC>(s, g, ph, rk, e, j, kx, kzp, nl, v, rhs_consts(s, g, ph, rk, kx, kzp), cf);
+  rhs_cf(s, e)[a] = cf;
+  if (INC && ghost) {
     const int qg = (j <= 1) ? j : (j >= g.ny ? j - g.ny + 2 : -1);
     if (qg >= 0) {
       const int gf = (e == 0) ? 0 : (e == 1 ? 2 : (e == 2 ? 1 : 3));
-      const double2 base = ghost[(long long)(4 * gf + qg) * g.sp + (long long)kzp * g.kxs + kxc];
-      cr = cadd(cr, csub(cuf, base));
+      const double2 base = ghost[(long long)(4 * gf + qg) * g.sp + (long long)kzp * g.kxs + kx];
+      cr = cadd(cr, csub(v.own, base));
     }
   }
   return cr;
@@ -483,16 +528,13 @@ __device__ __forceinline__ double2 rhs_point(const State& s, const Geom& g, cons
 // One CTA = KT kx columns of plane j; thread t owns column t % KT and the
 // z-set {lane + q N/8}.  Equation e: 0 -> u1, 1 -> u3, 2 -> u2, 3 -> th;
 // x-half inputs xh[2e] (N_e), xh[2e+1] (M_e); cr_e overwrites xh[2e].
-// SPEC (the substep without LES, either work type): no inverse z-pass; cr
-// goes out in FP64 as a packed spectral field (s.crs[e]) for the CN solve
-// in spectral space (k_thomas_spec).
-template <int N, typename R, bool EFAST, bool SPEC = false>
+template <int N, typename R, bool EFAST>
 __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS : 1))
     k_zpass_rhs(State s, Geom g, Phys ph, int rk, const double2* __restrict__ ghost) {
   // FP32 work type: write the increment cr - base (base = the state as the
   // inverse transforms saw it), so FP32 rounding scales with the substep's
   // change, not with the field
-  constexpr bool INC = sizeof(R) == sizeof(float) && !SPEC;
+  constexpr bool INC = sizeof(R) == sizeof(float);
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -529,7 +571,6 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
     C* xin_n = (C*)s.xh[2 * e];
     const C* xin_m = (const C*)s.xh[2 * e + 1];
     if (!in_rng(j, jlo, jhi)) {
-      if (SPEC) return;   // the spectral solve takes BC values on these planes
       if (active)
 #pragma unroll
         for (int q = 0; q < E; ++q) xin_n[h0 + (long long)(lane + q * T) * g.kxs] = mkc<C>(0, 0);
@@ -561,13 +602,8 @@ __global__ void __launch_bounds__(KT * FftShape<N>::T, (N <= 512 ? DB_LB_ZPASS :
       const double2 zmq = to_d2(sm_z[pidx(zz)]), zn = to_d2(vn[q]);
       const double2 nl = make_double2((zn.x - kzv * zmq.y) * inz, (zn.y + kzv * zmq.x) * inz);
       double2 cr = rhs_point<INC>(s, g, ph, rk, e, j, kxc, kzp, nl, ghost);
-      if (SPEC) {
-        s.crs[e][(long long)j * g.sp + (long long)kzp * g.kxs + kxc] = (kxc <= g.nkx) ? cr : make_double2(0.0, 0.0);
-        continue;
-      }
       vn[q] = from_d2<C>(cr);
     }
-    if (SPEC) return;
     __syncthreads();
     ZFFT(+1, vn);
     if (active)
@@ -733,13 +769,113 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // column: the BC rows carry their constant value in the (0,0) mode and zero
 // in every other mode.  The inverse x/z transforms of cr, the physical
 // solve and the forward transforms of the new state drop out, and the
-// solve runs in FP64 on both work types.  A spectral plane is viewed as
-// 2 sp doubles (real and imaginary parts are separate real columns of the
-// real matrix); one thread per column and equation (blockIdx.y, k_tri_coef
-// order th, u2, u1, u3) runs the plain Thomas sweeps with the shared LU
-// factors (row-coefficient loads uniform over a warp, batches of TB rows
-// with their loads issued first, g written into the state in place), cr from s.crs, the state updated in place.
-__global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ State s, Geom g) {
+// solve runs in FP64 on both work types.  Real and imaginary parts of a
+// mode are two real columns of the same real system, with the LU factors
+// k_tri_coef shares.
+//
+// k_rhs_cn: one thread per retained mode walks the planes upward and runs
+// the four equations (z-pass order 0 u1, 1 u3, 2 u2, 3 th) together,
+// joining the spectral RHS with the forward sweep: NL from the z-pass (or
+// its Z(N), Z(M) parts, SPLITZ), cr and cf (stored) by rhs_eval, the
+// explicit CN term from
+// the old state planes j-1..j+1 and y_j = v_j + a'_j y_{j-1}; y_j
+// overwrites NL of plane j.  The planes j-1, j, j+1 of cu1, cu3, cu2, cth
+// (the CN explicit terms and the cross terms of the RHS) and cp of planes
+// j-1, j stay in registers as the walk moves up, so each state plane is
+// loaded once for all four equations (13 loads per plane and mode, 17 with
+// SPLITZ), and
+// the state is only read (cf apart).  Every mode's thread is resident at
+// once (a second wave would walk all planes again with few threads).
+template <bool SPLITZ>
+__global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constant__ State s, Geom g, Phys ph, int rk,
+                                                            const __grid_constant__ FieldSet nl) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= g.sp) return;
+  const int np = g.np;
+  const long long sp = g.sp;
+  const int kzp = m / g.kxs, kx = m % g.kxs;
+  const RhsK kc = rhs_consts(s, g, ph, rk, kx, kzp);
+  const bool m0 = (m == 0);   // the (0,0) mode carries the BC constants
+  // z-pass order 0 u1, 1 u3, 2 u2, 3 th; k_tri_coef order th, u2, u1, u3
+  const double2* const U[4] = {s.cu1 + m, s.cu3 + m, s.cu2 + m, s.cth + m};
+  const int lo[4] = {g.jstart, g.jstart, 2, g.jstart_th};
+  const int hi[4] = {g.jend, g.jend, g.ny, g.jend_th};
+  const TriRow* const Rw[4] = {s.tri + 2 * np, s.tri + 3 * np, s.tri + np, s.tri};
+  double2 um[4], uc[4], y[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    um[e] = make_double2(0.0, 0.0);
+    uc[e] = U[e][0];
+    y[e] = make_double2(0.0, 0.0);
+  }
+  double2 pm = make_double2(0.0, 0.0);   // cp of plane j-1
+  for (int j = 0; j < np; ++j) {
+    const long long a = (long long)j * sp;
+    double2 un[4], nlv[4], zmv[4], cfo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const bool rr = in_rng(j, lo[e], hi[e]);
+      un[e] = (j + 1 < np) ? U[e][a + sp] : make_double2(0.0, 0.0);
+      nlv[e] = rr ? ((const double2*)nl.p[e])[a + m] : make_double2(0.0, 0.0);
+      if (SPLITZ) zmv[e] = rr ? ((const double2*)nl.p[4 + e])[a + m] : make_double2(0.0, 0.0);
+      cfo[e] = (rr && rk > 0) ? rhs_cf(s, e)[a + m] : make_double2(0.0, 0.0);
+    }
+    const double2 cpj = s.cp[a + m];
+    if (SPLITZ) {   // NL = Z(N) + i kz Z(M), both already scaled by 1/Nz
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        nlv[e] = make_double2(nlv[e].x - kc.kzv * zmv[e].y, nlv[e].y + kc.kzv * zmv[e].x);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const TriRow* row = Rw[e] + j;
+      double2 cr = make_double2(0.0, 0.0);
+      if (in_rng(j, lo[e], hi[e])) {
+        RhsIn v;
+        v.own = uc[e];
+        v.cu1 = uc[0];
+        v.cu3 = uc[1];
+        v.cth = uc[3];
+        v.cp = cpj;
+        v.nb2 = (e == 2) ? um[3] : uc[2];   // u2: cth of plane j-1; u1, u3: cu2 of plane j
+        v.nbp = (e == 2) ? pm : un[2];      // u2: cp of plane j-1;  u1, u3: cu2 of plane j+1
+        v.cfo = cfo[e];
+        double2 cf;
+        cr = rhs_eval<false>(s, g, ph, rk, e, j, kx, kzp, nlv[e], v, kc, cf);
+        rhs_cf(s, e)[a + m] = cf;
+      }
+      double2 w;
+      if (row->is_bc) {
+        w = make_double2(m0 ? row->bc : 0.0, 0.0);
+      } else {
+        w.x = cr.x + (row->cn_hi * (un[e].x - uc[e].x) - row->cn_lo * (uc[e].x - um[e].x));
+        w.y = cr.y + (row->cn_hi * (un[e].y - uc[e].y) - row->cn_lo * (uc[e].y - um[e].y));
+      }
+      if (j == 0) {
+        y[e] = w;
+      } else {
+        y[e].x = w.x + row->ap * y[e].x;
+        y[e].y = w.y + row->ap * y[e].y;
+      }
+      ((double2*)nl.p[e])[a + m] = y[e];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      um[e] = uc[e];
+      uc[e] = un[e];
+    }
+    pm = cpj;
+  }
+}
+
+// k_cn_back: back substitution per real column (2 sp doubles per plane)
+// and equation (blockIdx.y, k_tri_coef order th, u2, u1, u3) from the y
+// values k_rhs_cn left in the scratch, batches of TB planes loaded first;
+// the new state is written on the planes the reference's solve stores,
+// the others keep their values.  A non-finite new state is reported as
+// DB_FLAG_NONFINITE.
+__global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s, Geom g,
+                                                 const __grid_constant__ FieldSet nl) {
   constexpr int TB = 8;
   const long long ncol = 2 * g.sp;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -748,45 +884,19 @@ __global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ Sta
   const int np = g.np, Nyp = g.ny;
   const long long pp = ncol;
   const TriRow* Rw = s.tri + eq * np;
-  // z-pass equation order of s.crs: 0 u1, 1 u3, 2 u2, 3 th
   const int ze = (eq == 0) ? 3 : (eq == 1 ? 2 : (eq == 2 ? 0 : 1));
   double* u = (double*)((eq == 0) ? s.cth : (eq == 1 ? s.cu2 : (eq == 2 ? s.cu1 : s.cu3))) + c;
-  const double* r = (const double*)s.crs[ze] + c;
-  const bool m0 = (c == 0);   // real part of the (0,0) mode
+  const double* yv = (const double*)nl.p[ze] + c;
   const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
   const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-  const double k0 = u[0], k1 = u[pp], kb = u[(long long)(np - 2) * pp], kt = u[(long long)(np - 1) * pp];
-  double um = 0.0, uc = k0, y = 0.0;
-  for (int jb = 0; jb < np; jb += TB) {
-    double xr[TB], xu[TB];
-#pragma unroll
-    for (int q = 0; q < TB; ++q) {
-      const int j = jb + q;
-      xr[q] = (j < np) ? r[(long long)j * pp] : 0.0;
-      xu[q] = (j + 1 < np) ? u[(long long)(j + 1) * pp] : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < TB; ++q) {
-      const int j = jb + q;
-      if (j >= np) break;
-      const TriRow* row = Rw + j;
-      const double un = xu[q];
-      const double v = row->is_bc ? (m0 ? row->bc : 0.0)
-                                  : xr[q] + (row->cn_hi * (un - uc) - row->cn_lo * (uc - um));
-      y = (j == 0) ? v : v + row->ap * y;
-      u[(long long)j * pp] = y;
-      um = uc;
-      uc = un;
-    }
-  }
   double xn = 0.0;
-  bool bad = false;   // a non-finite new state (reported as DB_FLAG_NONFINITE)
+  bool bad = false;
   for (int jt = np - 1; jt >= 0; jt -= TB) {
     double xg[TB];
 #pragma unroll
     for (int q = 0; q < TB; ++q) {
       const int j = jt - q;
-      xg[q] = (j >= 0) ? u[(long long)j * pp] : 0.0;
+      xg[q] = (j >= 0) ? yv[(long long)j * pp] : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < TB; ++q) {
@@ -796,9 +906,7 @@ __global__ void __launch_bounds__(128) k_thomas_spec(const __grid_constant__ Sta
       const double xv = (j == np - 1) ? xg[q] * ib : xg[q] * ib - Rw[j].u * ib * xn;
       xn = xv;
       bad = bad || !(fabs(xv) <= 1.7976931348623157e308);
-      const bool st = (j >= lo && j <= hi);
-      const double old = (j == 0) ? k0 : (j == 1 ? k1 : (j == np - 2 ? kb : kt));
-      u[(long long)j * pp] = st ? xv : old;
+      if (j >= lo && j <= hi) u[(long long)j * pp] = xv;
     }
   }
   if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
@@ -1109,33 +1217,6 @@ static void go_zpass_t(const Geom& g, const Phys& ph, const State& s, int rk, co
   const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
   k_zpass_rhs<N, R, EFAST><<<grid, KT * T, smem, st>>>(s, g, ph, rk, ghost);
 }
-template <int N, typename R>
-static void go_zpass_spec_t(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  constexpr int T = FftShape<N>::T;
-  constexpr bool EFAST = sizeof(R) == sizeof(double);
-  size_t smem = (size_t)KT * (3 * padded(N) + 1) * sizeof(typename CplxOf<R>::type);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_zpass_rhs<N, R, EFAST, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const dim3 grid = EFAST ? dim3(4, g.kxs / KT, g.np) : dim3(g.kxs / KT, g.np, 4);
-  k_zpass_rhs<N, R, EFAST, true><<<grid, KT * T, smem, st>>>(s, g, ph, rk, nullptr);
-}
-// split form: Z(N_e) / Nz into s.crs[e], Z(M_e) / Nz into s.nls[4 + e], then
-// cr over s.crs[e] in place (k_rhs_modes)
-static void go_zpass_spec_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  const FieldSet nl = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
-  launch_fwd_z(g, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]), nl, 8, st);
-  k_rhs_modes<<<dim3(4, (g.nkzp * g.kxs + 255) / 256, g.np), 256, 0, st>>>(s, g, ph, rk, nl);
-}
-template <int N>
-static void go_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  if (g.prec) {
-    if (DB_ZSPEC_SPLIT_F32) go_zpass_spec_split(g, ph, s, rk, st);
-    else go_zpass_spec_t<N, float>(g, ph, s, rk, st);
-  } else {
-    if (DB_ZSPEC_SPLIT_F64) go_zpass_spec_split(g, ph, s, rk, st);
-    else go_zpass_spec_t<N, double>(g, ph, s, rk, st);
-  }
-}
 template <int N>
 static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
   const FieldSet nl = fset(s.nls[0], s.nls[1], s.nls[2], s.nls[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
@@ -1171,14 +1252,23 @@ cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int 
   DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, st);
   return cudaGetLastError();
 }
-cudaError_t launch_zpass_spec(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
-  if (!s.crs[0] || !s.nls[4]) return cudaErrorInvalidValue;
-  DB_DISPATCH_N2(g.nz, go_zpass_spec, g, ph, s, rk, st);
-  return cudaGetLastError();
+// without LES: the nonlinear terms into spectral scratch, then the spectral
+// RHS with the CN solves.  FP64 fields: Z(N_e) / Nz into s.crs[e] and
+// Z(M_e) / Nz into s.nls[4 + e] (k_fwd_z, 4-column CTAs), combined in
+// k_rhs_cn; FP32 fields: NL_e into s.crs[e] (k_fwd_z_nl).
+cudaError_t launch_zpass_spec(const Geom& g, const State& s, cudaStream_t st) {
+  if (!s.crs[0] || (!g.prec && !s.nls[4])) return cudaErrorInvalidValue;
+  if (!g.prec)
+    return launch_fwd_z(g, fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]),
+                        fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]), 8, st);
+  return launch_fwd_z_nl(g, fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]),
+                         fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3]), st);
 }
-cudaError_t launch_thomas_spec(const Geom& g, const State& s, cudaStream_t st) {
-  const long long ncol = 2 * g.sp;
-  k_thomas_spec<<<dim3((unsigned)((ncol + 127) / 128), 4), 128, 0, st>>>(s, g);
+cudaError_t launch_rhs_cn(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
+  const FieldSet nl = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
+  if (!g.prec) k_rhs_cn<true><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
+  else k_rhs_cn<false><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
+  k_cn_back<<<dim3((unsigned)((2 * g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
@@ -1191,6 +1281,10 @@ cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl
   const dim3 grid(16, 74);   // x: within a row, y: rows
   if (g.prec) k_courant_reduce<float><<<grid, 256, 0, st>>>(s, g, ph, ctl);
   else k_courant_reduce<double><<<grid, 256, 0, st>>>(s, g, ph, ctl);
+  k_courant_final<<<1, 1, 0, st>>>(s.sc, ph, ctl);
+  return cudaGetLastError();
+}
+cudaError_t launch_courant_final(const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
   k_courant_final<<<1, 1, 0, st>>>(s.sc, ph, ctl);
   return cudaGetLastError();
 }

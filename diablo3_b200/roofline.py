@@ -14,13 +14,22 @@ transforms of cr and of the new state drop out:
   inv_z      4 S  -> 4 Xh           cu1, cu2, cu3, cth to x-half
   inv_x      4 Xh -> 4 P            to physical u1, u2, u3, th
   products   4 P  -> 8 Xh           11 products + x-FFT, x-derivatives folded
-  zpass_rhs  8 Xh + 9 S -> 8 S      z-FFT, spectral RHS (cu, cp, cth, cf_old
-                                    in; cf and cr out)
-  thomas     8 S  -> 4 S            cr and cu in (CN explicit), cu out
-  courant    (3 S + 6 Xh + 6 P) / 3 u1..u3 to physical space and the CFL
-                                    reduction, on the third substep only
+  zpass_rhs  8 Xh -> 8 S            z-FFT of the 8 product fields (FP64:
+                                    Z(N_e), Z(M_e); the mixed path writes
+                                    the 4 terms NL_e = Z(N_e) + i kz Z(M_e):
+                                    8 Xh -> 4 S)
+  thomas     8 S + 9 S -> 8 S       spectral RHS joined with the CN solves:
+                                    Z(N), Z(M) (mixed: NL, 4 S), cu1, cu2,
+                                    cu3, cth, cp, cf_old in; cf and the new cu
+                                    out (the forward sweep's y values are a
+                                    round trip that is not counted)
+  courant    (3 S + 6 Xh) / 3       u1..u3 inverse z, then their inverse x
+                                    reducing the CFL terms (no physical
+                                    store), on the third substep only
   rem_div    4 S  -> 4 S            cu1, cu2, cu3, cp in and out
-At 512x257x512 this is ~46 P, i.e. ~370 B per grid point and substep.
+At 512x257x512 this is ~46 P, i.e. ~369 B per grid point and substep for
+FP64 (a z-pass fused with the RHS would save the 8 S of Z(N), Z(M): its
+FP64 form spills and ran slower).
 
 The reference's own sequence (cr to physical space, physical CN solves,
 new state back to Fourier space; the LES substep still runs it) adds
@@ -80,14 +89,15 @@ def stage_bytes(p) -> dict:
         return _physical_path_bytes(p)
     u = units(p)
     P, X, S = u["P"], u["Xh"], u["S"]
+    mixed = bool(getattr(p, "precision", 0))
     return {
         "inv_z": 4 * S + 4 * X,
         "inv_x": 4 * X + 4 * P,
         "products": 4 * P + 8 * X,
-        "zpass_rhs": 8 * X + 17 * S,
+        "zpass_rhs": 8 * X + (4 if mixed else 8) * S,
         "inv_x_r": 0.0,
-        "thomas": 12 * S,
-        "courant": ((3 * S + 6 * X + 6 * P) / 3.0) if p.variable_dt else 0.0,
+        "thomas": (21 if mixed else 25) * S,
+        "courant": ((3 * S + 6 * X) / 3.0) if p.variable_dt else 0.0,
         "fwd_x": 0.0,
         "fwd_z": 0.0,
         "rem_div": 8 * S,

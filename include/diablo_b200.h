@@ -373,9 +373,11 @@ enum db_stage {
   DB_ST_INV_Z = 0,     /* cu -> x-half, 4 fields      (fft.f90:322-337)   */
   DB_ST_INV_X = 1,     /* x-half -> u, 4 fields       (fft.f90:364-372)   */
   DB_ST_PRODUCTS = 2,  /* 11 products + x-FFT         (solver.f90:655-964) */
-  DB_ST_ZPASS_RHS = 3, /* z-FFT + spectral RHS + inverse z of cr          */
-  DB_ST_INV_X_R = 4,   /* cr x-half -> r, 4 fields                        */
-  DB_ST_THOMAS = 5,    /* CN explicit + Thomas, 4 eqs (solver.f90:1012-1233) */
+  DB_ST_ZPASS_RHS = 3, /* z-FFT + spectral RHS + inverse z of cr; without
+                          LES the z-FFT of the products only             */
+  DB_ST_INV_X_R = 4,   /* cr x-half -> r, 4 fields (with LES)             */
+  DB_ST_THOMAS = 5,    /* CN explicit + Thomas, 4 eqs (solver.f90:1012-1233);
+                          without LES with the spectral RHS, per mode     */
   DB_ST_COURANT = 6,   /* CFL reduction (rk_step 3)   (flow.f90:746-857)  */
   DB_ST_FWD_X = 7,     /* u -> x-half, 4 fields                           */
   DB_ST_FWD_Z = 8,     /* x-half -> cu, 4 fields                          */

@@ -201,7 +201,10 @@ def test_roofline_model_totals():
     u = roofline.units(p)
     total_p = roofline.substep_bytes(p) / u["P"]
     assert 40 < total_p < 50
-    assert b["thomas"] == 12 * u["S"]
+    assert b["thomas"] == 25 * u["S"] and b["zpass_rhs"] == 8 * u["Xh"] + 8 * u["S"]
+    bm = roofline.stage_bytes(make_params(nx=512, ny=257, nz=512, variable_dt=1, precision=1))
+    um = roofline.units(make_params(nx=512, ny=257, nz=512, precision=1))
+    assert bm["thomas"] == 21 * um["S"] and bm["zpass_rhs"] == 8 * um["Xh"] + 4 * um["S"]
     assert b["inv_x_r"] == b["fwd_x"] == b["fwd_z"] == 0
     ref_p = roofline.reference_substep_bytes(p) / u["P"]
     assert 60 < ref_p < 75
