@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
+
 import os
 import statistics
 import subprocess
@@ -35,44 +35,7 @@ METRIC = "grid-pt RK substeps/s on 1 B200: FP64 plain vs mixed+learned SGS at st
 UNIT = "grid-pt substeps/s"
 
 
-def workload_params(name: str):
-    from diablo3_b200.params import make_params
-    if name == "config1":
-        return make_params(
-            nx=512, ny=257, nz=512, lx=2 * math.pi, lz=2 * math.pi, ly=2.0,
-            re=5000.0, pr=1.0, ri=1.0, ro=1.0, delta=1.0, grav_y=1.0, ic_type=4, kick=1e-3,
-            delta_t=1e-3, variable_dt=1, cfl=0.5, update_dt=1, time_limit=1e9,
-            u_bc_ymin=0, w_bc_ymin=0, v_bc_ymin=0, th_bc_ymin=1,
-            u_bc_ymax=1, w_bc_ymax=1, v_bc_ymax=0, th_bc_ymax=1,
-            th_bc_ymin_c1=1.0, th_bc_ymax_c1=1.0)
-    if name == "slab":
-        p = workload_params("config1")
-        p.ny = 65  # 512x65x512: same planes, fields still > L2, for ncu captures
-        return p
-    if name == "config0":
-        p = workload_params("config1")
-        p.nx, p.ny, p.nz, p.re, p.variable_dt = 64, 65, 64, 1000.0, 0
-        return p
-    if name in ("config2", "config3"):
-        # finite front (IC_type 6, front width 0.5), AMD LES, CFL-limited dt
-        p = workload_params("config1")
-        p.ic_type, p.delta = 6, 0.5
-        p.use_les, p.les_model_type, p.create_new_flow = 1, 5, 0
-        if name == "config2":
-            p.nx, p.ny, p.nz, p.re = 256, 129, 256, 1e5
-        else:
-            p.nx, p.ny, p.nz, p.re = 128, 65, 128, 1e4
-        return p
-    raise ValueError(name)
-
-
-WORKLOAD_DESC = {
-    "config1": "plain FP64 DNS, infinite front, 512x257x512 (x,y,z), Re 5000, Ri 1 (M2=N2=f=1), CFL 0.5",
-    "config0": "plain FP64 DNS, infinite front, 64x65x64, Re 1000, fixed dt 1e-3",
-    "slab": "plain FP64 DNS, infinite front, 512x65x512 (profiling case), Re 5000, Ri 1, CFL 0.5",
-    "config2": "LES, finite front (IC 6, width 0.5), 256x129x256, Re 1e5, AMD closure, CFL 0.5",
-    "config3": "LES, finite front (IC 6, width 0.5), 128x65x128, Re 1e4, CFL 0.5",
-}
+from diablo3_b200.workloads import WORKLOAD_DESC, workload_params  # noqa: E402
 
 
 def workload_suffix(args) -> str:
@@ -372,13 +335,10 @@ def les_compare(config: str, steps: int, warmup: int, autotune: bool = True) -> 
     LES.  Config 3 (128x65x128): FP64 AMD LES against the mixed-precision
     LES with the learned closure (les_model_type 6).  Both arms run the same
     IC with CFL-limited dt; the comparison is simulated time per wall second.
-    The network of config 3 is fitted (tensor-core Adam) to AMD's eddy
-    coefficients on the FP64 run's own closure features: its weights do not
-    change its cost (AMD is evaluated at every point as the fallback), and
-    its accuracy against filtered DNS is what the closure tests establish."""
-    import numpy as np
+    The network of config 3 is the one trained on a resolved (512x257x512
+    FP64) run of the same flow filtered onto this grid; its accuracy against
+    the filtered resolved run is what the closure tests establish."""
     import torch
-    from diablo3_b200 import sgs_train
     from diablo3_b200.channel import Channel
     from diablo3_b200.grid import create_grid
     p64 = workload_params(config)
@@ -392,12 +352,10 @@ def les_compare(config: str, steps: int, warmup: int, autotune: bool = True) -> 
     ms_a, rate_a = _timed_run(a, stream, steps, warmup)
     net = None
     if config == "config3":
-        nu, ka, feat = a.les_eval(5, features=True)
-        rows = slice(3, p64.ny)
-        f = torch.from_numpy(np.ascontiguousarray(feat[rows].reshape(-1, 16))).cuda()
-        t = torch.from_numpy(np.stack([nu[rows, : p64.nz, : p64.nx].reshape(-1),
-                                       ka[rows, : p64.nz, : p64.nx].reshape(-1)], 1).astype(np.float32)).cuda()
-        net, _ = sgs_train.train(f, t, steps=300, batch=65536, lr=1e-3, seed=0)
+        # the network trained on a 512x257x512 FP64 DNS of this flow filtered
+        # 4x4x4 onto this grid (closure_study.run; weights in the package)
+        from diablo3_b200 import closure_study
+        net = closure_study.load_net(os.path.join(ROOT, "diablo3_b200", "data", "closure_config3.npz"))
     a.close()
     pm = workload_params(config)
     pm.precision = 1
@@ -424,7 +382,8 @@ def les_compare(config: str, steps: int, warmup: int, autotune: bool = True) -> 
         "candidate": {"arm": arm_b, "ms_per_step": ms_b, "sim_time_per_wall_s": rate_b,
                       "grid_pt_substeps_per_s": npts * 3 / (ms_b / 1e3)},
         "speedup_per_unit_sim_time": rate_b / rate_a,
-        "network": "fitted to AMD on the FP64 run's closure features (cost does not depend on the weights)"
+        "network": "trained on a 512x257x512 FP64 DNS of the flow filtered 4x4x4 onto this grid "
+                   "(diablo3_b200/closure_study.py, weights diablo3_b200/data/closure_config3.npz)"
         if net is not None else None,
         "clocks": clk,
     }

@@ -24,6 +24,20 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #endif
 // k_rhs_cn: minimum resident 32-thread CTAs per SM (13 keeps every mode's
 // thread of a 512x512 plane resident at once: 128 registers)
+// k_cn_back: one thread per mode (1) or per real column (0), planes per batch
+#ifndef DB_CNBACK_CPLX
+#define DB_CNBACK_CPLX 0
+#endif
+#ifndef DB_CNBACK_TB
+#define DB_CNBACK_TB 4
+#endif
+// k_rem_div: minimum resident CTAs per SM, planes per batch
+#ifndef DB_REMDIV_LB
+#define DB_REMDIV_LB 6
+#endif
+#ifndef DB_REMDIV_RB
+#define DB_REMDIV_RB 4
+#endif
 #ifndef DB_RHSCN_LB
 #define DB_RHSCN_LB 13
 #endif

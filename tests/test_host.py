@@ -307,3 +307,15 @@ def test_profile_error_measures():
     rows = slice(1, 4)
     assert np.isclose(F.profile_errors(les, ref, rows)["u1"], 1.0 / np.linalg.norm([1, 2, 3]))
     assert np.isclose(F.evolution_errors(les, ref0, ref, ref0, rows)["u1"], 1.0 / np.linalg.norm([1, 2, 3]))
+
+
+def test_config3_network_fixture():
+    """The DNS-trained closure network the 128x65x128 comparison loads
+    (diablo3_b200/closure_study.py made it): parameters, normalisation and
+    training range of the 16-64-64-64-2 network, all finite."""
+    import numpy as np
+    d = np.load(os.path.join(os.path.dirname(__file__), "..", "diablo3_b200", "data", "closure_config3.npz"))
+    shapes = {"params": (9538,), "mean": (16,), "std": (16,), "scale": (2,), "lo": (16,), "hi": (16,)}
+    for k, sh in shapes.items():
+        assert d[k].shape == sh and np.all(np.isfinite(d[k])), k
+    assert np.all(d["std"] > 0) and np.all(d["scale"] > 0) and np.all(d["hi"] >= d["lo"])
