@@ -165,6 +165,22 @@ class Channel:
         self._ck(self.L.db_bpe(self.h, n, _L.dptr(pdf), _L.dptr(edges), ctypes.byref(e)))
         return e.value, pdf, edges
 
+    def bin_ystar(self, field=None, nbin: int | None = None):
+        """Bin_Ystar_and_Write: (binned field, bin weights) over the
+        buoyancy bins of compute_BPE.  field: a physical array in the
+        reference layout (Nyp+2, Nz+2, Nx+2); None bins the kinetic energy
+        0.5 (u1^2 + u2^2 + u3^2) of the current state (KE_zstar)."""
+        n = int(nbin or self.p.nx)
+        out, w = np.zeros(n), np.zeros(n)
+        if field is None:
+            self._ck(self.L.db_bin_ystar(self.h, _L.DB_ZS_KE, None, n, _L.dptr(out), _L.dptr(w)))
+        else:
+            f = np.ascontiguousarray(field, np.float64)
+            assert f.shape == (self.p.ny + 2, self.p.nz + 2, self.p.nx + 2), f.shape
+            self._ck(self.L.db_bin_ystar(self.h, _L.DB_ZS_FIELD, _L.dptr(f.reshape(-1)), n, _L.dptr(out),
+                                         _L.dptr(w)))
+        return out, w
+
     def set_sgs_net(self, net):
         """Learned closure for les_model_type 6 (a SgsNet that outlives this channel)."""
         self._sgs = net

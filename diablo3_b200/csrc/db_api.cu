@@ -28,6 +28,10 @@ struct db_ctx {
   Phys ph;
   State s;
   cudaStream_t st = nullptr;
+  // side stream of the substep: the tridiagonal rows are factored there
+  // while the transforms and products run (a branch of the captured graph)
+  cudaStream_t st_side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool own_stream = false;
   int device = 0;
   std::vector<void*> allocs;
@@ -40,6 +44,7 @@ struct db_ctx {
   double* bud_out = nullptr;
   double* bud_pdf = nullptr;
   int bud_nbin = 0;
+  double* zs_field = nullptr;    // a caller's physical field for db_bin_ystar
   double* d_tab = nullptr;       // gy, gyf, dy, dyf, kx, kz tables
   double2* d_tw = nullptr;       // twiddles (Nx then Nz)
   float2* d_twf = nullptr;       // the same in FP32
@@ -200,6 +205,13 @@ static int init_impl(const db_params* p, const double* gy_in, void* stream, db_c
       return DB_ERR_CUDA;
     }
     c->own_stream = true;
+  }
+  if (cudaStreamCreateWithFlags(&c->st_side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    g_init_err = "db_init: no CUDA device";
+    db_finalize(c);
+    return DB_ERR_CUDA;
   }
   const int Nx = p->nx, Nyp = p->ny, Nz = p->nz, np = Nyp + 2;
   Geom& g = c->g;
@@ -435,6 +447,12 @@ extern "C" int db_finalize(db_ctx* c) {
       if (c->ev[r][k]) cudaEventDestroy(c->ev[r][k]);
   for (void* q : c->allocs) cudaFree(q);
   if (c->h_stage) cudaFreeHost(c->h_stage);
+  if (c->st_side) {
+    cudaStreamSynchronize(c->st_side);
+    cudaStreamDestroy(c->st_side);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   delete c;
   return DB_OK;
@@ -825,6 +843,12 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   // without eddy terms the CN matrices are the same in every column
   const bool spectral = !c->p.use_les || (!les && !c->eddy_live);
   mark(c, rk, 0);
+  // the implicit systems' rows (dt and rk only) on the side stream, joined
+  // before the solves
+  if ((e = cudaEventRecord(c->ev_fork, st))) return e;
+  if ((e = cudaStreamWaitEvent(c->st_side, c->ev_fork, 0))) return e;
+  if ((e = launch_tri_coef(g, c->ph, s, rk, c->st_side))) return e;
+  if ((e = cudaEventRecord(c->ev_join, c->st_side))) return e;
   if (les) {
     // les_chan / les_chan_th: ghost rows, then the state and its x and z
     // derivatives to physical space (les.f90:63-75, 555-569, 1209-1211)
@@ -862,10 +886,10 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
     // without eddy viscosity the CN matrices are the same in every column:
     // z-FFT of the products, then the spectral RHS and the CN solves on the
     // retained modes (FP64), no transforms of cr or u
-    if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
     if ((e = launch_zpass_spec(g, s, st))) return e;
     mark(c, rk, 4);
     mark(c, rk, 5);
+    if ((e = cudaStreamWaitEvent(st, c->ev_join, 0))) return e;
     if ((e = launch_rhs_cn(g, c->ph, s, rk, st))) return e;
     mark(c, rk, 6);
     n += 4;
@@ -883,7 +907,7 @@ static cudaError_t substep(db_ctx* c, int rk /* 0-based */, bool les) {
   } else {
     // z-FFT + spectral RHS + inverse z of cr
     const double2* ov = les ? s.ghost : nullptr;   // ghost rows the transforms saw
-    if ((e = launch_tri_coef(g, c->ph, s, rk, st))) return e;
+    if ((e = cudaStreamWaitEvent(st, c->ev_join, 0))) return e;
     if ((e = launch_zpass_rhs(g, c->ph, s, rk, st, ov))) return e;
     mark(c, rk, 4);
     // cr1 = xh[0], cr3 = xh[2], cr2 = xh[4], crth = xh[6] -> physical r
@@ -1617,6 +1641,47 @@ extern "C" int db_bpe(db_ctx* c, int nbin, double* pdf, double* th_bin, double* 
   if (pdf) std::copy(P.begin(), P.end(), pdf);
   if (th_bin) std::copy(B.begin(), B.end(), th_bin);
   if (bpe) *bpe = e;
+  return DB_OK;
+}
+
+// Bin_Ystar_and_Write (for/diagnostics.f90:1859-1950): a physical field
+// binned by the buoyancy with its background gradient (the bins of
+// compute_BPE), dyf-weighted, divided by the bins' weights
+extern "C" int db_bin_ystar(db_ctx* c, int kind, const double* field, int nbin, double* binned, double* weight) {
+  if (!c || nbin < 1 || nbin > (1 << 13) || !binned) return DB_ERR_ARG;
+  if (kind != DB_ZS_FIELD && kind != DB_ZS_KE) return fail(c, DB_ERR_ARG, "db_bin_ystar: unknown kind");
+  if (kind == DB_ZS_FIELD && !field) return fail(c, DB_ERR_ARG, "db_bin_ystar: no field");
+  const Geom& g = c->g;
+  if (c->bud_nbin < 2 * nbin) {
+    if (balloc(c, (void**)&c->bud_pdf, (size_t)2 * nbin * sizeof(double)))
+      return fail(c, DB_ERR_CUDA, "db_bin_ystar: out of device memory");
+    c->bud_nbin = 2 * nbin;
+  }
+  int rc = budget_fields(c);
+  if (rc) return rc;
+  const double* f0 = c->bud_phys[0];
+  if (kind == DB_ZS_FIELD) {
+    if (!c->zs_field && balloc(c, (void**)&c->zs_field, (size_t)g.np * g.pp * sizeof(double)))
+      return fail(c, DB_ERR_CUDA, "db_bin_ystar: out of device memory");
+    // reference physical layout real(0:Nx+1, 0:Nz+1, 0:Nyp+1): the Nx x Nz
+    // points of each plane
+    for (int j = 0; j < g.np; ++j)
+      CK(cudaMemcpy2DAsync(c->zs_field + (size_t)j * g.pp, (size_t)g.nx * sizeof(double),
+                           field + (size_t)j * (g.nz + 2) * (g.nx + 2), (size_t)(g.nx + 2) * sizeof(double),
+                           (size_t)g.nx * sizeof(double), (size_t)g.nz, cudaMemcpyHostToDevice, c->st));
+    f0 = c->zs_field;
+  }
+  CK(cudaMemsetAsync(c->bud_pdf, 0, (size_t)2 * nbin * sizeof(double), c->st));
+  CK(launch_bpe_pdf(g, c->ph, c->bud_phys[3], homogeneous_x(c), nbin, c->bud_pdf, c->st, c->bud_pdf + nbin, kind,
+                    f0, c->bud_phys[1], c->bud_phys[2]));
+  std::vector<double> h((size_t)2 * nbin);
+  CK(cudaMemcpyAsync(h.data(), c->bud_pdf, (size_t)2 * nbin * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->launches += 1 + 8;
+  for (int b = 0; b < nbin; ++b) {
+    binned[b] = h[(size_t)nbin + b] / h[b];   // 0/0 in an empty bin, as the reference divides
+    if (weight) weight[b] = h[b];
+  }
   return DB_OK;
 }
 

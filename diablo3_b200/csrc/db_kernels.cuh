@@ -24,19 +24,12 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #endif
 // k_rhs_cn: minimum resident 32-thread CTAs per SM (13 keeps every mode's
 // thread of a 512x512 plane resident at once: 128 registers)
-// k_cn_back: one thread per mode (1) or per real column (0), planes per batch
-#ifndef DB_CNBACK_CPLX
-#define DB_CNBACK_CPLX 0
-#endif
-#ifndef DB_CNBACK_TB
-#define DB_CNBACK_TB 4
-#endif
 // k_rem_div: minimum resident CTAs per SM, planes per batch
 #ifndef DB_REMDIV_LB
-#define DB_REMDIV_LB 6
+#define DB_REMDIV_LB 7
 #endif
 #ifndef DB_REMDIV_RB
-#define DB_REMDIV_RB 4
+#define DB_REMDIV_RB 3
 #endif
 #ifndef DB_RHSCN_LB
 #define DB_RHSCN_LB 13
@@ -230,7 +223,8 @@ cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSe
                           double* out, cudaStream_t st);
 // PDF of th + dTHdX (x - Lx/2) over planes jstart_th..jend_th (weights dyf)
 cudaError_t launch_bpe_pdf(const Geom& g, const Phys& ph, const double* th, int homx, int nbin, double* pdf,
-                           cudaStream_t st);
+                           cudaStream_t st, double* fbin = nullptr, int kind = 0, const double* f0 = nullptr,
+                           const double* f1 = nullptr, const double* f2 = nullptr);
 // k_pressure.cu: poisson_p_chan's term factors, physical products and the
 // Poisson solve of cp
 cudaError_t launch_pp_terms(const Geom& g, const State& s, int term, double2* w1, double2* w2, cudaStream_t st);

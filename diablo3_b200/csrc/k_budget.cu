@@ -188,9 +188,19 @@ __global__ void __launch_bounds__(256) k_vorticity(const __grid_constant__ State
 // PDF of the buoyancy with its background gradient (compute_BPE): weights
 // dyf(j) over the planes jstart_th..jend_th, into nbin bins; constant bins
 // over +-1.1 dTHdX Lx/2 with homogeneousX, else cos-spaced over +-Ro_inv
-__global__ void __launch_bounds__(256) k_bpe_pdf(const double* th, Geom g, Phys ph, int homx, int nbin, double* pdf) {
+// With fbin, also the dyf-weighted sum of a field per bin
+// (Bin_Ystar_and_Write, diagnostics.f90:1859-1950): kind 0 the field f0,
+// kind 1 the kinetic energy 0.5 (f0^2 + f1^2 + f2^2) of the physical u1, u2,
+// u3 at each point.
+__global__ void __launch_bounds__(256) k_bpe_pdf(const double* th, Geom g, Phys ph, int homx, int nbin, double* pdf,
+                                                 double* fbin, int kind, const double* f0, const double* f1,
+                                                 const double* f2) {
   extern __shared__ double hist[];
-  for (int b = threadIdx.x; b < nbin; b += blockDim.x) hist[b] = 0.0;
+  double* hf = hist + nbin;
+  for (int b = threadIdx.x; b < nbin; b += blockDim.x) {
+    hist[b] = 0.0;
+    if (fbin) hf[b] = 0.0;
+  }
   __syncthreads();
   const int j = g.jstart_th + blockIdx.y;
   const double dyfj = g.dyf[j];
@@ -209,11 +219,20 @@ __global__ void __launch_bounds__(256) k_bpe_pdf(const double* th, Geom g, Phys 
       const double c = -fmin(fmax(b, thmin), thmax) / (ph.ro_inv + 1.e-14);
       bin = min((int)(acos(c) * nbin / pi), nbin - 1);
     }
-    if (bin >= 0) atomicAdd(&hist[bin], dyfj);
+    if (bin >= 0) {
+      atomicAdd(&hist[bin], dyfj);
+      if (fbin) {
+        const long long q = (long long)j * g.pp + p;
+        const double v = kind == 1 ? 0.5 * (f0[q] * f0[q] + f1[q] * f1[q] + f2[q] * f2[q]) : f0[q];
+        atomicAdd(&hf[bin], v * dyfj);
+      }
+    }
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < nbin; b += blockDim.x)
+  for (int b = threadIdx.x; b < nbin; b += blockDim.x) {
     if (hist[b] != 0.0) atomicAdd(&pdf[b], hist[b]);
+    if (fbin && hf[b] != 0.0) atomicAdd(&fbin[b], hf[b]);
+  }
 }
 
 cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSet phys, int homx, double* mxy,
@@ -225,12 +244,14 @@ cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSe
 }
 
 cudaError_t launch_bpe_pdf(const Geom& g, const Phys& ph, const double* th, int homx, int nbin, double* pdf,
-                           cudaStream_t st) {
+                           cudaStream_t st, double* fbin, int kind, const double* f0, const double* f1,
+                           const double* f2) {
   const int nj = g.jend_th - g.jstart_th + 1;
   if (nj < 1 || nbin < 1) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)nbin * sizeof(double);
+  const size_t smem = (size_t)nbin * sizeof(double) * (fbin ? 2 : 1);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_bpe_pdf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_bpe_pdf<<<dim3(8, nj), 256, smem, st>>>(th, g, ph, homx, nbin, pdf);
+  k_bpe_pdf<<<dim3(8, nj), 256, smem, st>>>(th, g, ph, homx, nbin, pdf, fbin, kind, f0, f1, f2);
   return cudaGetLastError();
 }
 

@@ -911,53 +911,6 @@ __global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s
   }
   if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
 }
-// the same with one thread per mode (both parts, 16-byte loads): half the
-// threads, so a 512x512 plane's four equations fit one wave
-__global__ void __launch_bounds__(128) k_cn_back2(const __grid_constant__ State s, Geom g,
-                                                  const __grid_constant__ FieldSet nl) {
-  constexpr int TB = DB_CNBACK_TB;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int eq = blockIdx.y;
-  if (c >= g.sp) return;
-  const int np = g.np, Nyp = g.ny;
-  const long long pp = g.sp;
-  const TriRow* Rw = s.tri + eq * np;
-  const int ze = (eq == 0) ? 3 : (eq == 1 ? 2 : (eq == 2 ? 0 : 1));
-  double2* u = ((eq == 0) ? s.cth : (eq == 1 ? s.cu2 : (eq == 2 ? s.cu1 : s.cu3))) + c;
-  const double2* yv = (const double2*)nl.p[ze] + c;
-  const int lo = (eq == 0) ? g.jstart_th - 1 : (eq == 1 ? 1 : g.jstart - 1);
-  const int hi = (eq == 0) ? g.jend_th + 1 : (eq == 1 ? Nyp + 1 : g.jend + 1);
-  double xnr = 0.0, xni = 0.0;
-  bool bad = false;
-  for (int jt = np - 1; jt >= 0; jt -= TB) {
-    double2 xg[TB];
-#pragma unroll
-    for (int q = 0; q < TB; ++q) {
-      const int j = jt - q;
-      xg[q] = (j >= 0) ? yv[(long long)j * pp] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int q = 0; q < TB; ++q) {
-      const int j = jt - q;
-      if (j < 0) break;
-      const double ib = Rw[j].ibp;
-      double xr, xi;
-      if (j == np - 1) {
-        xr = xg[q].x * ib;
-        xi = xg[q].y * ib;
-      } else {
-        xr = xg[q].x * ib - Rw[j].u * ib * xnr;
-        xi = xg[q].y * ib - Rw[j].u * ib * xni;
-      }
-      xnr = xr;
-      xni = xi;
-      bad = bad || !(fabs(xr) <= 1.7976931348623157e308) || !(fabs(xi) <= 1.7976931348623157e308);
-      if (j >= lo && j <= hi) u[(long long)j * pp] = make_double2(xr, xi);
-    }
-  }
-  if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
-}
-
 // ---------------------------------------------------------------------------
 // rem_div factors: per (kx, kzp) column, rows 1..Nyp of the Poisson system
 // (solver.f90:1326-1333 with apply_BC_rem_div_mpi 2341-2368), forward
@@ -999,7 +952,9 @@ __global__ void k_pfac(Geom g, double2* pfac) {
 __global__ void __launch_bounds__(128, DB_REMDIV_LB) k_rem_div(const __grid_constant__ State s, Geom g, int rk,
                                                                 int update_cp) {
   // the rows of both sweeps are handled in batches of RB whose loads are all
-  // issued first (each thread keeps several rows in flight)
+  // issued first (each thread keeps several rows in flight); 72 registers,
+  // seven CTAs per SM: the 131 k threads of a 512x512 plane in one wave
+  // (at six, a partial second wave walked every row again)
   constexpr int RB = DB_REMDIV_RB;
   const int t = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   const int kx = t >> 1, part = t & 1;
@@ -1314,8 +1269,7 @@ cudaError_t launch_rhs_cn(const Geom& g, const Phys& ph, const State& s, int rk,
   const FieldSet nl = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
   if (!g.prec) k_rhs_cn<true><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
   else k_rhs_cn<false><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
-  if (DB_CNBACK_CPLX) k_cn_back2<<<dim3((unsigned)((g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl);
-  else k_cn_back<<<dim3((unsigned)((2 * g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl);
+  k_cn_back<<<dim3((unsigned)((2 * g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {

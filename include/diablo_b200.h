@@ -252,6 +252,20 @@ int db_budget(db_ctx* ctx, double* out);
  * 1, the bin edges th_bin[nbin + 1] and the BPE.  Any output may be NULL. */
 int db_bpe(db_ctx* ctx, int nbin, double* pdf, double* th_bin, double* bpe);
 
+/* A physical field binned into z* coordinates (Bin_Ystar_and_Write,
+ * for/diagnostics.f90:1859-1950, Winters et al. 1996): the points of planes
+ * jstart_th..jend_th go to the buoyancy bins of db_bpe (the buoyancy plus
+ * its background gradient), binned[b] = sum(field dyf) / sum(dyf) over bin
+ * b (0/0 for an empty bin, as the reference divides), weight[b] (may be
+ * NULL) = sum(dyf).  kind DB_ZS_FIELD: field is a host array in the
+ * reference physical layout real(0:Nx+1, 0:Nz+1, 0:Nyp+1) (e.g. the
+ * reference's shear2, thw, chi, epsilon or TKE integrands); DB_ZS_KE: the
+ * kinetic energy 0.5 (u1^2 + u2^2 + u3^2) of the current state (KE_zstar),
+ * field unused.  nbin <= 8192 (the reference uses Nx).  FP64 on both
+ * precision paths. */
+enum { DB_ZS_FIELD = 0, DB_ZS_KE = 1 };
+int db_bin_ystar(db_ctx* ctx, int kind, const double* field, int nbin, double* binned, double* weight);
+
 /*
  * Divergence removal that allocates nothing.  No counterpart in the
  * reference (it follows rem_div_chan's arithmetic, for/solver.f90:1302-1379,

@@ -233,3 +233,64 @@ def test_energy_budget_closes(Channel, precision):
     rel = float(np.abs(err).max() / scale)
     print(f"budget closure (precision {precision}): max |error| / max term = {rel:.3e}")
     assert rel <= 3e-2, rel   # measured 1.65e-2 on both precision paths
+
+
+def ref_bin_ystar(p, gy, st, field, nbin):
+    """Bin_Ystar_and_Write (for/diagnostics.f90:1859-1950) in numpy: field
+    [j][z][x] binned by the buoyancy with its background gradient."""
+    m, _, pi = _geom(p, gy)
+    dyf = m["dyf"]
+    th = to_phys(p, significant(p, st[4]))
+    gx = np.arange(p.nx) * p.lx / p.nx
+    s1 = th + _dthdx(p) * (gx - 0.5 * p.lx)[None, None, :]
+    homx = not (5 <= p.ic_type <= 8)
+    ro_inv = 1.0 / p.ro
+    pdf, fb = np.zeros(nbin), np.zeros(nbin)
+    jst, jet = _th_rows(p)
+    for j in range(jst, jet + 1):
+        b = s1[j].reshape(-1)
+        if homx:
+            thmin, thmax = -_dthdx(p) * 0.5 * p.lx * 1.1, _dthdx(p) * 0.5 * p.lx * 1.1
+            dth = (thmax - thmin) / nbin + 1e-14
+            bins = np.minimum(np.trunc((b - thmin) / dth).astype(int), nbin - 1)
+        else:
+            cc = -np.minimum(np.maximum(b, -ro_inv), ro_inv) / (ro_inv + 1e-14)
+            bins = np.minimum(np.trunc(np.arccos(cc) * nbin / pi).astype(int), nbin - 1)
+        ok = bins >= 0
+        np.add.at(pdf, bins[ok], dyf[j])
+        np.add.at(fb, bins[ok], field[j].reshape(-1)[ok] * dyf[j])
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return fb / pdf, pdf
+
+
+@pytest.mark.parametrize("case", ["infinite_front", "finite_front"])
+def test_bin_ystar_matches_reference_loops(Channel, case):
+    """db_bin_ystar of a caller's field (a smooth function of the point) and
+    of the kinetic energy against the reference's binning loop; bins whose
+    weight differs (points on a bin edge, FP rounding of the buoyancy) are
+    left out of the comparison and must be few."""
+    p = config0_params(**CASES[case])
+    gy = grid_for(p)
+    with Channel(p, gy) as ch:
+        ch.init_flow(seed=12)
+        ch.step(3)
+        st = ch.download_state()
+        z = np.arange(p.nz)[None, :, None]
+        x = np.arange(p.nx)[None, None, :]
+        jj = np.arange(p.ny + 2)[:, None, None]
+        fld = np.cos(0.3 * jj) + 0.01 * z + 0.002 * x * x
+        arr = np.zeros((p.ny + 2, p.nz + 2, p.nx + 2))
+        arr[:, : p.nz, : p.nx] = fld
+        got, w = ch.bin_ystar(arr)
+        ke, wk = ch.bin_ystar(None)
+    ref, wr = ref_bin_ystar(p, gy, st, np.broadcast_to(fld, (p.ny + 2, p.nz, p.nx)), p.nx)
+    u = [to_phys(p, significant(p, st[f])) for f in (0, 1, 2)]
+    kef = 0.5 * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    ke_ref, _ = ref_bin_ystar(p, gy, st, kef, p.nx)
+    same = np.isclose(w, wr, rtol=1e-12, atol=1e-300)
+    assert (~same).sum() <= 2, (~same).sum()
+    assert np.array_equal(np.isnan(got[same]), np.isnan(ref[same]))
+    ok = same & np.isfinite(ref)
+    assert ok.sum() > 0
+    assert np.allclose(got[ok], ref[ok], rtol=1e-10, atol=1e-12)
+    assert np.allclose(wk, w) and np.allclose(ke[ok], ke_ref[ok], rtol=1e-9, atol=1e-14)
