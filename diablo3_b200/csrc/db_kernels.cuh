@@ -133,7 +133,7 @@ struct State {
   double2* phi_g;                            // rem_div forward-sweep scratch (spectral)
   double2* nls[8];                           // z-pass scratch of the FP64 path: Z(N_e), Z(M_e), then cr_e (spectral)
   double2* crs[4];                           // cr of u1, u3, u2, th (spectral FP64) for the spectral CN solve (no LES)
-  double2* pfac;                             // rem_div factors (a', 1/b') per (kx,kz,j)
+  double2* pfac;                             // rem_div factors: a' then 1/b', each np x sp doubles
   TriRow* tri;                               // 4 equations x np rows (th, u2, u1, u3)
   DevScalars* sc;
   // LES (les_model_type 5), physical [j][z][x]; null without use_les

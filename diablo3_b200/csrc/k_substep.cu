@@ -914,8 +914,15 @@ __global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s
 // ---------------------------------------------------------------------------
 // rem_div factors: per (kx, kzp) column, rows 1..Nyp of the Poisson system
 // (solver.f90:1326-1333 with apply_BC_rem_div_mpi 2341-2368), forward
-// eliminated once: pfac[j] = (a'_j, 1/b'_j).
-__global__ void k_pfac(Geom g, double2* pfac) {
+// eliminated once: a'_j and 1/b'_j as two planes-by-modes arrays in the
+// pfac buffer (the forward sweep reads only a', the backward only 1/b').
+__device__ __forceinline__ double* pfac_a(const State& s, const Geom&) { return (double*)s.pfac; }
+__device__ __forceinline__ double* pfac_ib(const State& s, const Geom& g) {
+  return (double*)s.pfac + (long long)g.np * g.sp;
+}
+__global__ void k_pfac(Geom g, double2* pfac2) {
+  double* pa = (double*)pfac2;
+  double* pib = pa + (long long)g.np * g.sp;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   if (kx > g.nkx) return;
   const int Nyp = g.ny;
@@ -931,12 +938,14 @@ __global__ void k_pfac(Geom g, double2* pfac) {
   double l, d, u, lp, dp, up;
   row(1, lp, dp, up);
   double bprev = dp;
-  pfac[(long long)1 * g.sp + (long long)kzp * g.kxs + kx] = make_double2(0.0, 1.0 / dp);
+  pa[(long long)1 * g.sp + (long long)kzp * g.kxs + kx] = 0.0;
+  pib[(long long)1 * g.sp + (long long)kzp * g.kxs + kx] = 1.0 / dp;
   for (int j = 2; j <= Nyp; ++j) {
     row(j, l, d, u);
     const double a = -l / bprev;
     const double b = d + a * up;
-    pfac[(long long)j * g.sp + (long long)kzp * g.kxs + kx] = make_double2(a, 1.0 / b);
+    pa[(long long)j * g.sp + (long long)kzp * g.kxs + kx] = a;
+    pib[(long long)j * g.sp + (long long)kzp * g.kxs + kx] = 1.0 / b;
     bprev = b;
     up = u;
   }
@@ -969,6 +978,8 @@ __global__ void __launch_bounds__(128, DB_REMDIV_LB) k_rem_div(const __grid_cons
   double* u2 = reinterpret_cast<double*>(s.cu2);
   double* cpp = reinterpret_cast<double*>(s.cp);
   double* ph = reinterpret_cast<double*>(s.phi_g);
+  const double* pfa = pfac_a(s, g);
+  const double* pfb = pfac_ib(s, g);
   // d/dx, d/dz of the other part: Re(i k a) = -k Im a, Im(i k a) = k Re a
   const long long qo = 2 * c0 + (part ^ 1);
   const double sgn = part ? 1.0 : -1.0;
@@ -984,7 +995,7 @@ __global__ void __launch_bounds__(128, DB_REMDIV_LB) k_rem_div(const __grid_cons
     for (int c = 0; c < RB; ++c) {
       const int j = jb + c;
       const bool in = j <= Nyp, mid = j < Nyp;
-      pa[c] = in ? s.pfac[(long long)j * sp + c0].x : 0.0;
+      pa[c] = in ? pfa[(long long)j * sp + c0] : 0.0;
       u2n[c] = in ? u2[(long long)(j + 1) * qs + q0] : 0.0;
       a1[c] = mid ? u1[(long long)j * qs + qo] : 0.0;
       a3[c] = mid ? u3[(long long)j * qs + qo] : 0.0;
@@ -1011,7 +1022,7 @@ __global__ void __launch_bounds__(128, DB_REMDIV_LB) k_rem_div(const __grid_cons
       const int j = jt - c;
       const bool in = j >= 1;
       const long long a = (long long)j * qs;
-      ib[c] = in ? s.pfac[(long long)j * sp + c0].y : 0.0;
+      ib[c] = in ? pfb[(long long)j * sp + c0] : 0.0;
       gj[c] = in ? ph[a + q0] : 0.0;
       v1[c] = in ? u1[a + qo] : 0.0;
       v3[c] = in ? u3[a + qo] : 0.0;
