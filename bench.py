@@ -193,7 +193,8 @@ def run_reference(args) -> None:
 
 
 # --------------------------------------------------------------------------
-# config 4: 64 independent 128x65x128 channels, one graph launch per step
+# config 4: 64 independent 128x65x128 channels, one graph launch per step;
+# the members are batched (each kernel of the step launched once for all)
 
 def run_ensemble(args) -> None:
     import torch
@@ -206,20 +207,32 @@ def run_ensemble(args) -> None:
     gy = create_grid(ps[0].ny, lz=ps[0].ly, cs=1.5, grid_type=1)
     stream = torch.cuda.Stream()
     ens = Ensemble(ps, gy, stream=stream.cuda_stream)
-    for _ in range(args.warmup):
-        ens.step(1)
-    torch.cuda.synchronize()
+
+    def timed():
+        for _ in range(args.warmup):
+            ens.step(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ens.step(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    batched = ens.batched
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
     time.sleep(0.5)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        ens.step(1)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = timed()
     clk = clocks.stop()
+    kps = ens.kernels_per_step()
+    branches = None
+    if batched:   # the per-member graph branches on the same members, for comparison
+        ens.batched = False
+        ms_b = timed()
+        branches = {"ms_per_step": ms_b / args.steps, "kernels_per_step": ens.kernels_per_step(),
+                    "value": n_inst * ps[0].nx * ps[0].ny * ps[0].nz * 3 * args.steps / (ms_b / 1e3)}
     p0 = ps[0]
     npts = p0.nx * p0.ny * p0.nz
     value = n_inst * npts * 3 * args.steps / (ms / 1e3)
@@ -234,11 +247,14 @@ def run_ensemble(args) -> None:
                                f"Ri_i ~ U[0.5, 2], Re 2000), one CUDA graph launch per time step"
                                + (", mixed precision" if prec else ""),
                    "instances": n_inst, "grid_xyz": [p0.nx, p0.ny, p0.nz], "points": n_inst * npts,
-                   "parallelism": "single GPU, members on concurrent streams",
+                   "parallelism": ("single GPU, members batched: each kernel launched once for all members"
+                                   if batched else "single GPU, one graph branch per member"),
                    "l2": l2_note(n_inst * resident_bytes(p0))},
         "roofline": {"bound": "hbm", "kernel": "whole step, all members", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
         "clocks": clk,
+        "gpu_launches": kps * args.steps,
+        "per_member_graphs": branches,
     }
     print(json.dumps(line), flush=True)
     ens.close()
@@ -320,6 +336,10 @@ def _dns_timed(ch, p, stream, steps, rk, local, precision, les):
     return {
         "ms_max": ms_max, "value": value, "clocks": clk, "gpu_launches": int(n1.value - n0.value),
         "stages_ms_per_substep": {L.STAGES[i]: round(float(per_stage[i]), 4) for i in range(len(L.STAGES))},
+        "stages_note": ("without LES: zpass_rhs = the z-FFT of the product fields, thomas = the spectral "
+                        "RHS joined with the CN solves, courant = the third substep's CFL transforms "
+                        "(averaged over the three substeps)") if not getattr(p, "use_les", 0) else
+                       "with LES: the reference's stage sequence (physical CN solves)",
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "alg_bytes_per_launch": alg,

@@ -1027,8 +1027,11 @@ extern "C" int db_rk_steps(db_ctx* c, int nsteps) {
 }
 
 // ---------------------------------------------------------------------------
-// ensembles: one CUDA graph per time step that forks into every member's
-// stream, runs its step there and joins back
+// ensembles: one CUDA graph per time step.  Members of equal size without
+// LES at a fixed dt are batched: each kernel of the step is launched once
+// for all of them (launch_substep_batch, the members' arguments in a device
+// table).  Otherwise the graph forks into every member's stream, runs its
+// step there and joins back.
 
 struct db_ensemble {
   std::vector<db_ctx*> members;
@@ -1038,8 +1041,29 @@ struct db_ensemble {
   std::vector<cudaEvent_t> ev;                     // fork event + one join event per member
   long long kernels[2] = {0, 0};
   bool graph_eddy[2] = {false, false};             // eddy terms when each graph was captured
+  // batched form
+  bool can_batch = false, batched = false;
+  MemberArgs* tab = nullptr;                       // device table, one entry per member
+  cudaStream_t st_side = nullptr;                  // the implicit systems' rows
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaGraphExec_t bgraph = nullptr;
+  Geom g_cap{};                                    // member 0's geometry when bgraph was captured
+  long long bkernels = 0;
   std::string err;
 };
+
+// members that one batched launch per kernel can advance: the spectral
+// substep (no LES), fixed dt, the same grid and precision
+static bool batch_eligible(const std::vector<db_ctx*>& m) {
+  const db_ctx* a = m[0];
+  if (a->g.nx > 512 || (long long)m.size() > 65535 / MAXF) return false;
+  for (const db_ctx* c : m) {
+    if (c->p.use_les || c->p.variable_dt) return false;
+    if (c->g.nx != a->g.nx || c->g.ny != a->g.ny || c->g.nz != a->g.nz || c->g.prec != a->g.prec) return false;
+    if (!c->s.crs[0] || (!c->g.prec && !c->s.nls[4])) return false;
+  }
+  return true;
+}
 
 static int ensemble_create_impl(db_ctx** members, int n, void* stream, db_ensemble** out) {
   if (!members || n < 1 || !out) return DB_ERR_ARG;
@@ -1078,6 +1102,17 @@ static int ensemble_create_impl(db_ctx** members, int n, void* stream, db_ensemb
       g_init_err = "db_ensemble_create: event creation failed";
       return DB_ERR_CUDA;
     }
+  if (batch_eligible(e->members)) {
+    if (cudaMalloc((void**)&e->tab, (size_t)n * sizeof(MemberArgs)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->st_side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      db_ensemble_destroy(e);
+      g_init_err = "db_ensemble_create: out of device memory";
+      return DB_ERR_CUDA;
+    }
+    e->can_batch = e->batched = true;
+  }
   *out = e;
   return DB_OK;
 }
@@ -1091,8 +1126,16 @@ extern "C" int db_ensemble_destroy(db_ensemble* e) {
   if (e->st) cudaStreamSynchronize(e->st);
   for (int i = 0; i < 2; ++i)
     if (e->graph[i]) cudaGraphExecDestroy(e->graph[i]);
+  if (e->bgraph) cudaGraphExecDestroy(e->bgraph);
   for (auto v : e->ev)
     if (v) cudaEventDestroy(v);
+  if (e->st_side) {
+    cudaStreamSynchronize(e->st_side);
+    cudaStreamDestroy(e->st_side);
+  }
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->tab) cudaFree(e->tab);
   if (e->own_stream && e->st) cudaStreamDestroy(e->st);
   delete e;
   return DB_OK;
@@ -1100,8 +1143,93 @@ extern "C" int db_ensemble_destroy(db_ensemble* e) {
 
 extern "C" const char* db_ensemble_error(const db_ensemble* e) { return e ? e->err.c_str() : g_init_err.c_str(); }
 
+extern "C" int db_ensemble_set_batched(db_ensemble* e, int on) {
+  if (!e || (on && !e->can_batch)) return DB_ERR_ARG;
+  e->batched = on != 0;
+  return DB_OK;
+}
+
+extern "C" int db_ensemble_info(const db_ensemble* e, int* batched, long long* kernels_per_step) {
+  if (!e) return DB_ERR_ARG;
+  if (batched) *batched = e->batched ? 1 : 0;
+  if (kernels_per_step) *kernels_per_step = e->batched ? e->bkernels : e->kernels[0];
+  return DB_OK;
+}
+
+// the launch shapes of a captured batched graph follow member 0's tuning
+static bool same_shapes(const Geom& a, const Geom& b) {
+  return a.tune_xcps == b.tune_xcps && a.tune_xgrid == b.tune_xgrid && a.tune_zns == b.tune_zns &&
+         a.tune_pgrid == b.tune_pgrid;
+}
+
+static int ensemble_steps_batched(db_ensemble* e, int nsteps) {
+  const int n = (int)e->members.size();
+  db_ctx* c0 = e->members[0];
+  // the step stream follows whatever the members' own streams hold
+  for (int i = 0; i < n; ++i) {
+    if (cudaEventRecord(e->ev[1 + i], e->members[i]->st) != cudaSuccess ||
+        cudaStreamWaitEvent(e->st, e->ev[1 + i], 0) != cudaSuccess) {
+      e->err = "ensemble stream join failed";
+      return DB_ERR_CUDA;
+    }
+  }
+  if (e->bgraph && !same_shapes(e->g_cap, c0->g)) {
+    cudaGraphExecDestroy(e->bgraph);
+    e->bgraph = nullptr;
+  }
+  if (!e->bgraph) {
+    std::vector<MemberArgs> h(n);
+    for (int i = 0; i < n; ++i) h[i] = member_args(e->members[i]->g, e->members[i]->ph, e->members[i]->s);
+    if (cudaMemcpyAsync(e->tab, h.data(), (size_t)n * sizeof(MemberArgs), cudaMemcpyHostToDevice, e->st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(e->st) != cudaSuccess) {
+      e->err = "ensemble member table upload failed";
+      return DB_ERR_CUDA;
+    }
+    const Batch b{e->tab, n, 0, 0, 0};
+    cudaGraph_t gr;
+    if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      e->err = "ensemble capture could not start";
+      return DB_ERR_CUDA;
+    }
+    cudaError_t er = launch_steps_batch(b, 0, e->st);
+    for (int rk = 0; rk < 3 && er == cudaSuccess; ++rk)
+      er = launch_substep_batch(c0->g, b, rk, e->st, e->st_side, e->ev_fork, e->ev_join);
+    if (er == cudaSuccess) er = launch_steps_batch(b, 1, e->st);
+    cudaError_t er2 = cudaStreamEndCapture(e->st, &gr);
+    if (er != cudaSuccess || er2 != cudaSuccess) {
+      e->err = std::string("ensemble capture failed: ") + cudaGetErrorString(er != cudaSuccess ? er : er2);
+      return DB_ERR_CUDA;
+    }
+    er = cudaGraphInstantiate(&e->bgraph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (er != cudaSuccess) {
+      e->bgraph = nullptr;
+      e->err = std::string("ensemble graph instantiate failed: ") + cudaGetErrorString(er);
+      return DB_ERR_CUDA;
+    }
+    e->g_cap = c0->g;
+    // step scalars twice; per substep tri_coef, the two inverse passes,
+    // products, the z-pass, rhs_cn, cn_back and rem_div
+    e->bkernels = 2 + 3 * 8;
+  }
+  for (int it = 0; it < nsteps; ++it) {
+    if (cudaGraphLaunch(e->bgraph, e->st) != cudaSuccess) {
+      e->err = "ensemble graph launch failed";
+      return DB_ERR_CUDA;
+    }
+    for (db_ctx* c : e->members) c->time_step += 1;
+  }
+  if (cudaStreamSynchronize(e->st) != cudaSuccess) {
+    e->err = std::string("ensemble step failed: ") + cudaGetErrorString(cudaGetLastError());
+    return DB_ERR_CUDA;
+  }
+  return DB_OK;
+}
+
 extern "C" int db_ensemble_steps(db_ensemble* e, int nsteps) {
   if (!e || nsteps < 0) return DB_ERR_ARG;
+  if (e->batched) return ensemble_steps_batched(e, nsteps);
   db_ctx* c0 = e->members[0];
   for (db_ctx* c : e->members)
     if (need_net(c)) { e->err = c->err; return DB_ERR_STATE; }

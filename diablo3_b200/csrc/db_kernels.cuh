@@ -24,13 +24,6 @@ constexpr int KT = 4;           // kx columns per z-pass CTA (kxs is a multiple 
 #endif
 // k_rhs_cn: minimum resident 32-thread CTAs per SM (13 keeps every mode's
 // thread of a 512x512 plane resident at once: 128 registers)
-// k_rem_div: minimum resident CTAs per SM, planes per batch
-#ifndef DB_REMDIV_LB
-#define DB_REMDIV_LB 7
-#endif
-#ifndef DB_REMDIV_RB
-#define DB_REMDIV_RB 3
-#endif
 #ifndef DB_RHSCN_LB
 #define DB_RHSCN_LB 13
 #endif
@@ -171,6 +164,44 @@ __device__ __forceinline__ R ydiff(R a, R b, const double* pmean, int f, int np,
   const R dm = pmean ? (R)((pmean[(long long)f * np + ja] - pmean[(long long)f * np + jb]) * id) : (R)0;
   return fma(a - b, (R)id, dm);
 }
+
+// Member-batched launches (ensembles of equal-sized channels without LES):
+// one launch covers every member, the member index folded into a grid
+// dimension the kernel does not use otherwise; member m's state, geometry,
+// physics and the field sets of the batched transforms come from a device
+// table.  Kernels instantiated with B = false take their arguments as
+// before and ignore the table.
+enum { FS_CU4 = 0, FS_XH4, FS_U4, FS_XH8, FS_XH8Z, FS_NL, FS_NSLOT };
+struct MemberArgs {
+  State s;
+  Geom g;
+  Phys ph;
+  // FS_CU4 cu1, cu2, cu3, cth; FS_XH4 xh[0..3]; FS_U4 u1, u2, u3, th;
+  // FS_XH8 xh[0..7]; FS_XH8Z xh[0, 2, 4, 6, 1, 3, 5, 7] (the FP64 z-pass
+  // input order); FS_NL crs[0..3], nls[4..7]
+  FieldSet fs[FS_NSLOT];
+};
+struct Batch {
+  const MemberArgs* tab;   // device table of n members (null: one context)
+  int n;
+  int nf;                  // fields per member of a batched transform
+  int fin, fout;           // its field-set slots
+};
+// the table entry of one context
+MemberArgs member_args(const Geom& g, const Phys& ph, const State& s);
+// one substep's kernels for every member (spectral path: no LES, fixed dt),
+// with g member 0's geometry (launch shapes); tri_coef on st_side, joined
+// through the two events before the solves
+cudaError_t launch_substep_batch(const Geom& g, const Batch& b, int rk, cudaStream_t st, cudaStream_t st_side,
+                                 cudaEvent_t ev_fork, cudaEvent_t ev_join);
+// time_step += 1 (end = 0) or time += delta_t (end = 1) of every member
+cudaError_t launch_steps_batch(const Batch& b, int end, cudaStream_t st);
+// batched transforms (k_fft.cu): nf fields of every member from slot fin
+// to slot fout
+cudaError_t launch_inv_z_batch(const Geom& g, const Batch& b, cudaStream_t st);
+cudaError_t launch_inv_x_batch(const Geom& g, const Batch& b, cudaStream_t st);
+cudaError_t launch_fwd_z_batch(const Geom& g, const Batch& b, cudaStream_t st);
+cudaError_t launch_fwd_z_nl_batch(const Geom& g, const Batch& b, cudaStream_t st);
 
 // k_substep.cu; les: add the SGS forcing fields s.les to the products
 int sm_count();   // SMs of the current device (cached)

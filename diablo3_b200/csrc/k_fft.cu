@@ -114,9 +114,14 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_x(const __grid_constant_
 // Xh -> packed spectral (FP64), scaled by 1/Nz; sequence = one kx column of a plane.
 // accumulate: out = base + transform, base = out itself, or for rows 0, 1,
 // Nyp, Nyp+1 the ghost overlay (field f % 4) when one is given
-template <int N, typename R, bool ACC>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int accumulate,
-                                                          const double2* __restrict__ ghost) {
+// B: member-batched (blockIdx.z = member * nf + field)
+template <int N, typename R, bool ACC, bool B = false>
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant__ FieldSet in0, const __grid_constant__ FieldSet out0, Geom g0, int accumulate,
+                                                          const double2* __restrict__ ghost, const __grid_constant__ Batch bt) {
+  const int m = B ? (int)blockIdx.z / bt.nf : 0, f = B ? (int)blockIdx.z - m * bt.nf : (int)blockIdx.z;
+  const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
+  const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
+  const Geom& g = B ? bt.tab[m].g : g0;
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
   // and the exchanges use CTA barriers
   const int ns = blockDim.x / T;
   const int seq = threadIdx.x % ns, lane = threadIdx.x / ns;
-  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, f = blockIdx.z;
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y;
   const bool active = kx < g.kxs;
   C* sq = sm + seq * (padded(N) + 1);   // staggered so the ns columns use different banks
   const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
@@ -180,9 +185,15 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
 // row segments, where the halves of a 256-thread CTA hold 2 columns.)
 template <int N>
 constexpr int znl_threads() { return FftShape<N>::T >= 256 ? 2 * FftShape<N>::T : 256; }
-template <int N, typename R>
+// B: member-batched (blockIdx.z = member * 4 + equation)
+template <int N, typename R, bool B = false>
 __global__ void __launch_bounds__(znl_threads<N>(), FftShape<N>::T >= 256 ? 1 : DB_LB_FFT)
-    k_fwd_z_nl(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, int ns) {
+    k_fwd_z_nl(const __grid_constant__ FieldSet in0, const __grid_constant__ FieldSet out0, Geom g0, int ns,
+               const __grid_constant__ Batch bt) {
+  const int m = B ? (int)blockIdx.z >> 2 : 0, e = B ? (int)blockIdx.z & 3 : (int)blockIdx.z;
+  const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
+  const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
+  const Geom& g = B ? bt.tab[m].g : g0;
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -191,7 +202,7 @@ __global__ void __launch_bounds__(znl_threads<N>(), FftShape<N>::T >= 256 ? 1 : 
   const int half = threadIdx.x / (ns * T);   // 0: M, 1: N (whole warps)
   const int t = threadIdx.x % (ns * T);
   const int seq = t % ns, lane = t / ns;     // column-fastest, as k_fwd_z
-  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, e = blockIdx.z;
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y;
   const int jlo = (e == 2) ? 2 : (e == 3 ? g.jstart_th : g.jstart);
   const int jhi = (e == 2) ? g.ny : (e == 3 ? g.jend_th : g.jend);
   if (j < jlo || j > jhi) return;   // uniform over the CTA
@@ -230,9 +241,15 @@ __global__ void __launch_bounds__(znl_threads<N>(), FftShape<N>::T >= 256 ? 1 : 
 // transform, so the physical field holds the fluctuation about the mean
 // and its FP32 rounding scales with the fluctuation (the consumers add the
 // mean back)
-template <int N, typename R>
-__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g, unsigned dmask,
-                                                          const double2* __restrict__ ghost, double* __restrict__ mean) {
+// B: member-batched (blockIdx.z = member * nf + field; no dmask, ghost or mean)
+template <int N, typename R, bool B = false>
+__global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant__ FieldSet in0, const __grid_constant__ FieldSet out0, Geom g0, unsigned dmask,
+                                                          const double2* __restrict__ ghost, double* __restrict__ mean,
+                                                          const __grid_constant__ Batch bt) {
+  const int m = B ? (int)blockIdx.z / bt.nf : 0, f = B ? (int)blockIdx.z - m * bt.nf : (int)blockIdx.z;
+  const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
+  const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
+  const Geom& g = B ? bt.tab[m].g : g0;
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -240,7 +257,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant_
   constexpr int E = S::E, T = S::T;
   const int ns = blockDim.x / T;   // column-fastest mapping, as k_fwd_z
   const int seq = threadIdx.x % ns, lane = threadIdx.x / ns;
-  const int kx = blockIdx.x * ns + seq, j = blockIdx.y, f = blockIdx.z;
+  const int kx = blockIdx.x * ns + seq, j = blockIdx.y;
   const bool active = kx < g.kxs;
   C* sq = sm + seq * (padded(N) + 1);
   const C* twt = tw_z<R>(g);   // twiddles fetched per pass (fewer live registers)
@@ -368,10 +385,17 @@ struct CflArgs {
   DevScalars* sc;
 };
 
-template <int N, typename R, bool CFL>
-__global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g,
+// B: member-batched (blockIdx.y = member; each member's items over its own
+// gridDim.x CTAs; no dmask, not with CFL)
+template <int N, typename R, bool CFL, bool B = false>
+__global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in0, const __grid_constant__ FieldSet out0, Geom g0,
                                                       unsigned dmask, int nblk, int nitems,
-                                                      const __grid_constant__ CflArgs cf) {
+                                                      const __grid_constant__ CflArgs cf, const __grid_constant__ Batch bt) {
+  static_assert(!(B && CFL), "the CFL x-pass is not batched");
+  const int m = B ? (int)blockIdx.y : 0;
+  const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
+  const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
+  const Geom& g = B ? bt.tab[m].g : g0;
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -570,7 +594,7 @@ static void go_inv_x_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   smem_attr(k_inv_x_st<N, R, false>, smem);
   const int gmax = xpass_ctas_per_sm(g) * sm_count();
   const int grid = nitems < gmax ? nitems : gmax;
-  k_inv_x_st<N, R, false><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems, CflArgs{});
+  k_inv_x_st<N, R, false><<<grid, cps * FftShape<N>::T, smem, st>>>(in, out, g, dmask, nblk, nitems, CflArgs{}, Batch{});
 }
 template <int N, typename R>
 static void go_inv_x_cfl_t(const Geom& g, FieldSet in, const CflArgs& cf, cudaStream_t st) {
@@ -581,7 +605,7 @@ static void go_inv_x_cfl_t(const Geom& g, FieldSet in, const CflArgs& cf, cudaSt
   smem_attr(k_inv_x_st<N, R, true>, smem);
   const int gmax = xpass_ctas_per_sm(g) * sm_count();
   const int grid = nitems < gmax ? nitems : gmax;
-  k_inv_x_st<N, R, true><<<grid, cps * FftShape<N>::T, smem, st>>>(in, FieldSet{}, g, 0u, nblk, nitems, cf);
+  k_inv_x_st<N, R, true><<<grid, cps * FftShape<N>::T, smem, st>>>(in, FieldSet{}, g, 0u, nblk, nitems, cf, Batch{});
 }
 template <int N>
 static void go_inv_x_cfl(const Geom& g, FieldSet in, const CflArgs& cf, cudaStream_t st) {
@@ -597,10 +621,10 @@ static void go_fwd_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, int acc
   const dim3 grid((g.kxs + ns - 1) / ns, g.np, nf);
   if (acc) {
     smem_attr(k_fwd_z<N, R, true>, smem);
-    k_fwd_z<N, R, true><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 1, ghost);
+    k_fwd_z<N, R, true><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 1, ghost, Batch{});
   } else {
     smem_attr(k_fwd_z<N, R, false>, smem);
-    k_fwd_z<N, R, false><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 0, ghost);
+    k_fwd_z<N, R, false><<<grid, ns * FftShape<N>::T, smem, st>>>(in, out, g, 0, ghost, Batch{});
   }
 }
 template <int N, typename R>
@@ -611,7 +635,7 @@ static void go_inv_z_t(const Geom& g, FieldSet in, FieldSet out, int nf, unsigne
   size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
   smem_attr(k_inv_z<N, R>, smem);
   k_inv_z<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, nf), ns * FftShape<N>::T, smem, st>>>(in, out, g, dmask, ghost,
-                                                                                          mean);
+                                                                                          mean, Batch{});
 }
 template <int N, typename R>
 static void go_fwd_z_nl_t(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st) {
@@ -620,7 +644,7 @@ static void go_fwd_z_nl_t(const Geom& g, FieldSet in, FieldSet out, cudaStream_t
   const int ns = znl_threads<N>() / (2 * T);
   const size_t smem = (size_t)3 * ns * (padded(N) + 1) * sizeof(C);
   smem_attr(k_fwd_z_nl<N, R>, smem);
-  k_fwd_z_nl<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, 4), 2 * ns * T, smem, st>>>(in, out, g, ns);
+  k_fwd_z_nl<N, R><<<dim3((g.kxs + ns - 1) / ns, g.np, 4), 2 * ns * T, smem, st>>>(in, out, g, ns, Batch{});
 }
 template <int N>
 static void go_fwd_z_nl(const Geom& g, FieldSet in, FieldSet out, cudaStream_t st) {
@@ -679,6 +703,92 @@ cudaError_t launch_inv_z(const Geom& g, FieldSet in, FieldSet out, int nf, cudaS
                          const double2* ghost, double* mean) {
   if (nf < 1 || nf > MAXF) return cudaErrorInvalidValue;
   DB_DISPATCH_N(g.nz, go_inv_z, g, in, out, nf, dmask, ghost, mean, st);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// member-batched transforms: the shapes of the single-context launchers with
+// the member folded into blockIdx.z (z-passes) or blockIdx.y (x-pass, each
+// member's items over its own share of the persistent CTAs)
+
+template <int N, typename R>
+static void go_inv_x_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int cps = xpass_cps<N>(g);
+  const int nblk = (g.nz / 2) / cps, nitems = nblk * g.np * bt.nf;
+  const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
+  smem_attr(k_inv_x_st<N, R, false, true>, smem);
+  const int gmax = xpass_ctas_per_sm(g) * sm_count();
+  int gx = (gmax + bt.n - 1) / bt.n;
+  gx = gx < nitems ? gx : nitems;
+  k_inv_x_st<N, R, false, true><<<dim3(gx, bt.n), cps * FftShape<N>::T, smem, st>>>(
+      FieldSet{}, FieldSet{}, g, 0u, nblk, nitems, CflArgs{}, bt);
+}
+template <int N, typename R>
+static void go_inv_z_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int ns = zpass_ns<N>(g);
+  const size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
+  smem_attr(k_inv_z<N, R, true>, smem);
+  k_inv_z<N, R, true><<<dim3((g.kxs + ns - 1) / ns, g.np, bt.n * bt.nf), ns * FftShape<N>::T, smem, st>>>(
+      FieldSet{}, FieldSet{}, g, 0u, nullptr, nullptr, bt);
+}
+template <int N, typename R>
+static void go_fwd_z_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  const int ns = zpass_ns<N>(g);
+  const size_t smem = (size_t)ns * (padded(N) + 1) * sizeof(C);
+  smem_attr(k_fwd_z<N, R, false, true>, smem);
+  k_fwd_z<N, R, false, true><<<dim3((g.kxs + ns - 1) / ns, g.np, bt.n * bt.nf), ns * FftShape<N>::T, smem, st>>>(
+      FieldSet{}, FieldSet{}, g, 0, nullptr, bt);
+}
+template <int N, typename R>
+static void go_fwd_z_nl_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  constexpr int T = FftShape<N>::T;
+  const int ns = znl_threads<N>() / (2 * T);
+  const size_t smem = (size_t)3 * ns * (padded(N) + 1) * sizeof(C);
+  smem_attr(k_fwd_z_nl<N, R, true>, smem);
+  k_fwd_z_nl<N, R, true><<<dim3((g.kxs + ns - 1) / ns, g.np, 4 * bt.n), 2 * ns * T, smem, st>>>(
+      FieldSet{}, FieldSet{}, g, ns, bt);
+}
+template <int N>
+static void go_inv_x_b(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (g.prec) go_inv_x_bt<N, float>(g, bt, st); else go_inv_x_bt<N, double>(g, bt, st);
+}
+template <int N>
+static void go_inv_z_b(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (g.prec) go_inv_z_bt<N, float>(g, bt, st); else go_inv_z_bt<N, double>(g, bt, st);
+}
+template <int N>
+static void go_fwd_z_b(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (g.prec) go_fwd_z_bt<N, float>(g, bt, st); else go_fwd_z_bt<N, double>(g, bt, st);
+}
+template <int N>
+static void go_fwd_z_nl_b(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (g.prec) go_fwd_z_nl_bt<N, float>(g, bt, st); else go_fwd_z_nl_bt<N, double>(g, bt, st);
+}
+
+static bool batch_ok(const Batch& bt) { return bt.tab && bt.n >= 1 && bt.n <= 65535 / MAXF && bt.nf >= 1 && bt.nf <= MAXF; }
+
+cudaError_t launch_inv_x_batch(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (!batch_ok(bt)) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nx, go_inv_x_b, g, bt, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_inv_z_batch(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (!batch_ok(bt)) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nz, go_inv_z_b, g, bt, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_fwd_z_batch(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (!batch_ok(bt)) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nz, go_fwd_z_b, g, bt, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_fwd_z_nl_batch(const Geom& g, const Batch& bt, cudaStream_t st) {
+  if (!batch_ok(bt)) return cudaErrorInvalidValue;
+  DB_DISPATCH_N(g.nz, go_fwd_z_nl_b, g, bt, st);
   return cudaGetLastError();
 }
 

@@ -208,9 +208,13 @@ constexpr int prod_zr() { return FftShape<N>::T >= 64 ? 1 : 64 / FftShape<N>::T;
 template <int N>
 constexpr int prod_sq() { return padded(N) - 1; }
 
-template <int N, typename R>
-__global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_st(const __grid_constant__ State s, Geom g, int zr, int nzb,
-                                                        int jlen, int nitems) {
+// B: member-batched (blockIdx.y = member, its items over gridDim.x CTAs)
+template <int N, typename R, bool B = false>
+__global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_st(const __grid_constant__ State s0, Geom g0, int zr, int nzb,
+                                                        int jlen, int nitems, const MemberArgs* __restrict__ tab) {
+  const int mb = B ? (int)blockIdx.y : 0;
+  const State& s = B ? tab[mb].s : s0;
+  const Geom& g = B ? tab[mb].g : g0;
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -647,7 +651,15 @@ __global__ void __launch_bounds__(256) k_rhs_modes(const __grid_constant__ State
 // implicit systems: rows of the four equations (th, u2, u1, u3) -> tri[eq*np + j].
 // One CTA per equation: rows are filled in parallel in shared memory, the BC
 // rows and the forward elimination (a serial recurrence) by one thread.
-__global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, DevScalars* sc, int rk) {
+// B: member-batched (blockIdx.y = member)
+template <bool B = false>
+__global__ void __launch_bounds__(256) k_tri_coef(Geom g0, Phys ph0, TriRow* tri0, DevScalars* sc0, int rk,
+                                                  const MemberArgs* __restrict__ tab) {
+  const int mb = B ? (int)blockIdx.y : 0;
+  const Geom& g = B ? tab[mb].g : g0;
+  const Phys& ph = B ? tab[mb].ph : ph0;
+  TriRow* tri = B ? tab[mb].s.tri : tri0;
+  DevScalars* sc = B ? tab[mb].s.sc : sc0;
   extern __shared__ TriRow Rs[];
   const int eq = blockIdx.x;  // 0..3
   const int np = g.np, Nyp = g.ny;
@@ -786,9 +798,16 @@ __global__ void __launch_bounds__(256) k_tri_coef(Geom g, Phys ph, TriRow* tri, 
 // SPLITZ), and
 // the state is only read (cf apart).  Every mode's thread is resident at
 // once (a second wave would walk all planes again with few threads).
-template <bool SPLITZ>
-__global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constant__ State s, Geom g, Phys ph, int rk,
-                                                            const __grid_constant__ FieldSet nl) {
+// B: member-batched (blockIdx.y = member)
+template <bool SPLITZ, bool B = false>
+__global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constant__ State s0, Geom g0, Phys ph0, int rk,
+                                                            const __grid_constant__ FieldSet nl0,
+                                                            const MemberArgs* __restrict__ tab) {
+  const int mb = B ? (int)blockIdx.y : 0;
+  const State& s = B ? tab[mb].s : s0;
+  const Geom& g = B ? tab[mb].g : g0;
+  const Phys& ph = B ? tab[mb].ph : ph0;
+  const FieldSet& nl = B ? tab[mb].fs[FS_NL] : nl0;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= g.sp) return;
   const int np = g.np;
@@ -874,8 +893,14 @@ __global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constan
 // the new state is written on the planes the reference's solve stores,
 // the others keep their values.  A non-finite new state is reported as
 // DB_FLAG_NONFINITE.
-__global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s, Geom g,
-                                                 const __grid_constant__ FieldSet nl) {
+// B: member-batched (blockIdx.z = member)
+template <bool B = false>
+__global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s0, Geom g0,
+                                                 const __grid_constant__ FieldSet nl0, const MemberArgs* __restrict__ tab) {
+  const int mb = B ? (int)blockIdx.z : 0;
+  const State& s = B ? tab[mb].s : s0;
+  const Geom& g = B ? tab[mb].g : g0;
+  const FieldSet& nl = B ? tab[mb].fs[FS_NL] : nl0;
   constexpr int TB = 8;
   const long long ncol = 2 * g.sp;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -958,13 +983,19 @@ __global__ void k_pfac(Geom g, double2* pfac2) {
 // warp reads 16 consecutive modes).  Part 0 (phi real) sees the divergence
 // -kx Im u1 + Dy Re u2 - kz Im u3 and corrects Im u1, Im u3, Re u2, Re cp;
 // part 1 the other halves, so the two threads never touch the same value.
-__global__ void __launch_bounds__(128, DB_REMDIV_LB) k_rem_div(const __grid_constant__ State s, Geom g, int rk,
-                                                                int update_cp) {
-  // the rows of both sweeps are handled in batches of RB whose loads are all
-  // issued first (each thread keeps several rows in flight); 72 registers,
-  // seven CTAs per SM: the 131 k threads of a 512x512 plane in one wave
-  // (at six, a partial second wave walked every row again)
-  constexpr int RB = DB_REMDIV_RB;
+// The rows of both sweeps are handled in batches of RB whose loads are all
+// issued first (each thread keeps several rows in flight).  Large planes:
+// RB 3 at 72 registers, seven CTAs per SM, so the 131 k threads of a
+// 512x512 plane fit one wave (at six, a partial second wave walked every row
+// again); small planes, whose threads fit a wave anyway: RB 4 (more rows in
+// flight per thread), six CTAs per SM.  B: member-batched (blockIdx.z =
+// member).
+template <int RB, int LB, bool B = false>
+__global__ void __launch_bounds__(128, LB) k_rem_div(const __grid_constant__ State s0, Geom g0, int rk, int update_cp,
+                                                      const MemberArgs* __restrict__ tab) {
+  const int mb = B ? (int)blockIdx.z : 0;
+  const State& s = B ? tab[mb].s : s0;
+  const Geom& g = B ? tab[mb].g : g0;
   const int t = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   const int kx = t >> 1, part = t & 1;
   if (kx > g.nkx) return;
@@ -1136,6 +1167,14 @@ __global__ void k_apply_dt(DevScalars* sc) {
 
 __global__ void k_step_begin(DevScalars* sc) { sc->time_step += 1; }
 __global__ void k_step_end(DevScalars* sc) { sc->time += sc->delta_t; }
+// the same for every member of a batch (end = 0: begin)
+__global__ void k_steps_batch(const MemberArgs* __restrict__ tab, int n, int end) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  DevScalars* sc = tab[i].s.sc;
+  if (end) sc->time += sc->delta_t;
+  else sc->time_step += 1;
+}
 
 // max |div| at GYF rows 2..Nyp-1 (the rows rem_div zeroes)
 __global__ void k_divergence(const __grid_constant__ State s, Geom g) {
@@ -1195,7 +1234,7 @@ static void go_products_t(const Geom& g, const State& s, cudaStream_t st) {
     nch = (g.np + jlen - 1) / jlen;
     const int nitems = nzb * nch;
     const int grid = nitems < gmax ? nitems : gmax;
-    k_products_st<N, R><<<grid, 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr, nzb, jlen, nitems);
+    k_products_st<N, R><<<grid, 3 * FftShape<N>::T * zr, smem, st>>>(s, g, zr, nzb, jlen, nitems, nullptr);
   } else {
     const size_t smem = (size_t)3 * padded(N) * sizeof(C);
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_products<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1238,9 +1277,10 @@ static void go_zpass_split(const Geom& g, const Phys& ph, const State& s, int rk
 }
 template <int N>
 static void go_zpass(const Geom& g, const Phys& ph, const State& s, int rk, const double2* ghost, cudaStream_t st) {
+  // FP32: one fused kernel; FP64: the three stages (the fused FP64 kernel
+  // spills at 128 registers), over the spectral scratch db_init allocates
   if (g.prec) go_zpass_t<N, float>(g, ph, s, rk, ghost, st);
-  else if (s.nls[0]) go_zpass_split<N>(g, ph, s, rk, st);
-  else go_zpass_t<N, double>(g, ph, s, rk, nullptr, st);
+  else go_zpass_split<N>(g, ph, s, rk, st);
 }
 
 #define DB_DISPATCH_N2(n, FN, ...)                  \
@@ -1261,6 +1301,7 @@ cudaError_t launch_products(const Geom& g, const State& s, cudaStream_t st, bool
 }
 cudaError_t launch_zpass_rhs(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st,
                              const double2* ghost) {
+  if (!g.prec && !s.nls[0]) return cudaErrorInvalidValue;
   DB_DISPATCH_N2(g.nz, go_zpass, g, ph, s, rk, ghost, st);
   return cudaGetLastError();
 }
@@ -1278,15 +1319,15 @@ cudaError_t launch_zpass_spec(const Geom& g, const State& s, cudaStream_t st) {
 }
 cudaError_t launch_rhs_cn(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
   const FieldSet nl = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
-  if (!g.prec) k_rhs_cn<true><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
-  else k_rhs_cn<false><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl);
-  k_cn_back<<<dim3((unsigned)((2 * g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl);
+  if (!g.prec) k_rhs_cn<true><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl, nullptr);
+  else k_rhs_cn<false><<<(unsigned)((g.sp + 31) / 32), 32, 0, st>>>(s, g, ph, rk, nl, nullptr);
+  k_cn_back<><<<dim3((unsigned)((2 * g.sp + 127) / 128), 4), 128, 0, st>>>(s, g, nl, nullptr);
   return cudaGetLastError();
 }
 cudaError_t launch_tri_coef(const Geom& g, const Phys& ph, const State& s, int rk, cudaStream_t st) {
   const size_t smem = (size_t)g.np * sizeof(TriRow);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_tri_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_tri_coef<<<4, 256, smem, st>>>(g, ph, s.tri, s.sc, rk);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_tri_coef<>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_tri_coef<><<<4, 256, smem, st>>>(g, ph, s.tri, s.sc, rk, nullptr);
   return cudaGetLastError();
 }
 cudaError_t launch_courant(const Geom& g, const Phys& ph, const State& s, CflCtl ctl, cudaStream_t st) {
@@ -1301,7 +1342,9 @@ cudaError_t launch_courant_final(const Phys& ph, const State& s, CflCtl ctl, cud
   return cudaGetLastError();
 }
 cudaError_t launch_rem_div(const Geom& g, const State& s, int rk, int update_cp, cudaStream_t st) {
-  k_rem_div<<<dim3((2 * (g.nkx + 1) + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, rk, update_cp);
+  const dim3 grid((2 * (g.nkx + 1) + 127) / 128, g.nkzp);
+  if ((long long)grid.x * grid.y > 6LL * sm_count()) k_rem_div<3, 7><<<grid, 128, 0, st>>>(s, g, rk, update_cp, nullptr);
+  else k_rem_div<4, 6><<<grid, 128, 0, st>>>(s, g, rk, update_cp, nullptr);
   return cudaGetLastError();
 }
 cudaError_t launch_pfac(const Geom& g, const State& s, cudaStream_t st) {
@@ -1326,6 +1369,116 @@ cudaError_t launch_divergence(const Geom& g, const State& s, cudaStream_t st) {
 }
 cudaError_t launch_bc_vel_post(const Geom& g, const Phys& ph, const State& s, cudaStream_t st) {
   k_bc_vel_post<<<dim3((g.nkx + 1 + 127) / 128, g.nkzp), 128, 0, st>>>(s, g, ph);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// member-batched substep (ensembles without LES at a fixed dt): the kernels
+// of the spectral substep above, each launched once for every member
+
+MemberArgs member_args(const Geom& g, const Phys& ph, const State& s) {
+  MemberArgs a{};
+  a.s = s;
+  a.g = g;
+  a.ph = ph;
+  a.fs[FS_CU4] = fset(s.cu1, s.cu2, s.cu3, s.cth);
+  a.fs[FS_XH4] = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3]);
+  a.fs[FS_U4] = fset(s.u1, s.u2, s.u3, s.th);
+  a.fs[FS_XH8] = fset(s.xh[0], s.xh[1], s.xh[2], s.xh[3], s.xh[4], s.xh[5], s.xh[6], s.xh[7]);
+  a.fs[FS_XH8Z] = fset(s.xh[0], s.xh[2], s.xh[4], s.xh[6], s.xh[1], s.xh[3], s.xh[5], s.xh[7]);
+  a.fs[FS_NL] = fset(s.crs[0], s.crs[1], s.crs[2], s.crs[3], s.nls[4], s.nls[5], s.nls[6], s.nls[7]);
+  return a;
+}
+
+// products: one item (a z block over a plane range) per CTA; the plane
+// ranges minimise waves x planes walked per item (each range re-reads its
+// two neighbouring planes)
+template <int N, typename R>
+static cudaError_t go_products_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
+  using C = typename CplxOf<R>::type;
+  if constexpr (N <= 512) {
+    const int zr = prod_zr<N>() < g.nz ? prod_zr<N>() : g.nz;
+    constexpr int PROD_SLOTS = prod_slots<R>();
+    const size_t smem = (size_t)PROD_SLOTS * 4 * zr * N * sizeof(R) + (size_t)3 * zr * prod_sq<N>() * sizeof(C) +
+                        PROD_SLOTS * sizeof(uint64_t);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_products_st<N, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nzb = g.nz / zr;
+    const long long res = (long long)(PROD_SLOTS == 4 ? 2 : 3) * sm_count();
+    int best = 1;
+    long long bcost = -1;
+    for (int nch = 1; nch <= (g.np / 4 > 1 ? g.np / 4 : 1); ++nch) {
+      const int jl = (g.np + nch - 1) / nch, nc = (g.np + jl - 1) / jl;
+      const long long items = (long long)bt.n * nzb * nc;
+      const long long cost = (items + res - 1) / res * (jl + 2);
+      if (bcost < 0 || cost < bcost) { bcost = cost; best = nch; }
+    }
+    const int jlen = (g.np + best - 1) / best, nitems = nzb * ((g.np + jlen - 1) / jlen);
+    k_products_st<N, R, true><<<dim3(nitems, bt.n), 3 * FftShape<N>::T * zr, smem, st>>>(State{}, g, zr, nzb, jlen,
+                                                                                        nitems, bt.tab);
+    return cudaGetLastError();
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+template <int N>
+static cudaError_t go_products_b(const Geom& g, const Batch& bt, cudaStream_t st) {
+  return g.prec ? go_products_bt<N, float>(g, bt, st) : go_products_bt<N, double>(g, bt, st);
+}
+
+cudaError_t launch_steps_batch(const Batch& b, int end, cudaStream_t st) {
+  if (!b.tab || b.n < 1) return cudaErrorInvalidValue;
+  k_steps_batch<<<(b.n + 127) / 128, 128, 0, st>>>(b.tab, b.n, end);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_substep_batch(const Geom& g, const Batch& b, int rk, cudaStream_t st, cudaStream_t st_side,
+                                 cudaEvent_t ev_fork, cudaEvent_t ev_join) {
+  if (!b.tab || b.n < 1 || b.n > 65535 / MAXF || g.nx > 512) return cudaErrorInvalidValue;
+  cudaError_t e;
+  Batch bt = b;
+  // the implicit systems' rows on the side stream, joined before the solves
+  if ((e = cudaEventRecord(ev_fork, st))) return e;
+  if ((e = cudaStreamWaitEvent(st_side, ev_fork, 0))) return e;
+  const size_t tsm = (size_t)g.np * sizeof(TriRow);
+  if (tsm > 48 * 1024) cudaFuncSetAttribute(k_tri_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+  k_tri_coef<true><<<dim3(4, bt.n), 256, tsm, st_side>>>(g, Phys{}, nullptr, nullptr, rk, bt.tab);
+  if ((e = cudaGetLastError())) return e;
+  if ((e = cudaEventRecord(ev_join, st_side))) return e;
+  // velocity and buoyancy to physical space, products, z-pass of the products
+  bt.nf = 4; bt.fin = FS_CU4; bt.fout = FS_XH4;
+  if ((e = launch_inv_z_batch(g, bt, st))) return e;
+  bt.fin = FS_XH4; bt.fout = FS_U4;
+  if ((e = launch_inv_x_batch(g, bt, st))) return e;
+  cudaError_t pe = cudaSuccess;
+  switch (g.nx) {
+    case 16: pe = go_products_b<16>(g, bt, st); break;
+    case 32: pe = go_products_b<32>(g, bt, st); break;
+    case 64: pe = go_products_b<64>(g, bt, st); break;
+    case 128: pe = go_products_b<128>(g, bt, st); break;
+    case 256: pe = go_products_b<256>(g, bt, st); break;
+    case 512: pe = go_products_b<512>(g, bt, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (pe) return pe;
+  if (g.prec) {
+    bt.nf = 4; bt.fin = FS_XH8; bt.fout = FS_NL;
+    if ((e = launch_fwd_z_nl_batch(g, bt, st))) return e;
+  } else {
+    bt.nf = 8; bt.fin = FS_XH8Z; bt.fout = FS_NL;
+    if ((e = launch_fwd_z_batch(g, bt, st))) return e;
+  }
+  // spectral RHS + CN solves, projection
+  if ((e = cudaStreamWaitEvent(st, ev_join, 0))) return e;
+  const dim3 gr((unsigned)((g.sp + 31) / 32), bt.n);
+  if (!g.prec) k_rhs_cn<true, true><<<gr, 32, 0, st>>>(State{}, g, Phys{}, rk, FieldSet{}, bt.tab);
+  else k_rhs_cn<false, true><<<gr, 32, 0, st>>>(State{}, g, Phys{}, rk, FieldSet{}, bt.tab);
+  k_cn_back<true><<<dim3((unsigned)((2 * g.sp + 127) / 128), 4, bt.n), 128, 0, st>>>(State{}, g, FieldSet{}, bt.tab);
+  const dim3 grd((2 * (g.nkx + 1) + 127) / 128, g.nkzp, bt.n);
+  if ((long long)grd.x * grd.y * grd.z > 6LL * sm_count())
+    k_rem_div<3, 7, true><<<grd, 128, 0, st>>>(State{}, g, rk, 1, bt.tab);
+  else
+    k_rem_div<4, 6, true><<<grd, 128, 0, st>>>(State{}, g, rk, 1, bt.tab);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,8 @@
 """Ensembles of independent channels advanced by one CUDA graph per step
 (include/diablo_b200.h, db_ensemble_*): the data-generation runs of the
-learned closure (many small channels with different seeds and Ri)."""
+learned closure (many small channels with different seeds and Ri).  Members
+of one size without LES at a fixed dt are batched: each kernel of the step
+is launched once for all of them."""
 from __future__ import annotations
 
 import ctypes
@@ -52,6 +54,24 @@ class Ensemble:
         rc = self.L.db_ensemble_steps(self.h, nsteps)
         if rc != 0:
             raise _L.DiabloError(rc, self.L.db_ensemble_error(self.h).decode())
+
+    @property
+    def batched(self) -> bool:
+        """True when every kernel of a step is launched once for all members."""
+        b = ctypes.c_int()
+        self.L.db_ensemble_info(self.h, ctypes.byref(b), None)
+        return bool(b.value)
+
+    @batched.setter
+    def batched(self, on: bool):
+        rc = self.L.db_ensemble_set_batched(self.h, 1 if on else 0)
+        if rc != 0:
+            raise _L.DiabloError(rc, "members do not qualify for the batched form")
+
+    def kernels_per_step(self) -> int:
+        k = ctypes.c_longlong()
+        self.L.db_ensemble_info(self.h, None, ctypes.byref(k))
+        return int(k.value)
 
     def close(self):
         if getattr(self, "h", None):

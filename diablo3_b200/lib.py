@@ -39,6 +39,7 @@ EXPORTS = (
     "db_sgs_gradient", "db_sgs_train_step", "db_sgs_gemm_check", "db_set_sgs_net", "db_les_eval",
     "db_sgs_targets",
     "db_ensemble_create", "db_ensemble_steps", "db_ensemble_destroy", "db_ensemble_error",
+    "db_ensemble_set_batched", "db_ensemble_info",
     "db_set_wait_limit",
 )
 STAGES = ("inv_z", "inv_x", "products", "zpass_rhs", "inv_x_r", "thomas", "courant",
@@ -123,6 +124,8 @@ def load(path: str | None = None):
     L.db_ensemble_destroy.argtypes = [vp]
     L.db_ensemble_error.argtypes = [vp]
     L.db_ensemble_error.restype = ctypes.c_char_p
+    L.db_ensemble_set_batched.argtypes = [vp, ctypes.c_int]
+    L.db_ensemble_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]
     L.db_sgs_targets.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, vp, vp,
                                  ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:

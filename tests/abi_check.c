@@ -23,7 +23,7 @@ int main(void) {
       (entry)db_sgs_get, (entry)db_sgs_set_range, (entry)db_sgs_forward, (entry)db_sgs_gradient,
       (entry)db_sgs_train_step, (entry)db_sgs_gemm_check, (entry)db_set_sgs_net, (entry)db_les_eval,
       (entry)db_sgs_targets, (entry)db_ensemble_create, (entry)db_ensemble_steps, (entry)db_ensemble_destroy,
-      (entry)db_ensemble_error, (entry)db_autotune, (entry)db_get_tuning, (entry)db_set_tuning, (entry)db_set_timing, (entry)db_stage_times,
+      (entry)db_ensemble_error, (entry)db_ensemble_set_batched, (entry)db_ensemble_info, (entry)db_autotune, (entry)db_get_tuning, (entry)db_set_tuning, (entry)db_set_timing, (entry)db_stage_times,
       (entry)db_kernel_launches, (entry)db_set_wait_limit,
   };
   const int n = (int)(sizeof all / sizeof all[0]);

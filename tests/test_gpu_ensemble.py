@@ -49,3 +49,59 @@ def test_ensemble_mixed_precision_members_track_fp64():
             err = np.linalg.norm(a[f] - b[f]) / np.linalg.norm(b[f])
             assert err <= 1e-6, (i, f, err)
     ens.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batched_form_equals_member_graphs(precision):
+    """Members without LES at a fixed dt are batched (each kernel of the step
+    launched once for all of them, the member's arguments from a device
+    table); the per-member graph branches and the batched form give
+    bit-identical states.  nx != nz and unequal forcing per member."""
+    from diablo3_b200.ensemble import Ensemble
+    ps = [config0_params(nx=64, ny=33, nz=32, precision=precision, dthdx_override=m2)
+          for m2 in (0.6, 0.9, 1.4, 1.1)]
+    gy = grid_for(ps[0])
+    seeds = [11, 12, 13, 14]
+    a = Ensemble(ps, gy, seeds=seeds)
+    b = Ensemble(ps, gy, seeds=seeds)
+    assert a.batched and b.batched
+    b.batched = False
+    assert not b.batched
+    a.step(4)
+    b.step(4)
+    a.step(3)
+    b.step(3)
+    assert a.kernels_per_step() == 26
+    assert b.kernels_per_step() > 26 * len(ps)
+    for ma, mb, p in zip(a.members, b.members, ps):
+        sa, sb = channel_state(ma, p), channel_state(mb, p)
+        for f in STATE:
+            assert np.array_equal(sa[f], sb[f]), f
+        st_a, st_b = ma.status(), mb.status()
+        assert st_a.flags == st_b.flags == 0
+        assert st_a.time_step == st_b.time_step == 7
+        assert st_a.time == st_b.time
+    # the batched form again on the second ensemble continues identically
+    b.batched = True
+    a.step(2)
+    b.step(2)
+    for ma, mb, p in zip(a.members, b.members, ps):
+        assert np.array_equal(channel_state(ma, p)[0], channel_state(mb, p)[0])
+    a.close()
+    b.close()
+
+
+def test_batched_form_only_where_members_qualify():
+    """Members with a CFL-limited dt (or LES) step through the per-member
+    graph branches; asking for the batched form is an argument error."""
+    from diablo3_b200 import lib as L
+    from diablo3_b200.ensemble import Ensemble
+    ps = [config0_params(nx=32, ny=33, nz=32, variable_dt=1, dthdx_override=m2) for m2 in (0.8, 1.2)]
+    gy = grid_for(ps[0])
+    ens = Ensemble(ps, gy, seeds=[1, 2])
+    assert not ens.batched
+    with pytest.raises(L.DiabloError):
+        ens.batched = True
+    ens.step(2)
+    assert all(m.status().time_step == 2 and m.status().flags == 0 for m in ens.members)
+    ens.close()
