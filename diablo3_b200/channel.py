@@ -181,6 +181,15 @@ class Channel:
                                          _L.dptr(w)))
         return out, w
 
+    def les_stats(self) -> dict:
+        """The LES statistics (save_stats_LES_OOL's nu_sgs, kappa_sgs and
+        compute_TKE_diss_les's eps_sgs2), FP64: a dict of arrays over the
+        planes 0..Nyp+1 from the stored nu_t, kappa_t (les_eval() first
+        for those of the current state)."""
+        out = np.zeros((len(_L.LES_ROWS), self.p.ny + 2))
+        self._ck(self.L.db_les_stats(self.h, _L.dptr(out.reshape(-1))))
+        return {k: out[i].copy() for i, k in enumerate(_L.LES_ROWS)}
+
     def set_sgs_net(self, net):
         """Learned closure for les_model_type 6 (a SgsNet that outlives this channel)."""
         self._sgs = net

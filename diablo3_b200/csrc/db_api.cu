@@ -1731,6 +1731,22 @@ extern "C" int db_budget(db_ctx* c, double* out) {
   return DB_OK;
 }
 
+// save_stats_LES_OOL's means and compute_TKE_diss_les (k_budget.cu)
+extern "C" int db_les_stats(db_ctx* c, double* out) {
+  if (!c || !out) return DB_ERR_ARG;
+  if (!c->p.use_les || !c->s.nu_t) return fail(c, DB_ERR_ARG, "db_les_stats: not an LES context");
+  const int np = c->g.np;
+  if (!c->bud_out && balloc(c, (void**)&c->bud_out, (size_t)DB_NBUD * np * sizeof(double)))
+    return fail(c, DB_ERR_CUDA, "db_les_stats: out of device memory");
+  int rc = budget_fields(c);
+  if (rc) return rc;
+  CK(launch_les_stats(c->g, c->s, fset(c->bud_phys[0], c->bud_phys[1], c->bud_phys[2]), c->bud_out, c->st));
+  CK(cudaMemcpyAsync(out, c->bud_out, (size_t)DB_NLES * np * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->launches += 1 + 8;
+  return DB_OK;
+}
+
 extern "C" int db_bpe(db_ctx* c, int nbin, double* pdf, double* th_bin, double* bpe) {
   if (!c || nbin < 1 || nbin > (1 << 16)) return DB_ERR_ARG;
   if (c->bud_nbin < nbin) {

@@ -252,6 +252,9 @@ cudaError_t launch_thomas_les(const Geom& g, const State& s, int rk, cudaStream_
 // mxy scratch [3][np][Nx], out [DB_NBUD][np]
 cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSet phys, int homx, double* mxy,
                           double* out, cudaStream_t st);
+// save_stats_LES_OOL's plane means of nu_t, kappa_t and compute_TKE_diss_les
+// (out[3][np]) from the FP64 physical u1, u2, u3 (phys)
+cudaError_t launch_les_stats(const Geom& g, const State& s, FieldSet phys, double* out, cudaStream_t st);
 // PDF of th + dTHdX (x - Lx/2) over planes jstart_th..jend_th (weights dyf)
 cudaError_t launch_bpe_pdf(const Geom& g, const Phys& ph, const double* th, int homx, int nbin, double* pdf,
                            cudaStream_t st, double* fbin = nullptr, int kind = 0, const double* f0 = nullptr,

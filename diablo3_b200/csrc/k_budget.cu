@@ -235,6 +235,70 @@ __global__ void __launch_bounds__(256) k_bpe_pdf(const double* th, Geom g, Phys 
   }
 }
 
+// The LES statistics: the plane means of nu_t and kappa_t that les_chan and
+// les_chan_th write under flag_save_LES (for/les.f90:909-935, 1404-1430),
+// and compute_TKE_diss_les's eps_sgs2 (for/diagnostics.f90:2057-2118), the
+// implicitly stepped part of the SGS dissipation: at GY row j (2..Nyp) the
+// u1, u3 terms u_i d/dy(nu_t du_i/dy), formed at the GYF rows j and j - 1
+// and averaged onto GY, plus the u2 term at GY with nu_t averaged onto GYF.
+// FP64 physical u1, u2, u3 (phys.p[0..2]); nu_t, kappa_t at the context's
+// precision R.  One CTA per plane, FP64 sums; out[3][np], zero where a row
+// is not defined.
+template <typename R>
+__global__ void __launch_bounds__(256) k_les_stats(const __grid_constant__ State s, Geom g,
+                                                   const __grid_constant__ FieldSet phys, double* out) {
+  const int j = blockIdx.x, np = g.np, Nyp = g.ny;
+  const long long pp = g.pp;   // Nx * Nz points per plane
+  const R* nut = (const R*)s.nu_t;
+  const R* kat = (const R*)s.kappa_t;
+  const double* U1 = (const double*)phys.p[0];
+  const double* U2 = (const double*)phys.p[1];
+  const double* U3 = (const double*)phys.p[2];
+  const bool eps = (j >= 2 && j <= Nyp);
+  // s1 of compute_TKE_diss_les at GYF row jj (1..Nyp), point c of the plane
+  auto s1 = [&](int jj, long long c) -> double {
+    const long long o = (long long)jj * pp + c;
+    const double n0 = (double)nut[o], n1 = (double)nut[o + pp];
+    const double dyp = g.dy[jj + 1], dy0 = g.dy[jj], dyfj = g.dyf[jj];
+    const double t1 = (n1 * (U1[o + pp] - U1[o]) / dyp - n0 * (U1[o] - U1[o - pp]) / dy0) / dyfj;
+    const double t3 = (n1 * (U3[o + pp] - U3[o]) / dyp - n0 * (U3[o] - U3[o - pp]) / dy0) / dyfj;
+    return U1[o] * t1 + U3[o] * t3;
+  };
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (long long c = threadIdx.x; c < pp; c += blockDim.x) {
+    const long long o = (long long)j * pp + c;
+    acc[0] += (double)nut[o];
+    acc[1] += (double)kat[o];
+    if (eps) {
+      const double nj = (double)nut[o], njp = (double)nut[o + pp], njm = (double)nut[o - pp];
+      const double t2 = (0.5 * (nj + njp) * (U2[o + pp] - U2[o]) / g.dyf[j] -
+                         0.5 * (nj + njm) * (U2[o] - U2[o - pp]) / g.dyf[j - 1]) / g.dy[j];
+      acc[2] += 0.5 * (s1(j, c) + s1(j - 1, c)) + U2[o] * t2;
+    }
+  }
+  __shared__ double red[8][3];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double v = acc[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += red[k][threadIdx.x];
+    out[(long long)threadIdx.x * np + j] = (threadIdx.x < 2 || eps) ? v / (double)pp : 0.0;
+  }
+}
+
+cudaError_t launch_les_stats(const Geom& g, const State& s, FieldSet phys, double* out, cudaStream_t st) {
+  if (!s.nu_t || !s.kappa_t) return cudaErrorInvalidValue;
+  if (g.prec) k_les_stats<float><<<g.np, 256, 0, st>>>(s, g, phys, out);
+  else k_les_stats<double><<<g.np, 256, 0, st>>>(s, g, phys, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_budget(const Geom& g, const Phys& ph, const State& s, FieldSet phys, int homx, double* mxy,
                           double* out, cudaStream_t st) {
   k_zmeans<<<g.np, 256, 0, st>>>(s, g, phys, homx, mxy);

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libdiablo_b200.so")
 # enum db_field
 CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH, NU_T, KAPPA_T = range(11)
 DB_ZS_FIELD, DB_ZS_KE = 0, 1   # db_bin_ystar kinds
+LES_ROWS = ("nu_sgs", "kappa_sgs", "eps_sgs2")   # db_les_stats rows
 # rows of db_stats (include/diablo_b200.h order)
 NTUNE = 6   # DB_NTUNE
 STAT_ROWS = ("ume", "vme", "wme", "thme", "urms", "vrms", "wrms", "thrms", "uv", "wv", "uw", "thv", "epsilon", "chi")
@@ -32,7 +33,7 @@ EXPORTS = (
     "db_set_clock", "db_get_status", "db_clear_status",
     "db_fft_xz_to_fourier", "db_fft_xz_to_physical", "db_fft_xz_to_fourier_dev", "db_fft_xz_to_physical_dev",
     "db_rk_substep", "db_rk_steps", "db_rem_div", "db_apply_bc_vel_post",
-    "db_courant", "db_divergence", "db_stats", "db_budget", "db_bpe", "db_bin_ystar", "db_poisson_p",
+    "db_courant", "db_divergence", "db_stats", "db_budget", "db_bpe", "db_bin_ystar", "db_les_stats", "db_poisson_p",
     "db_autotune", "db_get_tuning", "db_set_tuning", "db_set_timing", "db_stage_times", "db_kernel_launches",
     "db_rem_div_static",
     "db_sgs_create", "db_sgs_destroy", "db_sgs_set", "db_sgs_get", "db_sgs_set_range", "db_sgs_forward",
@@ -99,6 +100,7 @@ def load(path: str | None = None):
     L.db_poisson_p.argtypes = [vp]
     L.db_bpe.argtypes = [vp, ctypes.c_int, dp, dp, dp]
     L.db_bin_ystar.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, dp, dp]
+    L.db_les_stats.argtypes = [vp, dp]
     L.db_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.db_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     L.db_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]

@@ -266,6 +266,18 @@ int db_bpe(db_ctx* ctx, int nbin, double* pdf, double* th_bin, double* bpe);
 enum { DB_ZS_FIELD = 0, DB_ZS_KE = 1 };
 int db_bin_ystar(db_ctx* ctx, int kind, const double* field, int nbin, double* binned, double* weight);
 
+/* The LES statistics of an LES context, FP64, out[DB_NLES][Nyp+2] (row r,
+ * plane j): DB_LS_NU and DB_LS_KAPPA the plane means of the stored nu_t and
+ * kappa_t (nu_sgs, kappa_sgs: les_chan for/les.f90:909-935, les_chan_th
+ * :1404-1430), DB_LS_EPS2 compute_TKE_diss_les's eps_sgs2
+ * (for/diagnostics.f90:2057-2118) at GY rows 2..Nyp from the current state
+ * and the stored nu_t (zero on the other planes).  nu_t and kappa_t are
+ * those of the closure's last evaluation (the last LES substep, or
+ * db_les_eval on the current state, as save_stats_LES_OOL runs les_chan
+ * before writing).  DB_ERR_ARG without use_les. */
+enum { DB_LS_NU = 0, DB_LS_KAPPA, DB_LS_EPS2, DB_NLES };
+int db_les_stats(db_ctx* ctx, double* out);
+
 /*
  * Divergence removal that allocates nothing.  No counterpart in the
  * reference (it follows rem_div_chan's arithmetic, for/solver.f90:1302-1379,

@@ -18,7 +18,7 @@ int main(void) {
       (entry)db_upload_state, (entry)db_download_state, (entry)db_upload_field, (entry)db_download_field,
       (entry)db_set_clock, (entry)db_get_status, (entry)db_clear_status, (entry)db_fft_xz_to_fourier, (entry)db_fft_xz_to_fourier_dev,
       (entry)db_fft_xz_to_physical, (entry)db_fft_xz_to_physical_dev, (entry)db_rk_substep, (entry)db_rk_steps, (entry)db_rem_div,
-      (entry)db_apply_bc_vel_post, (entry)db_courant, (entry)db_divergence, (entry)db_stats, (entry)db_budget, (entry)db_bpe, (entry)db_bin_ystar, (entry)db_poisson_p,
+      (entry)db_apply_bc_vel_post, (entry)db_courant, (entry)db_divergence, (entry)db_stats, (entry)db_budget, (entry)db_bpe, (entry)db_bin_ystar, (entry)db_les_stats, (entry)db_poisson_p,
       (entry)db_rem_div_static, (entry)db_sgs_create, (entry)db_sgs_destroy, (entry)db_sgs_set,
       (entry)db_sgs_get, (entry)db_sgs_set_range, (entry)db_sgs_forward, (entry)db_sgs_gradient,
       (entry)db_sgs_train_step, (entry)db_sgs_gemm_check, (entry)db_set_sgs_net, (entry)db_les_eval,

@@ -71,8 +71,8 @@ def test_batched_form_equals_member_graphs(precision):
     b.step(4)
     a.step(3)
     b.step(3)
-    assert a.kernels_per_step() == 26
-    assert b.kernels_per_step() > 26 * len(ps)
+    assert a.kernels_per_step() == 26                       # one launch per kernel for all members
+    assert b.kernels_per_step() > 2 * a.kernels_per_step()  # each member's own kernels
     for ma, mb, p in zip(a.members, b.members, ps):
         sa, sb = channel_state(ma, p), channel_state(mb, p)
         for f in STATE:

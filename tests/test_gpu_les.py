@@ -123,3 +123,61 @@ def test_les_eddy_field_round_trip(Channel):
         a[:, : p.nz, : p.nx] = rng.random((p.ny + 2, p.nz, p.nx))
         ch.upload_field(KAPPA_T, a)
         assert np.array_equal(ch.download_field(KAPPA_T), a)
+
+
+def _ref_les_stats(p, gy, st, nu, ka):
+    """nu_sgs, kappa_sgs (les.f90:909-935, 1404-1430) and eps_sgs2
+    (diagnostics.f90:2057-2118) by the reference's loops, in numpy."""
+    from _util import to_phys
+    from diablo3_b200.grid import metrics
+    m = metrics(np.asarray(gy, np.float64))
+    dy, dyf = m["dy"], m["dyf"]
+    u1, u2, u3 = (to_phys(p, significant(p, st[f])) for f in (0, 1, 2))   # (planes, z, x)
+    nut, kat = nu[:, : p.nz, : p.nx], ka[:, : p.nz, : p.nx]
+    n, Nyp, npl = p.nx * p.nz, p.ny, p.ny + 2
+    out = np.zeros((3, npl))
+    out[0] = nut.sum(axis=(1, 2)) / n
+    out[1] = kat.sum(axis=(1, 2)) / n
+    s1 = np.zeros_like(u1)
+    for j in range(1, Nyp + 1):
+        s1[j] = (u1[j] * ((nut[j + 1] * (u1[j + 1] - u1[j]) / dy[j + 1] - nut[j] * (u1[j] - u1[j - 1]) / dy[j])
+                          / dyf[j])
+                 + u3[j] * ((nut[j + 1] * (u3[j + 1] - u3[j]) / dy[j + 1] - nut[j] * (u3[j] - u3[j - 1]) / dy[j])
+                            / dyf[j]))
+    for j in range(2, Nyp + 1):
+        temp = (0.5 * (s1[j] + s1[j - 1])
+                + u2[j] * ((0.5 * (nut[j] + nut[j + 1]) * (u2[j + 1] - u2[j]) / dyf[j]
+                            - 0.5 * (nut[j] + nut[j - 1]) * (u2[j] - u2[j - 1]) / dyf[j - 1]) / dy[j]))
+        out[2, j] = temp.sum() / n
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_les_stats_match_reference_loops(Channel, precision):
+    """db_les_stats (nu_sgs, kappa_sgs, eps_sgs2) against the reference's
+    loops on the same state, with nu_t / kappa_t of the AMD closure
+    evaluated on that state (as save_stats_LES_OOL runs les_chan before it
+    writes).  Bar: 1e-10 of each row's largest value."""
+    p = les_params(precision=precision)
+    gy = grid_for(p)
+    with Channel(p, gy) as ch:
+        ch.init_flow(seed=5)
+        ch.step(3)
+        nu, ka = ch.les_eval(5)
+        st = ch.download_state()
+        got = ch.les_stats()
+    ref = _ref_les_stats(p, gy, st, nu, ka)
+    for i, k in enumerate(("nu_sgs", "kappa_sgs", "eps_sgs2")):
+        scale = np.abs(ref[i]).max()
+        assert scale > 0, k
+        err = np.abs(got[k] - ref[i]).max() / scale
+        assert err <= 1e-10, (k, err)
+    assert got["eps_sgs2"][0] == got["eps_sgs2"][1] == got["eps_sgs2"][-1] == 0.0
+
+
+def test_les_stats_needs_les(Channel):
+    from diablo3_b200 import lib as L
+    p = config0_params(nx=32, ny=33, nz=32)
+    with Channel(p, grid_for(p)) as ch:
+        with pytest.raises(L.DiabloError):
+            ch.les_stats()
