@@ -319,3 +319,21 @@ def test_config3_network_fixture():
     for k, sh in shapes.items():
         assert d[k].shape == sh and np.all(np.isfinite(d[k])), k
     assert np.all(d["std"] > 0) and np.all(d["scale"] > 0) and np.all(d["hi"] >= d["lo"])
+
+
+def test_workloads_and_closure_study_setups():
+    """The benchmark configurations and the closure study's DNS / LES
+    parameters (no GPU): sizes, closures and the 4x4x4 filter relation."""
+    from diablo3_b200 import closure_study
+    from diablo3_b200.workloads import WORKLOAD_DESC, workload_params
+    c1, c2, c3 = (workload_params(n) for n in ("config1", "config2", "config3"))
+    assert (c1.nx, c1.ny, c1.nz, c1.use_les) == (512, 257, 512, 0)
+    assert (c2.nx, c2.ny, c2.nz, c2.use_les, c2.les_model_type) == (256, 129, 256, 1, 5)
+    assert (c3.nx, c3.ny, c3.nz, c3.ic_type) == (128, 65, 128, 6)
+    assert set(WORKLOAD_DESC) >= {"config0", "config1", "slab", "config2", "config3"}
+    d = closure_study.dns_params()
+    assert (d.nx, d.ny, d.nz, d.use_les, d.variable_dt) == (512, 257, 512, 0, 0)
+    a, l = closure_study.les_params(5, 0), closure_study.les_params(6, 1)
+    assert (a.nx, a.ny, a.nz) == (d.nx // 4, d.ny // 4 + 1, d.nz // 4) == (l.nx, l.ny, l.nz)
+    assert (a.les_model_type, a.precision, l.les_model_type, l.precision) == (5, 0, 6, 1)
+    assert a.delta_t == l.delta_t == d.delta_t and a.re == d.re
