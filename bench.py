@@ -228,7 +228,7 @@ def run_ensemble(args) -> None:
     clk = clocks.stop()
     kps = ens.kernels_per_step()
     branches = None
-    if batched:   # the per-member graph branches on the same members, for comparison
+    if batched and not args.no_extras:   # the per-member graph branches on the same members, for comparison
         ens.batched = False
         ms_b = timed()
         branches = {"ms_per_step": ms_b / args.steps, "kernels_per_step": ens.kernels_per_step(),
@@ -438,7 +438,8 @@ def main():
     ap.add_argument("--les", action="store_true", help="AMD LES closure (les_model_type 5) on")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the mixed-precision DNS and the 128x65x128 LES comparison keys")
+                    help="skip the mixed-precision DNS and the 128x65x128 LES comparison keys "
+                         "(--config config4: the per-member graph comparison)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

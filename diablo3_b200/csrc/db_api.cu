@@ -1053,13 +1053,17 @@ struct db_ensemble {
 };
 
 // members that one batched launch per kernel can advance: the spectral
-// substep (no LES), fixed dt, the same grid and precision
+// substep (no LES), fixed dt, the same grid, solved planes and precision
 static bool batch_eligible(const std::vector<db_ctx*>& m) {
   const db_ctx* a = m[0];
   if (a->g.nx > 512 || (long long)m.size() > 65535 / MAXF) return false;
   for (const db_ctx* c : m) {
     if (c->p.use_les || c->p.variable_dt) return false;
     if (c->g.nx != a->g.nx || c->g.ny != a->g.ny || c->g.nz != a->g.nz || c->g.prec != a->g.prec) return false;
+    // the batched kernels take member 0's geometry (the planes each equation solves included)
+    if (c->g.jstart != a->g.jstart || c->g.jend != a->g.jend || c->g.jstart_th != a->g.jstart_th ||
+        c->g.jend_th != a->g.jend_th)
+      return false;
     if (!c->s.crs[0] || (!c->g.prec && !c->s.nls[4])) return false;
   }
   return true;

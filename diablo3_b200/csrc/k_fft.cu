@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_fwd_z(const __grid_constant_
   const int m = B ? (int)blockIdx.z / bt.nf : 0, f = B ? (int)blockIdx.z - m * bt.nf : (int)blockIdx.z;
   const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
   const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
-  const Geom& g = B ? bt.tab[m].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(znl_threads<N>(), FftShape<N>::T >= 256 ? 1 : 
   const int m = B ? (int)blockIdx.z >> 2 : 0, e = B ? (int)blockIdx.z & 3 : (int)blockIdx.z;
   const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
   const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
-  const Geom& g = B ? bt.tab[m].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256, DB_LB_FFT) k_inv_z(const __grid_constant_
   const int m = B ? (int)blockIdx.z / bt.nf : 0, f = B ? (int)blockIdx.z - m * bt.nf : (int)blockIdx.z;
   const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
   const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
-  const Geom& g = B ? bt.tab[m].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   using C = typename CplxOf<R>::type;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   C* sm = reinterpret_cast<C*>(sm_raw);
@@ -385,17 +385,17 @@ struct CflArgs {
   DevScalars* sc;
 };
 
-// B: member-batched (blockIdx.y = member; each member's items over its own
-// gridDim.x CTAs; no dmask, not with CFL)
+// B: member-batched (the persistent CTAs walk the items of every member,
+// member = item / nitems; g is member 0's geometry, the same for all; no
+// dmask, not with CFL)
 template <int N, typename R, bool CFL, bool B = false>
-__global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in0, const __grid_constant__ FieldSet out0, Geom g0,
+__global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ FieldSet in, const __grid_constant__ FieldSet out, Geom g,
                                                       unsigned dmask, int nblk, int nitems,
                                                       const __grid_constant__ CflArgs cf, const __grid_constant__ Batch bt) {
   static_assert(!(B && CFL), "the CFL x-pass is not batched");
-  const int m = B ? (int)blockIdx.y : 0;
-  const FieldSet& in = B ? bt.tab[m].fs[bt.fin] : in0;
-  const FieldSet& out = B ? bt.tab[m].fs[bt.fout] : out0;
-  const Geom& g = B ? bt.tab[m].g : g0;
+  const int ntot = B ? nitems * bt.n : nitems;
+  auto fs_in = [&](int it) -> const FieldSet& { return B ? bt.tab[it / nitems].fs[bt.fin] : in; };
+  auto fs_out = [&](int it) -> const FieldSet& { return B ? bt.tab[it / nitems].fs[bt.fout] : out; };
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -410,8 +410,9 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
   C* sq = xbuf + seq * padded(N);
   const C* twt = tw_x<R>(g);   // twiddles fetched per pass (fewer live registers)
   auto src = [&](int it) -> const C* {
-    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
-    return (const C*)in.p[f] + (long long)j * g.hp + (long long)(2 * ns * b) * g.kxs;
+    const int li = B ? it % nitems : it;
+    const int f = li / (g.np * nblk), r = li % (g.np * nblk), j = r / nblk, b = r % nblk;
+    return (const C*)fs_in(it).p[f] + (long long)j * g.hp + (long long)(2 * ns * b) * g.kxs;
   };
   // CFL: courant's gate (for/flow.f90:746-750) and plane range
   if (CFL && !cf.ctl.force && !(cf.ctl.variable_dt && (cf.sc->time_step % cf.ctl.update_dt) == 0)) return;
@@ -424,15 +425,15 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
     mbar_init(&mbar[1], 1);
   }
   __syncthreads();
-  if (threadIdx.x == 0 && (int)blockIdx.x < nitems) {
+  if (threadIdx.x == 0 && (int)blockIdx.x < ntot) {
     mbar_expect_tx(&mbar[0], item_bytes);
     bulk_g2s(stage0, src(blockIdx.x), item_bytes, &mbar[0]);
   }
   int k = 0;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++k) {
+  for (int it = blockIdx.x; it < ntot; it += gridDim.x, ++k) {
     const int s = k & 1;
     const int nxt = it + gridDim.x;
-    if (threadIdx.x == 0 && nxt < nitems) {
+    if (threadIdx.x == 0 && nxt < ntot) {
       fence_async_smem();
       mbar_expect_tx(&mbar[s ^ 1], item_bytes);
       bulk_g2s(reinterpret_cast<unsigned char*>(stage0) + (s ^ 1) * item_bytes, src(nxt), item_bytes, &mbar[s ^ 1]);
@@ -441,13 +442,14 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
         __syncthreads_and(mbar_wait_first(&mbar[s], (uint32_t)((k >> 1) & 1), g.wait_first, STAGE_WAIT) ? 1 : 0) != 0;
     if (!got) {   // record it, let the copies in flight land (bounded), leave
       if (threadIdx.x == 0) {
-        atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
+        atomicOr(B ? bt.tab[it / nitems].g.flags : g.flags, DB_FLAG_WAIT_TIMEOUT);
         mbar_wait(&mbar[s], (uint32_t)((k >> 1) & 1), STAGE_WAIT);
-        if (nxt < nitems) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
+        if (nxt < ntot) mbar_wait(&mbar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), STAGE_WAIT);
       }
       return;
     }
-    const int f = it / (g.np * nblk), r = it % (g.np * nblk), j = r / nblk, b = r % nblk;
+    const int li = B ? it % nitems : it;
+    const int f = li / (g.np * nblk), r = li % (g.np * nblk), j = r / nblk, b = r % nblk;
     if (CFL && (j < jlo || j > jhi)) {   // uniform over the CTA: not a courant plane
       __syncthreads();
       continue;
@@ -496,7 +498,7 @@ __global__ void __launch_bounds__(256, 2) k_inv_x_st(const __grid_constant__ Fie
         amax = fmax(amax, fmax(ta, tb));
       }
     } else {
-      R* ra = (R*)out.p[f] + (long long)j * g.pp + (long long)(2 * (ns * b + seq)) * g.nx;
+      R* ra = (R*)fs_out(it).p[f] + (long long)j * g.pp + (long long)(2 * (ns * b + seq)) * g.nx;
       R* rb = ra + g.nx;
 #pragma unroll
       for (int q = 0; q < E; ++q) {
@@ -719,10 +721,10 @@ static void go_inv_x_bt(const Geom& g, const Batch& bt, cudaStream_t st) {
   const size_t smem = 2 * (size_t)(2 * cps * g.kxs * sizeof(C)) + (size_t)cps * padded(N) * sizeof(C) + 16;
   smem_attr(k_inv_x_st<N, R, false, true>, smem);
   const int gmax = xpass_ctas_per_sm(g) * sm_count();
-  int gx = (gmax + bt.n - 1) / bt.n;
-  gx = gx < nitems ? gx : nitems;
-  k_inv_x_st<N, R, false, true><<<dim3(gx, bt.n), cps * FftShape<N>::T, smem, st>>>(
-      FieldSet{}, FieldSet{}, g, 0u, nblk, nitems, CflArgs{}, bt);
+  const long long ntot = (long long)nitems * bt.n;
+  const int grid = ntot < gmax ? (int)ntot : gmax;
+  k_inv_x_st<N, R, false, true><<<grid, cps * FftShape<N>::T, smem, st>>>(FieldSet{}, FieldSet{}, g, 0u, nblk,
+                                                                           nitems, CflArgs{}, bt);
 }
 template <int N, typename R>
 static void go_inv_z_bt(const Geom& g, const Batch& bt, cudaStream_t st) {

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_
                                                         int jlen, int nitems, const MemberArgs* __restrict__ tab) {
   const int mb = B ? (int)blockIdx.y : 0;
   const State& s = B ? tab[mb].s : s0;
-  const Geom& g = B ? tab[mb].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   using C = typename CplxOf<R>::type;
   using S = FftShape<N>;
   constexpr int E = S::E, T = S::T;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(192, prod_slots<R>() == 4 ? 2 : 3) k_products_
       }
       if (__syncthreads_and(ok ? 1 : 0) == 0) {   // a copy did not land in time: record, drain (bounded), leave
         if (threadIdx.x == 0) {
-          atomicOr(g.flags, DB_FLAG_WAIT_TIMEOUT);
+          atomicOr(B ? tab[mb].g.flags : g.flags, DB_FLAG_WAIT_TIMEOUT);
           for (int sl = 0; sl < PROD_SLOTS; ++sl)
             if (pend >> sl & 1u) mbar_wait(&mbar[sl], (par >> sl) & 1u, PROD_WAIT);
         }
@@ -656,7 +656,7 @@ template <bool B = false>
 __global__ void __launch_bounds__(256) k_tri_coef(Geom g0, Phys ph0, TriRow* tri0, DevScalars* sc0, int rk,
                                                   const MemberArgs* __restrict__ tab) {
   const int mb = B ? (int)blockIdx.y : 0;
-  const Geom& g = B ? tab[mb].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   const Phys& ph = B ? tab[mb].ph : ph0;
   TriRow* tri = B ? tab[mb].s.tri : tri0;
   DevScalars* sc = B ? tab[mb].s.sc : sc0;
@@ -805,7 +805,7 @@ __global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constan
                                                             const MemberArgs* __restrict__ tab) {
   const int mb = B ? (int)blockIdx.y : 0;
   const State& s = B ? tab[mb].s : s0;
-  const Geom& g = B ? tab[mb].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   const Phys& ph = B ? tab[mb].ph : ph0;
   const FieldSet& nl = B ? tab[mb].fs[FS_NL] : nl0;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s
                                                  const __grid_constant__ FieldSet nl0, const MemberArgs* __restrict__ tab) {
   const int mb = B ? (int)blockIdx.z : 0;
   const State& s = B ? tab[mb].s : s0;
-  const Geom& g = B ? tab[mb].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   const FieldSet& nl = B ? tab[mb].fs[FS_NL] : nl0;
   constexpr int TB = 8;
   const long long ncol = 2 * g.sp;
@@ -934,7 +934,7 @@ __global__ void __launch_bounds__(128) k_cn_back(const __grid_constant__ State s
       if (j >= lo && j <= hi) u[(long long)j * pp] = xv;
     }
   }
-  if (bad) atomicOr(g.flags, DB_FLAG_NONFINITE);
+  if (bad) atomicOr(B ? tab[mb].g.flags : g.flags, DB_FLAG_NONFINITE);
 }
 // ---------------------------------------------------------------------------
 // rem_div factors: per (kx, kzp) column, rows 1..Nyp of the Poisson system
@@ -995,7 +995,7 @@ __global__ void __launch_bounds__(128, LB) k_rem_div(const __grid_constant__ Sta
                                                       const MemberArgs* __restrict__ tab) {
   const int mb = B ? (int)blockIdx.z : 0;
   const State& s = B ? tab[mb].s : s0;
-  const Geom& g = B ? tab[mb].g : g0;
+  const Geom& g = g0;   // the same geometry for every member
   const int t = blockIdx.x * blockDim.x + threadIdx.x, kzp = blockIdx.y;
   const int kx = t >> 1, part = t & 1;
   if (kx > g.nkx) return;
