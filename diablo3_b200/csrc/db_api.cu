@@ -1044,8 +1044,14 @@ struct db_ensemble {
   // batched form
   bool can_batch = false, batched = false;
   MemberArgs* tab = nullptr;                       // device table, one entry per member
-  cudaStream_t st_side = nullptr;                  // the implicit systems' rows
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // the members split into groups of consecutive members, each group a
+  // chain of batched kernels on its own branch of the graph (one group's
+  // kernel boundaries overlap another's work)
+  int groups = 1, groups_cap = 0;                  // requested; in bgraph
+  static constexpr int kMaxGroups = 8;
+  cudaStream_t gst[kMaxGroups] = {}, gside[kMaxGroups] = {};   // group streams, the implicit systems' rows
+  cudaEvent_t gfork[kMaxGroups] = {}, gjoin[kMaxGroups] = {}, gdone[kMaxGroups] = {};
+  cudaEvent_t ev_start = nullptr;
   cudaGraphExec_t bgraph = nullptr;
   Geom g_cap{};                                    // member 0's geometry when bgraph was captured
   long long bkernels = 0;
@@ -1107,15 +1113,22 @@ static int ensemble_create_impl(db_ctx** members, int n, void* stream, db_ensemb
       return DB_ERR_CUDA;
     }
   if (batch_eligible(e->members)) {
-    if (cudaMalloc((void**)&e->tab, (size_t)n * sizeof(MemberArgs)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&e->st_side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    bool ok = cudaMalloc((void**)&e->tab, (size_t)n * sizeof(MemberArgs)) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < db_ensemble::kMaxGroups && ok; ++k)
+      ok = cudaStreamCreateWithFlags(&e->gst[k], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaStreamCreateWithFlags(&e->gside[k], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&e->gfork[k], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&e->gjoin[k], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&e->gdone[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
       db_ensemble_destroy(e);
       g_init_err = "db_ensemble_create: out of device memory";
       return DB_ERR_CUDA;
     }
     e->can_batch = e->batched = true;
+    // about 16 members per group, at most four groups
+    e->groups = std::max(1, std::min(4, n / 16));
   }
   *out = e;
   return DB_OK;
@@ -1133,12 +1146,16 @@ extern "C" int db_ensemble_destroy(db_ensemble* e) {
   if (e->bgraph) cudaGraphExecDestroy(e->bgraph);
   for (auto v : e->ev)
     if (v) cudaEventDestroy(v);
-  if (e->st_side) {
-    cudaStreamSynchronize(e->st_side);
-    cudaStreamDestroy(e->st_side);
+  for (int k = 0; k < db_ensemble::kMaxGroups; ++k) {
+    for (cudaStream_t q : {e->gst[k], e->gside[k]})
+      if (q) {
+        cudaStreamSynchronize(q);
+        cudaStreamDestroy(q);
+      }
+    for (cudaEvent_t v : {e->gfork[k], e->gjoin[k], e->gdone[k]})
+      if (v) cudaEventDestroy(v);
   }
-  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
-  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->ev_start) cudaEventDestroy(e->ev_start);
   if (e->tab) cudaFree(e->tab);
   if (e->own_stream && e->st) cudaStreamDestroy(e->st);
   delete e;
@@ -1147,15 +1164,16 @@ extern "C" int db_ensemble_destroy(db_ensemble* e) {
 
 extern "C" const char* db_ensemble_error(const db_ensemble* e) { return e ? e->err.c_str() : g_init_err.c_str(); }
 
-extern "C" int db_ensemble_set_batched(db_ensemble* e, int on) {
-  if (!e || (on && !e->can_batch)) return DB_ERR_ARG;
-  e->batched = on != 0;
+extern "C" int db_ensemble_set_batched(db_ensemble* e, int groups) {
+  if (!e || groups < 0 || (groups && !e->can_batch)) return DB_ERR_ARG;
+  e->batched = groups != 0;
+  if (groups) e->groups = std::min(std::min(groups, db_ensemble::kMaxGroups), (int)e->members.size());
   return DB_OK;
 }
 
-extern "C" int db_ensemble_info(const db_ensemble* e, int* batched, long long* kernels_per_step) {
+extern "C" int db_ensemble_info(const db_ensemble* e, int* groups, long long* kernels_per_step) {
   if (!e) return DB_ERR_ARG;
-  if (batched) *batched = e->batched ? 1 : 0;
+  if (groups) *groups = e->batched ? e->groups : 0;
   if (kernels_per_step) *kernels_per_step = e->batched ? e->bkernels : e->kernels[0];
   return DB_OK;
 }
@@ -1177,7 +1195,7 @@ static int ensemble_steps_batched(db_ensemble* e, int nsteps) {
       return DB_ERR_CUDA;
     }
   }
-  if (e->bgraph && !same_shapes(e->g_cap, c0->g)) {
+  if (e->bgraph && (!same_shapes(e->g_cap, c0->g) || e->groups_cap != e->groups)) {
     cudaGraphExecDestroy(e->bgraph);
     e->bgraph = nullptr;
   }
@@ -1190,16 +1208,26 @@ static int ensemble_steps_batched(db_ensemble* e, int nsteps) {
       e->err = "ensemble member table upload failed";
       return DB_ERR_CUDA;
     }
-    const Batch b{e->tab, n, 0, 0, 0};
     cudaGraph_t gr;
     if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
       e->err = "ensemble capture could not start";
       return DB_ERR_CUDA;
     }
-    cudaError_t er = launch_steps_batch(b, 0, e->st);
-    for (int rk = 0; rk < 3 && er == cudaSuccess; ++rk)
-      er = launch_substep_batch(c0->g, b, rk, e->st, e->st_side, e->ev_fork, e->ev_join);
-    if (er == cudaSuccess) er = launch_steps_batch(b, 1, e->st);
+    const int G = e->groups;
+    cudaError_t er = cudaEventRecord(e->ev_start, e->st);
+    for (int k = 0; k < G && er == cudaSuccess; ++k) {
+      // group k: members [n k / G, n (k + 1) / G)
+      const int m0 = (int)((long long)n * k / G), m1 = (int)((long long)n * (k + 1) / G);
+      const Batch b{e->tab + m0, m1 - m0, 0, 0, 0};
+      cudaStream_t q = e->gst[k];
+      er = cudaStreamWaitEvent(q, e->ev_start, 0);
+      if (er == cudaSuccess) er = launch_steps_batch(b, 0, q);
+      for (int rk = 0; rk < 3 && er == cudaSuccess; ++rk)
+        er = launch_substep_batch(c0->g, b, rk, q, e->gside[k], e->gfork[k], e->gjoin[k]);
+      if (er == cudaSuccess) er = launch_steps_batch(b, 1, q);
+      if (er == cudaSuccess) er = cudaEventRecord(e->gdone[k], q);
+      if (er == cudaSuccess) er = cudaStreamWaitEvent(e->st, e->gdone[k], 0);
+    }
     cudaError_t er2 = cudaStreamEndCapture(e->st, &gr);
     if (er != cudaSuccess || er2 != cudaSuccess) {
       e->err = std::string("ensemble capture failed: ") + cudaGetErrorString(er != cudaSuccess ? er : er2);
@@ -1213,9 +1241,10 @@ static int ensemble_steps_batched(db_ensemble* e, int nsteps) {
       return DB_ERR_CUDA;
     }
     e->g_cap = c0->g;
+    e->groups_cap = G;
     // step scalars twice; per substep tri_coef, the two inverse passes,
     // products, the z-pass, rhs_cn, cn_back and rem_div
-    e->bkernels = 2 + 3 * 8;
+    e->bkernels = (long long)G * (2 + 3 * 8);
   }
   for (int it = 0; it < nsteps; ++it) {
     if (cudaGraphLaunch(e->bgraph, e->st) != cudaSuccess) {

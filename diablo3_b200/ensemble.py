@@ -49,6 +49,7 @@ class Ensemble:
         if rc != 0:
             raise _L.DiabloError(rc, self.L.db_ensemble_error(None).decode())
         self.h = h
+        self._groups0 = self.groups   # the default grouping of the batched form (0: not batched)
 
     def step(self, nsteps: int = 1):
         rc = self.L.db_ensemble_steps(self.h, nsteps)
@@ -56,17 +57,26 @@ class Ensemble:
             raise _L.DiabloError(rc, self.L.db_ensemble_error(self.h).decode())
 
     @property
-    def batched(self) -> bool:
-        """True when every kernel of a step is launched once for all members."""
+    def groups(self) -> int:
+        """Groups of the batched form (each kernel of a step launched once per
+        group of members), 0 for the per-member graph branches."""
         b = ctypes.c_int()
         self.L.db_ensemble_info(self.h, ctypes.byref(b), None)
-        return bool(b.value)
+        return b.value
+
+    @groups.setter
+    def groups(self, n: int):
+        rc = self.L.db_ensemble_set_batched(self.h, int(n))
+        if rc != 0:
+            raise _L.DiabloError(rc, "members do not qualify for the batched form")
+
+    @property
+    def batched(self) -> bool:
+        return self.groups > 0
 
     @batched.setter
     def batched(self, on: bool):
-        rc = self.L.db_ensemble_set_batched(self.h, 1 if on else 0)
-        if rc != 0:
-            raise _L.DiabloError(rc, "members do not qualify for the batched form")
+        self.groups = (self._groups0 or 1) if on else 0
 
     def kernels_per_step(self) -> int:
         k = ctypes.c_longlong()

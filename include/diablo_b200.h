@@ -390,19 +390,22 @@ int db_ensemble_create(db_ctx** members, int n, void* cuda_stream, db_ensemble**
 int db_ensemble_steps(db_ensemble* ens, int nsteps);
 int db_ensemble_destroy(db_ensemble* ens);
 const char* db_ensemble_error(const db_ensemble* ens);
-/* Batched form: members of the same grid size and precision, without LES
- * and at a fixed dt (variable_dt 0), are advanced by one launch of each
- * kernel of the step for all of them (the member index is a grid
- * dimension; each member's pointers and parameters come from a device
- * table); their results are bit-identical to stepping each alone.  It is
- * used whenever the members qualify.  db_ensemble_set_batched(ens, 0)
- * selects the per-member graph branches instead, 1 the batched form again
- * (DB_ERR_ARG if the members do not qualify).  db_ensemble_info: *batched
- * 1 when the batched form is in use; *kernels_per_step the kernels one
+/* Batched form: members of the same grid size, solved planes and
+ * precision, without LES and at a fixed dt (variable_dt 0), are advanced by
+ * batched kernels: each kernel of the step is launched once for a group of
+ * consecutive members (the member index is a grid dimension; each member's
+ * pointers and parameters come from a device table), each group a chain
+ * of such launches on its own branch of the step's graph; results are
+ * bit-identical to stepping each member alone.  It is used whenever the
+ * members qualify, with n/16 groups (1 to 4).  db_ensemble_set_batched(ens,
+ * groups): 0 selects the per-member graph branches, groups >= 1 the batched
+ * form in that many groups (at most 8 and n; DB_ERR_ARG if the members do
+ * not qualify).  db_ensemble_info: *groups 0 for the per-member branches,
+ * else the batched form's group count; *kernels_per_step the kernels one
  * ensemble step launches for all members (0 before the first step).  In
  * the batched form the members' own kernel counters do not grow. */
-int db_ensemble_set_batched(db_ensemble* ens, int on);
-int db_ensemble_info(const db_ensemble* ens, int* batched, long long* kernels_per_step);
+int db_ensemble_set_batched(db_ensemble* ens, int groups);
+int db_ensemble_info(const db_ensemble* ens, int* groups, long long* kernels_per_step);
 
 /* ---- measurement hooks (no counterpart in the reference, which only
  * prints wall seconds per iteration, for/diablo.f90:101-107) ---- */

@@ -54,9 +54,9 @@ def test_ensemble_mixed_precision_members_track_fp64():
 @pytest.mark.parametrize("precision", [0, 1])
 def test_batched_form_equals_member_graphs(precision):
     """Members without LES at a fixed dt are batched (each kernel of the step
-    launched once for all of them, the member's arguments from a device
-    table); the per-member graph branches and the batched form give
-    bit-identical states.  nx != nz and unequal forcing per member."""
+    launched once per group of members, the member's arguments from a
+    device table); the per-member graph branches, one group and two groups
+    give bit-identical states.  nx != nz and unequal forcing per member."""
     from diablo3_b200.ensemble import Ensemble
     ps = [config0_params(nx=64, ny=33, nz=32, precision=precision, dthdx_override=m2)
           for m2 in (0.6, 0.9, 1.4, 1.1)]
@@ -64,23 +64,27 @@ def test_batched_form_equals_member_graphs(precision):
     seeds = [11, 12, 13, 14]
     a = Ensemble(ps, gy, seeds=seeds)
     b = Ensemble(ps, gy, seeds=seeds)
-    assert a.batched and b.batched
+    c = Ensemble(ps, gy, seeds=seeds)
+    assert a.batched and b.batched and a.groups == 1
     b.batched = False
-    assert not b.batched
-    a.step(4)
-    b.step(4)
-    a.step(3)
-    b.step(3)
+    c.groups = 2
+    assert not b.batched and c.groups == 2
+    for e in (a, b, c):
+        e.step(4)
+    for e in (a, b, c):
+        e.step(3)
     assert a.kernels_per_step() == 26                       # one launch per kernel for all members
+    assert c.kernels_per_step() == 2 * 26                   # one per kernel and group
     assert b.kernels_per_step() > 2 * a.kernels_per_step()  # each member's own kernels
-    for ma, mb, p in zip(a.members, b.members, ps):
-        sa, sb = channel_state(ma, p), channel_state(mb, p)
+    for ma, mb, mc, p in zip(a.members, b.members, c.members, ps):
+        sa, sb, sc = channel_state(ma, p), channel_state(mb, p), channel_state(mc, p)
         for f in STATE:
             assert np.array_equal(sa[f], sb[f]), f
-        st_a, st_b = ma.status(), mb.status()
-        assert st_a.flags == st_b.flags == 0
-        assert st_a.time_step == st_b.time_step == 7
-        assert st_a.time == st_b.time
+            assert np.array_equal(sc[f], sb[f]), f
+        st_a, st_b, st_c = ma.status(), mb.status(), mc.status()
+        assert st_a.flags == st_b.flags == st_c.flags == 0
+        assert st_a.time_step == st_b.time_step == st_c.time_step == 7
+        assert st_a.time == st_b.time == st_c.time
     # the batched form again on the second ensemble continues identically
     b.batched = True
     a.step(2)
@@ -89,6 +93,7 @@ def test_batched_form_equals_member_graphs(precision):
         assert np.array_equal(channel_state(ma, p)[0], channel_state(mb, p)[0])
     a.close()
     b.close()
+    c.close()
 
 
 def test_batched_form_only_where_members_qualify():
