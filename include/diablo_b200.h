@@ -397,7 +397,7 @@ const char* db_ensemble_error(const db_ensemble* ens);
  * pointers and parameters come from a device table), each group a chain
  * of such launches on its own branch of the step's graph; results are
  * bit-identical to stepping each member alone.  It is used whenever the
- * members qualify, with n/16 groups (1 to 4).  db_ensemble_set_batched(ens,
+ * members qualify, in one group.  db_ensemble_set_batched(ens,
  * groups): 0 selects the per-member graph branches, groups >= 1 the batched
  * form in that many groups (at most 8 and n; DB_ERR_ARG if the members do
  * not qualify).  db_ensemble_info: *groups 0 for the per-member branches,
