@@ -502,32 +502,36 @@ def main():
     dns = _dns_timed(ch, p, stream, args.steps, rk, local, args.precision, args.les)
     ms_max, value, clk = dns["ms_max"], dns["value"], dns["clocks"]
 
-    # end to end through the C-ABI with host buffers
+    # end to end through the C-ABI with host buffers: each step uploads the
+    # fields a full RK step reads and downloads the ones it writes (U, V, W,
+    # TH, P; the CF history is rebuilt inside the step)
     e2e = None
     if not args.no_e2e:
         host = {f: torch.empty(ch.new_spectral().shape, dtype=torch.complex128, pin_memory=True).numpy()
-                for f in L.STATE_FIELDS}
+                for f in L.STEP_FIELDS}
         ke = max(1, min(3, args.steps))
-        h2d_bytes, d2h_bytes = roofline.state_transfer_bytes(p)
+        h2d_bytes, d2h_bytes = roofline.state_transfer_bytes(p, len(L.STEP_FIELDS))
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         saved = ch.download_state()
-        for f in L.STATE_FIELDS:   # the first step's inputs, in the pinned buffers too
+        for f in L.STEP_FIELDS:   # the first step's inputs, in the pinned buffers too
             host[f][...] = saved[f]
         e0.record(stream)
         for _ in range(ke):
-            ch.upload_state(host)
+            for f in L.STEP_FIELDS:
+                ch.upload_field(f, host[f])
             ch.step(1)
-            for f in L.STATE_FIELDS:
+            for f in L.STEP_FIELDS:
                 ch._ck(ch.L.db_download_field(ch.h, f, L.dptr(host[f].view(np.float64).reshape(-1))))
         e1.record(stream)
         torch.cuda.synchronize()
         te = replicas.max_over_ranks(rk, e0.elapsed_time(e1))
         e2e = {"value": replicas.job_rate(npts, 3 * ke, rk, te), "unit": UNIT,
                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
-               "steps": ke, "path": "db_upload_state + db_rk_steps(1) + db_download_field x9, reference-layout host arrays"}
+               "steps": ke, "path": "db_upload_field x5 (CU1, CU2, CU3, CP, CTH) + db_rk_steps(1) + "
+                                    "db_download_field x5, reference-layout host arrays"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

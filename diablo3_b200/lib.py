@@ -25,6 +25,9 @@ STAT_ROWS = ("ume", "vme", "wme", "thme", "urms", "vrms", "wrms", "thrms", "uv",
 BUDGET_ROWS = ("tke", "uu_dudx", "wu_dwdx", "vu_dvdx", "vv_dvdy", "uv_dudy", "wv_dwdy", "epsilon_m",
                "omega_x", "omega_y", "omega_z")
 STATE_FIELDS = (CU1, CU2, CU3, CP, CTH, CF1, CF2, CF3, CFTH)
+# what a full RK step reads and writes: the CF history is rebuilt in its
+# first substep before any read (for/solver.f90:413, 487)
+STEP_FIELDS = (CU1, CU2, CU3, CP, CTH)
 
 # exported symbols, in header order
 EXPORTS = (

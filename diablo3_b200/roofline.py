@@ -114,13 +114,13 @@ def reference_substep_bytes(p) -> float:
     return float(sum(_physical_path_bytes(p).values()))
 
 
-def state_transfer_bytes(p) -> tuple:
-    """Bytes one db_upload_state and nine db_download_field move over PCIe,
-    (host to device, device to host): both ways the retained modes of each
-    reference-layout array (kx <= Nkx of the first 2 Nkz + 1 rows of every
-    plane); the download writes the zero padding on the host."""
+def state_transfer_bytes(p, nfields: int = 9) -> tuple:
+    """Bytes nfields db_upload_field and db_download_field calls move over
+    PCIe (host to device, device to host): both ways the retained modes of
+    each reference-layout array (kx <= Nkx of the first 2 Nkz + 1 rows of
+    every plane); the download writes the zero padding on the host."""
     nplanes = p.ny + 2
-    h2d = 9 * nplanes * (2 * (p.nz // 3) + 1) * (p.nx // 3 + 1) * 16
+    h2d = nfields * nplanes * (2 * (p.nz // 3) + 1) * (p.nx // 3 + 1) * 16
     return h2d, h2d
 
 
