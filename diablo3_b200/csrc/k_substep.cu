@@ -387,6 +387,12 @@ struct RhsIn {
   double2 nb2, nbp;     // e 0/1: cu2 of planes j and j+1; e 2: cth and cp of plane j-1
   double2 cfo;          // cf of the previous substep (rk > 0)
 };
+// a hint that brings the line holding p into L2 (p must be a valid global
+// address)
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(p)));
+}
+
 __device__ __forceinline__ RhsIn rhs_load(const State& s, const Geom& g, int rk, int e, long long a) {
   const double2 z = make_double2(0.0, 0.0);
   RhsIn v{z, z, z, z, z, z, z, z};
@@ -830,6 +836,20 @@ __global__ void __launch_bounds__(32, DB_RHSCN_LB) k_rhs_cn(const __grid_constan
   double2 pm = make_double2(0.0, 0.0);   // cp of plane j-1
   for (int j = 0; j < np; ++j) {
     const long long a = (long long)j * sp;
+    // the next plane's inputs into L2 while this plane is computed (the
+    // stores of y below keep the compiler from hoisting those loads, so
+    // without this every plane waits for DRAM)
+    if (j + 1 < np) {
+      const long long an = a + sp;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (j + 2 < np) prefetch_l2(U[e] + an + sp);
+        prefetch_l2((const double2*)nl.p[e] + an + m);
+        if (SPLITZ) prefetch_l2((const double2*)nl.p[4 + e] + an + m);
+        if (rk > 0) prefetch_l2(rhs_cf(s, e) + an + m);
+      }
+      prefetch_l2(s.cp + an + m);
+    }
     double2 un[4], nlv[4], zmv[4], cfo[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
