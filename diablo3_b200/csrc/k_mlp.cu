@@ -63,9 +63,11 @@ __device__ __forceinline__ float gelu_d(float x) {
 __device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : log1pf(expf(y)); }
 __device__ __forceinline__ float sigm(float y) { return 1.0f / (1.0f + expf(-y)); }
 
+// a in the low half, b in the high half, each rounded to nearest; the
+// paired conversion is one instruction for the two values
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  const __nv_bfloat16 x = __float2bfloat16_rn(a), y = __float2bfloat16_rn(b);
-  return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+  const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&v);
 }
 
 // 8 consecutive K values of one row into a K-major tile (one 16-byte store)
