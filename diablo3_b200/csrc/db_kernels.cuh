@@ -167,10 +167,11 @@ __device__ __forceinline__ R ydiff(R a, R b, const double* pmean, int f, int np,
 
 // Member-batched launches (ensembles of equal-sized channels without LES):
 // one launch covers every member, the member index folded into a grid
-// dimension the kernel does not use otherwise; member m's state, geometry,
-// physics and the field sets of the batched transforms come from a device
-// table.  Kernels instantiated with B = false take their arguments as
-// before and ignore the table.
+// dimension the kernel does not use otherwise; member m's state, physics
+// and the field sets of the batched transforms come from a device table,
+// the geometry is member 0's kernel parameter (the same for every member;
+// of the table's copy only the flags word is used).  Kernels instantiated
+// with B = false take their arguments as before and ignore the table.
 enum { FS_CU4 = 0, FS_XH4, FS_U4, FS_XH8, FS_XH8Z, FS_NL, FS_NSLOT };
 struct MemberArgs {
   State s;
