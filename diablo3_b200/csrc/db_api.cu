@@ -1113,14 +1113,8 @@ static int ensemble_create_impl(db_ctx** members, int n, void* stream, db_ensemb
       return DB_ERR_CUDA;
     }
   if (batch_eligible(e->members)) {
-    bool ok = cudaMalloc((void**)&e->tab, (size_t)n * sizeof(MemberArgs)) == cudaSuccess &&
-              cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
-    for (int k = 0; k < db_ensemble::kMaxGroups && ok; ++k)
-      ok = cudaStreamCreateWithFlags(&e->gst[k], cudaStreamNonBlocking) == cudaSuccess &&
-           cudaStreamCreateWithFlags(&e->gside[k], cudaStreamNonBlocking) == cudaSuccess &&
-           cudaEventCreateWithFlags(&e->gfork[k], cudaEventDisableTiming) == cudaSuccess &&
-           cudaEventCreateWithFlags(&e->gjoin[k], cudaEventDisableTiming) == cudaSuccess &&
-           cudaEventCreateWithFlags(&e->gdone[k], cudaEventDisableTiming) == cudaSuccess;
+    const bool ok = cudaMalloc((void**)&e->tab, (size_t)n * sizeof(MemberArgs)) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
       db_ensemble_destroy(e);
       g_init_err = "db_ensemble_create: out of device memory";
@@ -1185,9 +1179,30 @@ static bool same_shapes(const Geom& a, const Geom& b) {
          a.tune_pgrid == b.tune_pgrid;
 }
 
+// the streams and events of groups 0..G-1, created on first use
+static bool ensure_groups(db_ensemble* e, int G) {
+  for (int k = 0; k < G; ++k) {
+    for (cudaStream_t* q : {&e->gst[k], &e->gside[k]})
+      if (!*q && cudaStreamCreateWithFlags(q, cudaStreamNonBlocking) != cudaSuccess) {
+        *q = nullptr;
+        return false;
+      }
+    for (cudaEvent_t* v : {&e->gfork[k], &e->gjoin[k], &e->gdone[k]})
+      if (!*v && cudaEventCreateWithFlags(v, cudaEventDisableTiming) != cudaSuccess) {
+        *v = nullptr;
+        return false;
+      }
+  }
+  return true;
+}
+
 static int ensemble_steps_batched(db_ensemble* e, int nsteps) {
   const int n = (int)e->members.size();
   db_ctx* c0 = e->members[0];
+  if (!ensure_groups(e, e->groups)) {
+    e->err = "ensemble stream creation failed";
+    return DB_ERR_CUDA;
+  }
   // the step stream follows whatever the members' own streams hold
   for (int i = 0; i < n; ++i) {
     if (cudaEventRecord(e->ev[1 + i], e->members[i]->st) != cudaSuccess ||
